@@ -1,0 +1,839 @@
+// Host side of the C ABI (include/am24.h): handles, resident matrices, batch
+// stepping and the denseDataSolver drivers (batch and on-the-fly modes).
+//
+// The drivers restate c++/src/gpower/sparse_PCA_solver.h:36-243 around the
+// device step of am24_kernels.cu: the same settings mutation, batch-global or
+// per-start termination, best-start choice and final normalisation.  All
+// arithmetic of the AM step runs on the GPU; the host only decides control
+// flow from a few scalars it reads back per iteration.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cudaTypedefs.h>
+
+#include "am24.h"
+#include "am24_internal.h"
+
+using namespace am24;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+am24_status fail(am24_status s, const std::string &msg) {
+  g_last_error = msg;
+  return s;
+}
+
+#define AM24_CUDA(expr)                                                                  \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      if (e_ == cudaErrorMemoryAllocation) {                                             \
+        cudaGetLastError();                                                              \
+        return fail(AM24_ERR_OOM, std::string(#expr) + ": " + cudaGetErrorString(e_));  \
+      }                                                                                  \
+      return fail(AM24_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));   \
+    }                                                                                    \
+  } while (0)
+
+#define AM24_TRY(expr)                   \
+  do {                                   \
+    am24_status s_ = (expr);             \
+    if (s_ != AM24_OK) return s_;        \
+  } while (0)
+
+int round_up(int v, int a) { return (v + a - 1) / a * a; }
+
+// Scoped device allocations of one object.
+struct Allocs {
+  std::vector<void *> ptrs;
+  ~Allocs() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  am24_status get(T **out, size_t count) {
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(e == cudaErrorMemoryAllocation ? AM24_ERR_OOM : AM24_ERR_CUDA,
+                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    ptrs.push_back(p);
+    *out = static_cast<T *>(p);
+    return AM24_OK;
+  }
+};
+
+}  // namespace
+
+struct am24_handle_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  Allocs scratch;  // small per-handle buffers
+  double *ev_rows = nullptr;
+  size_t ev_rows_cap = 0;
+  double *ev_out = nullptr;
+};
+
+struct am24_matrix_s {
+  MatrixDev d{};
+  Allocs mem;
+};
+
+struct am24_batch_s {
+  BatchDev d{};
+  TensorMaps tm{};
+  am24_matrix mat = nullptr;
+  am24_settings s{};
+  int launches = 0;
+  Allocs mem;
+};
+
+namespace {
+
+am24_status make_map(am24_handle h, CUtensorMap *map, const float *base, int K, int rows, int ld,
+                     int box_rows) {
+  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = h->encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims,
+                         strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return fail(AM24_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+  return AM24_OK;
+}
+
+// Split-K factor for Z = B V: minimise rounds * (K blocks per unit + fixed
+// per-unit cost) over the persistent grid.
+void choose_splits(int tiles, int kb_total, int sms, int *splits, int *kbps) {
+  double best_cost = 1e300;
+  *splits = 1;
+  *kbps = kb_total;
+  for (int s = 1; s <= std::min(kb_total, 64); s++) {
+    const int per = (kb_total + s - 1) / s;
+    if (per < 4 && s > 1) break;
+    const int s_eff = (kb_total + per - 1) / per;
+    const long units = (long)tiles * s_eff;
+    const long rounds = (units + sms - 1) / sms;
+    const double cost = (double)rounds * (per + 8.0);
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      *splits = s_eff;
+      *kbps = per;
+    }
+  }
+}
+
+am24_status validate_settings(const am24_settings *s) {
+  if (!s) return fail(AM24_ERR_INVALID_ARG, "settings is NULL");
+  if (s->formulation < 0 || s->formulation > 7)
+    return fail(AM24_ERR_INVALID_ARG, "formulation must be 0..7");
+  if (s->max_iter < 0) return fail(AM24_ERR_INVALID_ARG, "max_iter must be >= 0");
+  if (s->total_starts < 1 && s->batch_size < 1)
+    return fail(AM24_ERR_INVALID_ARG, "total_starts and batch_size cannot both be < 1");
+  if (s->batch_size < 0) return fail(AM24_ERR_INVALID_ARG, "batch_size must be >= 0");
+  if (is_constrained(s->formulation) && s->constraint < 1)
+    return fail(AM24_ERR_INVALID_ARG, "constraint (s) must be >= 1 for constrained formulations");
+  if (s->start_mode != AM24_START_REFERENCE && s->start_mode != AM24_START_INJECTED)
+    return fail(AM24_ERR_INVALID_ARG, "unknown start_mode");
+  if (s->l1_mode != AM24_L1_REFERENCE_SCAN && s->l1_mode != AM24_L1_EXACT)
+    return fail(AM24_ERR_INVALID_ARG, "unknown l1_mode");
+  return AM24_OK;
+}
+
+StepParams step_params(const am24_settings &s, int it, int shift) {
+  StepParams p;
+  p.formulation = s.formulation;
+  p.constraint = s.constraint;
+  p.penalty = s.penalty;
+  p.tolerance = s.tolerance;
+  p.use_sort_hard = s.use_sort_hard;
+  p.l1_mode = s.l1_mode;
+  p.store_all = s.store_all;
+  p.it = it;
+  p.log_shift = shift;
+  p.timeout_ns = (unsigned long long)(s.timeout_ms ? s.timeout_ms : 5000u) * 1000000ull;
+  return p;
+}
+
+am24_status check_device_status(am24_batch b) {
+  int st = 0;
+  AM24_CUDA(cudaMemcpy(&st, b->d.status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "device-side wait timed out (code 0x%x)", st);
+    return fail(AM24_ERR_DEVICE_TIMEOUT, buf);
+  }
+  return AM24_OK;
+}
+
+// getSignleStartingPoint (c++/src/gpower/gpower_commons.h:22-47) for global
+// start index g, into a zeroed column x of length n, with the reference's
+// float arithmetic: constrained forms draw s (index, value) pairs from rand_r
+// seeded with g and scale by 1/sqrt(sum value^2); penalized forms draw
+// U[-1, 1] entries and do not normalise.
+void reference_start(float *x, unsigned n, bool constrained, unsigned s, unsigned g) {
+  unsigned seed = g;
+  if (constrained) {
+    float norm = 0.f;
+    for (unsigned i = 0; i < s; i++) {
+      unsigned idx = (unsigned)(int)((float)n * (float)rand_r(&seed) / (float)RAND_MAX);
+      if (idx == n) idx--;
+      const float tmp = (float)rand_r(&seed) / (float)RAND_MAX;
+      x[idx] = tmp;
+      norm += tmp * tmp;
+    }
+    const float f = 1.0f / std::sqrt(norm);
+    for (unsigned i = 0; i < n; i++) x[i] *= f;
+  } else {
+    for (unsigned i = 0; i < n; i++) {
+      float tmp = (float)rand_r(&seed) / (float)RAND_MAX;
+      tmp = -1.0f + 2.0f * tmp;
+      x[i] = tmp;
+    }
+  }
+}
+
+// Fills `cols` starting-point columns (global indices first..) into host
+// staging (n x cols, leading dimension n) from the caller's matrix or the
+// reference generator.
+void host_starts(const am24_settings &s, unsigned n, const float *start_points,
+                 const unsigned *global_idx, int cols, std::vector<float> &out) {
+  out.assign((size_t)n * cols, 0.f);
+  for (int c = 0; c < cols; c++) {
+    float *dst = &out[(size_t)c * n];
+    if (s.start_mode == AM24_START_INJECTED)
+      std::memcpy(dst, start_points + (size_t)global_idx[c] * n, sizeof(float) * n);
+    else
+      reference_start(dst, n, is_constrained(s.formulation), s.constraint, global_idx[c]);
+  }
+}
+
+am24_status upload_columns(am24_handle h, am24_batch b, const float *host, int cols,
+                           const int *slots) {
+  const MatrixDev &M = b->mat->d;
+  // stage through Vraw (raw GEMM output, free between steps), then split
+  for (int c = 0; c < cols; c++) {
+    AM24_CUDA(cudaMemcpyAsync(b->d.Vraw + (size_t)slots[c] * M.ldn, host + (size_t)c * M.n,
+                              sizeof(float) * M.n, cudaMemcpyHostToDevice, h->stream));
+    AM24_CUDA(launch_split_columns(b->d.Vraw + (size_t)slots[c] * M.ldn, M.ldn, M.n, 1,
+                                   b->d.V_hi + (size_t)slots[c] * M.ldn,
+                                   b->d.V_lo + (size_t)slots[c] * M.ldn, M.ldn, h->stream));
+  }
+  return AM24_OK;
+}
+
+}  // namespace
+
+// ============================================================== library
+extern "C" {
+
+uint32_t am24_abi_version(void) { return AM24_ABI_VERSION; }
+
+const char *am24_last_error(void) { return g_last_error.c_str(); }
+
+const char *am24_status_string(am24_status s) {
+  switch (s) {
+    case AM24_OK: return "ok";
+    case AM24_ERR_INVALID_ARG: return "invalid argument";
+    case AM24_ERR_OOM: return "out of device memory";
+    case AM24_ERR_CUDA: return "CUDA error";
+    case AM24_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    case AM24_ERR_UNSUPPORTED: return "unsupported";
+    case AM24_ERR_DEGENERATE: return "degenerate start (NaN objective)";
+  }
+  return "unknown status";
+}
+
+// OptimizationSettings() defaults (c++/src/class/optimization_settings.h:101-123).
+void am24_default_settings(am24_settings *s) {
+  if (!s) return;
+  std::memset(s, 0, sizeof *s);
+  s->formulation = AM24_L0_CONSTRAINED_L2_PCA;
+  s->tolerance = 0.01;
+  s->constraint = 10;
+  s->penalty = 0;
+  s->total_starts = 64;
+  s->batch_size = 64;
+  s->use_sort_hard = 0;
+  s->use_otf = 0;
+  s->max_iter = 20;
+  s->store_all = 0;
+  s->start_mode = AM24_START_REFERENCE;
+  s->l1_mode = AM24_L1_REFERENCE_SCAN;
+  s->timeout_ms = 5000;
+}
+
+// chceckInputAndModifyIt (c++/src/class/optimization_settings.h:156-168).
+am24_status am24_check_input(am24_settings *s, uint32_t n) {
+  if (!s) return fail(AM24_ERR_INVALID_ARG, "settings is NULL");
+  if (s->constraint > n) s->constraint = n;
+  if (s->batch_size == 0) s->batch_size = s->total_starts;
+  if (s->batch_size <= 0) return fail(AM24_ERR_INVALID_ARG, "batch_size must be positive");
+  s->total_batches = (uint32_t)(s->total_starts / s->batch_size);
+  if (s->total_batches * (uint32_t)s->batch_size < (uint32_t)std::max(s->total_starts, 0))
+    s->total_batches++;
+  s->total_starts = (int32_t)(s->total_batches * (uint32_t)s->batch_size);
+  return AM24_OK;
+}
+
+am24_status am24_create(am24_handle *out, int device) {
+  if (!out) return fail(AM24_ERR_INVALID_ARG, "handle pointer is NULL");
+  *out = nullptr;
+  int count = 0;
+  AM24_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count)
+    return fail(AM24_ERR_INVALID_ARG, "device index out of range");
+  AM24_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  AM24_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fail(AM24_ERR_UNSUPPORTED, std::string("needs an sm_100 (B200-class) GPU, found ") +
+                                          prop.name);
+  auto *h = new am24_handle_s();
+  h->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete h;
+    return fail(AM24_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return fail(AM24_ERR_CUDA, "cuTensorMapEncodeTiled entry point not available");
+  }
+  h->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  am24_status st = h->scratch.get(&h->ev_out, 1);
+  if (st != AM24_OK) {
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return AM24_OK;
+}
+
+am24_status am24_destroy(am24_handle h) {
+  if (!h) return AM24_OK;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return AM24_OK;
+}
+
+am24_status am24_sync(am24_handle h) {
+  if (!h) return fail(AM24_ERR_INVALID_ARG, "handle is NULL");
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  return AM24_OK;
+}
+
+// ============================================================== matrices
+am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, uint32_t m,
+                                   uint32_t n, int32_t on_device, am24_matrix *out) {
+  if (!h || !B || !out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  if (m == 0 || n == 0) return fail(AM24_ERR_INVALID_ARG, "m and n must be positive");
+  if (ldB < (int32_t)m) return fail(AM24_ERR_INVALID_ARG, "ldB must be >= m");
+  if (m > (1u << 30) || n > (1u << 30)) return fail(AM24_ERR_INVALID_ARG, "matrix too large");
+  AM24_CUDA(cudaSetDevice(h->device));
+  auto *mat = new am24_matrix_s();
+  MatrixDev &M = mat->d;
+  M.m = (int)m;
+  M.n = (int)n;
+  M.ldm = round_up((int)m, 32);
+  M.ldn = round_up((int)n, 32);
+  am24_status st;
+  const size_t c_elems = (size_t)n * M.ldm, t_elems = (size_t)m * M.ldn;
+  if ((st = mat->mem.get(&M.Bc_hi, c_elems)) != AM24_OK ||
+      (st = mat->mem.get(&M.Bc_lo, c_elems)) != AM24_OK ||
+      (st = mat->mem.get(&M.Bt_hi, t_elems)) != AM24_OK ||
+      (st = mat->mem.get(&M.Bt_lo, t_elems)) != AM24_OK) {
+    delete mat;
+    return st;
+  }
+  const float *src = B;
+  int ld_src = ldB;
+  float *staging = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (!on_device) {
+    e = cudaMallocAsync(reinterpret_cast<void **>(&staging), sizeof(float) * (size_t)m * n,
+                        h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(staging, sizeof(float) * m, B, sizeof(float) * (size_t)ldB,
+                            sizeof(float) * m, n, cudaMemcpyHostToDevice, h->stream);
+    src = staging;
+    ld_src = (int)m;
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bc_hi, 0, sizeof(float) * c_elems, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bc_lo, 0, sizeof(float) * c_elems, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bt_hi, 0, sizeof(float) * t_elems, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bt_lo, 0, sizeof(float) * t_elems, h->stream);
+  if (e == cudaSuccess) e = launch_prep_matrix(src, ld_src, M, h->stream);
+  if (staging) cudaFreeAsync(staging, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    delete mat;
+    return fail(e == cudaErrorMemoryAllocation ? AM24_ERR_OOM : AM24_ERR_CUDA,
+                std::string("matrix upload: ") + cudaGetErrorString(e));
+  }
+  *out = mat;
+  return AM24_OK;
+}
+
+am24_status am24_matrix_destroy(am24_handle h, am24_matrix mat) {
+  if (!mat) return AM24_OK;
+  if (h) {
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+  }
+  delete mat;
+  return AM24_OK;
+}
+
+// ============================================================== batches
+am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_settings *settings,
+                              uint32_t batch_size, am24_batch *out) {
+  if (!h || !mat || !out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  AM24_TRY(validate_settings(settings));
+  if (batch_size == 0 || batch_size > (1u << 20))
+    return fail(AM24_ERR_INVALID_ARG, "batch_size must be in [1, 2^20]");
+  if (is_constrained(settings->formulation) && settings->constraint > (uint32_t)mat->d.n)
+    return fail(AM24_ERR_INVALID_ARG, "constraint exceeds n (run am24_check_input first)");
+  AM24_CUDA(cudaSetDevice(h->device));
+  auto *b = new am24_batch_s();
+  b->mat = mat;
+  b->s = *settings;
+  const MatrixDev &M = mat->d;
+  BatchDev &d = b->d;
+  const int k = (int)batch_size;
+  d.k = k;
+  d.bn1 = pick_bn(k);
+  d.bn2 = pick_bn(k);
+  d.m_tiles1 = (M.m + BM - 1) / BM;
+  d.n_tiles1 = (k + d.bn1 - 1) / d.bn1;
+  d.m_tiles2 = (M.n + BM - 1) / BM;
+  d.n_tiles2 = (k + d.bn2 - 1) / d.bn2;
+  const int kb_total1 = (M.n + BK - 1) / BK;
+  choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
+  const int parts = d.m_tiles2 * 4;
+  d.log_capacity = std::max(settings->total_starts, k);
+  am24_status st;
+  auto &A = b->mem;
+  const size_t kv = (size_t)k * M.ldn, kz = (size_t)k * M.ldm;
+  if ((st = A.get(&d.V_hi, kv)) || (st = A.get(&d.V_lo, kv)) || (st = A.get(&d.Vraw, kv)) ||
+      (st = A.get(&d.Z_hi, kz)) || (st = A.get(&d.Z_lo, kz)) ||
+      (st = A.get(&d.ws, ws_floats(d.splits1, d.m_tiles1, d.n_tiles1, d.bn1))) ||
+      (st = A.get(&d.fz, k)) || (st = A.get(&d.obj_part, (size_t)k * parts)) ||
+      (st = A.get(&d.nnz_part, (size_t)k * parts)) || (st = A.get(&d.nnz, k)) ||
+      (st = A.get(&d.val, k)) || (st = A.get(&d.err, k)) || (st = A.get(&d.max_err, 1)) ||
+      (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
+      (st = A.get(&d.status, 1))) {
+    delete b;
+    return st;
+  }
+  cudaError_t e = cudaMemsetAsync(d.V_hi, 0, sizeof(float) * kv, h->stream);
+  if (!e) e = cudaMemsetAsync(d.V_lo, 0, sizeof(float) * kv, h->stream);
+  if (!e) e = cudaMemsetAsync(d.Vraw, 0, sizeof(float) * kv, h->stream);
+  if (!e) e = cudaMemsetAsync(d.Z_hi, 0, sizeof(float) * kz, h->stream);
+  if (!e) e = cudaMemsetAsync(d.Z_lo, 0, sizeof(float) * kz, h->stream);
+  if (!e) e = cudaMemsetAsync(d.val, 0, sizeof(float) * k, h->stream);
+  if (!e) e = cudaMemsetAsync(d.err, 0, sizeof(float) * k, h->stream);
+  if (!e) e = cudaMemsetAsync(d.fz, 0, sizeof(float) * k, h->stream);
+  if (!e) e = cudaMemsetAsync(d.nnz, 0, sizeof(uint32_t) * k, h->stream);
+  if (!e) e = cudaMemsetAsync(d.status, 0, sizeof(int), h->stream);
+  if (!e) e = cudaMemsetAsync(d.iters, 0xFF, sizeof(int) * d.log_capacity, h->stream);
+  if (!e) e = cudaMemsetAsync(d.cards, 0xFF, sizeof(int) * d.log_capacity, h->stream);
+  if (!e) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(AM24_ERR_CUDA, std::string("batch init: ") + cudaGetErrorString(e));
+  }
+  if ((st = make_map(h, &b->tm.a1_hi, M.Bt_hi, M.n, M.m, M.ldn, BM)) ||
+      (st = make_map(h, &b->tm.a1_lo, M.Bt_lo, M.n, M.m, M.ldn, BM)) ||
+      (st = make_map(h, &b->tm.b1_hi, d.V_hi, M.n, k, M.ldn, d.bn1)) ||
+      (st = make_map(h, &b->tm.b1_lo, d.V_lo, M.n, k, M.ldn, d.bn1)) ||
+      (st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM)) ||
+      (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM)) ||
+      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.bn2)) ||
+      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.bn2))) {
+    delete b;
+    return st;
+  }
+  b->launches = is_constrained(settings->formulation) ? 5 : 4;
+  *out = b;
+  return AM24_OK;
+}
+
+am24_status am24_batch_destroy(am24_handle h, am24_batch b) {
+  if (!b) return AM24_OK;
+  if (h) {
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+  }
+  delete b;
+  return AM24_OK;
+}
+
+am24_status am24_batch_load(am24_handle h, am24_batch b, const float *V, int32_t on_device) {
+  if (!h || !b || !V) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  const MatrixDev &M = b->mat->d;
+  const int k = b->d.k;
+  if (on_device) {
+    AM24_CUDA(cudaMemcpy2DAsync(b->d.Vraw, sizeof(float) * M.ldn, V, sizeof(float) * M.n,
+                                sizeof(float) * M.n, k, cudaMemcpyDeviceToDevice, h->stream));
+  } else {
+    AM24_CUDA(cudaMemcpy2DAsync(b->d.Vraw, sizeof(float) * M.ldn, V, sizeof(float) * M.n,
+                                sizeof(float) * M.n, k, cudaMemcpyHostToDevice, h->stream));
+  }
+  AM24_CUDA(launch_split_columns(b->d.Vraw, M.ldn, M.n, k, b->d.V_hi, b->d.V_lo, M.ldn, h->stream));
+  // ValueCoordinateHolder::reset (c++/src/utils/various.h:33-38)
+  AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
+  AM24_CUDA(cudaMemsetAsync(b->d.err, 0, sizeof(float) * k, h->stream));
+  return AM24_OK;
+}
+
+am24_status am24_batch_iterate(am24_handle h, am24_batch b, int32_t it0, int32_t iterations,
+                               float *max_error) {
+  if (!h || !b) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  for (int i = 0; i < iterations; i++) {
+    const StepParams p = step_params(b->s, it0 + i, 0);
+    AM24_CUDA(launch_am_step(b->mat->d, b->d, b->tm, p, h->stream, &b->launches));
+  }
+  if (max_error) {
+    AM24_CUDA(cudaMemcpyAsync(max_error, b->d.max_err, sizeof(float), cudaMemcpyDeviceToHost,
+                              h->stream));
+    AM24_CUDA(cudaStreamSynchronize(h->stream));
+    AM24_TRY(check_device_status(b));
+  }
+  return AM24_OK;
+}
+
+am24_status am24_batch_read(am24_handle h, am24_batch b, float *V, float *val, float *err,
+                            uint32_t *nnz) {
+  if (!h || !b) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  const MatrixDev &M = b->mat->d;
+  const int k = b->d.k;
+  if (V) {
+    AM24_CUDA(launch_combine_columns(b->d.V_hi, b->d.V_lo, M.ldn, M.n, k, b->d.Vraw, M.ldn,
+                                     h->stream));
+    AM24_CUDA(cudaMemcpy2DAsync(V, sizeof(float) * M.n, b->d.Vraw, sizeof(float) * M.ldn,
+                                sizeof(float) * M.n, k, cudaMemcpyDeviceToHost, h->stream));
+  }
+  if (val)
+    AM24_CUDA(cudaMemcpyAsync(val, b->d.val, sizeof(float) * k, cudaMemcpyDeviceToHost, h->stream));
+  if (err)
+    AM24_CUDA(cudaMemcpyAsync(err, b->d.err, sizeof(float) * k, cudaMemcpyDeviceToHost, h->stream));
+  if (nnz) {
+    if (is_constrained(b->s.formulation)) {
+      AM24_CUDA(cudaMemcpyAsync(nnz, b->d.nnz, sizeof(uint32_t) * k, cudaMemcpyDeviceToHost,
+                                h->stream));
+    } else {
+      // penalized forms count non-zeros in the GEMM epilogue partials
+      const int parts = b->d.m_tiles2 * 4;
+      std::vector<float> np((size_t)k * parts);
+      AM24_CUDA(cudaMemcpyAsync(np.data(), b->d.nnz_part, sizeof(float) * np.size(),
+                                cudaMemcpyDeviceToHost, h->stream));
+      AM24_CUDA(cudaStreamSynchronize(h->stream));
+      for (int j = 0; j < k; j++) {
+        double c = 0;
+        for (int q = 0; q < parts; q++) c += np[(size_t)j * parts + q];
+        nnz[j] = (uint32_t)c;
+      }
+    }
+  }
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  AM24_TRY(check_device_status(b));
+  return AM24_OK;
+}
+
+am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float *ms,
+                                  int32_t *kinds, int32_t *count) {
+  if (!h || !b || !ms || !kinds || !count) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  cudaEvent_t ev[9];
+  int made = 0;
+  am24_status st = AM24_OK;
+  for (; made < 9; made++)
+    if (cudaEventCreate(&ev[made]) != cudaSuccess) {
+      st = fail(AM24_ERR_CUDA, "cudaEventCreate failed");
+      break;
+    }
+  int nl = 0, kk[9] = {0};
+  if (st == AM24_OK) {
+    const StepParams p = step_params(b->s, it, 0);
+    cudaError_t e = launch_am_step(b->mat->d, b->d, b->tm, p, h->stream, &nl, ev, kk);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    for (int i = 0; e == cudaSuccess && i < nl; i++) e = cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+    if (e != cudaSuccess) st = fail(AM24_ERR_CUDA, std::string("timed step: ") + cudaGetErrorString(e));
+  }
+  for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
+  if (st != AM24_OK) return st;
+  for (int i = 0; i < nl; i++) kinds[i] = kk[i];
+  *count = nl;
+  return check_device_status(b);
+}
+
+void *am24_stream(am24_handle h) { return h ? static_cast<void *>(h->stream) : nullptr; }
+
+am24_status am24_batch_launches_per_step(am24_handle h, am24_batch b, int32_t *launches) {
+  if (!h || !b || !launches) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  *launches = b->launches;
+  return AM24_OK;
+}
+
+// ============================================================== solver
+am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
+                                    am24_settings *settings, am24_statistics *stats,
+                                    const float *start_points, float *fval_out) {
+  const auto t_call = std::chrono::steady_clock::now();
+  if (!h || !mat || !x || !settings) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  AM24_TRY(validate_settings(settings));
+  if (settings->start_mode == AM24_START_INJECTED && !start_points)
+    return fail(AM24_ERR_INVALID_ARG, "start_mode INJECTED needs start_points");
+  AM24_CUDA(cudaSetDevice(h->device));
+  const MatrixDev &M = mat->d;
+  const unsigned n = (unsigned)M.n;
+  AM24_TRY(am24_check_input(settings, n));
+  am24_settings &s = *settings;
+  const int bs = s.batch_size;
+
+  am24_batch b = nullptr;
+  AM24_TRY(am24_batch_create(h, mat, &s, (uint32_t)bs, &b));
+  struct BatchGuard {
+    am24_handle h;
+    am24_batch b;
+    ~BatchGuard() { am24_batch_destroy(h, b); }
+  } guard{h, b};
+
+  // best loading so far, kept as hi/lo planes; starts as the caller's x, which
+  // the reference returns normalised when no start ever improves on -1
+  Allocs local;
+  float *xb_hi = nullptr, *xb_lo = nullptr, *x_dev = nullptr;
+  double *ev_rows = nullptr;
+  AM24_TRY(local.get(&xb_hi, n));
+  AM24_TRY(local.get(&xb_lo, n));
+  AM24_TRY(local.get(&x_dev, n));
+  AM24_TRY(local.get(&ev_rows, (size_t)M.m));
+  AM24_CUDA(cudaMemcpyAsync(xb_hi, x, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+  AM24_CUDA(cudaMemsetAsync(xb_lo, 0, sizeof(float) * n, h->stream));
+
+  cudaEvent_t e0, e1;
+  AM24_CUDA(cudaEventCreate(&e0));
+  AM24_CUDA(cudaEventCreate(&e1));
+  struct EvGuard {
+    cudaEvent_t a, c;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(c);
+    }
+  } evg{e0, e1};
+
+  std::vector<float> staging, val(bs), err(bs);
+  std::vector<int> slots(bs);
+  std::vector<unsigned> gidx(bs);
+  float best = -1.f;
+  uint32_t total_it = 0;
+  uint64_t start_its = 0;
+  double compute_s = 0.0;
+  float last_max_err = 0.f;
+  int degenerate = 0;
+  const BatchDev &d = b->d;
+  auto take_best = [&](int j) -> am24_status {
+    AM24_CUDA(cudaMemcpyAsync(xb_hi, d.V_hi + (size_t)j * M.ldn, sizeof(float) * n,
+                              cudaMemcpyDeviceToDevice, h->stream));
+    AM24_CUDA(cudaMemcpyAsync(xb_lo, d.V_lo + (size_t)j * M.ldn, sizeof(float) * n,
+                              cudaMemcpyDeviceToDevice, h->stream));
+    return AM24_OK;
+  };
+
+  if (!s.use_otf) {
+    // ---------------------------------- batches (sparse_PCA_solver.h:171-232)
+    for (unsigned batch = 0; batch < s.total_batches; batch++) {
+      const unsigned shift = batch * (unsigned)bs;
+      for (int j = 0; j < bs; j++) {
+        gidx[j] = shift + j;
+        slots[j] = j;
+      }
+      host_starts(s, n, start_points, gidx.data(), bs, staging);
+      AM24_TRY(upload_columns(h, b, staging.data(), bs, slots.data()));
+      AM24_CUDA(cudaMemsetAsync(d.val, 0, sizeof(float) * bs, h->stream));
+      AM24_CUDA(cudaEventRecord(e0, h->stream));
+      int it = 0;
+      for (; it < s.max_iter; it++) {
+        total_it++;
+        const StepParams p = step_params(s, it, (int)shift);
+        AM24_CUDA(launch_am_step(M, b->d, b->tm, p, h->stream, &b->launches));
+        AM24_CUDA(cudaMemcpyAsync(&last_max_err, d.max_err, sizeof(float), cudaMemcpyDeviceToHost,
+                                  h->stream));
+        AM24_CUDA(cudaStreamSynchronize(h->stream));
+        AM24_TRY(check_device_status(b));
+        start_its += (uint64_t)bs;
+        if (it > 0 && (double)last_max_err < s.tolerance) break;
+      }
+      AM24_CUDA(cudaEventRecord(e1, h->stream));
+      AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * bs, cudaMemcpyDeviceToHost,
+                                h->stream));
+      AM24_CUDA(cudaStreamSynchronize(h->stream));
+      float ms = 0.f;
+      AM24_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      compute_s += ms * 1e-3;
+      int sel = 0;
+      float bv = val[0];
+      if (s.store_all && stats && stats->values && shift < stats->per_start_capacity)
+        stats->values[shift] = bv;
+      for (int i = 1; i < bs; i++) {
+        if (s.store_all && stats && stats->values && shift + i < stats->per_start_capacity)
+          stats->values[shift + i] = val[i];
+        if (val[i] > bv) {
+          bv = val[i];
+          sel = i;
+        }
+      }
+      for (int i = 0; i < bs; i++) degenerate += std::isnan(val[i]) ? 1 : 0;
+      if (best < bv) {
+        best = bv;
+        AM24_TRY(take_best(sel));
+      }
+    }
+  } else {
+    // ---------------------------------- on the fly (sparse_PCA_solver.h:83-168)
+    s.store_all = 0;
+    std::vector<unsigned> cur(bs, 0), order(bs);
+    for (int j = 0; j < bs; j++) {
+      order[j] = j;
+      gidx[j] = j;
+      slots[j] = j;
+    }
+    host_starts(s, n, start_points, gidx.data(), bs, staging);
+    AM24_TRY(upload_columns(h, b, staging.data(), bs, slots.data()));
+    AM24_CUDA(cudaMemsetAsync(d.val, 0, sizeof(float) * bs, h->stream));
+    unsigned generated = (unsigned)bs;
+    bool go = true;
+    AM24_CUDA(cudaEventRecord(e0, h->stream));
+    while (go) {
+      total_it++;
+      const StepParams p = step_params(s, 0, 0);
+      AM24_CUDA(launch_am_step(M, b->d, b->tm, p, h->stream, &b->launches));
+      AM24_CUDA(cudaMemcpyAsync(err.data(), d.err, sizeof(float) * bs, cudaMemcpyDeviceToHost,
+                                h->stream));
+      AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * bs, cudaMemcpyDeviceToHost,
+                                h->stream));
+      AM24_CUDA(cudaStreamSynchronize(h->stream));
+      AM24_TRY(check_device_status(b));
+      start_its += (uint64_t)bs;
+      go = false;
+      int nref = 0;
+      for (int i = 0; i < bs; i++) {
+        cur[i]++;
+        const bool conv = (double)err[i] < s.tolerance;  // termination_criteria with it = cur > 0
+        if (conv || cur[i] >= (unsigned)s.max_iter) {
+          if (best < val[i]) {
+            best = val[i];
+            AM24_TRY(take_best(i));
+          }
+          if (generated < (unsigned)s.total_starts) {
+            order[i] = generated++;
+            cur[i] = 0;
+            slots[nref] = i;
+            gidx[nref] = order[i];
+            nref++;
+            go = true;
+          }
+        } else {
+          go = true;
+        }
+      }
+      if (nref > 0) {
+        host_starts(s, n, start_points, gidx.data(), nref, staging);
+        AM24_TRY(upload_columns(h, b, staging.data(), nref, slots.data()));
+        for (int r = 0; r < nref; r++)
+          AM24_CUDA(cudaMemsetAsync(d.val + slots[r], 0, sizeof(float), h->stream));
+      }
+    }
+    AM24_CUDA(cudaEventRecord(e1, h->stream));
+    AM24_CUDA(cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    AM24_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    compute_s += ms * 1e-3;
+    for (int i = 0; i < bs; i++) degenerate += std::isnan(val[i]) ? 1 : 0;
+  }
+
+  // x <- x / ||x|| and its FP64 explained variance ||B x||^2
+  AM24_CUDA(launch_finalize_x(xb_hi, xb_lo, (int)n, x_dev, h->stream));
+  AM24_CUDA(launch_explained_variance(M, x_dev, ev_rows, h->ev_out, h->stream));
+  double ev = 0.0;
+  AM24_CUDA(cudaMemcpyAsync(x, x_dev, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+  AM24_CUDA(cudaMemcpyAsync(&ev, h->ev_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+
+  if (stats) {
+    stats->it = total_it;
+    stats->fval = best;
+    stats->error = last_max_err;
+    stats->total_true_computation_time = compute_s;
+    stats->n = n;
+    stats->total_threads_used = 1;
+    stats->explained_variance = ev;
+    stats->start_iterations = start_its;
+    stats->degenerate_starts = degenerate;
+    if (s.store_all && stats->per_start_capacity > 0) {
+      const int cap = std::min<int>((int)stats->per_start_capacity, d.log_capacity);
+      if (stats->iters)
+        AM24_CUDA(cudaMemcpy(stats->iters, d.iters, sizeof(int) * cap, cudaMemcpyDeviceToHost));
+      if (stats->cardinalities)
+        AM24_CUDA(
+            cudaMemcpy(stats->cardinalities, d.cards, sizeof(int) * cap, cudaMemcpyDeviceToHost));
+    }
+    stats->total_elapsed_time =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t_call).count();
+  }
+  if (fval_out) *fval_out = best;
+  return AM24_OK;
+}
+
+am24_status am24_solve_dense_f32(am24_handle h, const float *B, int32_t ldB, float *x, uint32_t m,
+                                 uint32_t n, am24_settings *settings, am24_statistics *stats,
+                                 const float *start_points, float *fval_out) {
+  const auto t0 = std::chrono::steady_clock::now();
+  am24_matrix mat = nullptr;
+  AM24_TRY(am24_matrix_create_f32(h, B, ldB, m, n, 0, &mat));
+  am24_status st = am24_solve_resident_f32(h, mat, x, settings, stats, start_points, fval_out);
+  am24_matrix_destroy(h, mat);
+  if (st == AM24_OK && stats)
+    stats->total_elapsed_time =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return st;
+}
+
+am24_status am24_solve_device_f32(am24_handle h, const float *d_B, int32_t ldB, float *x,
+                                  uint32_t m, uint32_t n, am24_settings *settings,
+                                  am24_statistics *stats, const float *start_points,
+                                  float *fval_out) {
+  const auto t0 = std::chrono::steady_clock::now();
+  am24_matrix mat = nullptr;
+  AM24_TRY(am24_matrix_create_f32(h, d_B, ldB, m, n, 1, &mat));
+  am24_status st = am24_solve_resident_f32(h, mat, x, settings, stats, start_points, fval_out);
+  am24_matrix_destroy(h, mat);
+  if (st == AM24_OK && stats)
+    stats->total_elapsed_time =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return st;
+}
+
+}  // extern "C"

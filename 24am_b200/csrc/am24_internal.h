@@ -1,0 +1,87 @@
+// Internal declarations shared by the kernels (am24_kernels.cu) and the host
+// driver (am24_api.cu).  Not part of the public ABI.
+#pragma once
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace am24 {
+
+// GEMM tiling: M tile is fixed at 128 (one TMEM lane per accumulator row).
+constexpr int BM = 128;
+constexpr int BK = 32;  // K slab per pipeline stage (128-byte rows, 128B swizzle)
+
+// Formulation helpers (c++/src/class/optimization_settings.h:125-153).
+inline bool is_constrained(int f) { return f >= 0 && f <= 3; }
+inline bool is_l1_constrained(int f) { return f == 2 || f == 3; }
+inline bool is_l1_variance(int f) { return f == 1 || f == 3 || f == 5 || f == 7; }
+inline bool is_l1_penalized(int f) { return f == 6 || f == 7; }
+
+// Layout of one resident data matrix.  B (m x n) is kept in two K-major
+// orientations, each as a TF32 hi plane and an exact FP32 remainder plane:
+//   Bc: n rows (features) of m samples, leading dimension ldm  -> A of V = B^T Z
+//   Bt: m rows (samples) of n features, leading dimension ldn  -> A of Z = B V
+struct MatrixDev {
+  int m, n, ldm, ldn;
+  float *Bc_hi, *Bc_lo, *Bt_hi, *Bt_lo;
+};
+
+// Per-batch device state for k starting points.
+struct BatchDev {
+  int k;          // starting points in the batch
+  int bn1, bn2;   // GEMM N tiles (Z = B V and V = B^T Z)
+  int splits1;    // split-K factor of Z = B V
+  int kbps1;      // K blocks per split of Z = B V
+  int m_tiles1, n_tiles1, m_tiles2, n_tiles2;
+  float *V_hi, *V_lo;   // k x ldn loadings (GEMM-1 B operand, threshold output)
+  float *Z_hi, *Z_lo;   // k x ldm sample-space vectors (GEMM-2 B operand)
+  float *Vraw;          // k x ldn raw B^T Z (constrained forms)
+  float *ws;            // split-K partial tiles of Z = B V
+  float *fz;            // per start: ||y||_2 or ||y||_1 from the Z reduction
+  float *obj_part;      // per start x (m_tiles2*4): penalized objective partials
+  float *nnz_part;      // per start x (m_tiles2*4): penalized non-zero partials
+  uint32_t *nnz;        // per start: non-zeros after thresholding
+  float *val, *err;     // ValueCoordinateHolder val / current_error
+  float *max_err;       // batch maximum relative change (1 float)
+  int *iters, *cards;   // storeIterationsForAllPoints logs (total_starts each)
+  int log_capacity;
+  int *status;          // device status word (bounded-wait timeouts)
+};
+
+struct StepParams {
+  int formulation;
+  unsigned constraint;
+  double penalty;
+  double tolerance;
+  int use_sort_hard;
+  int l1_mode;
+  int store_all;
+  int it;             // iteration index within the batch (termination_criteria)
+  int log_shift;      // batch shift of the per-start logs
+  unsigned long long timeout_ns;
+};
+
+struct TensorMaps {
+  CUtensorMap a1_hi, a1_lo, b1_hi, b1_lo;  // Z = B V :  A = Bt, B = V
+  CUtensorMap a2_hi, a2_lo, b2_hi, b2_lo;  // V = B^T Z: A = Bc, B = Z
+};
+
+// ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
+int num_sms();
+cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st);
+cudaError_t launch_split_columns(const float *src, int ld_src, int rows, int cols, float *hi,
+                                 float *lo, int ld_dst, cudaStream_t st);
+// ev (optional, >= 9 events): ev[i] is recorded before launch i and
+// ev[launches] after the last one; kinds[i] (optional) gets each launch's kind.
+cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm,
+                           const StepParams &p, cudaStream_t st, int *launches,
+                           cudaEvent_t *ev = nullptr, int *kinds = nullptr);
+cudaError_t launch_finalize_x(const float *hi, const float *lo, int n, float *x, cudaStream_t st);
+cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double *partial,
+                                      double *out, cudaStream_t st);
+cudaError_t launch_combine_columns(const float *hi, const float *lo, int ld, int rows,
+                                   int cols, float *dst, int ld_dst, cudaStream_t st);
+int pick_bn(int k);
+size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn);
+
+}  // namespace am24

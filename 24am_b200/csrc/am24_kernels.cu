@@ -1,0 +1,1015 @@
+// Device kernels of one AM step and their launchers.
+//
+// One step for a batch of k starting points (reference:
+// perform_one_iteration_for_{constrained,penalized}_pca,
+// c++/src/gpower/gpower_commons.h:68-177):
+//
+//   1. gemm1     Z = B V            tcgen05 3xTF32, split-K partial tiles
+//   2. z_reduce  sum the split partials; L1 variance: ||z||_1 and z <- sgn(z);
+//                L2 variance: ||z||_2 (constrained) or z <- z/||z|| (penalized);
+//                writes Z as TF32 hi/lo planes for gemm2
+//   3. gemm2     V = B^T Z          tcgen05 3xTF32; penalized forms apply the
+//                threshold, the per-start objective and non-zero count in the
+//                epilogue; constrained forms store raw V
+//   4. select    constrained only: per-start radix select of the s-th largest
+//                |v| (L0) or the L1-ball level w (L1), normalisation
+//   5. finalize  per-start objective, relative change, logs, batch maximum
+//
+// Every reduction has a fixed order, so a step is bitwise reproducible.
+#include <cfloat>
+#include <climits>
+#include <cstdio>
+
+#include "am24_internal.h"
+#include "gemm_tf32x3.cuh"
+
+namespace am24 {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+// K slabs (of BK) accumulated in TMEM before promotion to registers
+constexpr int GEMM_PROMO = 4;
+
+// x rounded to the nearest TF32 value (low 13 mantissa bits zero).  With
+// lo = x - hi exact in FP32, x = hi + lo bit for bit, and lo takes either sign,
+// so whatever the tensor core does with lo's low bits is unbiased.
+__device__ __forceinline__ float tf32_hi(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+__device__ __forceinline__ void split_store(float x, float *hi, float *lo) {
+  const float h = tf32_hi(x);
+  *hi = h;
+  *lo = x - h;
+}
+// sgn with sgn(0) = 0 (c++/src/utils/various.h:44-46)
+__device__ __forceinline__ float sgnf(float v) { return (float)((v > 0.f) - (v < 0.f)); }
+__device__ __forceinline__ uint32_t abs_key(float v) { return __float_as_uint(v) & 0x7FFFFFFFu; }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+// Block-wide sum, result valid in every thread.  `red` holds >= 32 T.
+template <typename T>
+__device__ T block_sum(T v, T *red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  T r = (lane < nw) ? red[lane] : T(0);
+  if (w == 0) r = warp_sum(r);
+  if (threadIdx.x == 0) red[0] = r;
+  __syncthreads();
+  r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// 32 lanes each hold v[0..31] (one per column); afterwards lane L returns the
+// sum over all lanes of v[L].  31 shuffles instead of 32 x 5.
+__device__ __forceinline__ float transpose_reduce32(float (&v)[32], int lane) {
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < off; i++) {
+      const float send = upper ? v[i] : v[i + off];
+      const float keep = upper ? v[i + off] : v[i];
+      v[i] = keep + __shfl_xor_sync(FULL, send, off);
+    }
+  }
+  return v[0];
+}
+
+// ------------------------------------------------------------ GEMM epilogues
+// Z = B V split-K partial tile: ws[unit][col][row], whole 128 x bn tile.
+struct EpiPartial {
+  float *ws;
+  int bn;
+  __device__ void begin(const Unit &, int, int) {}
+  __device__ void end(const Unit &, int, int) {}
+  __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
+    float *base = ws + (size_t)t.index * ((size_t)bn * BM) + row;
+#pragma unroll
+    for (int j = 0; j < 32; j++) base[(size_t)(col0 + j) * BM] = r[j];
+  }
+};
+
+// V = B^T Z raw output (constrained forms): out[col * ld + row].
+struct EpiRaw {
+  float *out;
+  int ld, M, N, bn;
+  __device__ void begin(const Unit &, int, int) {}
+  __device__ void end(const Unit &, int, int) {}
+  __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
+    const int gi = t.mt * BM + row;
+    if (gi >= M) return;
+    const int c0 = t.nt * bn + col0;
+#pragma unroll
+    for (int j = 0; j < 32; j++)
+      if (c0 + j < N) out[(size_t)(c0 + j) * ld + gi] = r[j];
+  }
+};
+
+// V = B^T Z with the penalty threshold fused (penalized forms).
+//   L1 (c++/src/gpower/sparse_PCA_thresholding.h:26-47): d = |v| - gamma (in
+//      double, gamma is a double there), x = sgn(v) d if d > 0, objective term d^2.
+//   L0 (:68-87): d = v^2 - gamma, x = v if d > 0, objective term d.
+// Writes x as hi/lo planes and, per start and per (m-tile, warp), the partial
+// objective and non-zero count, summed in fixed order by the finalize kernel.
+template <bool L1>
+struct EpiPenalty {
+  float *V_hi, *V_lo;
+  float *obj_part, *nnz_part;
+  int ld, M, N, bn, parts;  // parts = m_tiles * 4
+  double gamma;
+  __device__ void begin(const Unit &, int, int) {}
+  __device__ void end(const Unit &, int, int) {}
+  // r holds this thread's 32 values (row `row`, columns col0..col0+31) and is
+  // overwritten with the objective terms.
+  __device__ void chunk(const Unit &t, int q, int lane, int row, int col0, float (&r)[32]) {
+    const int gi = t.mt * BM + row;
+    const bool rv = gi < M;
+    const int c0 = t.nt * bn + col0;
+    float mycnt = 0.f;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const float v = r[j];
+      float x, o;
+      if (L1) {
+        const float d = (float)((double)fabsf(v) - gamma);
+        const bool keep = d > 0.f;
+        x = keep ? d * sgnf(v) : 0.f;
+        o = keep ? __fmul_rn(d, d) : 0.f;
+      } else {
+        const float d = (float)((double)__fmul_rn(v, v) - gamma);
+        const bool keep = d > 0.f;
+        x = keep ? v : 0.f;
+        o = keep ? d : 0.f;
+      }
+      const bool valid = rv && (c0 + j < N);
+      r[j] = valid ? o : 0.f;
+      const unsigned nz = __ballot_sync(FULL, valid && x != 0.f);
+      if (lane == j) mycnt = (float)__popc(nz);
+      if (valid) {
+        const size_t off = (size_t)(c0 + j) * ld + gi;
+        split_store(x, V_hi + off, V_lo + off);
+      }
+    }
+    const float so = transpose_reduce32(r, lane);
+    const int col = c0 + lane;
+    if (col < N) {
+      obj_part[(size_t)col * parts + t.mt * 4 + q] = so;
+      nnz_part[(size_t)col * parts + t.mt * 4 + q] = mycnt;
+    }
+  }
+};
+
+// ------------------------------------------------------------ operand prep
+// Bc[c * ldm + r] = split(B[c * ldB + r]): one block per feature column.
+__global__ void prep_copy_kernel(const float *__restrict__ B, int ldB, int m, float *__restrict__ hi,
+                                 float *__restrict__ lo, int ldm) {
+  const size_t c = blockIdx.x;
+  for (int r = threadIdx.x; r < m; r += blockDim.x)
+    split_store(B[c * ldB + r], hi + c * ldm + r, lo + c * ldm + r);
+}
+
+// Bt[r * ldn + c] = split(B[c * ldB + r]): 32 x 32 tiles through shared memory.
+__global__ void prep_transpose_kernel(const float *__restrict__ B, int ldB, int m, int n,
+                                      float *__restrict__ hi, float *__restrict__ lo, int ldn) {
+  __shared__ float tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int c = c0 + y, r = r0 + threadIdx.x;
+    tile[y][threadIdx.x] = (c < n && r < m) ? B[(size_t)c * ldB + r] : 0.f;
+  }
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int r = r0 + y, c = c0 + threadIdx.x;
+    if (r < m && c < n) {
+      const size_t off = (size_t)r * ldn + c;
+      split_store(tile[threadIdx.x][y], hi + off, lo + off);
+    }
+  }
+}
+
+__global__ void split_columns_kernel(const float *__restrict__ src, int ld_src, int rows,
+                                     float *__restrict__ hi, float *__restrict__ lo, int ld_dst) {
+  const size_t c = blockIdx.x;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x)
+    split_store(src[c * ld_src + r], hi + c * ld_dst + r, lo + c * ld_dst + r);
+}
+
+__global__ void combine_columns_kernel(const float *__restrict__ hi, const float *__restrict__ lo,
+                                       int ld, int rows, float *__restrict__ dst, int ld_dst) {
+  const size_t c = blockIdx.x;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) dst[c * ld_dst + r] = hi[c * ld + r] + lo[c * ld + r];
+}
+
+// ------------------------------------------------------------ Z reduction
+// MODE 0: L2 variance, constrained  -> z = y, fz = ||y||_2  (gpower_commons.h:100)
+// MODE 1: L1 variance               -> z = sgn(y), fz = ||y||_1 (:85-86, :156)
+// MODE 2: L2 variance, penalized    -> z = y * (1/||y||_2)     (:163-164)
+template <int MODE>
+__global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__ ws, int splits,
+                                                       int m_tiles, int n_tiles, int bn, int m,
+                                                       float *__restrict__ Z_hi,
+                                                       float *__restrict__ Z_lo, int ldm,
+                                                       float *__restrict__ fz) {
+  __shared__ double red[32];
+  const int j = blockIdx.x;
+  const int nt = j / bn, c = j - nt * bn;
+  const size_t unit_stride = (size_t)bn * BM;
+  float *zh = Z_hi + (size_t)j * ldm;
+  float *zl = Z_lo + (size_t)j * ldm;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const int mt = i >> 7, r = i & 127;
+    float y = 0.f;
+    for (int s = 0; s < splits; s++) {
+      const size_t u = ((size_t)s * m_tiles + mt) * n_tiles + nt;
+      y += ws[u * unit_stride + (size_t)c * BM + r];
+    }
+    if (MODE == 1) {
+      acc += (double)fabsf(y);
+      zh[i] = sgnf(y);
+      zl[i] = 0.f;
+    } else {
+      acc += (double)y * (double)y;
+      split_store(y, zh + i, zl + i);
+    }
+  }
+  const double tot = block_sum(acc, red);
+  if (MODE == 2) {
+    const float inv = 1.0f / (float)sqrt(tot);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      const float y = zh[i] + zl[i];  // exact: this thread wrote both planes
+      split_store(y * inv, zh + i, zl + i);
+    }
+  } else if (threadIdx.x == 0) {
+    fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
+  }
+}
+
+// ------------------------------------------------------------ radix select
+struct SelResult {
+  uint32_t key;  // bit pattern of |v| at the requested descending rank
+  uint32_t gt;   // number of keys strictly greater
+  uint32_t eq;   // number of keys equal
+};
+
+template <bool CACHED>
+__device__ __forceinline__ uint32_t col_key(const float *__restrict__ g, const float *s, int i) {
+  return abs_key(CACHED ? s[i] : g[i]);
+}
+
+// Key of descending rank `rank` (1 = largest) among |col[0..n)|, by three
+// histogram passes over 11, 11 and 9 key bits.  All threads of the block
+// call it; hist has 2048 entries, res 4.
+template <bool CACHED>
+__device__ SelResult block_select(const float *__restrict__ colg, const float *cols, int n,
+                                  uint32_t rank, uint32_t *hist, uint32_t *res) {
+  uint32_t prefix = 0, pmask = 0, gt = 0, need = rank, eq = 0;
+#pragma unroll 1
+  for (int lvl = 0; lvl < 3; lvl++) {
+    const int sh = (lvl == 0) ? 20 : (lvl == 1) ? 9 : 0;
+    const uint32_t nb = (lvl == 2) ? 512u : 2048u;
+    const uint32_t bmask = nb - 1;
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t key = col_key<CACHED>(colg, cols, i);
+      if ((key & pmask) == prefix) {
+        const uint32_t bin = (key >> sh) & bmask;
+        const unsigned peers = __match_any_sync(__activemask(), bin);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], __popc(peers));
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      uint32_t running = 0, fbin = 0, fcum = 0, feq = 0;
+      bool found = false;
+      for (int base = (int)nb - 32; base >= 0 && !found; base -= 32) {
+        const uint32_t b = base + 31 - lane;
+        const uint32_t c = hist[b];
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(FULL, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const uint32_t total = __shfl_sync(FULL, incl, 31);
+        if (running + total >= need) {
+          const unsigned ballot = __ballot_sync(FULL, running + incl >= need);
+          const int f = __ffs(ballot) - 1;
+          const uint32_t inc_f = __shfl_sync(FULL, incl, f);
+          const uint32_t c_f = __shfl_sync(FULL, c, f);
+          fbin = base + 31 - f;
+          fcum = running + inc_f - c_f;
+          feq = c_f;
+          found = true;
+        } else {
+          running += total;
+        }
+      }
+      if (lane == 0) {
+        res[0] = fbin;
+        res[1] = fcum;
+        res[2] = feq;
+      }
+    }
+    __syncthreads();
+    const uint32_t bin = res[0];
+    gt += res[1];
+    need -= res[1];
+    eq = res[2];
+    prefix |= bin << sh;
+    pmask |= bmask << sh;
+    __syncthreads();
+  }
+  return SelResult{prefix, gt, eq};
+}
+
+// ------------------------------------------------------------ L0 constraint
+// k_hard_thresholding (c++/src/utils/thresh_functions.h:121-145): level = the
+// s-th largest |v| (with multiplicity, as the sorting variant :92-98 defines
+// it), keep |v| >= level, then x <- x / ||x|| (c++/src/gpower/gpower_commons.h:111).
+template <bool CACHED>
+__global__ void __launch_bounds__(512) hard_select_kernel(const float *__restrict__ Vraw, int ldv,
+                                                          int n, unsigned s,
+                                                          float *__restrict__ V_hi,
+                                                          float *__restrict__ V_lo,
+                                                          uint32_t *__restrict__ nnz_out) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
+  uint32_t *res = hist + 2048;
+  double *red = reinterpret_cast<double *>(res + 8);
+  float *cache = reinterpret_cast<float *>(red + 32);
+  const int j = blockIdx.x;
+  const float *colg = Vraw + (size_t)j * ldv;
+  if (CACHED) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) cache[i] = colg[i];
+    __syncthreads();
+  }
+  const SelResult sel = block_select<CACHED>(colg, cache, n, s, hist, res);
+  const uint32_t thr = sel.key;
+  double ss = 0.0, cnt = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = CACHED ? cache[i] : colg[i];
+    if (abs_key(v) >= thr) {
+      ss += (double)v * (double)v;
+      cnt += 1.0;
+    }
+  }
+  ss = block_sum(ss, red);
+  cnt = block_sum(cnt, red);
+  const float inv = 1.0f / (float)sqrt(ss);
+  float *vh = V_hi + (size_t)j * ldv;
+  float *vl = V_lo + (size_t)j * ldv;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = CACHED ? cache[i] : colg[i];
+    const float x = (abs_key(v) >= thr) ? v * inv : 0.f;
+    split_store(x, vh + i, vl + i);
+  }
+  if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
+}
+
+// ------------------------------------------------------------ L1 constraint
+constexpr int SOFT_C = 2048;  // sorted-candidate chunk (power of two for the bitonic sort)
+constexpr int SOFT_THREADS = 512;
+
+struct SoftSmem {
+  static constexpr size_t HIST = 2048 * 4, RES = 128, RED = 32 * 8, CAND = SOFT_C * 4,
+                          P = SOFT_C * 8;
+  static constexpr size_t FIXED = HIST + RES + RED + CAND + 2 * P + 64;
+};
+
+// Unfused double arithmetic (no FMA contraction), as host C++ evaluates it.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+// (S1 - t l) / sqrt(S2 - 2 l S1 + t l^2): ||(|v| - l)_+||_1 / ||(|v| - l)_+||_2 over the
+// top t entries, in the reference's operation order (thresh_functions.h:193-204).
+__device__ __forceinline__ double ratio_at(double S1, double S2, double t, double l) {
+  const double num = dsub(S1, dmul(t, l));
+  const double den = __dadd_rn(dsub(S2, dmul(dmul(2.0, l), S1)), dmul(dmul(t, l), l));
+  return __ddiv_rn(num, __dsqrt_rn(den));
+}
+
+// Inclusive prefix sums of cand[0..total) (0 beyond), in double, offset by
+// (o1, o2) for the values and their squares.  4 items per thread.
+__device__ void block_scan2(const float *cand, int total, double o1, double o2, double *p1,
+                            double *p2, double *red) {
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int base = t * (SOFT_C / SOFT_THREADS);
+  double a[SOFT_C / SOFT_THREADS], b[SOFT_C / SOFT_THREADS];
+  double s1 = 0, s2 = 0;
+#pragma unroll
+  for (int q = 0; q < SOFT_C / SOFT_THREADS; q++) {
+    const double v = (base + q < total) ? (double)cand[base + q] : 0.0;
+    s1 += v;
+    s2 += v * v;
+    a[q] = s1;
+    b[q] = s2;
+  }
+  // exclusive scan of (s1, s2) over threads
+  double x1 = s1, x2 = s2;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y1 = __shfl_up_sync(FULL, x1, o), y2 = __shfl_up_sync(FULL, x2, o);
+    if (lane >= o) {
+      x1 += y1;
+      x2 += y2;
+    }
+  }
+  __syncthreads();
+  if (lane == 31) {
+    red[w] = x1;
+    red[16 + w] = x2;
+  }
+  __syncthreads();
+  double w1 = 0, w2 = 0;
+  for (int i = 0; i < w; i++) {
+    w1 += red[i];
+    w2 += red[16 + i];
+  }
+  const double e1 = o1 + w1 + x1 - s1, e2 = o2 + w2 + x2 - s2;
+#pragma unroll
+  for (int q = 0; q < SOFT_C / SOFT_THREADS; q++) {
+    p1[base + q] = e1 + a[q];
+    p2[base + q] = e2 + b[q];
+  }
+  __syncthreads();
+}
+
+__device__ void bitonic_sort_desc(float *a) {
+  for (int k = 2; k <= SOFT_C; k <<= 1) {
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      for (int i = threadIdx.x; i < SOFT_C; i += blockDim.x) {
+        const int ixj = i ^ jj;
+        if (ixj > i) {
+          const float x = a[i], y = a[ixj];
+          const bool first_block = (i & k) == 0;
+          if (first_block ? (x < y) : (x > y)) {
+            a[i] = y;
+            a[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// soft_thresholding (c++/src/utils/thresh_functions.h:162-254): the level w
+// and x = sgn(v)(|v| - w)_+, then x <- x / ||x||.
+//
+// The reference sorts |v| and scans it from the top, stopping at the first
+// index i where one of three predicates holds (:197-216).  Here the sorted
+// order is produced a chunk of SOFT_C ranks at a time: a radix select finds
+// the key at the chunk's last rank, one pass gathers the keys between the
+// previous and this boundary (ties handled by counts, since only values
+// matter), a bitonic sort orders the chunk, double-precision prefix sums give
+// S1 and S2 at every rank, and every rank's predicates are evaluated in
+// parallel; the smallest breaking rank wins.  Most columns stop in the first
+// chunk; a column that never breaks is walked to its end, as the reference
+// does (then w is the '+' root of the last step).
+// EXACT: instead of the reference predicates, stop at the first segment whose
+// lower knot already satisfies ||.||_1/||.||_2 >= sqrt(s) and take the root
+// inside it: the exact L1-ball/sphere projection.
+template <bool CACHED, bool EXACT>
+__global__ void __launch_bounds__(SOFT_THREADS) soft_select_kernel(
+    const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ V_hi,
+    float *__restrict__ V_lo, uint32_t *__restrict__ nnz_out) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
+  uint32_t *res = hist + 2048;
+  double *red = reinterpret_cast<double *>(dsm + SoftSmem::HIST + SoftSmem::RES);
+  float *cand = reinterpret_cast<float *>(dsm + SoftSmem::HIST + SoftSmem::RES + SoftSmem::RED);
+  double *p1 = reinterpret_cast<double *>(reinterpret_cast<uint8_t *>(cand) + SoftSmem::CAND);
+  double *p2 = p1 + SOFT_C;
+  volatile uint32_t *misc = reinterpret_cast<volatile uint32_t *>(p2 + SOFT_C);  // 16 words
+  float *cache = reinterpret_cast<float *>(dsm + SoftSmem::FIXED);
+
+  const int j = blockIdx.x;
+  const float *colg = Vraw + (size_t)j * ldv;
+  if (CACHED) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) cache[i] = colg[i];
+    __syncthreads();
+  }
+  // sqrt(s), sqrt(s)^2, ||v||_inf - 1e-6 as the double-precision reference forms them
+  const double sq = __dsqrt_rn((double)s);
+  const double sq2 = __dmul_rn(sq, sq);
+  const SelResult top = block_select<CACHED>(colg, cache, n, 1u, hist, res);
+  const double linfty = (double)__uint_as_float(top.key);
+  const double lim = __dsub_rn(linfty, 0.000001);
+
+  uint32_t consumed = 0, khi = 0xFFFFFFFFu, ge_hi = 0;
+  double S1 = 0.0, S2 = 0.0;
+  double w = 0.0;
+  __shared__ double w_sh;
+  while (true) {
+    const uint32_t R = min(consumed + (uint32_t)SOFT_C, (uint32_t)n);
+    const uint32_t total = R - consumed;
+    const SelResult lo = block_select<CACHED>(colg, cache, n, R, hist, res);
+    if (threadIdx.x == 0) misc[0] = 0;
+    __syncthreads();
+    if (lo.key == khi) {
+      const float v = __uint_as_float(khi);
+      for (uint32_t q = threadIdx.x; q < total; q += blockDim.x) cand[q] = v;
+    } else {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t key = col_key<CACHED>(colg, cache, i);
+        if (key > lo.key && key < khi) {
+          const uint32_t slot = atomicAdd((uint32_t *)&misc[0], 1u);
+          cand[slot] = __uint_as_float(key);
+        }
+      }
+      __syncthreads();
+      const uint32_t nb = misc[0];
+      const uint32_t c_hi = ge_hi - consumed;
+      const uint32_t c_lo = R - lo.gt;
+      const float vhi = __uint_as_float(khi), vlo = __uint_as_float(lo.key);
+      for (uint32_t q = threadIdx.x; q < c_hi + c_lo; q += blockDim.x)
+        cand[nb + q] = (q < c_hi) ? vhi : vlo;
+    }
+    for (uint32_t q = total + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
+    __syncthreads();
+    bitonic_sort_desc(cand);
+    block_scan2(cand, (int)total, S1, S2, p1, p2, red);
+
+    const uint32_t E = (R == (uint32_t)n) ? total : total - 1;
+    uint32_t best = 0xFFFFFFFFu;
+    double bw = 0.0;
+    double w_last = 0.0;
+    for (uint32_t q = threadIdx.x; q < E; q += blockDim.x) {
+      const uint32_t g = consumed + q;
+      const double t = (double)(g + 1);
+      const double hi = (double)cand[q];
+      const double lov = (q + 1 < total) ? (double)cand[q + 1] : 0.0;
+      const double S1i = p1[q], S2i = p2[q];
+      if (!EXACT) {
+        // Same operations, order and (unfused) rounding as the reference's
+        // expressions at thresh_functions.h:193-213; several of its breaks are
+        // decided by the last bit (e.g. a zero discriminant at the first step).
+        const double S1p = q ? p1[q - 1] : S1, S2p = q ? p2[q - 1] : S2;
+        const double left = ratio_at(S1i, S2i, t, hi);
+        const double rprev = (g == 0) ? sq : ratio_at(S1p, S2p, t - 1.0, hi);
+        const double a = dmul(t, dsub(t, sq2));
+        const double b = dsub(dmul(dmul(2.0, S1i), sq2), dmul(dmul(2.0, t), S1i));
+        const double c = dsub(dmul(S1i, S1i), dmul(sq2, S2i));
+        const double disc = __dsqrt_rn(dsub(dmul(b, b), dmul(dmul(4.0, a), c)));
+        const double wm = __ddiv_rn(dsub(-b, disc), dmul(2.0, a));
+        const double wp = __ddiv_rn(__dadd_rn(-b, disc), dmul(2.0, a));
+        if (g + 1 == (uint32_t)n) w_last = wp;
+        double cw = 0.0;
+        bool hit = false;
+        if (left > sq && rprev < sq) {
+          hit = true;
+          cw = hi;
+        } else if (wm > lov && wm < hi) {
+          hit = true;
+          cw = wm;
+        } else if (wp > lov && wp < hi && wp < lim) {
+          hit = true;
+          cw = wp;
+        }
+        if (hit && g < best) {
+          best = g;
+          bw = cw;
+        }
+      } else {
+        const double rlo = (S1i - t * lov) / sqrt(S2i - 2.0 * lov * S1i + t * lov * lov);
+        if (rlo >= sq && g < best) {
+          const double a = t * (t - sq2);
+          const double b = 2.0 * S1i * sq2 - 2.0 * t * S1i;
+          const double c = S1i * S1i - sq2 * S2i;
+          double lam;
+          if (a == 0.0) {
+            lam = -c / b;
+          } else {
+            const double disc = sqrt(fmax(b * b - 4.0 * a * c, 0.0));
+            const double r1 = (-b - disc) / (2.0 * a), r2 = (-b + disc) / (2.0 * a);
+            // the genuine root keeps every one of the t entries above it
+            const bool ok1 = r1 >= lov && r1 <= hi, ok2 = r2 >= lov && r2 <= hi;
+            lam = ok1 ? r1 : ok2 ? r2 : fmin(fmax(r1, lov), hi);
+          }
+          best = g;
+          bw = lam;
+        }
+      }
+    }
+    // block minimum of the breaking rank
+    uint32_t mb = best;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mb = min(mb, __shfl_xor_sync(FULL, mb, o));
+    if ((threadIdx.x & 31) == 0) res[4 + (threadIdx.x >> 5)] = mb;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t m2 = 0xFFFFFFFFu;
+      for (int i = 0; i < (int)(blockDim.x >> 5); i++) m2 = min(m2, res[4 + i]);
+      misc[1] = m2;
+    }
+    __syncthreads();
+    const uint32_t brk = misc[1];
+    if (brk != 0xFFFFFFFFu) {
+      if (best == brk) w_sh = bw;
+      __syncthreads();
+      w = w_sh;
+      break;
+    }
+    if (R == (uint32_t)n) {
+      // never stopped: the reference keeps the '+' root of its last step;
+      // the exact projection with ratio < sqrt(s) everywhere is lambda = 0
+      if (!EXACT && consumed + E - 1 == (uint32_t)n - 1 && threadIdx.x == (E - 1) % blockDim.x)
+        w_sh = w_last;
+      if (EXACT && threadIdx.x == 0) w_sh = 0.0;
+      __syncthreads();
+      w = w_sh;
+      break;
+    }
+    consumed += E;
+    S1 = p1[E - 1];
+    S2 = p2[E - 1];
+    khi = lo.key;
+    ge_hi = lo.gt + lo.eq;
+    __syncthreads();
+  }
+
+  // x = sgn(v)(|v| - w)_+ with w kept in double: a level that lands within
+  // rounding of the largest |v| still leaves that entry non-zero, as in the
+  // reference's double arithmetic.
+  double ss = 0.0, cnt = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = CACHED ? cache[i] : colg[i];
+    const double d = (double)fabsf(v) - w;
+    if (d > 0.0) {
+      const float x = (float)d * sgnf(v);
+      ss += (double)x * (double)x;
+      cnt += 1.0;
+    }
+  }
+  ss = block_sum(ss, red);
+  cnt = block_sum(cnt, red);
+  const float inv = 1.0f / (float)sqrt(ss);
+  float *vh = V_hi + (size_t)j * ldv;
+  float *vl = V_lo + (size_t)j * ldv;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = CACHED ? cache[i] : colg[i];
+    const double d = (double)fabsf(v) - w;
+    const float x = (d > 0.0) ? (float)d * sgnf(v) : 0.f;
+    split_store(x * inv, vh + i, vl + i);
+  }
+  if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
+}
+
+// ------------------------------------------------------------ finalize
+// Per start: objective f, relative change |f - f0| / f0
+// (c++/src/utils/termination_criteria.h:30-36), the storeIterationsForAllPoints
+// logs (c++/src/gpower/gpower_commons.h:120-130), and the batch maximum that
+// ignores NaN changes (:132-133).  One block.
+struct FinalizeArgs {
+  int k, formulation, parts, it, store_all, log_shift, log_capacity;
+  double tolerance;
+  const float *fz;
+  const float *obj_part, *nnz_part;
+  const uint32_t *nnz_sel;
+  float *val, *err, *max_err;
+  int *iters, *cards;
+};
+
+__global__ void __launch_bounds__(1024) finalize_kernel(FinalizeArgs a) {
+  __shared__ float redf[32];
+  const bool cons = a.formulation <= 3;
+  const bool l1pen = a.formulation >= 6;
+  float lm = 0.f;
+  for (int j = threadIdx.x; j < a.k; j += blockDim.x) {
+    float f;
+    uint32_t nz;
+    if (cons) {
+      f = a.fz[j];
+      nz = a.nnz_sel[j];
+    } else {
+      double acc = 0.0, c = 0.0;
+      for (int q = 0; q < a.parts; q++) {
+        acc += (double)a.obj_part[(size_t)j * a.parts + q];
+        c += (double)a.nnz_part[(size_t)j * a.parts + q];
+      }
+      f = l1pen ? (float)sqrt(acc) : (float)acc;
+      nz = (uint32_t)c;
+    }
+    const float f0 = a.val[j];
+    const float e = fabsf(f - f0) / f0;
+    a.err[j] = e;
+    a.val[j] = f;
+    if (lm < e) lm = e;
+    if (a.store_all) {
+      // the penalized thresholding calls log into slot j of every batch
+      // (gpower_commons.h:170,173 leave the batch shift at 0)
+      const int slot = cons ? a.log_shift + j : j;
+      if (slot < a.log_capacity) {
+        const bool done = a.it > 0 && (double)e < a.tolerance;
+        if (done && a.iters[slot] == -1) {
+          a.iters[slot] = a.it;
+          a.cards[slot] = (int)nz;
+        } else if (!done && a.iters[slot] != -1) {
+          a.iters[slot] = -1;
+        }
+      }
+    }
+  }
+  // block max with the reference's `if (max < e) max = e` (NaN never wins)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float y = __shfl_xor_sync(FULL, lm, o);
+    if (lm < y) lm = y;
+  }
+  if ((threadIdx.x & 31) == 0) redf[threadIdx.x >> 5] = lm;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++)
+      if (m < redf[i]) m = redf[i];
+    *a.max_err = m;
+  }
+}
+
+// x = v / ||v|| with v = hi + lo (c++/src/gpower/sparse_PCA_solver.h:236-237).
+__global__ void finalize_x_kernel(const float *__restrict__ h, const float *__restrict__ l, int n,
+                                  float *__restrict__ x) {
+  __shared__ double red[32];
+  double ss = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = h[i] + l[i];
+    ss += (double)v * (double)v;
+  }
+  ss = block_sum(ss, red);
+  const float inv = 1.0f / (float)sqrt(ss);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (h[i] + l[i]) * inv;
+}
+
+// y_r = sum_c B[r, c] x_c in FP64, one warp per sample row of Bt (hi + lo = B exactly).
+__global__ void ev_rows_kernel(const float *__restrict__ hi, const float *__restrict__ lo, int ld,
+                               int m, int n, const float *__restrict__ x,
+                               double *__restrict__ y) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= m) return;
+  const float *h = hi + (size_t)warp * ld;
+  const float *l = lo + (size_t)warp * ld;
+  double acc = 0.0;
+  for (int c = lane; c < n; c += 32) acc += ((double)h[c] + (double)l[c]) * (double)x[c];
+  acc = warp_sum(acc);
+  if (lane == 0) y[warp] = acc;
+}
+
+__global__ void ev_sum_kernel(const double *__restrict__ y, int m, double *__restrict__ out) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) acc += y[i] * y[i];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) *out = acc;
+}
+
+// ------------------------------------------------------------ GEMM launch
+struct GemmCfg {
+  int bn, stages;
+};
+
+template <int BN, int ST, class Epi>
+cudaError_t run_gemm(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
+                     const CUtensorMap &b_lo, const GemmShape &sh, const Epi &epi,
+                     cudaStream_t st) {
+  using L = GemmSmem<BN, BK, ST>;
+  auto kern = gemm_tf32x3_kernel<BN, BK, ST, GEMM_PROMO, Epi>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int grid = sh.num_units < num_sms() ? sh.num_units : num_sms();
+  kern<<<grid, GEMM_THREADS, L::TOTAL, st>>>(a_hi, a_lo, b_hi, b_lo, sh, epi);
+  return cudaGetLastError();
+}
+
+template <class Epi>
+cudaError_t dispatch_gemm(int bn, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
+                          const CUtensorMap &b_hi, const CUtensorMap &b_lo, const GemmShape &sh,
+                          const Epi &epi, cudaStream_t st) {
+  switch (bn) {
+    case 256: return run_gemm<256, 2>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+    case 128: return run_gemm<128, 3>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+    case 64: return run_gemm<64, 4>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <bool CACHED_OK, class F1, class F2>
+cudaError_t launch_select(bool cached, size_t smem_fixed, int n, int grid, int threads, F1 kc, F2 kg,
+                          cudaStream_t st, const float *Vraw, int ld, unsigned s, float *vh,
+                          float *vl, uint32_t *nnz) {
+  if (cached) {
+    const size_t smem = smem_fixed + (size_t)n * 4;
+    cudaError_t e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kc<<<grid, threads, smem, st>>>(Vraw, ld, n, s, vh, vl, nnz);
+  } else {
+    cudaError_t e =
+        cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fixed);
+    if (e != cudaSuccess) return e;
+    kg<<<grid, threads, smem_fixed, st>>>(Vraw, ld, n, s, vh, vl, nnz);
+  }
+  return cudaGetLastError();
+}
+
+constexpr size_t SMEM_LIMIT = 227 * 1024;
+constexpr size_t HARD_FIXED = 2048 * 4 + 32 + 32 * 8 + 64;
+
+}  // namespace
+
+int num_sms() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 1;
+  }
+  return sms;
+}
+
+int pick_bn(int k) { return k > 128 ? 256 : (k > 64 ? 128 : 64); }
+
+size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn) {
+  return (size_t)splits * m_tiles * n_tiles * bn * BM;
+}
+
+cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st) {
+  prep_copy_kernel<<<M.n, 256, 0, st>>>(B, ldB, M.m, M.Bc_hi, M.Bc_lo, M.ldm);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 grid((M.n + 31) / 32, (M.m + 31) / 32);
+  prep_transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(B, ldB, M.m, M.n, M.Bt_hi, M.Bt_lo, M.ldn);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split_columns(const float *src, int ld_src, int rows, int cols, float *hi,
+                                 float *lo, int ld_dst, cudaStream_t st) {
+  if (cols <= 0) return cudaSuccess;
+  split_columns_kernel<<<cols, 256, 0, st>>>(src, ld_src, rows, hi, lo, ld_dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine_columns(const float *hi, const float *lo, int ld, int rows, int cols,
+                                   float *dst, int ld_dst, cudaStream_t st) {
+  if (cols <= 0) return cudaSuccess;
+  combine_columns_kernel<<<cols, 256, 0, st>>>(hi, lo, ld, rows, dst, ld_dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_x(const float *hi, const float *lo, int n, float *x, cudaStream_t st) {
+  finalize_x_kernel<<<1, 1024, 0, st>>>(hi, lo, n, x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double *partial,
+                                      double *out, cudaStream_t st) {
+  const int threads = 256;
+  const int blocks = (M.m * 32 + threads - 1) / threads;
+  ev_rows_kernel<<<blocks, threads, 0, st>>>(M.Bt_hi, M.Bt_lo, M.ldn, M.m, M.n, x, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  ev_sum_kernel<<<1, 1024, 0, st>>>(partial, M.m, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm,
+                           const StepParams &p, cudaStream_t st, int *launches, cudaEvent_t *ev,
+                           int *kinds) {
+  cudaError_t e;
+  int nl = 0;
+  const int f = p.formulation;
+  auto mark = [&](int kind) -> cudaError_t {
+    if (kinds) kinds[nl] = kind;
+    return ev ? cudaEventRecord(ev[nl], st) : cudaSuccess;
+  };
+  // 1. Z = B V (split-K partials)
+  GemmShape g1;
+  g1.M = M.m;
+  g1.N = b.k;
+  g1.K = M.n;
+  g1.m_tiles = b.m_tiles1;
+  g1.n_tiles = b.n_tiles1;
+  g1.kb_total = (M.n + BK - 1) / BK;
+  g1.kb_per_split = b.kbps1;
+  g1.splits = b.splits1;
+  g1.num_units = g1.splits * g1.m_tiles * g1.n_tiles;
+  g1.timeout_ns = p.timeout_ns;
+  g1.status = b.status;
+  EpiPartial ep{b.ws, b.bn1};
+  if ((e = mark(0)) != cudaSuccess) return e;
+  e = dispatch_gemm(b.bn1, tm.a1_hi, tm.a1_lo, tm.b1_hi, tm.b1_lo, g1, ep, st);
+  if (e != cudaSuccess) return e;
+  nl++;
+  // 2. reduce + sign / normalise
+  const int mode = is_l1_variance(f) ? 1 : (is_constrained(f) ? 0 : 2);
+  if ((e = mark(1)) != cudaSuccess) return e;
+  if (mode == 0)
+    z_reduce_kernel<0><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz);
+  else if (mode == 1)
+    z_reduce_kernel<1><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz);
+  else
+    z_reduce_kernel<2><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  nl++;
+  // 3. V = B^T Z
+  GemmShape g2;
+  g2.M = M.n;
+  g2.N = b.k;
+  g2.K = M.m;
+  g2.m_tiles = b.m_tiles2;
+  g2.n_tiles = b.n_tiles2;
+  g2.kb_total = (M.m + BK - 1) / BK;
+  g2.kb_per_split = g2.kb_total;
+  g2.splits = 1;
+  g2.num_units = g2.m_tiles * g2.n_tiles;
+  g2.timeout_ns = p.timeout_ns;
+  g2.status = b.status;
+  const int parts = b.m_tiles2 * 4;
+  if ((e = mark(2)) != cudaSuccess) return e;
+  if (is_constrained(f)) {
+    EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
+    e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, er, st);
+  } else if (is_l1_penalized(f)) {
+    EpiPenalty<true> pe{b.V_hi, b.V_lo, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
+                        p.penalty};
+    e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
+  } else {
+    EpiPenalty<false> pe{b.V_hi, b.V_lo, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
+                         p.penalty};
+    e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
+  }
+  if (e != cudaSuccess) return e;
+  nl++;
+  // 4. constrained: selection / projection + normalisation
+  if (is_constrained(f)) {
+    if ((e = mark(3)) != cudaSuccess) return e;
+    if (!is_l1_constrained(f)) {
+      const bool cached = HARD_FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
+      e = launch_select<true>(cached, HARD_FIXED, M.n, b.k, 512, hard_select_kernel<true>,
+                              hard_select_kernel<false>, st, b.Vraw, M.ldn, p.constraint, b.V_hi,
+                              b.V_lo, b.nnz);
+    } else {
+      const bool cached = SoftSmem::FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
+      if (p.l1_mode == 0)
+        e = launch_select<true>(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
+                                soft_select_kernel<true, false>, soft_select_kernel<false, false>,
+                                st, b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz);
+      else
+        e = launch_select<true>(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
+                                soft_select_kernel<true, true>, soft_select_kernel<false, true>,
+                                st, b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz);
+    }
+    if (e != cudaSuccess) return e;
+    nl++;
+  }
+  // 5. finalize
+  FinalizeArgs fa;
+  fa.k = b.k;
+  fa.formulation = f;
+  fa.parts = parts;
+  fa.it = p.it;
+  fa.store_all = p.store_all;
+  fa.log_shift = p.log_shift;
+  fa.log_capacity = b.log_capacity;
+  fa.tolerance = p.tolerance;
+  fa.fz = b.fz;
+  fa.obj_part = b.obj_part;
+  fa.nnz_part = b.nnz_part;
+  fa.nnz_sel = b.nnz;
+  fa.val = b.val;
+  fa.err = b.err;
+  fa.max_err = b.max_err;
+  fa.iters = b.iters;
+  fa.cards = b.cards;
+  if ((e = mark(4)) != cudaSuccess) return e;
+  finalize_kernel<<<1, 1024, 0, st>>>(fa);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  nl++;
+  if (ev && (e = cudaEventRecord(ev[nl], st)) != cudaSuccess) return e;
+  if (launches) *launches = nl;
+  return cudaSuccess;
+}
+
+}  // namespace am24

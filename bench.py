@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the AM sparse-PCA hot path (start-iterations per second).
+
+Workload (one GPU): n = 2000 samples x p = 50000 features, low-rank (r = 50,
+256 non-zeros per loading) plus N(0, 0.1^2) noise, seeded and generated on
+the device; k = 1024 starting points U[-1, 1] normalised; all 8 formulations:
+s = 16 for the constraint forms, gamma = 0.1 x max column 2-norm (L2-variance
+penalties) or 0.1 x max column 1-norm (L1-variance penalties).  FP32 data,
+3xTF32 tensor-core products with FP32 accumulation.
+
+A step is one AM iteration of every formulation over its k starts, i.e.
+8 x 1024 start-iterations.  `value` = start-iterations/s of the whole job with
+the data resident in HBM (device-timed with CUDA events on the library's
+stream, max over ranks).  `e2e` is the same metric through the public
+one-call API am24_solve_dense_f32 with host (pinned) buffers, host<->device
+copies included, each formulation solved to its own convergence (maxIter 200,
+tol 1e-6).  `roofline` is for the dominant kernel, from per-kernel CUDA events
+inside the timed steps.  `cpu_baseline` times the reference's own CPU solver
+(built from its sources, multithreaded OpenBLAS) on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU under torchrun; every rank runs the same
+workload on its own starting points (start sharding, weak scaling, no
+collective on the data path).
+"""
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = 2000, 50000, 50, 256, 1024
+S_CONS, GAMMA_C, SEED = 16, 0.1, 1
+E2E_MAX_IT, E2E_TOL = 200, 1e-6
+CPU_SAMPLE_STARTS, CPU_SAMPLE_ITERS = 64, 3
+WORKLOAD = (f"config-1 AM step: n={N_SAMPLES} samples x p={P_FEATURES} features (r={RANK}, "
+            f"{NNZ_V} nnz/loading), k={STARTS} starts, 8 formulations, plain FP32 path")
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, \
+            "fallback"
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` on this workload from the committed ncu
+    summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "am_step_config1.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(rf"^traffic_bytes_per_launch\s+{re.escape(kernel)}\s+([0-9.eE+]+)", txt, re.M)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        self.gpu = ids[gpu] if gpu < len(ids) else str(gpu)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_reference(B_host, steps, per_step_iters, starts):
+    """The reference's own denseDataSolver<float> (oracle/_ref, OpenBLAS,
+    all host threads) on n x p = B_host, `starts` starting points per
+    formulation, `per_step_iters` iterations; returns (start-it/s, cores, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle as po
+    cores = os.cpu_count() or 1
+    kind = "reference"
+    blas = "openblas"
+    if not po.ref_available(blas):
+        blas = "naive"
+    if not po.ref_available(blas):
+        kind = "port"
+    gam = {}
+    col2 = float(np.sqrt((B_host.astype(np.float64) ** 2).sum(0)).max())
+    col1 = float(np.abs(B_host).sum(0, dtype=np.float64).max())
+    gam = {4: GAMMA_C * col2, 6: GAMMA_C * col2, 5: GAMMA_C * col1, 7: GAMMA_C * col1}
+    if kind == "reference":
+        po.ref_set_threads(cores, blas)
+    total_its, total_s = 0, 0.0
+    for _ in range(steps):
+        for f in range(8):
+            s = po.make_settings(f, constraint=S_CONS, penalty=gam.get(f, 0.0), tolerance=0.0,
+                                 max_iter=per_step_iters, total_starts=starts, batch_size=starts)
+            if kind == "reference":
+                r = po.ref_solve(B_host, s, blas=blas)
+                total_s += r["compute_time"]
+            else:
+                t0 = time.perf_counter()
+                r = po.oracle_solve(B_host, s)
+                total_s += time.perf_counter() - t0
+                cores = 1
+            total_its += starts * int(r["it"])
+    return total_its / total_s, cores, kind, total_its, total_s
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+    am = importlib.import_module("24am_b200")
+    wl = am.workloads
+    import torch
+    if torch.cuda.is_available():
+        B = wl.low_rank_data_torch(N_SAMPLES, P_FEATURES, RANK, NNZ_V, SEED).cpu().numpy()
+    else:
+        B = wl.low_rank_data(N_SAMPLES, P_FEATURES, RANK, NNZ_V, SEED, dtype=np.float32).T.copy()
+    B_host = np.asfortranarray(B.T)  # n x p column-major
+    cpu_reference(B_host, args.warmup, 1, CPU_SAMPLE_STARTS)  # untimed warm-up steps
+    t0 = time.time()
+    v, cores, kind, its, secs = cpu_reference(B_host, args.steps, 1, CPU_SAMPLE_STARTS)
+    wall = time.time() - t0
+    sample = (f"{args.steps} steps x 8 formulations x 1 iteration x {CPU_SAMPLE_STARTS} starts "
+              f"on the full {N_SAMPLES}x{P_FEATURES} matrix ({its} start-iterations, "
+              f"{secs:.1f} s compute)")
+    line = {"impl": "reference", "metric": "start-iterations/s", "value": v,
+            "unit": "start-it/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N_SAMPLES, "p": P_FEATURES,
+                       "starts": CPU_SAMPLE_STARTS, "s": S_CONS, "gamma_factor": GAMMA_C},
+            "cpu_baseline": {"value": v, "unit": "start-it/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "start-it/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    am = importlib.import_module("24am_b200")
+    wl = am.workloads
+    solver = am.Solver(local)
+    stream = torch.cuda.ExternalStream(solver.stream())
+
+    Dt = wl.low_rank_data_torch(N_SAMPLES, P_FEATURES, RANK, NNZ_V, SEED)  # (p, n): B col-major
+    col2 = float(Dt.double().norm(dim=1).max())
+    col1 = float(Dt.double().abs().sum(dim=1).max())
+    gam = wl.penalty_gammas(col2, col1, GAMMA_C)
+    torch.cuda.synchronize()
+    M = am.Matrix(solver, None, on_device_ptr=Dt.data_ptr(), m=N_SAMPLES, n=P_FEATURES,
+                  ldB=N_SAMPLES)
+    batches, starts = [], []
+    for f in range(8):
+        V = wl.uniform_starts_torch(P_FEATURES, STARTS, seed=1000 + SEED + 17 * rank + f)
+        torch.cuda.synchronize()
+        st = am.OptimizationSettings(formulation=f, constraintParameter=S_CONS,
+                                     penaltyParameter=gam.get(f, 0.0), tolerance=E2E_TOL,
+                                     maximumIterations=E2E_MAX_IT, totalStartingPoints=STARTS,
+                                     batchSize=STARTS)
+        b = M.batch(st, STARTS)
+        b.load(device_ptr=V.data_ptr())
+        batches.append(b)
+        starts.append(V)
+    launches_per_step = sum(b.launches_per_step() for b in batches)
+
+    def step(it):
+        for b in batches:
+            b.iterate(it, 1, sync=False)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for i in range(args.warmup):
+        step(i)
+    solver.sync()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for i in range(args.steps):
+            step(args.warmup + i)
+        e1.record(stream)
+        solver.sync()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    its_per_step = 8 * STARTS
+    value = its_per_step * args.steps * world / (ms_max * 1e-3)
+
+    # per-kernel CUDA events inside the same kind of steps
+    per_kind = {}
+    for i in range(max(1, min(args.steps, 5))):
+        for f, b in enumerate(batches):
+            for kind, kms in b.step_timed(args.warmup + args.steps + i):
+                key = kind if kind not in ("gemm_BtZ", "select") else (
+                    f"{kind}_{'cons' if f <= 3 else 'pen'}")
+                per_kind.setdefault(key, []).append(kms)
+    totals = {k: sum(v) for k, v in per_kind.items()}
+    dom = max(totals, key=totals.get)
+    pk, pk_kind = peaks()
+    tf32x3_peak = pk["bf16_tflops_sustained"] / 2.0 / 3.0
+    avg_ms = statistics.mean(per_kind[dom])
+    if dom.startswith("gemm"):
+        flops = 2.0 * N_SAMPLES * P_FEATURES * STARTS
+        achieved = flops / (avg_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": tf32x3_peak, "unit": "TFLOP/s",
+                "frac": achieved / tf32x3_peak, "traffic": profiled_traffic(dom),
+                "kernel": dom, "avg_launch_ms": avg_ms,
+                "peak_note": f"{pk_kind} bf16 sustained {pk['bf16_tflops_sustained']} TF/s "
+                             "/2 (TF32 rate) /3 (three TF32 MMAs per FP32 product); "
+                             "achieved counts 2*n*p*k dense FLOPs per launch"}
+    else:
+        byts = 4.0 * P_FEATURES * STARTS * 3
+        achieved = byts / (avg_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"], "traffic": profiled_traffic(dom),
+                "kernel": dom, "avg_launch_ms": avg_ms}
+    breakdown = {k: {"launches": len(v), "avg_ms": statistics.mean(v),
+                     "share": totals[k] / sum(totals.values())} for k, v in per_kind.items()}
+
+    # e2e through the one-call public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        Bh = Dt.cpu().pin_memory()  # (p, n) contiguous == n x p column-major
+        x = torch.zeros(P_FEATURES, dtype=torch.float32).pin_memory()
+        t_e2e, its_e2e, h2d, d2h = 0.0, 0, 0, 0
+        for _ in range(max(1, args.e2e_steps)):
+            for f in range(8):
+                Vh = starts[f].cpu().pin_memory()
+                st = am.OptimizationSettings(formulation=f, constraintParameter=S_CONS,
+                                             penaltyParameter=gam.get(f, 0.0), tolerance=E2E_TOL,
+                                             maximumIterations=E2E_MAX_IT,
+                                             totalStartingPoints=STARTS, batchSize=STARTS,
+                                             startMode=am.START_INJECTED)
+                s_c = st.to_c()
+                stc = am.am24_statistics()
+                fv = C.c_float()
+                barrier()
+                t0 = time.perf_counter()
+                am.check(am.lib().am24_solve_dense_f32(
+                    solver.h, C.c_void_p(Bh.data_ptr()), N_SAMPLES, C.c_void_p(x.data_ptr()),
+                    N_SAMPLES, P_FEATURES, C.byref(s_c), C.byref(stc),
+                    C.c_void_p(Vh.data_ptr()), C.byref(fv)))
+                t_e2e += time.perf_counter() - t0
+                its_e2e += int(stc.start_iterations)
+                h2d += Bh.numel() * 4 + Vh.numel() * 4
+                d2h += x.numel() * 4
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        steps_e2e = max(1, args.e2e_steps)
+        e2e = {"value": its_e2e * world / float(tt.item()), "unit": "start-it/s",
+               "h2d_bytes_per_step": h2d // steps_e2e, "d2h_bytes_per_step": d2h // steps_e2e,
+               "solves_per_step": 8, "start_iterations": its_e2e,
+               "note": "am24_solve_dense_f32 per formulation, maxIter 200, tol 1e-6, "
+                       "pinned host B and starts, wall clock around each call"}
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu:
+        Bnp = Dt.cpu().numpy().T  # n x p view, column-major
+        import numpy as np
+        Bnp = np.asfortranarray(Bnp)
+        v, cores, kind, its, secs = cpu_reference(Bnp, 1, CPU_SAMPLE_ITERS, CPU_SAMPLE_STARTS)
+        cpu = {"value": v, "unit": "start-it/s", "cores": cores, "kind": kind,
+               "sample": f"8 formulations x {CPU_SAMPLE_ITERS} iterations x "
+                         f"{CPU_SAMPLE_STARTS} starts on the full matrix ({its} start-iterations, "
+                         f"{secs:.1f} s compute, reference denseDataSolver<float> + OpenBLAS)"}
+
+    if rank == 0:
+        line = {"metric": "start-iterations/s", "value": value, "unit": "start-it/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "n": N_SAMPLES, "p": P_FEATURES,
+                           "starts_per_gpu": STARTS, "formulations": 8, "s": S_CONS,
+                           "gamma_factor": GAMMA_C, "precision": "3xTF32 products, FP32 accumulate",
+                           "l2": "inputs larger than L2 (B as 4 FP32 planes = 1.6 GB)",
+                           "parallelism": f"start-sharded x{world}, no data-path collective"},
+                "roofline": roof, "kernels": breakdown, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches_per_step * args.steps,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    for b in batches:
+        b.close()
+    M.close()
+    solver.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

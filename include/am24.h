@@ -1,0 +1,206 @@
+/*
+ * am24.h -- C ABI of the B200-native alternating-maximization (AM) sparse-PCA
+ * core.  Plain C types only (no CUDA or torch types), so any FFI can bind it.
+ *
+ * The library replaces the reference's (optml/24am) dense AM solver:
+ *   SPCASolver::MulticoreSolver::denseDataSolver<F>(const F* B, int ldB, F* x,
+ *       unsigned m, unsigned n, OptimizationSettings*, OptimizationStatistics*)
+ *       -- c++/src/gpower/sparse_PCA_solver.h:36-40
+ *   SPCASolver::GPUSolver::denseDataSolver<F>(cublasHandle_t&, m, n,
+ *       thrust::device_vector<F>& d_B, thrust::host_vector<F>& h_x, settings*,
+ *       stats*, LD_M, LD_N) -- c++/src/gpugpower/gpu_sparse_PCA_solver.h:29-35
+ * The C++ adapter in include/am24/sparse_PCA_solver.h keeps those exact
+ * signatures on top of this ABI.
+ *
+ * Conventions (as in the reference): B is the m x n data matrix, m samples by
+ * n features, column-major with leading dimension ldB >= m.  x receives the n
+ * loadings of the best starting point, normalised to unit 2-norm.  Each
+ * starting point is an n-vector; a batch of them is n x k column-major.
+ *
+ * Every call returns an am24_status; am24_last_error() describes the last
+ * failure on the calling thread.  Handles are independent (one CUDA stream
+ * each); one handle must not be used from two threads at once.
+ */
+#ifndef AM24_H
+#define AM24_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AM24_ABI_VERSION 1
+
+typedef enum {
+  AM24_OK = 0,
+  AM24_ERR_INVALID_ARG = 1,    /* bad size, pointer, formulation or parameter */
+  AM24_ERR_OOM = 2,            /* device allocation failed */
+  AM24_ERR_CUDA = 3,           /* CUDA runtime/driver error */
+  AM24_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait gave up */
+  AM24_ERR_UNSUPPORTED = 5,    /* device is not sm_100 or feature not built */
+  AM24_ERR_DEGENERATE = 6      /* informational: some start produced a NaN objective */
+} am24_status;
+
+/* SPCA_Formulation (c++/src/class/optimization_settings.h:27-37), same values. */
+typedef enum {
+  AM24_L0_CONSTRAINED_L2_PCA = 0,
+  AM24_L0_CONSTRAINED_L1_PCA = 1,
+  AM24_L1_CONSTRAINED_L2_PCA = 2,
+  AM24_L1_CONSTRAINED_L1_PCA = 3,
+  AM24_L0_PENALIZED_L2_PCA = 4,
+  AM24_L0_PENALIZED_L1_PCA = 5,
+  AM24_L1_PENALIZED_L2_PCA = 6,
+  AM24_L1_PENALIZED_L1_PCA = 7
+} am24_formulation;
+
+/* How starting points are produced. */
+typedef enum {
+  AM24_START_REFERENCE = 0, /* the reference generator: rand_r seeded with the global
+                               start index (c++/src/gpower/gpower_commons.h:22-47) */
+  AM24_START_INJECTED = 1   /* caller-supplied n x total_starts matrix */
+} am24_start_mode;
+
+/* L1-constraint projection (the soft-thresholding level w). */
+typedef enum {
+  AM24_L1_REFERENCE_SCAN = 0, /* the reference's first-break scan
+                                 (c++/src/utils/thresh_functions.h:162-218) */
+  AM24_L1_EXACT = 1           /* exact ||x||_1/||x||_2 = sqrt(s) projection */
+} am24_l1_mode;
+
+/* Mirror of OptimizationSettings (c++/src/class/optimization_settings.h:71-123),
+ * fields the dense AM path reads, fixed-width.  am24_default_settings() gives the
+ * reference's defaults.  total_starts, batch_size, constraint, total_batches and
+ * store_all are rewritten by a solve exactly as the reference rewrites them. */
+typedef struct {
+  int32_t formulation;     /* am24_formulation */
+  uint32_t constraint;     /* constraintParameter s (default 10) */
+  double penalty;          /* penaltyParameter gamma (default 0) */
+  double tolerance;        /* default 0.01 */
+  int32_t max_iter;        /* maximumIterations (default 20) */
+  int32_t total_starts;    /* totalStartingPoints (default 64) */
+  int32_t batch_size;      /* batchSize (default 64) */
+  int32_t use_otf;         /* useOTF (default 0) */
+  int32_t use_sort_hard;   /* useSortForHardThresholding (default 0) */
+  int32_t store_all;       /* storeIterationsForAllPoints (default 0) */
+  uint32_t total_batches;  /* totalBatches: output */
+  int32_t verbose;
+  /* extensions */
+  int32_t start_mode;      /* am24_start_mode (default AM24_START_REFERENCE) */
+  int32_t l1_mode;         /* am24_l1_mode (default AM24_L1_REFERENCE_SCAN) */
+  uint32_t timeout_ms;     /* bound on any device-side wait (default 5000) */
+  uint32_t reserved[7];
+} am24_settings;
+
+/* Mirror of OptimizationStatistics (c++/src/class/optimization_statistics.h:27-46).
+ * The per-start arrays are caller-provided (NULL = not wanted) with capacity
+ * per_start_capacity; they are filled when settings.store_all is set, as the
+ * reference fills values/iters/cardinalities. */
+typedef struct {
+  uint32_t it;                         /* total (batch-)iterations */
+  double fval;                         /* best objective (the return value) */
+  double error;                        /* last batch-maximum relative change */
+  double total_true_computation_time;  /* seconds spent iterating */
+  double total_elapsed_time;           /* seconds for the whole call */
+  uint32_t n;                          /* length of x */
+  int32_t total_threads_used;          /* 1 (one device stream) */
+  double *values;
+  int32_t *iters;
+  int32_t *cardinalities;
+  uint32_t per_start_capacity;
+  /* extensions */
+  double explained_variance;  /* ||B x||_2^2 of the returned x, FP64 on the device */
+  uint64_t start_iterations;  /* AM steps summed over starting points */
+  int32_t degenerate_starts;  /* starts whose final objective was NaN */
+  uint32_t reserved[7];
+} am24_statistics;
+
+typedef struct am24_handle_s *am24_handle;
+typedef struct am24_matrix_s *am24_matrix;
+typedef struct am24_batch_s *am24_batch;
+
+/* ---- library / handle ---------------------------------------------------- */
+uint32_t am24_abi_version(void);
+const char *am24_last_error(void);
+const char *am24_status_string(am24_status s);
+void am24_default_settings(am24_settings *s);
+/* chceckInputAndModifyIt (c++/src/class/optimization_settings.h:156-168):
+ * s <= n, batch 0 -> total, total rounded up to whole batches. Host only. */
+am24_status am24_check_input(am24_settings *s, uint32_t n);
+
+am24_status am24_create(am24_handle *h, int device);
+am24_status am24_destroy(am24_handle h);
+
+/* ---- one-call solves (drop-in for denseDataSolver) ------------------------ */
+/* Host B, host x.  start_points (n x total_starts after rounding, column-major)
+ * is read when settings->start_mode == AM24_START_INJECTED, else ignored.
+ * *fval_out (may be NULL) receives the returned objective. */
+am24_status am24_solve_dense_f32(am24_handle h, const float *B, int32_t ldB, float *x,
+                                 uint32_t m, uint32_t n, am24_settings *settings,
+                                 am24_statistics *stats, const float *start_points,
+                                 float *fval_out);
+/* Same with B already in device memory (the reference GPU console's entry,
+ * c++/src/gpugpower/gpu_sparse_PCA_solver.h:29-35): d_B column-major with
+ * leading dimension ldB (the reference pads it to 128 B: LD_M). */
+am24_status am24_solve_device_f32(am24_handle h, const float *d_B, int32_t ldB, float *x,
+                                  uint32_t m, uint32_t n, am24_settings *settings,
+                                  am24_statistics *stats, const float *start_points,
+                                  float *fval_out);
+
+/* ---- resident data matrices ---------------------------------------------- */
+/* Copies B (host, or device when on_device != 0) into the handle's layout and
+ * keeps it until am24_matrix_destroy. */
+am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, uint32_t m,
+                                   uint32_t n, int32_t on_device, am24_matrix *out);
+am24_status am24_matrix_destroy(am24_handle h, am24_matrix mat);
+am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
+                                    am24_settings *settings, am24_statistics *stats,
+                                    const float *start_points, float *fval_out);
+
+/* ---- batch stepping (one AM iteration at a time) -------------------------- */
+/* A batch of batch_size starting points on a resident matrix.  `settings` must
+ * already have passed am24_check_input. */
+am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_settings *settings,
+                              uint32_t batch_size, am24_batch *out);
+am24_status am24_batch_destroy(am24_handle h, am24_batch b);
+/* Loads n x batch_size starting points (host, or device when on_device != 0)
+ * and resets the per-start values to 0 (ValueCoordinateHolder::reset). */
+am24_status am24_batch_load(am24_handle h, am24_batch b, const float *V, int32_t on_device);
+/* Runs `iterations` AM steps with iteration indices it0, it0+1, ... on the
+ * handle's stream.  When max_error is non-NULL the call synchronizes and
+ * stores the batch-maximum relative change of the last step there. */
+am24_status am24_batch_iterate(am24_handle h, am24_batch b, int32_t it0, int32_t iterations,
+                               float *max_error);
+/* Copies the current state to the host (any pointer may be NULL): loadings
+ * V (n x batch_size), per-start objective val, relative change err and
+ * number of non-zero loadings nnz. */
+am24_status am24_batch_read(am24_handle h, am24_batch b, float *V, float *val, float *err,
+                            uint32_t *nnz);
+/* Number of kernel launches one am24_batch_iterate step issues. */
+am24_status am24_batch_launches_per_step(am24_handle h, am24_batch b, int32_t *launches);
+/* Synchronizes the handle's stream. */
+am24_status am24_sync(am24_handle h);
+/* The handle's CUDA stream (a cudaStream_t), for callers that record their own
+ * events around library work. */
+void *am24_stream(am24_handle h);
+
+/* Kernel kinds reported by am24_batch_step_timed. */
+typedef enum {
+  AM24_KERNEL_GEMM_BV = 0,   /* Z = B V, tensor cores, split-K partial tiles */
+  AM24_KERNEL_Z_REDUCE = 1,  /* split-K sum, sign / norm / normalise of Z */
+  AM24_KERNEL_GEMM_BTZ = 2,  /* V = B^T Z, tensor cores (+ penalty epilogue) */
+  AM24_KERNEL_SELECT = 3,    /* top-s select or L1-ball level, normalise (constrained) */
+  AM24_KERNEL_FINALIZE = 4   /* per-start objective, change, logs, batch maximum */
+} am24_kernel_kind;
+/* One AM step like am24_batch_iterate(h, b, it, 1, NULL), with a CUDA event
+ * recorded on the handle's stream before and after every kernel.  Synchronizes,
+ * then writes each launch's duration (ms) to ms[i] and its am24_kernel_kind to
+ * kinds[i] (both with room for 8) and the number of launches to *count. */
+am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float *ms,
+                                  int32_t *kinds, int32_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AM24_H */

@@ -71,7 +71,26 @@ def oracle_lib():
     return _load(os.path.join(HERE, "liboracle.so"))
 
 
+def _openblas_dir():
+    import site
+    for d in site.getsitepackages() + [site.getusersitepackages()]:
+        cand = os.path.join(d, "opencv_python_headless.libs")
+        if os.path.isdir(cand):
+            return cand
+    return None
+
+
 def ref_lib(blas="naive"):
+    if blas == "openblas" and "openblas-deps" not in _LIBS:
+        # OpenBLAS's own runtime dependencies sit beside it; load them first so
+        # the dynamic loader finds them by soname.
+        d = _openblas_dir()
+        if d:
+            for prefix in ("libquadmath", "libgfortran"):
+                for f in sorted(os.listdir(d)):
+                    if f.startswith(prefix):
+                        C.CDLL(os.path.join(d, f), mode=C.RTLD_GLOBAL)
+        _LIBS["openblas-deps"] = True
     return _load(os.path.join(HERE, "_ref", f"libref24_{blas}.so"))
 
 
@@ -140,6 +159,14 @@ def ref_solve(B, settings, V_all=None, blas="naive"):
     lib = ref_lib(blas)
     fn = ("ref_dense_solver_" if V_all is None else "ref_solver_injected_") + _dt(B.dtype)
     return _solve(lib, fn, B, settings, V_all)
+
+
+def ref_set_threads(n, blas="naive"):
+    """OpenMP threads of the reference build (1 = reproducible reference starts)."""
+    lib = ref_lib(blas)
+    lib.ref_set_threads(C.c_int(int(n)))
+    lib.ref_total_threads.restype = C.c_uint
+    return lib.ref_total_threads()
 
 
 def ref_init_threads(blas="naive"):
@@ -229,29 +256,20 @@ def ref_hard_threshold(x, k, use_sort=False, blas="naive"):
     return _thr(ref_lib(blas), "ref_k_hard_thresholding", x, C.c_uint(k), C.c_int(int(use_sort)))
 
 
+def _workloads():
+    import importlib.util
+    path = os.path.join(os.path.dirname(HERE), "24am_b200", "workloads.py")
+    spec = importlib.util.spec_from_file_location("am24_workloads", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def low_rank_data(n, p, r, nnz_v, seed, noise=0.1, dtype=np.float64):
-    """The low-rank-plus-noise generator of the benchmark workloads, as the
-    reference lays data out (m = n samples x p features, column-major):
-    D = sum_{k<r} sigma_k u_k v_k^T + N(0, noise^2), sigma_k = 10*0.8^k,
-    u_k ~ N(0, I_n)/||.||, v_k with nnz_v uniform random indices of N(0,1)
-    values, normalised; columns centred."""
-    rng = np.random.default_rng(seed)
-    D = rng.standard_normal((n, p)) * noise
-    for k in range(r):
-        u = rng.standard_normal(n)
-        u /= np.linalg.norm(u)
-        v = np.zeros(p)
-        idx = rng.choice(p, size=min(nnz_v, p), replace=False)
-        v[idx] = rng.standard_normal(idx.size)
-        v /= np.linalg.norm(v)
-        D += 10.0 * 0.8 ** k * np.outer(u, v)
-    D -= D.mean(axis=0, keepdims=True)
-    return np.asfortranarray(D.astype(dtype))
+    """The benchmark workloads' low-rank-plus-noise generator (24am_b200/workloads.py)."""
+    return _workloads().low_rank_data(n, p, r, nnz_v, seed, noise, dtype)
 
 
 def uniform_starts(p, k, seed, dtype=np.float64):
-    """Starting points i.i.d. U[-1, 1] (density 1), each column normalised."""
-    rng = np.random.default_rng(seed)
-    V = rng.uniform(-1.0, 1.0, size=(p, k))
-    V /= np.linalg.norm(V, axis=0, keepdims=True)
-    return np.asfortranarray(V.astype(dtype))
+    """Starting points i.i.d. U[-1, 1], each column normalised (24am_b200/workloads.py)."""
+    return _workloads().uniform_starts(p, k, seed, dtype)

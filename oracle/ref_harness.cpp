@@ -240,6 +240,12 @@ extern "C" {
 /* Sets TOTAL_THREADS and the thread-private my_thread_id
  * (c++/src/utils/openmp_helper.h:44-67) so per-thread error maxima do not race. */
 void ref_init_threads(void) { init_random_seeds(); }
+/* OpenMP team size for the reference's parallel regions; 1 makes its own
+ * starting points reproducible (they share a global seed across threads). */
+void ref_set_threads(int n) {
+  omp_set_num_threads(n > 0 ? n : 1);
+  init_random_seeds();
+}
 unsigned ref_total_threads(void) { return TOTAL_THREADS; }
 
 float ref_dense_solver_f32(const float *B, int ldB, float *x, unsigned m, unsigned n,

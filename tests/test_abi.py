@@ -1,0 +1,73 @@
+"""The C ABI without a GPU: the library loads, exports every entry point of
+include/am24.h, mirrors the reference's settings logic, and reports errors."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+
+def test_exports_every_declared_symbol(am):
+    L = am.lib()
+    syms = am.header_symbols()
+    assert len(syms) >= 19
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing
+    assert L.am24_abi_version() == 1
+
+
+def test_default_settings_are_reference_defaults(am):
+    """OptimizationSettings() (c++/src/class/optimization_settings.h:101-123)."""
+    s = am.am24_settings()
+    am.lib().am24_default_settings(C.byref(s))
+    assert (s.tolerance, s.constraint, s.penalty, s.total_starts, s.batch_size) == (0.01, 10, 0.0, 64, 64)
+    assert (s.max_iter, s.use_otf, s.use_sort_hard, s.store_all) == (20, 0, 0, 0)
+    assert s.start_mode == am.START_REFERENCE and s.l1_mode == am.L1_REFERENCE_SCAN
+
+
+def test_check_input_matches_reference(am, po):
+    """chceckInputAndModifyIt (c++/src/class/optimization_settings.h:156-168)
+    against the oracle's restatement, over random settings."""
+    rng = np.random.default_rng(3)
+    for _ in range(300):
+        n = int(rng.integers(1, 500))
+        total = int(rng.integers(1, 300))
+        bs = int(rng.integers(0, 70))
+        s_par = int(rng.integers(1, 1000))
+        a = am.am24_settings()
+        am.lib().am24_default_settings(C.byref(a))
+        a.total_starts, a.batch_size, a.constraint = total, bs, s_par
+        st = am.lib().am24_check_input(C.byref(a), n)
+        b = po.make_settings(0, constraint=s_par, total_starts=total, batch_size=bs)
+        po.oracle_lib().orc_check_input(C.byref(b), C.c_uint(n))
+        assert st == 0
+        assert (a.total_starts, a.batch_size, a.constraint, a.total_batches) == \
+               (b.total_starts, b.batch_size, b.constraint, b.total_batches)
+
+
+def test_python_mirror_settings(am):
+    s = am.OptimizationSettings(totalStartingPoints=100, batchSize=64, constraintParameter=500)
+    s.chceckInputAndModifyIt(300)
+    assert (s.totalStartingPoints, s.totalBatches, s.constraintParameter) == (128, 2, 300)
+    assert am.OptimizationSettings(formulation=am.L1_penalized_L2_PCA).isL1PenalizedProblem()
+    assert not am.OptimizationSettings(formulation=am.L0_penalized_L2_PCA).isConstrainedProblem()
+
+
+def test_errors_are_reported(am):
+    L = am.lib()
+    assert L.am24_check_input(None, 10) == 1
+    assert "NULL" in am.last_error()
+    x = np.zeros(3, np.float32)
+    s = am.am24_settings()
+    L.am24_default_settings(C.byref(s))
+    assert L.am24_solve_dense_f32(None, None, 1, x.ctypes.data_as(C.c_void_p), 1, 3, C.byref(s),
+                                  None, None, None) == 1
+    assert L.am24_status_string(4).decode() == "device-side wait timed out"
+
+
+def test_no_gpu_fails_loudly(am):
+    """Without a usable sm_100 device the library refuses; there is no CPU path."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(am.Am24Error):
+        am.Solver(0)

@@ -1,0 +1,105 @@
+"""One AM step on the GPU (am24_batch_iterate) against one oracle step in FP64
+on the same FP32 data and starting points: every formulation, ragged shapes."""
+import numpy as np
+import pytest
+
+import parity
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(200, 300, 64), (257, 1000, 130), (33, 70, 1), (129, 4097, 257), (1000, 5000, 256)]
+
+
+def gammas(B):
+    Bd = B.astype(np.float64)
+    c2 = np.linalg.norm(Bd, axis=0).max()
+    c1 = np.abs(Bd).sum(0).max()
+    # the scale of B^T sgn(B x) (L1 variance) and of B^T (B x / ||B x||) (L2)
+    return {4: (0.02 * c2) ** 2, 5: (0.05 * c1) ** 2, 6: 0.05 * c2, 7: 0.05 * c1}
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("formulation", range(8))
+def test_step_matches_oracle(solver, po, shape, formulation):
+    m, n, k = shape
+    B = po.low_rank_data(m, n, 8, 30, seed=m + n, dtype=np.float32)
+    B64 = B.astype(np.float64)
+    V0 = po.uniform_starts(n, k, seed=n, dtype=np.float32)
+    s = min(16, n)
+    g = gammas(B).get(formulation, 0.0)
+    import importlib
+    am = importlib.import_module("24am_b200")
+    st = am.OptimizationSettings(formulation=formulation, constraintParameter=s, penaltyParameter=g,
+                                 tolerance=1e-6, maximumIterations=10, totalStartingPoints=k,
+                                 batchSize=k)
+    M = solver.matrix(B)
+    b = M.batch(st, k)
+    val_prev = np.linspace(1.0, 2.0, k).astype(np.float32)
+    b.load(V0)
+    b.iterate(0, 1)
+    V1, val, err, nnz = b.read()
+    os_ = po.make_settings(formulation, constraint=s, penalty=g, tolerance=1e-6, max_iter=10,
+                           total_starts=k, batch_size=k)
+    Vo, Zo, valo, erro, _ = po.oracle_iteration(B64, V0.astype(np.float64), os_, np.zeros(k))
+    # the raw B^T z the oracle thresholded, for the conditioning checks
+    Z = B64 @ V0.astype(np.float64)
+    if formulation in (1, 3, 5, 7):
+        Z = np.sign(Z)
+    elif formulation >= 4:
+        Z = Z / np.linalg.norm(Z, axis=0)
+    Vraw = B64.T @ Z
+    bad = 0
+    for j in range(k):
+        v = Vraw[:, j]
+        if formulation in (0, 1):
+            ill = parity.hard_ill_conditioned(v, s)
+        elif formulation in (2, 3):
+            # the reference scan's first step (t = 1) has a discriminant of exactly
+            # zero in exact arithmetic, so stopping there is decided by the last
+            # bit of the largest |v|; a 1-sparse result on either side is that case
+            ill = (parity.soft_ill_conditioned(po, v, s) or
+                   po.oracle_soft_level(v, s)[1] == 0 or
+                   (nnz[j] == 1 and np.count_nonzero(Vo[:, j]) > 1))
+        else:
+            ill = parity.penalty_ill_conditioned(v, g, formulation >= 6)
+        if ill:
+            bad += 1
+            continue
+        assert np.array_equal(V1[:, j] != 0, Vo[:, j] != 0), f"support differs in column {j}"
+        # thresholds subtract from |v|; errors scale with |v| before the threshold,
+        # relative to the normalisation the formulation applies
+        if formulation <= 1:
+            scale = np.abs(Vo[:, j]).max()
+        elif formulation <= 3:
+            scale = parity.soft_scale(po, v, s)
+        else:
+            scale = np.abs(v).max()
+        assert np.abs(V1[:, j] - Vo[:, j]).max() <= 1e-5 * scale, f"column {j}"
+        assert nnz[j] == np.count_nonzero(Vo[:, j])
+        sc = parity.objective_scale(formulation, v, g)
+        tol = 1e-5 * (sc if sc is not None else abs(valo[j]))
+        assert abs(val[j] - valo[j]) <= tol + 1e-30, f"objective of column {j}"
+    assert bad <= max(2, k // 10), f"{bad} ill-conditioned columns of {k}"
+    b.close()
+    M.close()
+
+
+def test_step_is_deterministic(solver, po):
+    import importlib
+    am = importlib.import_module("24am_b200")
+    B = po.low_rank_data(500, 3000, 8, 30, seed=1, dtype=np.float32)
+    V0 = po.uniform_starts(3000, 200, seed=2, dtype=np.float32)
+    M = solver.matrix(B)
+    outs = []
+    for f in (0, 3, 4, 7):
+        st = am.OptimizationSettings(formulation=f, constraintParameter=16, penaltyParameter=0.5,
+                                     totalStartingPoints=200, batchSize=200)
+        for _ in range(2):
+            b = M.batch(st, 200)
+            b.load(V0)
+            b.iterate(0, 3)
+            outs.append(b.read())
+            b.close()
+        a, c = outs[-2], outs[-1]
+        for x, y in zip(a, c):
+            assert np.array_equal(x, y, equal_nan=True)
