@@ -38,11 +38,18 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = 2000, 50000, 50, 256, 1024
+SIZES = {  # (n samples, p features, rank, nnz per loading, starts)
+    "config1": (2000, 50000, 50, 256, 1024),
+    # profiling case: same kernels, B planes 262 MB (> L2), a few GB on the device
+    "small": (2000, 8192, 50, 256, 1024),
+}
+N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = SIZES["config1"]
 S_CONS, GAMMA_C, SEED = 16, 0.1, 1
 E2E_MAX_IT, E2E_TOL = 200, 1e-6
 CPU_SAMPLE_STARTS, CPU_SAMPLE_ITERS = 64, 3
-WORKLOAD = (f"config-1 AM step: n={N_SAMPLES} samples x p={P_FEATURES} features (r={RANK}, "
+def workload_name():
+    tag = "config-1" if (N_SAMPLES, P_FEATURES) == SIZES["config1"][:2] else "profiling case"
+    return (f"{tag} AM step: n={N_SAMPLES} samples x p={P_FEATURES} features (r={RANK}, "
             f"{NNZ_V} nnz/loading), k={STARTS} starts, 8 formulations, plain FP32 path")
 
 
@@ -80,7 +87,8 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu):
+    def __init__(self, gpu, period_ms=100):
+        self.period = str(int(period_ms))
         vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
         ids = [v.strip() for v in vis.split(",") if v.strip()]
         self.gpu = ids[gpu] if gpu < len(ids) else str(gpu)
@@ -90,7 +98,7 @@ class ClockSampler:
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", self.period],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
@@ -188,7 +196,7 @@ def run_reference_arm(args):
             "unit": "start-it/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": N_SAMPLES, "p": P_FEATURES,
+            "config": {"workload": workload_name(), "n": N_SAMPLES, "p": P_FEATURES,
                        "starts": CPU_SAMPLE_STARTS, "s": S_CONS, "gamma_factor": GAMMA_C},
             "cpu_baseline": {"value": v, "unit": "start-it/s", "cores": cores, "kind": kind,
                              "sample": sample},
@@ -249,7 +257,7 @@ def run_ours(args):
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(local, args.clock_ms) as clk:
         e0.record(stream)
         for i in range(args.steps):
             step(args.warmup + i)
@@ -349,7 +357,7 @@ def run_ours(args):
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "n": N_SAMPLES, "p": P_FEATURES,
+                "config": {"workload": workload_name(), "n": N_SAMPLES, "p": P_FEATURES,
                            "starts_per_gpu": STARTS, "formulations": 8, "s": S_CONS,
                            "gamma_factor": GAMMA_C, "precision": "3xTF32 products, FP32 accumulate",
                            "l2": "inputs larger than L2 (B as 4 FP32 planes = 1.6 GB)",
@@ -370,13 +378,17 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--clock-ms", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--size", default="config1", choices=sorted(SIZES))
     args = ap.parse_args()
+    global N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS
+    N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = SIZES[args.size]
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

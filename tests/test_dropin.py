@@ -1,0 +1,103 @@
+"""The C++ drop-in boundary: the adapter headers compile against reference-style
+callers, and the console reproduces the reference console's runs."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CONSOLE = os.path.join(ROOT, "24am_b200", "am24_console")
+GOLDEN = os.path.join(ROOT, "tests", "golden", "reference_small_csv.npz")
+
+CALLER = r'''
+#include <am24/sparse_PCA_solver.h>
+#include <vector>
+using namespace SolverStructures;
+// the shape of the reference's multicore console call (multicore_console.cpp:35)
+template <typename F> F run(std::vector<F>& B, unsigned m, unsigned n, OptimizationSettings* s) {
+  OptimizationStatistics* st = new OptimizationStatistics();
+  std::vector<F> x(n, 0);
+  F f = SPCASolver::MulticoreSolver::denseDataSolver(&B[0], m, &x[0], m, n, s, st);
+  delete st;
+  return f;
+}
+int main() {
+  OptimizationSettings s; s.formulation = L1_penalized_L2_PCA;
+  std::vector<float> Bf(6, 1.f); std::vector<double> Bd(6, 1.0);
+  return (run(Bf, 2, 3, &s) == run(Bd, 2, 3, &s)) ? 0 : 0;
+}
+'''
+
+GPU_CALLER = r'''
+#include <am24/gpu_sparse_PCA_solver.h>
+// the shape of the reference GPU console's call (gpu_console.cu:132)
+int call(cublasHandle_t& h, thrust::device_vector<float>& d_B, thrust::host_vector<float>& x,
+         SolverStructures::OptimizationSettings* s, SolverStructures::OptimizationStatistics* st) {
+  return SPCASolver::GPUSolver::denseDataSolver(h, 2u, 3u, d_B, x, s, st, 32u, 32u);
+}
+'''
+
+
+def test_adapter_compiles_for_reference_callers(tmp_path):
+    src = tmp_path / "caller.cpp"
+    src.write_text(CALLER)
+    subprocess.run(["g++", "-std=c++14", "-Wall", "-Werror", f"-I{ROOT}/include", "-c", str(src),
+                    "-o", str(tmp_path / "caller.o")], check=True)
+
+
+def test_gpu_adapter_compiles_with_nvcc(tmp_path):
+    src = tmp_path / "gcaller.cu"
+    src.write_text(GPU_CALLER)
+    subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                    f"-I{ROOT}/include", "-c", str(src), "-o", str(tmp_path / "g.o")], check=True)
+
+
+def test_console_usage_without_required_flags():
+    r = subprocess.run([CONSOLE], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stdout
+
+
+def _write_csv(path, B):
+    with open(path, "w") as f:
+        for row in B:
+            f.write(",".join(repr(float(v)) for v in row) + "\n")
+
+
+def _read_x(path, n):
+    x = np.zeros(n)
+    for line in open(path):
+        i, v = line.strip().split(",")
+        x[int(i)] = float(v)
+    return x
+
+
+def _read_fval(path):
+    for line in open(path):
+        if line.startswith("Objective value:"):
+            return float(line.split(":")[1])
+    raise AssertionError("no objective in " + path)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,flags", [
+    ("small_f1_s3", ["-f", "1", "-s", "3"]),
+    ("small_f1_s2_l1000_r64", ["-l", "1000", "-r", "64", "-f", "1", "-s", "2"]),
+    ("small_f1_s2_l1000_r64_otf", ["-l", "1000", "-r", "64", "-u", "1", "-f", "1", "-s", "2"]),
+])
+def test_console_matches_reference_console_runs(name, flags):
+    """The reference Makefile's console runs on datasets/small.csv
+    (c++/multicore.mk:18-21), against outputs the reference itself produced."""
+    z = np.load(GOLDEN)
+    B = z["B"]
+    with tempfile.TemporaryDirectory() as d:
+        csv = os.path.join(d, "small.csv")
+        _write_csv(csv, B)
+        out = os.path.join(d, "res")
+        subprocess.run([CONSOLE, "-i", csv, "-o", out, "-v", "true", "-d", "double"] + flags,
+                       check=True, timeout=120)
+        x = _read_x(out + "_x", B.shape[1])
+        f = _read_fval(out + "_optimizationStatistics")
+    assert abs(f - float(z[f"{name}.fval"])) <= 1e-5 * abs(float(z[f"{name}.fval"]))
+    assert np.allclose(x, z[f"{name}.x"], atol=1e-5)

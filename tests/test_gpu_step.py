@@ -58,8 +58,7 @@ def test_step_matches_oracle(solver, po, shape, formulation):
             # zero in exact arithmetic, so stopping there is decided by the last
             # bit of the largest |v|; a 1-sparse result on either side is that case
             ill = (parity.soft_ill_conditioned(po, v, s) or
-                   po.oracle_soft_level(v, s)[1] == 0 or
-                   (nnz[j] == 1 and np.count_nonzero(Vo[:, j]) > 1))
+                   (nnz[j] == 1) != (np.count_nonzero(Vo[:, j]) == 1))
         else:
             ill = parity.penalty_ill_conditioned(v, g, formulation >= 6)
         if ill:
