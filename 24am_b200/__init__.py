@@ -107,7 +107,7 @@ _SIGS = {
     "am24_batch_step_timed": (C.c_int, [_VP, _VP, C.c_int32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
 }
-KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize"]
+KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV"]
 
 _lib = None
 
@@ -412,7 +412,12 @@ class Batch:
         cnt = C.c_int32()
         check(lib().am24_batch_step_timed(self.matrix.solver.h, self.bh, int(it), ms, kinds,
                                           C.byref(cnt)))
-        return [(KERNEL_KINDS[kinds[i]], ms[i]) for i in range(cnt.value)]
+        out = []
+        for i in range(cnt.value):
+            k = kinds[i]
+            name = KERNEL_KINDS[k & 0xFF] + ("(skipped)" if k & 0x100 else "")
+            out.append((name, ms[i]))
+        return out
 
     def launches_per_step(self):
         v = C.c_int32()

@@ -230,8 +230,11 @@ am24_status upload_columns(am24_handle h, am24_batch b, const float *host, int c
                               sizeof(float) * M.n, cudaMemcpyHostToDevice, h->stream));
     AM24_CUDA(launch_split_columns(b->d.Vraw + (size_t)slots[c] * M.ldn, M.ldn, M.n, 1,
                                    b->d.V_hi + (size_t)slots[c] * M.ldn,
-                                   b->d.V_lo + (size_t)slots[c] * M.ldn, M.ldn, h->stream));
+                                   b->d.V_lo + (size_t)slots[c] * M.ldn, M.ldn, h->stream,
+                                   b->d.vmask + (size_t)slots[c] * (M.ldn / 32)));
   }
+  // new starts are dense: the next Z = B V runs on the tensor cores
+  AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));
   return AM24_OK;
 }
 
@@ -444,7 +447,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.nnz_part, (size_t)k * parts)) || (st = A.get(&d.nnz, k)) ||
       (st = A.get(&d.val, k)) || (st = A.get(&d.err, k)) || (st = A.get(&d.max_err, 1)) ||
       (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
-      (st = A.get(&d.status, 1))) {
+      (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||
+      (st = A.get(&d.max_nnz, 1))) {
     delete b;
     return st;
   }
@@ -458,6 +462,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.fz, 0, sizeof(float) * k, h->stream);
   if (!e) e = cudaMemsetAsync(d.nnz, 0, sizeof(uint32_t) * k, h->stream);
   if (!e) e = cudaMemsetAsync(d.status, 0, sizeof(int), h->stream);
+  if (!e) e = cudaMemsetAsync(d.vmask, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
+  if (!e) e = cudaMemsetAsync(d.max_nnz, 0xFF, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.iters, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaMemsetAsync(d.cards, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaStreamSynchronize(h->stream);
@@ -476,7 +482,9 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
     delete b;
     return st;
   }
-  b->launches = is_constrained(settings->formulation) ? 5 : 4;
+  // a gather over V's non-zeros beats the dense product while they are few
+  d.sparse_cap = (uint32_t)std::min(4096, M.n / 32);
+  b->launches = is_constrained(settings->formulation) ? 6 : 5;
   *out = b;
   return AM24_OK;
 }
@@ -502,7 +510,9 @@ am24_status am24_batch_load(am24_handle h, am24_batch b, const float *V, int32_t
     AM24_CUDA(cudaMemcpy2DAsync(b->d.Vraw, sizeof(float) * M.ldn, V, sizeof(float) * M.n,
                                 sizeof(float) * M.n, k, cudaMemcpyHostToDevice, h->stream));
   }
-  AM24_CUDA(launch_split_columns(b->d.Vraw, M.ldn, M.n, k, b->d.V_hi, b->d.V_lo, M.ldn, h->stream));
+  AM24_CUDA(launch_split_columns(b->d.Vraw, M.ldn, M.n, k, b->d.V_hi, b->d.V_lo, M.ldn, h->stream,
+                                 b->d.vmask));
+  AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));  // dense starts
   // ValueCoordinateHolder::reset (c++/src/utils/various.h:33-38)
   AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
   AM24_CUDA(cudaMemsetAsync(b->d.err, 0, sizeof(float) * k, h->stream));
@@ -575,7 +585,11 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
       break;
     }
   int nl = 0, kk[9] = {0};
-  if (st == AM24_OK) {
+  uint32_t gate = 0;
+  if (st == AM24_OK &&
+      cudaMemcpyAsync(&gate, b->d.max_nnz, sizeof gate, cudaMemcpyDeviceToHost, h->stream) ==
+          cudaSuccess &&
+      cudaStreamSynchronize(h->stream) == cudaSuccess) {
     const StepParams p = step_params(b->s, it, 0);
     cudaError_t e = launch_am_step(b->mat->d, b->d, b->tm, p, h->stream, &nl, ev, kk);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -584,7 +598,13 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
   }
   for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
   if (st != AM24_OK) return st;
-  for (int i = 0; i < nl; i++) kinds[i] = kk[i];
+  // mark the Z = B V kernels that the gate turned into no-ops
+  const bool sparse = gate <= b->d.sparse_cap;
+  for (int i = 0; i < nl; i++) {
+    const bool skipped = sparse ? (kk[i] == AM24_KERNEL_GEMM_BV || kk[i] == AM24_KERNEL_Z_REDUCE)
+                                : (kk[i] == AM24_KERNEL_GATHER_BV);
+    kinds[i] = kk[i] | (skipped ? AM24_KERNEL_SKIPPED : 0);
+  }
   *count = nl;
   return check_device_status(b);
 }

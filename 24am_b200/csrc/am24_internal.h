@@ -41,6 +41,9 @@ struct BatchDev {
   float *obj_part;      // per start x (m_tiles2*4): penalized objective partials
   float *nnz_part;      // per start x (m_tiles2*4): penalized non-zero partials
   uint32_t *nnz;        // per start: non-zeros after thresholding
+  uint32_t *vmask;      // k x (ldn/32): bit r of word w set iff V[32w + r] != 0
+  uint32_t *max_nnz;    // largest non-zero count of the last step (0xFFFFFFFF: dense V)
+  uint32_t sparse_cap;  // Z = B V runs as a gather when max_nnz <= sparse_cap
   float *val, *err;     // ValueCoordinateHolder val / current_error
   float *max_err;       // batch maximum relative change (1 float)
   int *iters, *cards;   // storeIterationsForAllPoints logs (total_starts each)
@@ -69,8 +72,11 @@ struct TensorMaps {
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
 int num_sms();
 cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st);
+// dst hi/lo planes of `cols` columns from src, and their non-zero masks
+// (mask may be null; otherwise mask + c * (ld_dst / 32) per column).
 cudaError_t launch_split_columns(const float *src, int ld_src, int rows, int cols, float *hi,
-                                 float *lo, int ld_dst, cudaStream_t st);
+                                 float *lo, int ld_dst, cudaStream_t st,
+                                 uint32_t *mask = nullptr);
 // ev (optional, >= 9 events): ev[i] is recorded before launch i and
 // ev[launches] after the last one; kinds[i] (optional) gets each launch's kind.
 cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm,

@@ -130,6 +130,7 @@ struct EpiPenalty {
   float *obj_part, *nnz_part;
   int ld, M, N, bn, parts;  // parts = m_tiles * 4
   double gamma;
+  uint32_t *vmask;  // non-zero bitmask words, ld / 32 per column
   __device__ void begin(const Unit &, int, int) {}
   __device__ void end(const Unit &, int, int) {}
   // r holds this thread's 32 values (row `row`, columns col0..col0+31) and is
@@ -139,6 +140,7 @@ struct EpiPenalty {
     const bool rv = gi < M;
     const int c0 = t.nt * bn + col0;
     float mycnt = 0.f;
+    uint32_t mymask = 0u;
 #pragma unroll
     for (int j = 0; j < 32; j++) {
       const float v = r[j];
@@ -157,7 +159,10 @@ struct EpiPenalty {
       const bool valid = rv && (c0 + j < N);
       r[j] = valid ? o : 0.f;
       const unsigned nz = __ballot_sync(FULL, valid && x != 0.f);
-      if (lane == j) mycnt = (float)__popc(nz);
+      if (lane == j) {
+        mycnt = (float)__popc(nz);
+        mymask = nz;
+      }
       if (valid) {
         const size_t off = (size_t)(c0 + j) * ld + gi;
         split_store(x, V_hi + off, V_lo + off);
@@ -168,6 +173,7 @@ struct EpiPenalty {
     if (col < N) {
       obj_part[(size_t)col * parts + t.mt * 4 + q] = so;
       nnz_part[(size_t)col * parts + t.mt * 4 + q] = mycnt;
+      if (t.mt * 4 + q < (ld >> 5)) vmask[(size_t)col * (ld >> 5) + t.mt * 4 + q] = mymask;
     }
   }
 };
@@ -200,11 +206,20 @@ __global__ void prep_transpose_kernel(const float *__restrict__ B, int ldB, int 
   }
 }
 
+// One block per column: hi/lo planes and, when mask is given, the column's
+// non-zero bitmask (ld_dst / 32 words; rows beyond `rows` count as zero).
 __global__ void split_columns_kernel(const float *__restrict__ src, int ld_src, int rows,
-                                     float *__restrict__ hi, float *__restrict__ lo, int ld_dst) {
+                                     float *__restrict__ hi, float *__restrict__ lo, int ld_dst,
+                                     uint32_t *__restrict__ mask) {
   const size_t c = blockIdx.x;
-  for (int r = threadIdx.x; r < rows; r += blockDim.x)
-    split_store(src[c * ld_src + r], hi + c * ld_dst + r, lo + c * ld_dst + r);
+  const int lane = threadIdx.x & 31;
+  for (int base = threadIdx.x & ~31; base < ld_dst; base += blockDim.x) {
+    const int r = base + lane;
+    const float v = (r < rows) ? src[c * ld_src + r] : 0.f;
+    if (r < rows) split_store(v, hi + c * ld_dst + r, lo + c * ld_dst + r);
+    const unsigned nz = __ballot_sync(FULL, v != 0.f);
+    if (mask && lane == 0) mask[c * (ld_dst >> 5) + (base >> 5)] = nz;
+  }
 }
 
 __global__ void combine_columns_kernel(const float *__restrict__ hi, const float *__restrict__ lo,
@@ -222,8 +237,10 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
                                                        int m_tiles, int n_tiles, int bn, int m,
                                                        float *__restrict__ Z_hi,
                                                        float *__restrict__ Z_lo, int ldm,
-                                                       float *__restrict__ fz) {
+                                                       float *__restrict__ fz,
+                                                       const uint32_t *gate, uint32_t gate_max) {
   __shared__ double red[32];
+  if (*gate <= gate_max) return;  // the gather kernel produced Z this step
   const int j = blockIdx.x;
   const int nt = j / bn, c = j - nt * bn;
   const size_t unit_stride = (size_t)bn * BM;
@@ -252,6 +269,119 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       const float y = zh[i] + zl[i];  // exact: this thread wrote both planes
       split_store(y * inv, zh + i, zl + i);
+    }
+  } else if (threadIdx.x == 0) {
+    fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
+  }
+}
+
+// ------------------------------------------------------------ sparse Z = B V
+constexpr int GATHER_THREADS = 256;
+constexpr int GATHER_ROWS = 8;  // samples per thread per pass
+constexpr int GATHER_CAP = 4096;
+
+// Z = B V for one start when V's column has few non-zeros: runs instead of
+// gemm1 + z_reduce when the previous step left at most gate_max non-zeros in
+// every column (*gate).  The column's non-zero rows are listed in index order
+// from its bitmask, then z = sum_q v_q B[:, q] is accumulated with FP32 FMAs in
+// that fixed order (deterministic), and the same sign / norm / normalise
+// step as z_reduce_kernel<MODE> finishes the column.
+template <int MODE>
+__global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
+    const float *__restrict__ Bc_hi, const float *__restrict__ Bc_lo, int ldm, int m, int ldn,
+    const float *__restrict__ V_hi, const float *__restrict__ V_lo,
+    const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi, float *__restrict__ Z_lo,
+    float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max) {
+  __shared__ int idx[GATHER_CAP];
+  __shared__ float val[GATHER_CAP];
+  __shared__ uint32_t wsum[GATHER_THREADS / 32];
+  __shared__ double red[32];
+  if (*gate > gate_max) return;  // dense V: gemm1 + z_reduce handle this step
+  const int j = blockIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int words = ldn >> 5;
+  const uint32_t *mk = vmask + (size_t)j * words;
+  // each thread owns a contiguous run of mask words, so the block-wide
+  // exclusive scan of their popcounts lists rows in index order
+  const int per = (words + GATHER_THREADS - 1) / GATHER_THREADS;
+  const int w0 = min(words, threadIdx.x * per), w1 = min(words, w0 + per);
+  uint32_t cnt = 0;
+  for (int q = w0; q < w1; q++) cnt += __popc(mk[q]);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  uint32_t off = incl - cnt;
+  for (int i = 0; i < w; i++) off += wsum[i];
+  uint32_t total = 0;
+  for (int i = 0; i < GATHER_THREADS / 32; i++) total += wsum[i];
+  if (total > (uint32_t)GATHER_CAP) total = GATHER_CAP;  // cannot happen below the gate
+  const float *vh = V_hi + (size_t)j * ldn;
+  const float *vl = V_lo + (size_t)j * ldn;
+  for (int q = w0; q < w1; q++) {
+    uint32_t bits = mk[q];
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const int r = q * 32 + b;
+      if (off < (uint32_t)GATHER_CAP) {
+        idx[off] = r;
+        val[off] = vh[r] + vl[r];
+      }
+      off++;
+    }
+  }
+  __syncthreads();
+  double acc = 0.0;
+  float y[GATHER_ROWS];
+  float *zh = Z_hi + (size_t)j * ldm;
+  float *zl = Z_lo + (size_t)j * ldm;
+  const int chunk = GATHER_THREADS * GATHER_ROWS;
+  const bool one_pass = m <= chunk;
+  for (int base = 0; base < m; base += chunk) {
+#pragma unroll
+    for (int r = 0; r < GATHER_ROWS; r++) y[r] = 0.f;
+    for (uint32_t q = 0; q < total; q++) {
+      const float v = val[q];
+      const size_t row = (size_t)idx[q] * ldm;
+#pragma unroll
+      for (int r = 0; r < GATHER_ROWS; r++) {
+        const int i = base + r * GATHER_THREADS + threadIdx.x;
+        if (i < m) y[r] = fmaf(v, Bc_hi[row + i] + Bc_lo[row + i], y[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < GATHER_ROWS; r++) {
+      const int i = base + r * GATHER_THREADS + threadIdx.x;
+      if (i >= m) continue;
+      if (MODE == 1) {
+        acc += (double)fabsf(y[r]);
+        zh[i] = sgnf(y[r]);
+        zl[i] = 0.f;
+      } else {
+        acc += (double)y[r] * (double)y[r];
+        if (!(MODE == 2 && one_pass)) split_store(y[r], zh + i, zl + i);
+      }
+    }
+  }
+  const double tot = block_sum(acc, red);
+  if (MODE == 2) {
+    const float inv = 1.0f / (float)sqrt(tot);
+    if (one_pass) {
+#pragma unroll
+      for (int r = 0; r < GATHER_ROWS; r++) {
+        const int i = r * GATHER_THREADS + threadIdx.x;
+        if (i < m) split_store(y[r] * inv, zh + i, zl + i);
+      }
+    } else {
+      for (int i = threadIdx.x; i < m; i += GATHER_THREADS) {
+        const float v = zh[i] + zl[i];
+        split_store(v * inv, zh + i, zl + i);
+      }
     }
   } else if (threadIdx.x == 0) {
     fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
@@ -338,35 +468,246 @@ __device__ SelResult block_select(const float *__restrict__ colg, const float *c
   return SelResult{prefix, gt, eq};
 }
 
+// Stages col[0..n) (plus up to 3 floats of the 16-byte-rounded tail, which
+// lie in the column's padding) into shared memory with one bulk copy per
+// 32 KB.  If the copy does not land within the bound, raises *status and
+// falls back to plain loads.
+__device__ void stage_column(float *cache, const float *__restrict__ colg, int n, uint64_t *bar,
+                             int *status) {
+  const uint32_t bytes = ((uint32_t)n * 4u + 15u) & ~15u;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(bar, bytes);
+    for (uint32_t off = 0; off < bytes; off += 32768u)
+      bulk_load(reinterpret_cast<uint8_t *>(cache) + off,
+                reinterpret_cast<const uint8_t *>(colg) + off, min(32768u, bytes - off), bar);
+  }
+  const uint64_t t0 = global_timer_ns();
+  bool ok = true;
+  while (!mbar_try_wait(bar, 0)) {
+    if (global_timer_ns() - t0 > 2000000000ull) {
+      ok = false;
+      break;
+    }
+  }
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicCAS(status, 0, 0x201);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) cache[i] = colg[i];
+    __syncthreads();
+  }
+}
+
+// x_i = f(v_i) written as hi/lo planes with 16-byte stores (column bases are
+// 128-byte aligned) and the column's non-zero bitmask.  Each warp writes 128
+// consecutive entries per step (4 mask words); entries past n read the zero
+// padding of the staged column (the column's padding rows are zero).
+template <class Fn>
+__device__ __forceinline__ void write_column(const float *cache, int n, float *vh, float *vl,
+                                             uint32_t *mask, Fn fn) {
+  const int n4 = (n + 3) >> 2;
+  const int lane = threadIdx.x & 31;
+  const float4 *c4 = reinterpret_cast<const float4 *>(cache);
+  float4 *h4 = reinterpret_cast<float4 *>(vh);
+  float4 *l4 = reinterpret_cast<float4 *>(vl);
+  for (int base = threadIdx.x & ~31; base < n4; base += blockDim.x) {
+    const int i = base + lane;
+    uint32_t nib = 0;
+    if (i < n4) {
+      const float4 v = c4[i];
+      float4 h, l;
+      float x;
+      x = fn(v.x); h.x = tf32_hi(x); l.x = x - h.x; nib |= (x != 0.f) ? 1u : 0u;
+      x = fn(v.y); h.y = tf32_hi(x); l.y = x - h.y; nib |= (x != 0.f) ? 2u : 0u;
+      x = fn(v.z); h.z = tf32_hi(x); l.z = x - h.z; nib |= (x != 0.f) ? 4u : 0u;
+      x = fn(v.w); h.w = tf32_hi(x); l.w = x - h.w; nib |= (x != 0.f) ? 8u : 0u;
+      h4[i] = h;
+      l4[i] = l;
+    }
+    // 8 lanes x 4 entries -> one 32-bit mask word
+    uint32_t word = nib << (4 * (lane & 7));
+    word |= __shfl_xor_sync(FULL, word, 1);
+    word |= __shfl_xor_sync(FULL, word, 2);
+    word |= __shfl_xor_sync(FULL, word, 4);
+    if ((lane & 7) == 0 && 4 * i < ((n + 31) & ~31)) mask[(4 * i) >> 5] = word;
+  }
+}
+
+// Same as write_column, reading the column from global memory (entries up to
+// the next multiple of 32 are read; they lie in the column's zero padding).
+template <class Fn>
+__device__ __forceinline__ void write_column_global(const float *__restrict__ colg, int n,
+                                                    float *vh, float *vl, uint32_t *mask, Fn fn) {
+  const int lane = threadIdx.x & 31;
+  const int n32 = (n + 31) & ~31;
+  for (int base = threadIdx.x & ~31; base < n32; base += blockDim.x) {
+    const int i = base + lane;
+    const float x = fn(colg[i]);
+    split_store(x, vh + i, vl + i);
+    const unsigned nz = __ballot_sync(FULL, x != 0.f);
+    if (lane == 0) mask[base >> 5] = nz;
+  }
+}
+
+// Warp 0 walks the histogram from the top bin down and finds the bin holding
+// descending rank `need` (1-based): res[0] = bin, res[1] = count of keys in
+// higher bins, res[2] = count in the bin.  All threads call; result after the
+// trailing barrier.
+__device__ void find_rank_bin(const uint32_t *hist, int nb, uint32_t need, uint32_t *res) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    uint32_t running = 0, fbin = 0, fcum = running, feq = 0;
+    bool found = false;
+    for (int base = nb - 32; base >= 0 && !found; base -= 32) {
+      const uint32_t c = hist[base + 31 - lane];
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const uint32_t total = __shfl_sync(FULL, incl, 31);
+      if (running + total >= need) {
+        const unsigned ballot = __ballot_sync(FULL, running + incl >= need);
+        const int f = __ffs(ballot) - 1;
+        const uint32_t inc_f = __shfl_sync(FULL, incl, f);
+        const uint32_t c_f = __shfl_sync(FULL, c, f);
+        fbin = base + 31 - f;
+        fcum = running + inc_f - c_f;
+        feq = c_f;
+        found = true;
+      } else {
+        running += total;
+      }
+    }
+    if (!found) {  // fewer than `need` keys: every bin lies above
+      fbin = 0;
+      fcum = running;
+      feq = 0;
+    }
+    if (lane == 0) {
+      res[0] = fbin;
+      res[1] = fcum;
+      res[2] = feq;
+    }
+  }
+  __syncthreads();
+}
+
+// Top-11-bit histogram of |col| keys into hist[2048] (warp-aggregated adds).
+template <bool CACHED>
+__device__ void key_histogram(const float *__restrict__ colg, const float *cols, int n,
+                              uint32_t *hist) {
+  for (int b = threadIdx.x; b < 2048; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t bin = col_key<CACHED>(colg, cols, i) >> 20;
+    const unsigned peers = __match_any_sync(__activemask(), bin);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], __popc(peers));
+  }
+  __syncthreads();
+}
+
+// Descending bitonic sort of a[0..len), len a power of two.
+template <typename T>
+__device__ void bitonic_desc(T *a, int len) {
+  for (int k = 2; k <= len; k <<= 1) {
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        const int ixj = i ^ jj;
+        if (ixj > i) {
+          const T x = a[i], y = a[ixj];
+          const bool first_block = (i & k) == 0;
+          if (first_block ? (x < y) : (x > y)) {
+            a[i] = y;
+            a[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // ------------------------------------------------------------ L0 constraint
 // k_hard_thresholding (c++/src/utils/thresh_functions.h:121-145): level = the
 // s-th largest |v| (with multiplicity, as the sorting variant :92-98 defines
 // it), keep |v| >= level, then x <- x / ||x|| (c++/src/gpower/gpower_commons.h:111).
+constexpr int HARD_CAND = 4096;  // candidates resolved in shared memory
+
+// k_hard_thresholding (c++/src/utils/thresh_functions.h:121-145): level = the
+// s-th largest |v| (with multiplicity, as the sorting variant :92-98 defines
+// it), keep |v| >= level, then x <- x / ||x|| (c++/src/gpower/gpower_commons.h:111).
+//
+// Common case, three passes over the column: (1) histogram of the top 11 bits
+// of |v| finds the bin holding rank s; (2) keys above that bin are kept for
+// sure (their squares are summed on the way), keys in the bin are gathered
+// into shared memory and sorted there to give the exact level and the rest of
+// the norm; (3) the normalised loadings are written.  A bin too full for shared
+// memory falls back to the exact three-level radix select.
 template <bool CACHED>
-__global__ void __launch_bounds__(512) hard_select_kernel(const float *__restrict__ Vraw, int ldv,
-                                                          int n, unsigned s,
-                                                          float *__restrict__ V_hi,
-                                                          float *__restrict__ V_lo,
-                                                          uint32_t *__restrict__ nnz_out) {
+__global__ void __launch_bounds__(512, 1) hard_select_kernel(const float *__restrict__ Vraw,
+                                                             int ldv, int n, unsigned s,
+                                                             float *__restrict__ V_hi,
+                                                             float *__restrict__ V_lo,
+                                                             uint32_t *__restrict__ nnz_out,
+                                                             int *status,
+                                                             uint32_t *__restrict__ vmask) {
   extern __shared__ __align__(16) uint8_t dsm[];
   uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
-  uint32_t *res = hist + 2048;
+  uint32_t *cand = hist + 2048;
+  uint32_t *res = cand + HARD_CAND;
   double *red = reinterpret_cast<double *>(res + 8);
-  float *cache = reinterpret_cast<float *>(red + 32);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(red + 32);
+  float *cache = reinterpret_cast<float *>(bar + 2);
   const int j = blockIdx.x;
   const float *colg = Vraw + (size_t)j * ldv;
-  if (CACHED) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) cache[i] = colg[i];
-    __syncthreads();
-  }
-  const SelResult sel = block_select<CACHED>(colg, cache, n, s, hist, res);
-  const uint32_t thr = sel.key;
+  if (CACHED) stage_column(cache, colg, n, bar, status);
+  key_histogram<CACHED>(colg, cache, n, hist);
+  find_rank_bin(hist, 2048, s, res);
+  const uint32_t b1 = res[0], above = res[1], in_bin = res[2];
+  __syncthreads();
+  uint32_t thr;
   double ss = 0.0, cnt = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float v = CACHED ? cache[i] : colg[i];
-    if (abs_key(v) >= thr) {
-      ss += (double)v * (double)v;
-      cnt += 1.0;
+  if (in_bin <= (uint32_t)HARD_CAND) {
+    if (threadIdx.x == 0) res[3] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t key = col_key<CACHED>(colg, cache, i);
+      const uint32_t bin = key >> 20;
+      if (bin > b1) {
+        const double v = (double)__uint_as_float(key);
+        ss += v * v;
+        cnt += 1.0;
+      } else if (bin == b1) {
+        cand[atomicAdd(&res[3], 1u)] = key;
+      }
+    }
+    __syncthreads();
+    const int nc = (int)res[3];
+    int len = 1;
+    while (len < nc) len <<= 1;
+    for (int q = nc + threadIdx.x; q < len; q += blockDim.x) cand[q] = 0u;
+    __syncthreads();
+    bitonic_desc(cand, len);
+    thr = cand[s - above - 1];
+    for (int q = threadIdx.x; q < nc; q += blockDim.x)
+      if (cand[q] >= thr) {
+        const double v = (double)__uint_as_float(cand[q]);
+        ss += v * v;
+        cnt += 1.0;
+      }
+  } else {
+    thr = block_select<CACHED>(colg, cache, n, s, hist, res).key;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float v = CACHED ? cache[i] : colg[i];
+      if (abs_key(v) >= thr) {
+        ss += (double)v * (double)v;
+        cnt += 1.0;
+      }
     }
   }
   ss = block_sum(ss, red);
@@ -374,22 +715,25 @@ __global__ void __launch_bounds__(512) hard_select_kernel(const float *__restric
   const float inv = 1.0f / (float)sqrt(ss);
   float *vh = V_hi + (size_t)j * ldv;
   float *vl = V_lo + (size_t)j * ldv;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float v = CACHED ? cache[i] : colg[i];
-    const float x = (abs_key(v) >= thr) ? v * inv : 0.f;
-    split_store(x, vh + i, vl + i);
+  uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
+  if (CACHED) {
+    write_column(cache, n, vh, vl, mk,
+                 [=](float v) { return (abs_key(v) >= thr) ? v * inv : 0.f; });
+  } else {
+    write_column_global(colg, n, vh, vl, mk,
+                        [=](float v) { return (abs_key(v) >= thr) ? v * inv : 0.f; });
   }
   if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
 }
 
 // ------------------------------------------------------------ L1 constraint
-constexpr int SOFT_C = 2048;  // sorted-candidate chunk (power of two for the bitonic sort)
+constexpr int SOFT_C = 1024;  // sorted-candidate chunk (power of two for the bitonic sort)
 constexpr int SOFT_THREADS = 512;
 
 struct SoftSmem {
   static constexpr size_t HIST = 2048 * 4, RES = 128, RED = 32 * 8, CAND = SOFT_C * 4,
                           P = SOFT_C * 8;
-  static constexpr size_t FIXED = HIST + RES + RED + CAND + 2 * P + 64;
+  static constexpr size_t FIXED = HIST + RES + RED + CAND + 2 * P + 64 + 16;  // + mbarrier
 };
 
 // Unfused double arithmetic (no FMA contraction), as host C++ evaluates it.
@@ -468,26 +812,123 @@ __device__ void bitonic_sort_desc(float *a) {
   }
 }
 
+// Evaluates the reference scan's stopping predicates (or, EXACT, the exact
+// projection's segment test) at chunk positions q in [0, E) of a descending
+// sorted chunk; global rank index g = base + q.  p1/p2 are inclusive prefix
+// sums including everything before the chunk (S1, S2).  The value below
+// position q is cand[q + 1], or lo_after for the chunk's last position.
+// Per thread: the smallest stopping g found and its level; w_last gets the
+// '+' root at g = n - 1 (the reference's level when it never stops).
+template <bool EXACT>
+__device__ void eval_chunk(const float *cand, const double *p1, const double *p2, uint32_t total,
+                           uint32_t E, uint32_t base, uint32_t n, double S1, double S2,
+                           double lo_after, double sq, double sq2, double lim, uint32_t &best,
+                           double &bw, double &w_last) {
+  for (uint32_t q = threadIdx.x; q < E; q += blockDim.x) {
+    const uint32_t g = base + q;
+    const double t = (double)(g + 1);
+    const double hi = (double)cand[q];
+    const double lov = (q + 1 < total) ? (double)cand[q + 1] : lo_after;
+    const double S1i = p1[q], S2i = p2[q];
+    if (!EXACT) {
+      // Same operations, order and (unfused) rounding as the reference's
+      // expressions at thresh_functions.h:193-213; several of its stops are
+      // decided by the last bit (e.g. a zero discriminant at the first step).
+      const double S1p = q ? p1[q - 1] : S1, S2p = q ? p2[q - 1] : S2;
+      const double left = ratio_at(S1i, S2i, t, hi);
+      const double rprev = (g == 0) ? sq : ratio_at(S1p, S2p, t - 1.0, hi);
+      const double a = dmul(t, dsub(t, sq2));
+      const double b = dsub(dmul(dmul(2.0, S1i), sq2), dmul(dmul(2.0, t), S1i));
+      const double c = dsub(dmul(S1i, S1i), dmul(sq2, S2i));
+      const double disc = __dsqrt_rn(dsub(dmul(b, b), dmul(dmul(4.0, a), c)));
+      const double wm = __ddiv_rn(dsub(-b, disc), dmul(2.0, a));
+      const double wp = __ddiv_rn(__dadd_rn(-b, disc), dmul(2.0, a));
+      if (g + 1 == n) w_last = wp;
+      double cw = 0.0;
+      bool hit = false;
+      if (left > sq && rprev < sq) {
+        hit = true;
+        cw = hi;
+      } else if (wm > lov && wm < hi) {
+        hit = true;
+        cw = wm;
+      } else if (wp > lov && wp < hi && wp < lim) {
+        hit = true;
+        cw = wp;
+      }
+      if (hit && g < best) {
+        best = g;
+        bw = cw;
+      }
+    } else {
+      const double rlo = (S1i - t * lov) / sqrt(S2i - 2.0 * lov * S1i + t * lov * lov);
+      if (rlo >= sq && g < best) {
+        const double a = t * (t - sq2);
+        const double b = 2.0 * S1i * sq2 - 2.0 * t * S1i;
+        const double c = S1i * S1i - sq2 * S2i;
+        double lam;
+        if (a == 0.0) {
+          lam = -c / b;
+        } else {
+          const double disc = sqrt(fmax(b * b - 4.0 * a * c, 0.0));
+          const double r1 = (-b - disc) / (2.0 * a), r2 = (-b + disc) / (2.0 * a);
+          // the genuine root keeps every one of the t entries above it
+          const bool ok1 = r1 >= lov && r1 <= hi, ok2 = r2 >= lov && r2 <= hi;
+          lam = ok1 ? r1 : ok2 ? r2 : fmin(fmax(r1, lov), hi);
+        }
+        best = g;
+        bw = lam;
+      }
+    }
+  }
+}
+
+// Block minimum of the per-thread stopping rank; the owning thread publishes
+// its level.  Returns the rank (0xFFFFFFFF when nobody stopped) and sets *w.
+__device__ uint32_t resolve_stop(uint32_t best, double bw, uint32_t *res,
+                                 volatile uint32_t *misc, double *w_sh, double *w) {
+  uint32_t mb = best;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mb = min(mb, __shfl_xor_sync(FULL, mb, o));
+  if ((threadIdx.x & 31) == 0) res[4 + (threadIdx.x >> 5)] = mb;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t m2 = 0xFFFFFFFFu;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) m2 = min(m2, res[4 + i]);
+    misc[1] = m2;
+  }
+  __syncthreads();
+  const uint32_t brk = misc[1];
+  if (brk != 0xFFFFFFFFu && best == brk) *w_sh = bw;
+  __syncthreads();
+  if (brk != 0xFFFFFFFFu) *w = *w_sh;
+  __syncthreads();
+  return brk;
+}
+
 // soft_thresholding (c++/src/utils/thresh_functions.h:162-254): the level w
 // and x = sgn(v)(|v| - w)_+, then x <- x / ||x||.
 //
 // The reference sorts |v| and scans it from the top, stopping at the first
-// index i where one of three predicates holds (:197-216).  Here the sorted
-// order is produced a chunk of SOFT_C ranks at a time: a radix select finds
-// the key at the chunk's last rank, one pass gathers the keys between the
-// previous and this boundary (ties handled by counts, since only values
-// matter), a bitonic sort orders the chunk, double-precision prefix sums give
-// S1 and S2 at every rank, and every rank's predicates are evaluated in
-// parallel; the smallest breaking rank wins.  Most columns stop in the first
-// chunk; a column that never breaks is walked to its end, as the reference
-// does (then w is the '+' root of the last step).
-// EXACT: instead of the reference predicates, stop at the first segment whose
-// lower knot already satisfies ||.||_1/||.||_2 >= sqrt(s) and take the root
-// inside it: the exact L1-ball/sphere projection.
+// index i where one of three predicates holds (:197-216).  Common case, three
+// passes over the column: a histogram of the top 11 bits of |v| picks the
+// highest bins holding at most SOFT_C values; one pass gathers them (and the
+// largest value below them); they are sorted in shared memory, prefix sums
+// in double give S1 and S2 at every rank, and all ranks' predicates are
+// evaluated at once -- the smallest stopping rank wins, and the norm comes
+// from the gathered values; a last pass writes the loadings.  When the stop
+// lies deeper, the column is walked exactly a chunk of SOFT_C ranks at a time
+// (radix select of each chunk boundary, ties by count); a column that never
+// stops is walked to its end as in the reference (w is then the '+' root of
+// the last step).
+// EXACT: stop at the first segment whose lower knot already gives
+// ||.||_1/||.||_2 >= sqrt(s) and take the root inside it -- the exact
+// L1-ball / unit-sphere projection.
 template <bool CACHED, bool EXACT>
-__global__ void __launch_bounds__(SOFT_THREADS) soft_select_kernel(
+__global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ V_hi,
-    float *__restrict__ V_lo, uint32_t *__restrict__ nnz_out) {
+    float *__restrict__ V_lo, uint32_t *__restrict__ nnz_out, int *status,
+    uint32_t *__restrict__ vmask) {
   extern __shared__ __align__(16) uint8_t dsm[];
   uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
   uint32_t *res = hist + 2048;
@@ -496,164 +937,149 @@ __global__ void __launch_bounds__(SOFT_THREADS) soft_select_kernel(
   double *p1 = reinterpret_cast<double *>(reinterpret_cast<uint8_t *>(cand) + SoftSmem::CAND);
   double *p2 = p1 + SOFT_C;
   volatile uint32_t *misc = reinterpret_cast<volatile uint32_t *>(p2 + SOFT_C);  // 16 words
+  double *w_sh = reinterpret_cast<double *>(const_cast<uint32_t *>(misc) + 8);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(dsm + SoftSmem::FIXED - 16);
   float *cache = reinterpret_cast<float *>(dsm + SoftSmem::FIXED);
 
   const int j = blockIdx.x;
   const float *colg = Vraw + (size_t)j * ldv;
-  if (CACHED) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) cache[i] = colg[i];
-    __syncthreads();
-  }
-  // sqrt(s), sqrt(s)^2, ||v||_inf - 1e-6 as the double-precision reference forms them
+  if (CACHED) stage_column(cache, colg, n, bar, status);
+  // sqrt(s), sqrt(s)^2 as the double-precision reference forms them
   const double sq = __dsqrt_rn((double)s);
   const double sq2 = __dmul_rn(sq, sq);
-  const SelResult top = block_select<CACHED>(colg, cache, n, 1u, hist, res);
-  const double linfty = (double)__uint_as_float(top.key);
-  const double lim = __dsub_rn(linfty, 0.000001);
+  const uint32_t NONE = 0xFFFFFFFFu;
 
-  uint32_t consumed = 0, khi = 0xFFFFFFFFu, ge_hi = 0;
-  double S1 = 0.0, S2 = 0.0;
+  // ---- fast path: the highest bins holding at most SOFT_C values
+  key_histogram<CACHED>(colg, cache, n, hist);
+  find_rank_bin(hist, 2048, (uint32_t)SOFT_C + 1u, res);
+  const bool whole = (uint32_t)n <= (uint32_t)SOFT_C;
+  const uint32_t bstar = whole ? 0u : res[0] + 1u;  // gather bins >= bstar
+  const uint32_t c = whole ? (uint32_t)n : res[1];
+  __syncthreads();
   double w = 0.0;
-  __shared__ double w_sh;
-  while (true) {
-    const uint32_t R = min(consumed + (uint32_t)SOFT_C, (uint32_t)n);
-    const uint32_t total = R - consumed;
-    const SelResult lo = block_select<CACHED>(colg, cache, n, R, hist, res);
-    if (threadIdx.x == 0) misc[0] = 0;
-    __syncthreads();
-    if (lo.key == khi) {
-      const float v = __uint_as_float(khi);
-      for (uint32_t q = threadIdx.x; q < total; q += blockDim.x) cand[q] = v;
-    } else {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint32_t key = col_key<CACHED>(colg, cache, i);
-        if (key > lo.key && key < khi) {
-          const uint32_t slot = atomicAdd((uint32_t *)&misc[0], 1u);
-          cand[slot] = __uint_as_float(key);
-        }
-      }
-      __syncthreads();
-      const uint32_t nb = misc[0];
-      const uint32_t c_hi = ge_hi - consumed;
-      const uint32_t c_lo = R - lo.gt;
-      const float vhi = __uint_as_float(khi), vlo = __uint_as_float(lo.key);
-      for (uint32_t q = threadIdx.x; q < c_hi + c_lo; q += blockDim.x)
-        cand[nb + q] = (q < c_hi) ? vhi : vlo;
-    }
-    for (uint32_t q = total + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
-    __syncthreads();
-    bitonic_sort_desc(cand);
-    block_scan2(cand, (int)total, S1, S2, p1, p2, red);
-
-    const uint32_t E = (R == (uint32_t)n) ? total : total - 1;
-    uint32_t best = 0xFFFFFFFFu;
-    double bw = 0.0;
-    double w_last = 0.0;
-    for (uint32_t q = threadIdx.x; q < E; q += blockDim.x) {
-      const uint32_t g = consumed + q;
-      const double t = (double)(g + 1);
-      const double hi = (double)cand[q];
-      const double lov = (q + 1 < total) ? (double)cand[q + 1] : 0.0;
-      const double S1i = p1[q], S2i = p2[q];
-      if (!EXACT) {
-        // Same operations, order and (unfused) rounding as the reference's
-        // expressions at thresh_functions.h:193-213; several of its breaks are
-        // decided by the last bit (e.g. a zero discriminant at the first step).
-        const double S1p = q ? p1[q - 1] : S1, S2p = q ? p2[q - 1] : S2;
-        const double left = ratio_at(S1i, S2i, t, hi);
-        const double rprev = (g == 0) ? sq : ratio_at(S1p, S2p, t - 1.0, hi);
-        const double a = dmul(t, dsub(t, sq2));
-        const double b = dsub(dmul(dmul(2.0, S1i), sq2), dmul(dmul(2.0, t), S1i));
-        const double c = dsub(dmul(S1i, S1i), dmul(sq2, S2i));
-        const double disc = __dsqrt_rn(dsub(dmul(b, b), dmul(dmul(4.0, a), c)));
-        const double wm = __ddiv_rn(dsub(-b, disc), dmul(2.0, a));
-        const double wp = __ddiv_rn(__dadd_rn(-b, disc), dmul(2.0, a));
-        if (g + 1 == (uint32_t)n) w_last = wp;
-        double cw = 0.0;
-        bool hit = false;
-        if (left > sq && rprev < sq) {
-          hit = true;
-          cw = hi;
-        } else if (wm > lov && wm < hi) {
-          hit = true;
-          cw = wm;
-        } else if (wp > lov && wp < hi && wp < lim) {
-          hit = true;
-          cw = wp;
-        }
-        if (hit && g < best) {
-          best = g;
-          bw = cw;
-        }
-      } else {
-        const double rlo = (S1i - t * lov) / sqrt(S2i - 2.0 * lov * S1i + t * lov * lov);
-        if (rlo >= sq && g < best) {
-          const double a = t * (t - sq2);
-          const double b = 2.0 * S1i * sq2 - 2.0 * t * S1i;
-          const double c = S1i * S1i - sq2 * S2i;
-          double lam;
-          if (a == 0.0) {
-            lam = -c / b;
-          } else {
-            const double disc = sqrt(fmax(b * b - 4.0 * a * c, 0.0));
-            const double r1 = (-b - disc) / (2.0 * a), r2 = (-b + disc) / (2.0 * a);
-            // the genuine root keeps every one of the t entries above it
-            const bool ok1 = r1 >= lov && r1 <= hi, ok2 = r2 >= lov && r2 <= hi;
-            lam = ok1 ? r1 : ok2 ? r2 : fmin(fmax(r1, lov), hi);
-          }
-          best = g;
-          bw = lam;
-        }
-      }
-    }
-    // block minimum of the breaking rank
-    uint32_t mb = best;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mb = min(mb, __shfl_xor_sync(FULL, mb, o));
-    if ((threadIdx.x & 31) == 0) res[4 + (threadIdx.x >> 5)] = mb;
-    __syncthreads();
+  uint32_t brk = NONE;
+  bool have_norm = false;
+  double ss = 0.0, cnt = 0.0;
+  if (c > 0) {
     if (threadIdx.x == 0) {
-      uint32_t m2 = 0xFFFFFFFFu;
-      for (int i = 0; i < (int)(blockDim.x >> 5); i++) m2 = min(m2, res[4 + i]);
-      misc[1] = m2;
+      misc[0] = 0;
+      misc[2] = 0;
     }
     __syncthreads();
-    const uint32_t brk = misc[1];
-    if (brk != 0xFFFFFFFFu) {
-      if (best == brk) w_sh = bw;
-      __syncthreads();
-      w = w_sh;
-      break;
+    uint32_t below = 0;  // largest key under the gathered bins
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t key = col_key<CACHED>(colg, cache, i);
+      if ((key >> 20) >= bstar) cand[atomicAdd((uint32_t *)&misc[0], 1u)] = __uint_as_float(key);
+      else below = max(below, key);
     }
-    if (R == (uint32_t)n) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) below = max(below, __shfl_xor_sync(FULL, below, o));
+    if ((threadIdx.x & 31) == 0) atomicMax((uint32_t *)&misc[2], below);
+    for (uint32_t q = c + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
+    __syncthreads();
+    const double lo_after = (c == (uint32_t)n) ? 0.0 : (double)__uint_as_float(misc[2]);
+    bitonic_sort_desc(cand);
+    block_scan2(cand, (int)c, 0.0, 0.0, p1, p2, red);
+    const double lim = __dsub_rn((double)cand[0], 0.000001);  // ||v||_inf - 1e-6
+    uint32_t best = NONE;
+    double bw = 0.0, w_last = 0.0;
+    eval_chunk<EXACT>(cand, p1, p2, c, c, 0, (uint32_t)n, 0.0, 0.0, lo_after, sq, sq2, lim, best,
+                      bw, w_last);
+    brk = resolve_stop(best, bw, res, misc, w_sh, &w);
+    if (brk == NONE && c == (uint32_t)n) {
       // never stopped: the reference keeps the '+' root of its last step;
       // the exact projection with ratio < sqrt(s) everywhere is lambda = 0
-      if (!EXACT && consumed + E - 1 == (uint32_t)n - 1 && threadIdx.x == (E - 1) % blockDim.x)
-        w_sh = w_last;
-      if (EXACT && threadIdx.x == 0) w_sh = 0.0;
+      if (!EXACT && threadIdx.x == (c - 1) % blockDim.x) *w_sh = w_last;
+      if (EXACT && threadIdx.x == 0) *w_sh = 0.0;
       __syncthreads();
-      w = w_sh;
-      break;
+      w = *w_sh;
+      brk = (uint32_t)n;
+      __syncthreads();
     }
-    consumed += E;
-    S1 = p1[E - 1];
-    S2 = p2[E - 1];
-    khi = lo.key;
-    ge_hi = lo.gt + lo.eq;
-    __syncthreads();
+    if (brk != NONE) {
+      // every value above w sits in the gathered chunk
+      for (uint32_t q = threadIdx.x; q < c; q += blockDim.x) {
+        const double d = (double)cand[q] - w;
+        if (d > 0.0) {
+          const double x = (double)(float)d;
+          ss += x * x;
+          cnt += 1.0;
+        }
+      }
+      have_norm = true;
+    }
+  }
+
+  // ---- exact walk, a chunk of SOFT_C ranks at a time
+  if (brk == NONE) {
+    const SelResult top = block_select<CACHED>(colg, cache, n, 1u, hist, res);
+    const double lim = __dsub_rn((double)__uint_as_float(top.key), 0.000001);
+    uint32_t consumed = 0, khi = NONE, ge_hi = 0;
+    double S1 = 0.0, S2 = 0.0;
+    while (true) {
+      const uint32_t R = min(consumed + (uint32_t)SOFT_C, (uint32_t)n);
+      const uint32_t total = R - consumed;
+      const SelResult lo = block_select<CACHED>(colg, cache, n, R, hist, res);
+      if (threadIdx.x == 0) misc[0] = 0;
+      __syncthreads();
+      if (lo.key == khi) {
+        const float v = __uint_as_float(khi);
+        for (uint32_t q = threadIdx.x; q < total; q += blockDim.x) cand[q] = v;
+      } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          const uint32_t key = col_key<CACHED>(colg, cache, i);
+          if (key > lo.key && key < khi)
+            cand[atomicAdd((uint32_t *)&misc[0], 1u)] = __uint_as_float(key);
+        }
+        __syncthreads();
+        const uint32_t nb = misc[0];
+        const uint32_t c_hi = ge_hi - consumed;
+        const uint32_t c_lo = R - lo.gt;
+        const float vhi = __uint_as_float(khi), vlo = __uint_as_float(lo.key);
+        for (uint32_t q = threadIdx.x; q < c_hi + c_lo; q += blockDim.x)
+          cand[nb + q] = (q < c_hi) ? vhi : vlo;
+      }
+      for (uint32_t q = total + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
+      __syncthreads();
+      bitonic_sort_desc(cand);
+      block_scan2(cand, (int)total, S1, S2, p1, p2, red);
+      const uint32_t E = (R == (uint32_t)n) ? total : total - 1;
+      uint32_t best = NONE;
+      double bw = 0.0, w_last = 0.0;
+      eval_chunk<EXACT>(cand, p1, p2, total, E, consumed, (uint32_t)n, S1, S2, 0.0, sq, sq2, lim,
+                        best, bw, w_last);
+      brk = resolve_stop(best, bw, res, misc, w_sh, &w);
+      if (brk != NONE) break;
+      if (R == (uint32_t)n) {
+        if (!EXACT && consumed + E - 1 == (uint32_t)n - 1 && threadIdx.x == (E - 1) % blockDim.x)
+          *w_sh = w_last;
+        if (EXACT && threadIdx.x == 0) *w_sh = 0.0;
+        __syncthreads();
+        w = *w_sh;
+        __syncthreads();
+        break;
+      }
+      consumed += E;
+      S1 = p1[E - 1];
+      S2 = p2[E - 1];
+      khi = lo.key;
+      ge_hi = lo.gt + lo.eq;
+      __syncthreads();
+    }
   }
 
   // x = sgn(v)(|v| - w)_+ with w kept in double: a level that lands within
   // rounding of the largest |v| still leaves that entry non-zero, as in the
   // reference's double arithmetic.
-  double ss = 0.0, cnt = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float v = CACHED ? cache[i] : colg[i];
-    const double d = (double)fabsf(v) - w;
-    if (d > 0.0) {
-      const float x = (float)d * sgnf(v);
-      ss += (double)x * (double)x;
-      cnt += 1.0;
+  if (!have_norm) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float v = CACHED ? cache[i] : colg[i];
+      const double d = (double)fabsf(v) - w;
+      if (d > 0.0) {
+        const double x = (double)(float)d;
+        ss += x * x;
+        cnt += 1.0;
+      }
     }
   }
   ss = block_sum(ss, red);
@@ -661,11 +1087,15 @@ __global__ void __launch_bounds__(SOFT_THREADS) soft_select_kernel(
   const float inv = 1.0f / (float)sqrt(ss);
   float *vh = V_hi + (size_t)j * ldv;
   float *vl = V_lo + (size_t)j * ldv;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float v = CACHED ? cache[i] : colg[i];
+  auto soft = [=](float v) {
     const double d = (double)fabsf(v) - w;
-    const float x = (d > 0.0) ? (float)d * sgnf(v) : 0.f;
-    split_store(x * inv, vh + i, vl + i);
+    return ((d > 0.0) ? (float)d * sgnf(v) : 0.f) * inv;
+  };
+  uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
+  if (CACHED) {
+    write_column(cache, n, vh, vl, mk, soft);
+  } else {
+    write_column_global(colg, n, vh, vl, mk, soft);
   }
   if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
 }
@@ -682,62 +1112,57 @@ struct FinalizeArgs {
   const float *obj_part, *nnz_part;
   const uint32_t *nnz_sel;
   float *val, *err, *max_err;
+  uint32_t *max_nnz;
   int *iters, *cards;
 };
 
-__global__ void __launch_bounds__(1024) finalize_kernel(FinalizeArgs a) {
-  __shared__ float redf[32];
+// One warp per start; the batch maximum is an atomicMax on the bit pattern
+// of the (non-negative, non-NaN) changes, zeroed before the step -- max is
+// order-independent, so the result is deterministic.
+__global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= a.k) return;
   const bool cons = a.formulation <= 3;
   const bool l1pen = a.formulation >= 6;
-  float lm = 0.f;
-  for (int j = threadIdx.x; j < a.k; j += blockDim.x) {
-    float f;
-    uint32_t nz;
-    if (cons) {
-      f = a.fz[j];
-      nz = a.nnz_sel[j];
-    } else {
-      double acc = 0.0, c = 0.0;
-      for (int q = 0; q < a.parts; q++) {
-        acc += (double)a.obj_part[(size_t)j * a.parts + q];
-        c += (double)a.nnz_part[(size_t)j * a.parts + q];
-      }
-      f = l1pen ? (float)sqrt(acc) : (float)acc;
-      nz = (uint32_t)c;
+  float f;
+  uint32_t nz;
+  if (cons) {
+    f = a.fz[j];
+    nz = a.nnz_sel[j];
+  } else {
+    // fixed order: lane-strided partial sums, then a butterfly
+    double acc = 0.0, c = 0.0;
+    for (int q = lane; q < a.parts; q += 32) {
+      acc += (double)a.obj_part[(size_t)j * a.parts + q];
+      c += (double)a.nnz_part[(size_t)j * a.parts + q];
     }
-    const float f0 = a.val[j];
-    const float e = fabsf(f - f0) / f0;
-    a.err[j] = e;
-    a.val[j] = f;
-    if (lm < e) lm = e;
-    if (a.store_all) {
-      // the penalized thresholding calls log into slot j of every batch
-      // (gpower_commons.h:170,173 leave the batch shift at 0)
-      const int slot = cons ? a.log_shift + j : j;
-      if (slot < a.log_capacity) {
-        const bool done = a.it > 0 && (double)e < a.tolerance;
-        if (done && a.iters[slot] == -1) {
-          a.iters[slot] = a.it;
-          a.cards[slot] = (int)nz;
-        } else if (!done && a.iters[slot] != -1) {
-          a.iters[slot] = -1;
-        }
+    acc = warp_sum(acc);
+    c = warp_sum(c);
+    f = l1pen ? (float)sqrt(acc) : (float)acc;
+    nz = (uint32_t)c;
+  }
+  if (lane != 0) return;
+  atomicMax(a.max_nnz, nz);
+  const float f0 = a.val[j];
+  const float e = fabsf(f - f0) / f0;
+  a.err[j] = e;
+  a.val[j] = f;
+  // the reference's `if (max < e) max = e`: NaN never wins
+  if (e > 0.f) atomicMax(reinterpret_cast<unsigned int *>(a.max_err), __float_as_uint(e));
+  if (a.store_all) {
+    // the penalized thresholding calls log into slot j of every batch
+    // (gpower_commons.h:170,173 leave the batch shift at 0)
+    const int slot = cons ? a.log_shift + j : j;
+    if (slot < a.log_capacity) {
+      const bool done = a.it > 0 && (double)e < a.tolerance;
+      if (done && a.iters[slot] == -1) {
+        a.iters[slot] = a.it;
+        a.cards[slot] = (int)nz;
+      } else if (!done && a.iters[slot] != -1) {
+        a.iters[slot] = -1;
       }
     }
-  }
-  // block max with the reference's `if (max < e) max = e` (NaN never wins)
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const float y = __shfl_xor_sync(FULL, lm, o);
-    if (lm < y) lm = y;
-  }
-  if ((threadIdx.x & 31) == 0) redf[threadIdx.x >> 5] = lm;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float m = 0.f;
-    for (int i = 0; i < (int)(blockDim.x >> 5); i++)
-      if (m < redf[i]) m = redf[i];
-    *a.max_err = m;
   }
 }
 
@@ -812,26 +1237,26 @@ cudaError_t dispatch_gemm(int bn, const CUtensorMap &a_hi, const CUtensorMap &a_
   }
 }
 
-template <bool CACHED_OK, class F1, class F2>
+template <class F1, class F2>
 cudaError_t launch_select(bool cached, size_t smem_fixed, int n, int grid, int threads, F1 kc, F2 kg,
                           cudaStream_t st, const float *Vraw, int ld, unsigned s, float *vh,
-                          float *vl, uint32_t *nnz) {
+                          float *vl, uint32_t *nnz, int *status, uint32_t *vmask) {
   if (cached) {
-    const size_t smem = smem_fixed + (size_t)n * 4;
+    const size_t smem = smem_fixed + ((size_t)n * 4 + 15) / 16 * 16;
     cudaError_t e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kc<<<grid, threads, smem, st>>>(Vraw, ld, n, s, vh, vl, nnz);
+    kc<<<grid, threads, smem, st>>>(Vraw, ld, n, s, vh, vl, nnz, status, vmask);
   } else {
     cudaError_t e =
         cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fixed);
     if (e != cudaSuccess) return e;
-    kg<<<grid, threads, smem_fixed, st>>>(Vraw, ld, n, s, vh, vl, nnz);
+    kg<<<grid, threads, smem_fixed, st>>>(Vraw, ld, n, s, vh, vl, nnz, status, vmask);
   }
   return cudaGetLastError();
 }
 
 constexpr size_t SMEM_LIMIT = 227 * 1024;
-constexpr size_t HARD_FIXED = 2048 * 4 + 32 + 32 * 8 + 64;
+constexpr size_t HARD_FIXED = 2048 * 4 + HARD_CAND * 4 + 32 + 32 * 8 + 16;  // + mbarrier
 
 }  // namespace
 
@@ -862,9 +1287,9 @@ cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream
 }
 
 cudaError_t launch_split_columns(const float *src, int ld_src, int rows, int cols, float *hi,
-                                 float *lo, int ld_dst, cudaStream_t st) {
+                                 float *lo, int ld_dst, cudaStream_t st, uint32_t *mask) {
   if (cols <= 0) return cudaSuccess;
-  split_columns_kernel<<<cols, 256, 0, st>>>(src, ld_src, rows, hi, lo, ld_dst);
+  split_columns_kernel<<<cols, 256, 0, st>>>(src, ld_src, rows, hi, lo, ld_dst, mask);
   return cudaGetLastError();
 }
 
@@ -901,6 +1326,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     if (kinds) kinds[nl] = kind;
     return ev ? cudaEventRecord(ev[nl], st) : cudaSuccess;
   };
+  if ((e = cudaMemsetAsync(b.max_err, 0, sizeof(float), st)) != cudaSuccess) return e;
   // 1. Z = B V (split-K partials)
   GemmShape g1;
   g1.M = M.m;
@@ -914,23 +1340,42 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g1.num_units = g1.splits * g1.m_tiles * g1.n_tiles;
   g1.timeout_ns = p.timeout_ns;
   g1.status = b.status;
+  g1.gate = b.max_nnz;
+  g1.gate_max = b.sparse_cap;
+  const int mode = is_l1_variance(f) ? 1 : (is_constrained(f) ? 0 : 2);
+  // 1a. sparse V (every column <= sparse_cap non-zeros last step): gather
+  if ((e = mark(5)) != cudaSuccess) return e;
+  if (mode == 0)
+    gather_bv_kernel<0><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc_hi, M.Bc_lo, M.ldm, M.m, M.ldn,
+                                                        b.V_hi, b.V_lo, b.vmask, b.Z_hi, b.Z_lo,
+                                                        b.fz, b.max_nnz, b.sparse_cap);
+  else if (mode == 1)
+    gather_bv_kernel<1><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc_hi, M.Bc_lo, M.ldm, M.m, M.ldn,
+                                                        b.V_hi, b.V_lo, b.vmask, b.Z_hi, b.Z_lo,
+                                                        b.fz, b.max_nnz, b.sparse_cap);
+  else
+    gather_bv_kernel<2><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc_hi, M.Bc_lo, M.ldm, M.m, M.ldn,
+                                                        b.V_hi, b.V_lo, b.vmask, b.Z_hi, b.Z_lo,
+                                                        b.fz, b.max_nnz, b.sparse_cap);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  nl++;
+  // 1b. dense V: tensor-core Z = B V (split-K partials) ...
   EpiPartial ep{b.ws, b.bn1};
   if ((e = mark(0)) != cudaSuccess) return e;
   e = dispatch_gemm(b.bn1, tm.a1_hi, tm.a1_lo, tm.b1_hi, tm.b1_lo, g1, ep, st);
   if (e != cudaSuccess) return e;
   nl++;
-  // 2. reduce + sign / normalise
-  const int mode = is_l1_variance(f) ? 1 : (is_constrained(f) ? 0 : 2);
+  // 2. ... then reduce + sign / normalise
   if ((e = mark(1)) != cudaSuccess) return e;
   if (mode == 0)
     z_reduce_kernel<0><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
-                                             b.Z_hi, b.Z_lo, M.ldm, b.fz);
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap);
   else if (mode == 1)
     z_reduce_kernel<1><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
-                                             b.Z_hi, b.Z_lo, M.ldm, b.fz);
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap);
   else
     z_reduce_kernel<2><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
-                                             b.Z_hi, b.Z_lo, M.ldm, b.fz);
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   // 3. V = B^T Z
@@ -946,6 +1391,8 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g2.num_units = g2.m_tiles * g2.n_tiles;
   g2.timeout_ns = p.timeout_ns;
   g2.status = b.status;
+  g2.gate = nullptr;
+  g2.gate_max = 0;
   const int parts = b.m_tiles2 * 4;
   if ((e = mark(2)) != cudaSuccess) return e;
   if (is_constrained(f)) {
@@ -953,11 +1400,11 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, er, st);
   } else if (is_l1_penalized(f)) {
     EpiPenalty<true> pe{b.V_hi, b.V_lo, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
-                        p.penalty};
+                        p.penalty, b.vmask};
     e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
   } else {
     EpiPenalty<false> pe{b.V_hi, b.V_lo, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
-                         p.penalty};
+                         p.penalty, b.vmask};
     e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
   }
   if (e != cudaSuccess) return e;
@@ -967,19 +1414,19 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     if ((e = mark(3)) != cudaSuccess) return e;
     if (!is_l1_constrained(f)) {
       const bool cached = HARD_FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
-      e = launch_select<true>(cached, HARD_FIXED, M.n, b.k, 512, hard_select_kernel<true>,
-                              hard_select_kernel<false>, st, b.Vraw, M.ldn, p.constraint, b.V_hi,
-                              b.V_lo, b.nnz);
+      e = launch_select(cached, HARD_FIXED, M.n, b.k, 512, hard_select_kernel<true>,
+                        hard_select_kernel<false>, st, b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo,
+                        b.nnz, b.status, b.vmask);
     } else {
       const bool cached = SoftSmem::FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
       if (p.l1_mode == 0)
-        e = launch_select<true>(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
-                                soft_select_kernel<true, false>, soft_select_kernel<false, false>,
-                                st, b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz);
+        e = launch_select(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
+                          soft_select_kernel<true, false>, soft_select_kernel<false, false>, st,
+                          b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz, b.status, b.vmask);
       else
-        e = launch_select<true>(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
-                                soft_select_kernel<true, true>, soft_select_kernel<false, true>,
-                                st, b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz);
+        e = launch_select(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
+                          soft_select_kernel<true, true>, soft_select_kernel<false, true>, st,
+                          b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz, b.status, b.vmask);
     }
     if (e != cudaSuccess) return e;
     nl++;
@@ -1003,8 +1450,11 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   fa.max_err = b.max_err;
   fa.iters = b.iters;
   fa.cards = b.cards;
+  fa.max_nnz = b.max_nnz;
+  // Z = B V of this step has read max_nnz; finalize sets it for the next step
+  if ((e = cudaMemsetAsync(b.max_nnz, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
   if ((e = mark(4)) != cudaSuccess) return e;
-  finalize_kernel<<<1, 1024, 0, st>>>(fa);
+  finalize_kernel<<<(b.k + 7) / 8, 256, 0, st>>>(fa);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   if (ev && (e = cudaEventRecord(ev[nl], st)) != cudaSuccess) return e;

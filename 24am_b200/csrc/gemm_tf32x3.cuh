@@ -55,6 +55,10 @@ struct GemmShape {
   int num_units;     // splits * m_tiles * n_tiles
   unsigned long long timeout_ns;
   int *status;
+  // Optional gate: when gate != nullptr and *gate <= gate_max the launch does
+  // nothing (another kernel of the step covers the work).
+  const uint32_t *gate;
+  uint32_t gate_max;
 };
 
 struct Unit {
@@ -120,6 +124,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  if (shape.gate && *shape.gate <= shape.gate_max) return;  // uniform over the grid
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {

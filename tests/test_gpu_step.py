@@ -102,3 +102,43 @@ def test_step_is_deterministic(solver, po):
         a, c = outs[-2], outs[-1]
         for x, y in zip(a, c):
             assert np.array_equal(x, y, equal_nan=True)
+
+
+@pytest.mark.parametrize("formulation", range(8))
+def test_steps_through_sparse_gather_match_oracle(solver, po, formulation):
+    """Three steps: after the first, V is sparse and Z = B V runs as the gather
+    kernel (every column at most min(4096, n/32) non-zeros); the loadings stay
+    with the oracle's."""
+    import importlib
+    am = importlib.import_module("24am_b200")
+    m, n, k = 300, 4096, 96
+    B = po.low_rank_data(m, n, 8, 30, seed=77, dtype=np.float32)
+    B64 = B.astype(np.float64)
+    V0 = po.uniform_starts(n, k, seed=78, dtype=np.float32)
+    s = 12
+    g = {4: 2.0, 5: 2000.0, 6: 1.0, 7: 40.0}.get(formulation, 0.0)
+    st = am.OptimizationSettings(formulation=formulation, constraintParameter=s,
+                                 penaltyParameter=g, tolerance=1e-6, maximumIterations=10,
+                                 totalStartingPoints=k, batchSize=k)
+    M = solver.matrix(B)
+    b = M.batch(st, k)
+    b.load(V0)
+    os_ = po.make_settings(formulation, constraint=s, penalty=g, tolerance=1e-6, max_iter=10,
+                           total_starts=k, batch_size=k)
+    Vo, val_o = V0.astype(np.float64), np.zeros(k)
+    kinds = []
+    for it in range(3):
+        kinds.append([name for name, _ in b.step_timed(it)])
+        Vo, _, val_o, _, _ = po.oracle_iteration(B64, Vo, os_, val_o, it=it)
+    V, val, err, nnz = b.read()
+    assert "gemm_BV" in kinds[0] and "gather_BV(skipped)" in kinds[0]
+    if formulation <= 3 or np.count_nonzero(Vo, axis=0).max() <= n // 32:
+        assert "gather_BV" in kinds[2], kinds[2]
+    ok = 0
+    for j in range(k):
+        same = np.array_equal(V[:, j] != 0, Vo[:, j] != 0)
+        close = np.abs(V[:, j] - Vo[:, j]).max() <= 1e-4 * max(np.abs(Vo[:, j]).max(), 1e-30)
+        ok += same and close and abs(val[j] - val_o[j]) <= 1e-4 * abs(val_o[j]) + 1e-20
+    assert ok >= 0.9 * k, f"{ok} of {k} starts agree after 3 steps"
+    b.close()
+    M.close()
