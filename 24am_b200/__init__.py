@@ -107,7 +107,7 @@ _SIGS = {
     "am24_batch_step_timed": (C.c_int, [_VP, _VP, C.c_int32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
 }
-KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV"]
+KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV", "densify"]
 
 _lib = None
 
@@ -407,8 +407,8 @@ class Batch:
 
     def step_timed(self, it=0):
         """One step with per-kernel CUDA-event durations: [(kind, ms), ...]."""
-        ms = (C.c_float * 8)()
-        kinds = (C.c_int32 * 8)()
+        ms = (C.c_float * 16)()
+        kinds = (C.c_int32 * 16)()
         cnt = C.c_int32()
         check(lib().am24_batch_step_timed(self.matrix.solver.h, self.bh, int(it), ms, kinds,
                                           C.byref(cnt)))

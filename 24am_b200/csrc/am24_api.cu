@@ -100,16 +100,18 @@ struct am24_batch_s {
 
 namespace {
 
+// K-major FP32 operand [rows][ld], loaded as bk x box_rows tiles; the swizzle
+// matches the row length (bk * 4 bytes) and the GEMM's smem descriptors.
 am24_status make_map(am24_handle h, CUtensorMap *map, const float *base, int K, int rows, int ld,
-                     int box_rows) {
+                     int box_rows, int bk) {
   cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
-  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  cuuint32_t box[2] = {(cuuint32_t)bk, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = h->encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims,
                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                         bk == 32 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
     return fail(AM24_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
   return AM24_OK;
@@ -228,10 +230,10 @@ am24_status upload_columns(am24_handle h, am24_batch b, const float *host, int c
   for (int c = 0; c < cols; c++) {
     AM24_CUDA(cudaMemcpyAsync(b->d.Vraw + (size_t)slots[c] * M.ldn, host + (size_t)c * M.n,
                               sizeof(float) * M.n, cudaMemcpyHostToDevice, h->stream));
-    AM24_CUDA(launch_split_columns(b->d.Vraw + (size_t)slots[c] * M.ldn, M.ldn, M.n, 1,
-                                   b->d.V_hi + (size_t)slots[c] * M.ldn,
-                                   b->d.V_lo + (size_t)slots[c] * M.ldn, M.ldn, h->stream,
-                                   b->d.vmask + (size_t)slots[c] * (M.ldn / 32)));
+    AM24_CUDA(launch_load_columns(b->d.Vraw + (size_t)slots[c] * M.ldn, M.ldn, M.n, 1,
+                                  b->d.Vx + (size_t)slots[c] * M.ldn, M.ldn,
+                                  b->d.vmask + (size_t)slots[c] * (M.ldn / 32), h->stream));
+    AM24_CUDA(cudaMemsetAsync(b->d.sel_hint + slots[c], 0, sizeof(float), h->stream));
   }
   // new starts are dense: the next Z = B V runs on the tensor cores
   AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));
@@ -366,7 +368,8 @@ am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, u
   if ((st = mat->mem.get(&M.Bc_hi, c_elems)) != AM24_OK ||
       (st = mat->mem.get(&M.Bc_lo, c_elems)) != AM24_OK ||
       (st = mat->mem.get(&M.Bt_hi, t_elems)) != AM24_OK ||
-      (st = mat->mem.get(&M.Bt_lo, t_elems)) != AM24_OK) {
+      (st = mat->mem.get(&M.Bt_lo, t_elems)) != AM24_OK ||
+      (st = mat->mem.get(&M.Bc, c_elems)) != AM24_OK) {
     delete mat;
     return st;
   }
@@ -387,6 +390,7 @@ am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, u
   if (e == cudaSuccess) e = cudaMemsetAsync(M.Bc_lo, 0, sizeof(float) * c_elems, h->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(M.Bt_hi, 0, sizeof(float) * t_elems, h->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(M.Bt_lo, 0, sizeof(float) * t_elems, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bc, 0, sizeof(float) * c_elems, h->stream);
   if (e == cudaSuccess) e = launch_prep_matrix(src, ld_src, M, h->stream);
   if (staging) cudaFreeAsync(staging, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -433,14 +437,17 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   d.n_tiles1 = (k + d.bn1 - 1) / d.bn1;
   d.m_tiles2 = (M.n + BM - 1) / BM;
   d.n_tiles2 = (k + d.bn2 - 1) / d.bn2;
-  const int kb_total1 = (M.n + BK - 1) / BK;
+  d.bk = BK_DEFAULT;
+  if (const char *e = getenv("AM24_GEMM_BK")) d.bk = (atoi(e) == 16) ? 16 : 32;
+  const int kb_total1 = (M.n + d.bk - 1) / d.bk;
   choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
   const int parts = d.m_tiles2 * 4;
   d.log_capacity = std::max(settings->total_starts, k);
   am24_status st;
   auto &A = b->mem;
   const size_t kv = (size_t)k * M.ldn, kz = (size_t)k * M.ldm;
-  if ((st = A.get(&d.V_hi, kv)) || (st = A.get(&d.V_lo, kv)) || (st = A.get(&d.Vraw, kv)) ||
+  if ((st = A.get(&d.Vx, kv)) || (st = A.get(&d.V_hi, kv)) || (st = A.get(&d.V_lo, kv)) ||
+      (st = A.get(&d.Vraw, kv)) ||
       (st = A.get(&d.Z_hi, kz)) || (st = A.get(&d.Z_lo, kz)) ||
       (st = A.get(&d.ws, ws_floats(d.splits1, d.m_tiles1, d.n_tiles1, d.bn1))) ||
       (st = A.get(&d.fz, k)) || (st = A.get(&d.obj_part, (size_t)k * parts)) ||
@@ -448,11 +455,12 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.val, k)) || (st = A.get(&d.err, k)) || (st = A.get(&d.max_err, 1)) ||
       (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
       (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||
-      (st = A.get(&d.max_nnz, 1))) {
+      (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.sel_hint, k))) {
     delete b;
     return st;
   }
-  cudaError_t e = cudaMemsetAsync(d.V_hi, 0, sizeof(float) * kv, h->stream);
+  cudaError_t e = cudaMemsetAsync(d.Vx, 0, sizeof(float) * kv, h->stream);
+  if (!e) e = cudaMemsetAsync(d.V_hi, 0, sizeof(float) * kv, h->stream);
   if (!e) e = cudaMemsetAsync(d.V_lo, 0, sizeof(float) * kv, h->stream);
   if (!e) e = cudaMemsetAsync(d.Vraw, 0, sizeof(float) * kv, h->stream);
   if (!e) e = cudaMemsetAsync(d.Z_hi, 0, sizeof(float) * kz, h->stream);
@@ -464,6 +472,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.status, 0, sizeof(int), h->stream);
   if (!e) e = cudaMemsetAsync(d.vmask, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
   if (!e) e = cudaMemsetAsync(d.max_nnz, 0xFF, sizeof(uint32_t), h->stream);
+  if (!e) e = cudaMemsetAsync(d.sel_hint, 0, sizeof(float) * k, h->stream);
   if (!e) e = cudaMemsetAsync(d.iters, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaMemsetAsync(d.cards, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaStreamSynchronize(h->stream);
@@ -471,20 +480,20 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
     delete b;
     return fail(AM24_ERR_CUDA, std::string("batch init: ") + cudaGetErrorString(e));
   }
-  if ((st = make_map(h, &b->tm.a1_hi, M.Bt_hi, M.n, M.m, M.ldn, BM)) ||
-      (st = make_map(h, &b->tm.a1_lo, M.Bt_lo, M.n, M.m, M.ldn, BM)) ||
-      (st = make_map(h, &b->tm.b1_hi, d.V_hi, M.n, k, M.ldn, d.bn1)) ||
-      (st = make_map(h, &b->tm.b1_lo, d.V_lo, M.n, k, M.ldn, d.bn1)) ||
-      (st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM)) ||
-      (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM)) ||
-      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.bn2)) ||
-      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.bn2))) {
+  if ((st = make_map(h, &b->tm.a1_hi, M.Bt_hi, M.n, M.m, M.ldn, BM, d.bk)) ||
+      (st = make_map(h, &b->tm.a1_lo, M.Bt_lo, M.n, M.m, M.ldn, BM, d.bk)) ||
+      (st = make_map(h, &b->tm.b1_hi, d.V_hi, M.n, k, M.ldn, d.bn1, d.bk)) ||
+      (st = make_map(h, &b->tm.b1_lo, d.V_lo, M.n, k, M.ldn, d.bn1, d.bk)) ||
+      (st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM, d.bk)) ||
+      (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM, d.bk)) ||
+      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.bn2, d.bk)) ||
+      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.bn2, d.bk))) {
     delete b;
     return st;
   }
   // a gather over V's non-zeros beats the dense product while they are few
   d.sparse_cap = (uint32_t)std::min(4096, M.n / 32);
-  b->launches = is_constrained(settings->formulation) ? 6 : 5;
+  b->launches = is_constrained(settings->formulation) ? 7 : 6;
   *out = b;
   return AM24_OK;
 }
@@ -510,9 +519,9 @@ am24_status am24_batch_load(am24_handle h, am24_batch b, const float *V, int32_t
     AM24_CUDA(cudaMemcpy2DAsync(b->d.Vraw, sizeof(float) * M.ldn, V, sizeof(float) * M.n,
                                 sizeof(float) * M.n, k, cudaMemcpyHostToDevice, h->stream));
   }
-  AM24_CUDA(launch_split_columns(b->d.Vraw, M.ldn, M.n, k, b->d.V_hi, b->d.V_lo, M.ldn, h->stream,
-                                 b->d.vmask));
+  AM24_CUDA(launch_load_columns(b->d.Vraw, M.ldn, M.n, k, b->d.Vx, M.ldn, b->d.vmask, h->stream));
   AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));  // dense starts
+  AM24_CUDA(cudaMemsetAsync(b->d.sel_hint, 0, sizeof(float) * k, h->stream));      // no hints
   // ValueCoordinateHolder::reset (c++/src/utils/various.h:33-38)
   AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
   AM24_CUDA(cudaMemsetAsync(b->d.err, 0, sizeof(float) * k, h->stream));
@@ -541,8 +550,8 @@ am24_status am24_batch_read(am24_handle h, am24_batch b, float *V, float *val, f
   const MatrixDev &M = b->mat->d;
   const int k = b->d.k;
   if (V) {
-    AM24_CUDA(launch_combine_columns(b->d.V_hi, b->d.V_lo, M.ldn, M.n, k, b->d.Vraw, M.ldn,
-                                     h->stream));
+    AM24_CUDA(launch_masked_copy(b->d.Vx, b->d.vmask, M.ldn, M.n, k, b->d.Vraw, M.ldn,
+                                 h->stream));
     AM24_CUDA(cudaMemcpy2DAsync(V, sizeof(float) * M.n, b->d.Vraw, sizeof(float) * M.ldn,
                                 sizeof(float) * M.n, k, cudaMemcpyDeviceToHost, h->stream));
   }
@@ -576,15 +585,15 @@ am24_status am24_batch_read(am24_handle h, am24_batch b, float *V, float *val, f
 am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float *ms,
                                   int32_t *kinds, int32_t *count) {
   if (!h || !b || !ms || !kinds || !count) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  cudaEvent_t ev[9];
+  cudaEvent_t ev[17];
   int made = 0;
   am24_status st = AM24_OK;
-  for (; made < 9; made++)
+  for (; made < 17; made++)
     if (cudaEventCreate(&ev[made]) != cudaSuccess) {
       st = fail(AM24_ERR_CUDA, "cudaEventCreate failed");
       break;
     }
-  int nl = 0, kk[9] = {0};
+  int nl = 0, kk[17] = {0};
   uint32_t gate = 0;
   if (st == AM24_OK &&
       cudaMemcpyAsync(&gate, b->d.max_nnz, sizeof gate, cudaMemcpyDeviceToHost, h->stream) ==
@@ -601,7 +610,8 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
   // mark the Z = B V kernels that the gate turned into no-ops
   const bool sparse = gate <= b->d.sparse_cap;
   for (int i = 0; i < nl; i++) {
-    const bool skipped = sparse ? (kk[i] == AM24_KERNEL_GEMM_BV || kk[i] == AM24_KERNEL_Z_REDUCE)
+    const bool skipped = sparse ? (kk[i] == AM24_KERNEL_GEMM_BV || kk[i] == AM24_KERNEL_Z_REDUCE ||
+                                   kk[i] == AM24_KERNEL_DENSIFY)
                                 : (kk[i] == AM24_KERNEL_GATHER_BV);
     kinds[i] = kk[i] | (skipped ? AM24_KERNEL_SKIPPED : 0);
   }
@@ -644,14 +654,12 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
   // best loading so far, kept as hi/lo planes; starts as the caller's x, which
   // the reference returns normalised when no start ever improves on -1
   Allocs local;
-  float *xb_hi = nullptr, *xb_lo = nullptr, *x_dev = nullptr;
+  float *xb = nullptr, *x_dev = nullptr;
   double *ev_rows = nullptr;
-  AM24_TRY(local.get(&xb_hi, n));
-  AM24_TRY(local.get(&xb_lo, n));
+  AM24_TRY(local.get(&xb, n));
   AM24_TRY(local.get(&x_dev, n));
   AM24_TRY(local.get(&ev_rows, (size_t)M.m));
-  AM24_CUDA(cudaMemcpyAsync(xb_hi, x, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
-  AM24_CUDA(cudaMemsetAsync(xb_lo, 0, sizeof(float) * n, h->stream));
+  AM24_CUDA(cudaMemcpyAsync(xb, x, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
 
   cudaEvent_t e0, e1;
   AM24_CUDA(cudaEventCreate(&e0));
@@ -675,10 +683,8 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
   int degenerate = 0;
   const BatchDev &d = b->d;
   auto take_best = [&](int j) -> am24_status {
-    AM24_CUDA(cudaMemcpyAsync(xb_hi, d.V_hi + (size_t)j * M.ldn, sizeof(float) * n,
-                              cudaMemcpyDeviceToDevice, h->stream));
-    AM24_CUDA(cudaMemcpyAsync(xb_lo, d.V_lo + (size_t)j * M.ldn, sizeof(float) * n,
-                              cudaMemcpyDeviceToDevice, h->stream));
+    AM24_CUDA(launch_masked_copy(d.Vx + (size_t)j * M.ldn, d.vmask + (size_t)j * (M.ldn / 32),
+                                 M.ldn, (int)n, 1, xb, (int)n, h->stream));
     return AM24_OK;
   };
 
@@ -795,7 +801,7 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
   }
 
   // x <- x / ||x|| and its FP64 explained variance ||B x||^2
-  AM24_CUDA(launch_finalize_x(xb_hi, xb_lo, (int)n, x_dev, h->stream));
+  AM24_CUDA(launch_finalize_x(xb, (int)n, x_dev, h->stream));
   AM24_CUDA(launch_explained_variance(M, x_dev, ev_rows, h->ev_out, h->stream));
   double ev = 0.0;
   AM24_CUDA(cudaMemcpyAsync(x, x_dev, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));

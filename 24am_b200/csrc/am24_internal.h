@@ -9,7 +9,9 @@ namespace am24 {
 
 // GEMM tiling: M tile is fixed at 128 (one TMEM lane per accumulator row).
 constexpr int BM = 128;
-constexpr int BK = 32;  // K slab per pipeline stage (128-byte rows, 128B swizzle)
+// K slab per pipeline stage: 32 (128-byte rows, 128B swizzle, fewer deeper
+// stages) or 16 (64-byte rows, 64B swizzle, twice the stages).
+constexpr int BK_DEFAULT = 16;
 
 // Formulation helpers (c++/src/class/optimization_settings.h:125-153).
 inline bool is_constrained(int f) { return f >= 0 && f <= 3; }
@@ -24,16 +26,21 @@ inline bool is_l1_penalized(int f) { return f == 6 || f == 7; }
 struct MatrixDev {
   int m, n, ldm, ldn;
   float *Bc_hi, *Bc_lo, *Bt_hi, *Bt_lo;
+  float *Bc;  // plain FP32 B, n rows of ldm samples: the gather Z = B V reads it
 };
 
 // Per-batch device state for k starting points.
 struct BatchDev {
   int k;          // starting points in the batch
   int bn1, bn2;   // GEMM N tiles (Z = B V and V = B^T Z)
+  int bk;         // GEMM K slab (16 or 32)
   int splits1;    // split-K factor of Z = B V
   int kbps1;      // K blocks per split of Z = B V
   int m_tiles1, n_tiles1, m_tiles2, n_tiles2;
-  float *V_hi, *V_lo;   // k x ldn loadings (GEMM-1 B operand, threshold output)
+  float *Vx;            // k x ldn loadings; entry i of a column is defined only
+                        // where its vmask bit is set (zero elsewhere)
+  float *V_hi, *V_lo;   // k x ldn dense TF32 hi/lo planes of V: the B operand of the
+                        // tensor-core Z = B V, filled by densify on dense steps only
   float *Z_hi, *Z_lo;   // k x ldm sample-space vectors (GEMM-2 B operand)
   float *Vraw;          // k x ldn raw B^T Z (constrained forms)
   float *ws;            // split-K partial tiles of Z = B V
@@ -41,6 +48,7 @@ struct BatchDev {
   float *obj_part;      // per start x (m_tiles2*4): penalized objective partials
   float *nnz_part;      // per start x (m_tiles2*4): penalized non-zero partials
   uint32_t *nnz;        // per start: non-zeros after thresholding
+  float *sel_hint;      // per start: last threshold level (0 = none), a search hint
   uint32_t *vmask;      // k x (ldn/32): bit r of word w set iff V[32w + r] != 0
   uint32_t *max_nnz;    // largest non-zero count of the last step (0xFFFFFFFF: dense V)
   uint32_t sparse_cap;  // Z = B V runs as a gather when max_nnz <= sparse_cap
@@ -72,21 +80,21 @@ struct TensorMaps {
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
 int num_sms();
 cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st);
-// dst hi/lo planes of `cols` columns from src, and their non-zero masks
-// (mask may be null; otherwise mask + c * (ld_dst / 32) per column).
-cudaError_t launch_split_columns(const float *src, int ld_src, int rows, int cols, float *hi,
-                                 float *lo, int ld_dst, cudaStream_t st,
-                                 uint32_t *mask = nullptr);
-// ev (optional, >= 9 events): ev[i] is recorded before launch i and
+// Loadings of `cols` columns from src (rows entries each) into dst and their
+// non-zero masks (mask + c * (ld_dst / 32) per column).
+cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols, float *dst,
+                                int ld_dst, uint32_t *mask, cudaStream_t st);
+// dst[c][i] = mask bit i of column c ? Vx[c][i] : 0 for i < rows.
+cudaError_t launch_masked_copy(const float *Vx, const uint32_t *mask, int ld, int rows, int cols,
+                               float *dst, int ld_dst, cudaStream_t st);
+// ev (optional, >= 17 events): ev[i] is recorded before launch i and
 // ev[launches] after the last one; kinds[i] (optional) gets each launch's kind.
 cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm,
                            const StepParams &p, cudaStream_t st, int *launches,
                            cudaEvent_t *ev = nullptr, int *kinds = nullptr);
-cudaError_t launch_finalize_x(const float *hi, const float *lo, int n, float *x, cudaStream_t st);
+cudaError_t launch_finalize_x(const float *v, int n, float *x, cudaStream_t st);
 cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double *partial,
                                       double *out, cudaStream_t st);
-cudaError_t launch_combine_columns(const float *hi, const float *lo, int ld, int rows,
-                                   int cols, float *dst, int ld_dst, cudaStream_t st);
 int pick_bn(int k);
 size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn);
 

@@ -28,8 +28,8 @@ namespace am24 {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-// K slabs (of BK) accumulated in TMEM before promotion to registers
-constexpr int GEMM_PROMO = 4;
+// K elements accumulated in TMEM before promotion to registers
+constexpr int GEMM_PROMO_K = 128;
 
 // x rounded to the nearest TF32 value (low 13 mantissa bits zero).  With
 // lo = x - hi exact in FP32, x = hi + lo bit for bit, and lo takes either sign,
@@ -92,11 +92,13 @@ __device__ __forceinline__ float transpose_reduce32(float (&v)[32], int lane) {
 // Z = B V split-K partial tile: ws[unit][col][row], whole 128 x bn tile.
 struct EpiPartial {
   float *ws;
-  int bn;
+  int bn, m_tiles, n_tiles;  // m_tiles: 128-row blocks of C
   __device__ void begin(const Unit &, int, int) {}
   __device__ void end(const Unit &, int, int) {}
   __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
-    float *base = ws + (size_t)t.index * ((size_t)bn * BM) + row;
+    if (t.m0 >= m_tiles * BM) return;  // a 2-CTA tile's second half can lie past the last block
+    const size_t slot = ((size_t)t.split * m_tiles + t.m0 / BM) * n_tiles + t.nt;
+    float *base = ws + slot * ((size_t)bn * BM) + row;
 #pragma unroll
     for (int j = 0; j < 32; j++) base[(size_t)(col0 + j) * BM] = r[j];
   }
@@ -109,7 +111,7 @@ struct EpiRaw {
   __device__ void begin(const Unit &, int, int) {}
   __device__ void end(const Unit &, int, int) {}
   __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
-    const int gi = t.mt * BM + row;
+    const int gi = t.m0 + row;
     if (gi >= M) return;
     const int c0 = t.nt * bn + col0;
 #pragma unroll
@@ -122,11 +124,12 @@ struct EpiRaw {
 //   L1 (c++/src/gpower/sparse_PCA_thresholding.h:26-47): d = |v| - gamma (in
 //      double, gamma is a double there), x = sgn(v) d if d > 0, objective term d^2.
 //   L0 (:68-87): d = v^2 - gamma, x = v if d > 0, objective term d.
-// Writes x as hi/lo planes and, per start and per (m-tile, warp), the partial
-// objective and non-zero count, summed in fixed order by the finalize kernel.
+// Writes the non-zero x and the non-zero bitmask and, per start and per
+// (m-tile, warp), the partial objective and non-zero count, summed in fixed
+// order by the finalize kernel.
 template <bool L1>
 struct EpiPenalty {
-  float *V_hi, *V_lo;
+  float *Vx;
   float *obj_part, *nnz_part;
   int ld, M, N, bn, parts;  // parts = m_tiles * 4
   double gamma;
@@ -136,8 +139,10 @@ struct EpiPenalty {
   // r holds this thread's 32 values (row `row`, columns col0..col0+31) and is
   // overwritten with the objective terms.
   __device__ void chunk(const Unit &t, int q, int lane, int row, int col0, float (&r)[32]) {
-    const int gi = t.mt * BM + row;
+    if (t.m0 >= M) return;  // a 2-CTA tile's second half can lie past the last row
+    const int gi = t.m0 + row;
     const bool rv = gi < M;
+    const int mb = t.m0 / BM;  // 128-row block
     const int c0 = t.nt * bn + col0;
     float mycnt = 0.f;
     uint32_t mymask = 0u;
@@ -163,17 +168,14 @@ struct EpiPenalty {
         mycnt = (float)__popc(nz);
         mymask = nz;
       }
-      if (valid) {
-        const size_t off = (size_t)(c0 + j) * ld + gi;
-        split_store(x, V_hi + off, V_lo + off);
-      }
+      if (valid && x != 0.f) Vx[(size_t)(c0 + j) * ld + gi] = x;  // zeros live in the mask
     }
     const float so = transpose_reduce32(r, lane);
     const int col = c0 + lane;
     if (col < N) {
-      obj_part[(size_t)col * parts + t.mt * 4 + q] = so;
-      nnz_part[(size_t)col * parts + t.mt * 4 + q] = mycnt;
-      if (t.mt * 4 + q < (ld >> 5)) vmask[(size_t)col * (ld >> 5) + t.mt * 4 + q] = mymask;
+      obj_part[(size_t)col * parts + mb * 4 + q] = so;
+      nnz_part[(size_t)col * parts + mb * 4 + q] = mycnt;
+      if (mb * 4 + q < (ld >> 5)) vmask[(size_t)col * (ld >> 5) + mb * 4 + q] = mymask;
     }
   }
 };
@@ -181,10 +183,13 @@ struct EpiPenalty {
 // ------------------------------------------------------------ operand prep
 // Bc[c * ldm + r] = split(B[c * ldB + r]): one block per feature column.
 __global__ void prep_copy_kernel(const float *__restrict__ B, int ldB, int m, float *__restrict__ hi,
-                                 float *__restrict__ lo, int ldm) {
+                                 float *__restrict__ lo, float *__restrict__ full, int ldm) {
   const size_t c = blockIdx.x;
-  for (int r = threadIdx.x; r < m; r += blockDim.x)
-    split_store(B[c * ldB + r], hi + c * ldm + r, lo + c * ldm + r);
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    const float v = B[c * ldB + r];
+    split_store(v, hi + c * ldm + r, lo + c * ldm + r);
+    full[c * ldm + r] = v;
+  }
 }
 
 // Bt[r * ldn + c] = split(B[c * ldB + r]): 32 x 32 tiles through shared memory.
@@ -206,26 +211,43 @@ __global__ void prep_transpose_kernel(const float *__restrict__ B, int ldB, int 
   }
 }
 
-// One block per column: hi/lo planes and, when mask is given, the column's
-// non-zero bitmask (ld_dst / 32 words; rows beyond `rows` count as zero).
-__global__ void split_columns_kernel(const float *__restrict__ src, int ld_src, int rows,
-                                     float *__restrict__ hi, float *__restrict__ lo, int ld_dst,
-                                     uint32_t *__restrict__ mask) {
+// One block per column: dst = src (rows entries, zero up to ld_dst) and the
+// column's non-zero bitmask (ld_dst / 32 words).
+__global__ void load_columns_kernel(const float *__restrict__ src, int ld_src, int rows,
+                                    float *__restrict__ dst, int ld_dst,
+                                    uint32_t *__restrict__ mask) {
   const size_t c = blockIdx.x;
   const int lane = threadIdx.x & 31;
   for (int base = threadIdx.x & ~31; base < ld_dst; base += blockDim.x) {
     const int r = base + lane;
     const float v = (r < rows) ? src[c * ld_src + r] : 0.f;
-    if (r < rows) split_store(v, hi + c * ld_dst + r, lo + c * ld_dst + r);
+    dst[c * ld_dst + r] = v;
     const unsigned nz = __ballot_sync(FULL, v != 0.f);
-    if (mask && lane == 0) mask[c * (ld_dst >> 5) + (base >> 5)] = nz;
+    if (lane == 0) mask[c * (ld_dst >> 5) + (base >> 5)] = nz;
   }
 }
 
-__global__ void combine_columns_kernel(const float *__restrict__ hi, const float *__restrict__ lo,
-                                       int ld, int rows, float *__restrict__ dst, int ld_dst) {
+__global__ void masked_copy_kernel(const float *__restrict__ Vx, const uint32_t *__restrict__ mask,
+                                   int ld, int rows, float *__restrict__ dst, int ld_dst) {
   const size_t c = blockIdx.x;
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) dst[c * ld_dst + r] = hi[c * ld + r] + lo[c * ld + r];
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    const bool on = (mask[c * (ld >> 5) + (r >> 5)] >> (r & 31)) & 1u;
+    dst[c * ld_dst + r] = on ? Vx[c * ld + r] : 0.f;
+  }
+}
+
+// Dense TF32 hi/lo planes of V for the tensor-core Z = B V; does nothing on
+// steps where the gather kernel takes Z = B V (*gate <= gate_max).
+__global__ void densify_kernel(const float *__restrict__ Vx, const uint32_t *__restrict__ mask,
+                               int ld, int rows, float *__restrict__ V_hi,
+                               float *__restrict__ V_lo, const uint32_t *gate,
+                               uint32_t gate_max) {
+  if (*gate <= gate_max) return;
+  const size_t c = blockIdx.x;
+  for (int r = threadIdx.x; r < ld; r += blockDim.x) {
+    const bool on = r < rows && ((mask[c * (ld >> 5) + (r >> 5)] >> (r & 31)) & 1u);
+    split_store(on ? Vx[c * ld + r] : 0.f, V_hi + c * ld + r, V_lo + c * ld + r);
+  }
 }
 
 // ------------------------------------------------------------ Z reduction
@@ -288,10 +310,9 @@ constexpr int GATHER_CAP = 4096;
 // step as z_reduce_kernel<MODE> finishes the column.
 template <int MODE>
 __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
-    const float *__restrict__ Bc_hi, const float *__restrict__ Bc_lo, int ldm, int m, int ldn,
-    const float *__restrict__ V_hi, const float *__restrict__ V_lo,
-    const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi, float *__restrict__ Z_lo,
-    float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max) {
+    const float *__restrict__ Bc, int ldm, int m, int ldn,
+    const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
+    float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max) {
   __shared__ int idx[GATHER_CAP];
   __shared__ float val[GATHER_CAP];
   __shared__ uint32_t wsum[GATHER_THREADS / 32];
@@ -320,8 +341,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
   uint32_t total = 0;
   for (int i = 0; i < GATHER_THREADS / 32; i++) total += wsum[i];
   if (total > (uint32_t)GATHER_CAP) total = GATHER_CAP;  // cannot happen below the gate
-  const float *vh = V_hi + (size_t)j * ldn;
-  const float *vl = V_lo + (size_t)j * ldn;
+  const float *vx = Vx + (size_t)j * ldn;
   for (int q = w0; q < w1; q++) {
     uint32_t bits = mk[q];
     while (bits) {
@@ -330,7 +350,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
       const int r = q * 32 + b;
       if (off < (uint32_t)GATHER_CAP) {
         idx[off] = r;
-        val[off] = vh[r] + vl[r];
+        val[off] = vx[r];
       }
       off++;
     }
@@ -351,7 +371,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
 #pragma unroll
       for (int r = 0; r < GATHER_ROWS; r++) {
         const int i = base + r * GATHER_THREADS + threadIdx.x;
-        if (i < m) y[r] = fmaf(v, Bc_hi[row + i] + Bc_lo[row + i], y[r]);
+        if (i < m) y[r] = fmaf(v, Bc[row + i], y[r]);
       }
     }
 #pragma unroll
@@ -501,31 +521,26 @@ __device__ void stage_column(float *cache, const float *__restrict__ colg, int n
   }
 }
 
-// x_i = f(v_i) written as hi/lo planes with 16-byte stores (column bases are
-// 128-byte aligned) and the column's non-zero bitmask.  Each warp writes 128
-// consecutive entries per step (4 mask words); entries past n read the zero
-// padding of the staged column (the column's padding rows are zero).
+// x_i = f(v_i) for a column staged in shared memory: the non-zero x_i are
+// stored (only they are defined; the bitmask says which) and the column's
+// non-zero bitmask is written.  Each warp covers 128 consecutive entries per
+// step (4 mask words); entries past n read the staged column's zero padding.
 template <class Fn>
-__device__ __forceinline__ void write_column(const float *cache, int n, float *vh, float *vl,
-                                             uint32_t *mask, Fn fn) {
+__device__ __forceinline__ void write_column(const float *cache, int n, float *vx, uint32_t *mask,
+                                             Fn fn) {
   const int n4 = (n + 3) >> 2;
   const int lane = threadIdx.x & 31;
   const float4 *c4 = reinterpret_cast<const float4 *>(cache);
-  float4 *h4 = reinterpret_cast<float4 *>(vh);
-  float4 *l4 = reinterpret_cast<float4 *>(vl);
   for (int base = threadIdx.x & ~31; base < n4; base += blockDim.x) {
     const int i = base + lane;
     uint32_t nib = 0;
     if (i < n4) {
       const float4 v = c4[i];
-      float4 h, l;
-      float x;
-      x = fn(v.x); h.x = tf32_hi(x); l.x = x - h.x; nib |= (x != 0.f) ? 1u : 0u;
-      x = fn(v.y); h.y = tf32_hi(x); l.y = x - h.y; nib |= (x != 0.f) ? 2u : 0u;
-      x = fn(v.z); h.z = tf32_hi(x); l.z = x - h.z; nib |= (x != 0.f) ? 4u : 0u;
-      x = fn(v.w); h.w = tf32_hi(x); l.w = x - h.w; nib |= (x != 0.f) ? 8u : 0u;
-      h4[i] = h;
-      l4[i] = l;
+      const float x0 = fn(v.x), x1 = fn(v.y), x2 = fn(v.z), x3 = fn(v.w);
+      if (x0 != 0.f) { vx[4 * i] = x0; nib |= 1u; }
+      if (x1 != 0.f) { vx[4 * i + 1] = x1; nib |= 2u; }
+      if (x2 != 0.f) { vx[4 * i + 2] = x2; nib |= 4u; }
+      if (x3 != 0.f) { vx[4 * i + 3] = x3; nib |= 8u; }
     }
     // 8 lanes x 4 entries -> one 32-bit mask word
     uint32_t word = nib << (4 * (lane & 7));
@@ -540,13 +555,13 @@ __device__ __forceinline__ void write_column(const float *cache, int n, float *v
 // the next multiple of 32 are read; they lie in the column's zero padding).
 template <class Fn>
 __device__ __forceinline__ void write_column_global(const float *__restrict__ colg, int n,
-                                                    float *vh, float *vl, uint32_t *mask, Fn fn) {
+                                                    float *vx, uint32_t *mask, Fn fn) {
   const int lane = threadIdx.x & 31;
   const int n32 = (n + 31) & ~31;
   for (int base = threadIdx.x & ~31; base < n32; base += blockDim.x) {
     const int i = base + lane;
     const float x = fn(colg[i]);
-    split_store(x, vh + i, vl + i);
+    if (x != 0.f) vx[i] = x;
     const unsigned nz = __ballot_sync(FULL, x != 0.f);
     if (lane == 0) mask[base >> 5] = nz;
   }
@@ -611,6 +626,43 @@ __device__ void key_histogram(const float *__restrict__ colg, const float *cols,
   __syncthreads();
 }
 
+// Block-wide: the keys >= bound go to cand (the first `cap` of them, in any
+// order) and the count of all of them is returned (it may exceed cap);
+// res[1] gets the largest key below the bound.  res[0..1] are scratch.
+template <bool CACHED>
+__device__ uint32_t gather_keys_above(const float *__restrict__ colg, const float *cols, int n,
+                                      uint32_t bound, uint32_t *cand, uint32_t cap,
+                                      uint32_t *res) {
+  if (threadIdx.x == 0) {
+    res[0] = 0;
+    res[1] = 0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  uint32_t below = 0;
+  for (int base = threadIdx.x & ~31; base < n; base += blockDim.x) {
+    const int i = base + lane;
+    const uint32_t key = (i < n) ? col_key<CACHED>(colg, cols, i) : 0u;
+    const bool take = (i < n) && key >= bound;
+    if (!take) below = max(below, key);
+    const unsigned bal = __ballot_sync(FULL, take);
+    if (bal) {
+      uint32_t wbase = 0;
+      if (lane == 0) wbase = atomicAdd(&res[0], (uint32_t)__popc(bal));
+      wbase = __shfl_sync(FULL, wbase, 0);
+      if (take) {
+        const uint32_t pos = wbase + __popc(bal & ((1u << lane) - 1u));
+        if (pos < cap) cand[pos] = key;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) below = max(below, __shfl_xor_sync(FULL, below, o));
+  if (lane == 0) atomicMax(&res[1], below);
+  __syncthreads();
+  return res[0];
+}
+
 // Descending bitonic sort of a[0..len), len a power of two.
 template <typename T>
 __device__ void bitonic_desc(T *a, int len) {
@@ -637,25 +689,27 @@ __device__ void bitonic_desc(T *a, int len) {
 // s-th largest |v| (with multiplicity, as the sorting variant :92-98 defines
 // it), keep |v| >= level, then x <- x / ||x|| (c++/src/gpower/gpower_commons.h:111).
 constexpr int HARD_CAND = 4096;  // candidates resolved in shared memory
+constexpr int HARD_THREADS = 1024;
+// fraction of the previous level used as the gather bound of the hinted search
+constexpr float HINT_FRACTION = 0.9f;
 
 // k_hard_thresholding (c++/src/utils/thresh_functions.h:121-145): level = the
 // s-th largest |v| (with multiplicity, as the sorting variant :92-98 defines
 // it), keep |v| >= level, then x <- x / ||x|| (c++/src/gpower/gpower_commons.h:111).
 //
-// Common case, three passes over the column: (1) histogram of the top 11 bits
-// of |v| finds the bin holding rank s; (2) keys above that bin are kept for
-// sure (their squares are summed on the way), keys in the bin are gathered
-// into shared memory and sorted there to give the exact level and the rest of
-// the norm; (3) the normalised loadings are written.  A bin too full for shared
-// memory falls back to the exact three-level radix select.
+// The column is staged in shared memory by a bulk copy.  Level search:
+// (a) with the previous step's level as a hint, one pass gathers |v| >= hint/2;
+// when that holds s to HARD_CAND values, sorting them gives the exact level
+// and the norm; otherwise (b) a histogram of the top 11 bits of |v| finds the
+// bin holding rank s, keys above it are kept for sure, keys in it are gathered
+// and sorted; a bin too full for shared memory falls back to (c) the exact
+// three-level radix select.  Last, the non-zero loadings and the bitmask are
+// written.
 template <bool CACHED>
-__global__ void __launch_bounds__(512, 1) hard_select_kernel(const float *__restrict__ Vraw,
-                                                             int ldv, int n, unsigned s,
-                                                             float *__restrict__ V_hi,
-                                                             float *__restrict__ V_lo,
-                                                             uint32_t *__restrict__ nnz_out,
-                                                             int *status,
-                                                             uint32_t *__restrict__ vmask) {
+__global__ void __launch_bounds__(HARD_THREADS, 1) hard_select_kernel(
+    const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
+    uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
+    float *__restrict__ hints) {
   extern __shared__ __align__(16) uint8_t dsm[];
   uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
   uint32_t *cand = hist + 2048;
@@ -666,12 +720,39 @@ __global__ void __launch_bounds__(512, 1) hard_select_kernel(const float *__rest
   const int j = blockIdx.x;
   const float *colg = Vraw + (size_t)j * ldv;
   if (CACHED) stage_column(cache, colg, n, bar, status);
+  uint32_t thr = 0;
+  double ss = 0.0, cnt = 0.0;
+  // (a) the previous step's level: as the iterates settle the s-th largest
+  // moves little, so one pass gathering |v| >= HINT_FRACTION * level usually
+  // holds the exact answer (and few enough values to sort cheaply)
+  bool done = false;
+  const float hint = hints[j];
+  if (hint > 0.f) {
+    const uint32_t c = gather_keys_above<CACHED>(colg, cache, n, abs_key(HINT_FRACTION * hint),
+                                                 cand, HARD_CAND, res);
+    if (c >= s && c <= (uint32_t)HARD_CAND) {
+      int len = 1;
+      while (len < (int)c) len <<= 1;
+      for (int q = c + threadIdx.x; q < len; q += blockDim.x) cand[q] = 0u;
+      __syncthreads();
+      bitonic_desc(cand, len);
+      thr = cand[s - 1];
+      for (int q = threadIdx.x; q < (int)c; q += blockDim.x)
+        if (cand[q] >= thr) {
+          const double v = (double)__uint_as_float(cand[q]);
+          ss += v * v;
+          cnt += 1.0;
+        }
+      done = true;
+    }
+    __syncthreads();
+  }
+  // (b) histogram of the top 11 key bits, then the bin holding rank s
+  if (!done) {
   key_histogram<CACHED>(colg, cache, n, hist);
   find_rank_bin(hist, 2048, s, res);
   const uint32_t b1 = res[0], above = res[1], in_bin = res[2];
   __syncthreads();
-  uint32_t thr;
-  double ss = 0.0, cnt = 0.0;
   if (in_bin <= (uint32_t)HARD_CAND) {
     if (threadIdx.x == 0) res[3] = 0;
     __syncthreads();
@@ -710,17 +791,17 @@ __global__ void __launch_bounds__(512, 1) hard_select_kernel(const float *__rest
       }
     }
   }
+  }
+  if (threadIdx.x == 0) hints[j] = __uint_as_float(thr);
   ss = block_sum(ss, red);
   cnt = block_sum(cnt, red);
   const float inv = 1.0f / (float)sqrt(ss);
-  float *vh = V_hi + (size_t)j * ldv;
-  float *vl = V_lo + (size_t)j * ldv;
+  float *vx = Vx + (size_t)j * ldv;
   uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
   if (CACHED) {
-    write_column(cache, n, vh, vl, mk,
-                 [=](float v) { return (abs_key(v) >= thr) ? v * inv : 0.f; });
+    write_column(cache, n, vx, mk, [=](float v) { return (abs_key(v) >= thr) ? v * inv : 0.f; });
   } else {
-    write_column_global(colg, n, vh, vl, mk,
+    write_column_global(colg, n, vx, mk,
                         [=](float v) { return (abs_key(v) >= thr) ? v * inv : 0.f; });
   }
   if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
@@ -926,9 +1007,9 @@ __device__ uint32_t resolve_stop(uint32_t best, double bw, uint32_t *res,
 // L1-ball / unit-sphere projection.
 template <bool CACHED, bool EXACT>
 __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
-    const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ V_hi,
-    float *__restrict__ V_lo, uint32_t *__restrict__ nnz_out, int *status,
-    uint32_t *__restrict__ vmask) {
+    const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
+    uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
+    float *__restrict__ hints) {
   extern __shared__ __align__(16) uint8_t dsm[];
   uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
   uint32_t *res = hist + 2048;
@@ -949,18 +1030,65 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
   const double sq2 = __dmul_rn(sq, sq);
   const uint32_t NONE = 0xFFFFFFFFu;
 
-  // ---- fast path: the highest bins holding at most SOFT_C values
-  key_histogram<CACHED>(colg, cache, n, hist);
-  find_rank_bin(hist, 2048, (uint32_t)SOFT_C + 1u, res);
-  const bool whole = (uint32_t)n <= (uint32_t)SOFT_C;
-  const uint32_t bstar = whole ? 0u : res[0] + 1u;  // gather bins >= bstar
-  const uint32_t c = whole ? (uint32_t)n : res[1];
-  __syncthreads();
   double w = 0.0;
   uint32_t brk = NONE;
   bool have_norm = false;
   double ss = 0.0, cnt = 0.0;
-  if (c > 0) {
+  // ---- hinted path: gather |v| >= HINT_FRACTION * (previous step's level)
+  const float hint = hints[j];
+  if (hint > 0.f) {
+    const uint32_t c = gather_keys_above<CACHED>(colg, cache, n, abs_key(HINT_FRACTION * hint),
+                                                 reinterpret_cast<uint32_t *>(cand), SOFT_C, res);
+    const uint32_t below_key = res[1];
+    __syncthreads();
+    if (c > 0 && c <= (uint32_t)SOFT_C) {
+      int len = 1;
+      while (len < (int)c) len <<= 1;
+      for (uint32_t q = c + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
+      __syncthreads();
+      const double lo_after = (c == (uint32_t)n) ? 0.0 : (double)__uint_as_float(below_key);
+      bitonic_desc(cand, len);
+      block_scan2(cand, (int)c, 0.0, 0.0, p1, p2, red);
+      const double lim = __dsub_rn((double)cand[0], 0.000001);  // ||v||_inf - 1e-6
+      uint32_t best = NONE;
+      double bw = 0.0, w_last = 0.0;
+      eval_chunk<EXACT>(cand, p1, p2, c, c, 0, (uint32_t)n, 0.0, 0.0, lo_after, sq, sq2, lim,
+                        best, bw, w_last);
+      brk = resolve_stop(best, bw, res, misc, w_sh, &w);
+      if (brk == NONE && c == (uint32_t)n) {
+        if (!EXACT && threadIdx.x == (c - 1) % blockDim.x) *w_sh = w_last;
+        if (EXACT && threadIdx.x == 0) *w_sh = 0.0;
+        __syncthreads();
+        w = *w_sh;
+        brk = (uint32_t)n;
+        __syncthreads();
+      }
+      if (brk != NONE) {
+        for (uint32_t q = threadIdx.x; q < c; q += blockDim.x) {
+          const double d = (double)cand[q] - w;
+          if (d > 0.0) {
+            const double x = (double)(float)d;
+            ss += x * x;
+            cnt += 1.0;
+          }
+        }
+        have_norm = true;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- fast path: the highest bins holding at most SOFT_C values
+  uint32_t c = 0, bstar = 0;
+  if (brk == NONE) {
+    key_histogram<CACHED>(colg, cache, n, hist);
+    find_rank_bin(hist, 2048, (uint32_t)SOFT_C + 1u, res);
+    const bool whole = (uint32_t)n <= (uint32_t)SOFT_C;
+    bstar = whole ? 0u : res[0] + 1u;  // gather bins >= bstar
+    c = whole ? (uint32_t)n : res[1];
+    __syncthreads();
+  }
+  if (brk == NONE && c > 0) {
     if (threadIdx.x == 0) {
       misc[0] = 0;
       misc[2] = 0;
@@ -1068,6 +1196,7 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
     }
   }
 
+  if (threadIdx.x == 0) hints[j] = (float)w;
   // x = sgn(v)(|v| - w)_+ with w kept in double: a level that lands within
   // rounding of the largest |v| still leaves that entry non-zero, as in the
   // reference's double arithmetic.
@@ -1085,17 +1214,16 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
   ss = block_sum(ss, red);
   cnt = block_sum(cnt, red);
   const float inv = 1.0f / (float)sqrt(ss);
-  float *vh = V_hi + (size_t)j * ldv;
-  float *vl = V_lo + (size_t)j * ldv;
+  float *vx = Vx + (size_t)j * ldv;
   auto soft = [=](float v) {
     const double d = (double)fabsf(v) - w;
     return ((d > 0.0) ? (float)d * sgnf(v) : 0.f) * inv;
   };
   uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
   if (CACHED) {
-    write_column(cache, n, vh, vl, mk, soft);
+    write_column(cache, n, vx, mk, soft);
   } else {
-    write_column_global(colg, n, vh, vl, mk, soft);
+    write_column_global(colg, n, vx, mk, soft);
   }
   if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
 }
@@ -1166,18 +1294,14 @@ __global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs a) {
   }
 }
 
-// x = v / ||v|| with v = hi + lo (c++/src/gpower/sparse_PCA_solver.h:236-237).
-__global__ void finalize_x_kernel(const float *__restrict__ h, const float *__restrict__ l, int n,
-                                  float *__restrict__ x) {
+// x = v / ||v|| (c++/src/gpower/sparse_PCA_solver.h:236-237).
+__global__ void finalize_x_kernel(const float *__restrict__ v, int n, float *__restrict__ x) {
   __shared__ double red[32];
   double ss = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float v = h[i] + l[i];
-    ss += (double)v * (double)v;
-  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) ss += (double)v[i] * (double)v[i];
   ss = block_sum(ss, red);
   const float inv = 1.0f / (float)sqrt(ss);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (h[i] + l[i]) * inv;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = v[i] * inv;
 }
 
 // y_r = sum_c B[r, c] x_c in FP64, one warp per sample row of Bt (hi + lo = B exactly).
@@ -1208,12 +1332,12 @@ struct GemmCfg {
   int bn, stages;
 };
 
-template <int BN, int ST, class Epi>
+template <int BN, int BKT, int ST, class Epi>
 cudaError_t run_gemm(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
                      const CUtensorMap &b_lo, const GemmShape &sh, const Epi &epi,
                      cudaStream_t st) {
-  using L = GemmSmem<BN, BK, ST>;
-  auto kern = gemm_tf32x3_kernel<BN, BK, ST, GEMM_PROMO, Epi>;
+  using L = GemmSmem<BN, BKT, ST>;
+  auto kern = gemm_tf32x3_kernel<BN, BKT, ST, GEMM_PROMO_K / BKT, Epi>;
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
@@ -1225,32 +1349,41 @@ cudaError_t run_gemm(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUt
   return cudaGetLastError();
 }
 
+// Stages per (N tile, K slab) fill ~192 KB of shared memory.
 template <class Epi>
-cudaError_t dispatch_gemm(int bn, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
+cudaError_t dispatch_gemm(int bn, int bk, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
                           const CUtensorMap &b_hi, const CUtensorMap &b_lo, const GemmShape &sh,
                           const Epi &epi, cudaStream_t st) {
-  switch (bn) {
-    case 256: return run_gemm<256, 2>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
-    case 128: return run_gemm<128, 3>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
-    case 64: return run_gemm<64, 4>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
-    default: return cudaErrorInvalidValue;
+  if (bk == 32) {
+    switch (bn) {
+      case 256: return run_gemm<256, 32, 2>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+      case 128: return run_gemm<128, 32, 3>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+      case 64: return run_gemm<64, 32, 4>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+    }
+  } else if (bk == 16) {
+    switch (bn) {
+      case 256: return run_gemm<256, 16, 4>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+      case 128: return run_gemm<128, 16, 6>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+      case 64: return run_gemm<64, 16, 8>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+    }
   }
+  return cudaErrorInvalidValue;
 }
 
 template <class F1, class F2>
 cudaError_t launch_select(bool cached, size_t smem_fixed, int n, int grid, int threads, F1 kc, F2 kg,
-                          cudaStream_t st, const float *Vraw, int ld, unsigned s, float *vh,
-                          float *vl, uint32_t *nnz, int *status, uint32_t *vmask) {
+                          cudaStream_t st, const float *Vraw, int ld, unsigned s, float *vx,
+                          uint32_t *nnz, int *status, uint32_t *vmask, float *hints) {
   if (cached) {
     const size_t smem = smem_fixed + ((size_t)n * 4 + 15) / 16 * 16;
     cudaError_t e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kc<<<grid, threads, smem, st>>>(Vraw, ld, n, s, vh, vl, nnz, status, vmask);
+    kc<<<grid, threads, smem, st>>>(Vraw, ld, n, s, vx, nnz, status, vmask, hints);
   } else {
     cudaError_t e =
         cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fixed);
     if (e != cudaSuccess) return e;
-    kg<<<grid, threads, smem_fixed, st>>>(Vraw, ld, n, s, vh, vl, nnz, status, vmask);
+    kg<<<grid, threads, smem_fixed, st>>>(Vraw, ld, n, s, vx, nnz, status, vmask, hints);
   }
   return cudaGetLastError();
 }
@@ -1278,7 +1411,7 @@ size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn) {
 }
 
 cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st) {
-  prep_copy_kernel<<<M.n, 256, 0, st>>>(B, ldB, M.m, M.Bc_hi, M.Bc_lo, M.ldm);
+  prep_copy_kernel<<<M.n, 256, 0, st>>>(B, ldB, M.m, M.Bc_hi, M.Bc_lo, M.Bc, M.ldm);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   dim3 grid((M.n + 31) / 32, (M.m + 31) / 32);
@@ -1286,22 +1419,22 @@ cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream
   return cudaGetLastError();
 }
 
-cudaError_t launch_split_columns(const float *src, int ld_src, int rows, int cols, float *hi,
-                                 float *lo, int ld_dst, cudaStream_t st, uint32_t *mask) {
+cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols, float *dst,
+                                int ld_dst, uint32_t *mask, cudaStream_t st) {
   if (cols <= 0) return cudaSuccess;
-  split_columns_kernel<<<cols, 256, 0, st>>>(src, ld_src, rows, hi, lo, ld_dst, mask);
+  load_columns_kernel<<<cols, 256, 0, st>>>(src, ld_src, rows, dst, ld_dst, mask);
   return cudaGetLastError();
 }
 
-cudaError_t launch_combine_columns(const float *hi, const float *lo, int ld, int rows, int cols,
-                                   float *dst, int ld_dst, cudaStream_t st) {
+cudaError_t launch_masked_copy(const float *Vx, const uint32_t *mask, int ld, int rows, int cols,
+                               float *dst, int ld_dst, cudaStream_t st) {
   if (cols <= 0) return cudaSuccess;
-  combine_columns_kernel<<<cols, 256, 0, st>>>(hi, lo, ld, rows, dst, ld_dst);
+  masked_copy_kernel<<<cols, 256, 0, st>>>(Vx, mask, ld, rows, dst, ld_dst);
   return cudaGetLastError();
 }
 
-cudaError_t launch_finalize_x(const float *hi, const float *lo, int n, float *x, cudaStream_t st) {
-  finalize_x_kernel<<<1, 1024, 0, st>>>(hi, lo, n, x);
+cudaError_t launch_finalize_x(const float *v, int n, float *x, cudaStream_t st) {
+  finalize_x_kernel<<<1, 1024, 0, st>>>(v, n, x);
   return cudaGetLastError();
 }
 
@@ -1334,7 +1467,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g1.K = M.n;
   g1.m_tiles = b.m_tiles1;
   g1.n_tiles = b.n_tiles1;
-  g1.kb_total = (M.n + BK - 1) / BK;
+  g1.kb_total = (M.n + b.bk - 1) / b.bk;
   g1.kb_per_split = b.kbps1;
   g1.splits = b.splits1;
   g1.num_units = g1.splits * g1.m_tiles * g1.n_tiles;
@@ -1346,23 +1479,28 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   // 1a. sparse V (every column <= sparse_cap non-zeros last step): gather
   if ((e = mark(5)) != cudaSuccess) return e;
   if (mode == 0)
-    gather_bv_kernel<0><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc_hi, M.Bc_lo, M.ldm, M.m, M.ldn,
-                                                        b.V_hi, b.V_lo, b.vmask, b.Z_hi, b.Z_lo,
-                                                        b.fz, b.max_nnz, b.sparse_cap);
+    gather_bv_kernel<0><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
+                                                        b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
+                                                        b.max_nnz, b.sparse_cap);
   else if (mode == 1)
-    gather_bv_kernel<1><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc_hi, M.Bc_lo, M.ldm, M.m, M.ldn,
-                                                        b.V_hi, b.V_lo, b.vmask, b.Z_hi, b.Z_lo,
-                                                        b.fz, b.max_nnz, b.sparse_cap);
+    gather_bv_kernel<1><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
+                                                        b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
+                                                        b.max_nnz, b.sparse_cap);
   else
-    gather_bv_kernel<2><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc_hi, M.Bc_lo, M.ldm, M.m, M.ldn,
-                                                        b.V_hi, b.V_lo, b.vmask, b.Z_hi, b.Z_lo,
-                                                        b.fz, b.max_nnz, b.sparse_cap);
+    gather_bv_kernel<2><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
+                                                        b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
+                                                        b.max_nnz, b.sparse_cap);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
-  // 1b. dense V: tensor-core Z = B V (split-K partials) ...
-  EpiPartial ep{b.ws, b.bn1};
+  // 1b. dense V: TF32 hi/lo planes, tensor-core Z = B V (split-K partials) ...
+  if ((e = mark(6)) != cudaSuccess) return e;
+  densify_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_hi, b.V_lo, b.max_nnz,
+                                      b.sparse_cap);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  nl++;
+  EpiPartial ep{b.ws, b.bn1, b.m_tiles1, b.n_tiles1};
   if ((e = mark(0)) != cudaSuccess) return e;
-  e = dispatch_gemm(b.bn1, tm.a1_hi, tm.a1_lo, tm.b1_hi, tm.b1_lo, g1, ep, st);
+  e = dispatch_gemm(b.bn1, b.bk, tm.a1_hi, tm.a1_lo, tm.b1_hi, tm.b1_lo, g1, ep, st);
   if (e != cudaSuccess) return e;
   nl++;
   // 2. ... then reduce + sign / normalise
@@ -1385,7 +1523,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g2.K = M.m;
   g2.m_tiles = b.m_tiles2;
   g2.n_tiles = b.n_tiles2;
-  g2.kb_total = (M.m + BK - 1) / BK;
+  g2.kb_total = (M.m + b.bk - 1) / b.bk;
   g2.kb_per_split = g2.kb_total;
   g2.splits = 1;
   g2.num_units = g2.m_tiles * g2.n_tiles;
@@ -1397,15 +1535,15 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if ((e = mark(2)) != cudaSuccess) return e;
   if (is_constrained(f)) {
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
-    e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, er, st);
+    e = dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, er, st);
   } else if (is_l1_penalized(f)) {
-    EpiPenalty<true> pe{b.V_hi, b.V_lo, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
-                        p.penalty, b.vmask};
-    e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
+    EpiPenalty<true> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts, p.penalty,
+                        b.vmask};
+    e = dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
   } else {
-    EpiPenalty<false> pe{b.V_hi, b.V_lo, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
+    EpiPenalty<false> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
                          p.penalty, b.vmask};
-    e = dispatch_gemm(b.bn2, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
+    e = dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
   }
   if (e != cudaSuccess) return e;
   nl++;
@@ -1414,19 +1552,19 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     if ((e = mark(3)) != cudaSuccess) return e;
     if (!is_l1_constrained(f)) {
       const bool cached = HARD_FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
-      e = launch_select(cached, HARD_FIXED, M.n, b.k, 512, hard_select_kernel<true>,
-                        hard_select_kernel<false>, st, b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo,
-                        b.nnz, b.status, b.vmask);
+      e = launch_select(cached, HARD_FIXED, M.n, b.k, HARD_THREADS, hard_select_kernel<true>,
+                        hard_select_kernel<false>, st, b.Vraw, M.ldn, p.constraint, b.Vx, b.nnz,
+                        b.status, b.vmask, b.sel_hint);
     } else {
       const bool cached = SoftSmem::FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
       if (p.l1_mode == 0)
         e = launch_select(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
                           soft_select_kernel<true, false>, soft_select_kernel<false, false>, st,
-                          b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz, b.status, b.vmask);
+                          b.Vraw, M.ldn, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint);
       else
         e = launch_select(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
                           soft_select_kernel<true, true>, soft_select_kernel<false, true>, st,
-                          b.Vraw, M.ldn, p.constraint, b.V_hi, b.V_lo, b.nnz, b.status, b.vmask);
+                          b.Vraw, M.ldn, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint);
     }
     if (e != cudaSuccess) return e;
     nl++;

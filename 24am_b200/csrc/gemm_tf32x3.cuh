@@ -61,8 +61,12 @@ struct GemmShape {
   uint32_t gate_max;
 };
 
+// One work unit as an epilogue sees it: rows [m0, m0 + 128) of C (this CTA's
+// accumulator lanes), columns [nt * BN, nt * BN + BN), K blocks [kb0, kb1) of
+// split `split`.
 struct Unit {
   int mt, nt, split, kb0, kb1, index;
+  int m0;
 };
 
 __device__ __forceinline__ Unit decode_unit(const GemmShape &s, int u) {
@@ -75,6 +79,7 @@ __device__ __forceinline__ Unit decode_unit(const GemmShape &s, int u) {
   r.kb0 = r.split * s.kb_per_split;
   r.kb1 = min(s.kb_total, r.kb0 + s.kb_per_split);
   r.index = u;
+  r.m0 = r.mt * GEMM_BM;
   return r;
 }
 

@@ -193,14 +193,15 @@ typedef enum {
   AM24_KERNEL_SELECT = 3,    /* top-s select or L1-ball level, normalise (constrained) */
   AM24_KERNEL_FINALIZE = 4,  /* per-start objective, change, logs, batch maximum */
   AM24_KERNEL_GATHER_BV = 5, /* Z = B V as a gather over V's non-zeros (sparse steps) */
+  AM24_KERNEL_DENSIFY = 6,   /* dense TF32 hi/lo planes of V for the tensor-core Z = B V */
   AM24_KERNEL_SKIPPED = 0x100 /* or-ed into a kind: the launch returned at once */
 } am24_kernel_kind;
 /* One AM step like am24_batch_iterate(h, b, it, 1, NULL), with a CUDA event
  * recorded on the handle's stream before and after every kernel.  Synchronizes,
  * then writes each launch's duration (ms) to ms[i] and its am24_kernel_kind to
- * kinds[i] (both with room for 8) and the number of launches to *count.  Z = B V
- * has two kernels per step (gather and tensor-core GEMM + reduction); the one
- * the step does not need returns at once. */
+ * kinds[i] (both with room for 16) and the number of launches to *count.  Z = B V
+ * has two paths per step (gather; or densify + tensor-core GEMM + reduction);
+ * the kernels of the path the step does not need return at once. */
 am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float *ms,
                                   int32_t *kinds, int32_t *count);
 
