@@ -100,6 +100,8 @@ _SIGS = {
     "am24_batch_destroy": (C.c_int, [_VP, _VP]),
     "am24_batch_load": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
     "am24_batch_iterate": (C.c_int, [_VP, _VP, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
+    "am24_batch_iterate_static_ws": (C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
+                                               C.POINTER(C.c_float)]),
     "am24_batch_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "am24_batch_launches_per_step": (C.c_int, [_VP, _VP, C.POINTER(C.c_int32)]),
     "am24_sync": (C.c_int, [_VP]),
@@ -393,6 +395,15 @@ class Batch:
         me = C.c_float()
         check(lib().am24_batch_iterate(self.matrix.solver.h, self.bh, int(it0), int(iterations),
                                        C.byref(me) if sync else None))
+        return me.value if sync else None
+
+    def iterate_static_ws(self, it0=0, iterations=1, sync=True):
+        """iterate() with the split-K workspace in the library's static device
+        array (am24_batch_iterate_static_ws)."""
+        me = C.c_float()
+        check(lib().am24_batch_iterate_static_ws(self.matrix.solver.h, self.bh, int(it0),
+                                                 int(iterations),
+                                                 C.byref(me) if sync else None))
         return me.value if sync else None
 
     def read(self):

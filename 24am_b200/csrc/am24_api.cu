@@ -12,7 +12,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -860,6 +862,75 @@ am24_status am24_solve_device_f32(am24_handle h, const float *d_B, int32_t ldB, 
     stats->total_elapsed_time =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return st;
+}
+
+}  // extern "C"
+
+// ---- split-K workspace in a file-scope device array ------------------------
+// am24_batch_iterate_static_ws runs the step of am24_batch_iterate with the
+// split-K partial tiles of the dense Z = B V product in this array instead of
+// the batch's own workspace.  Nothing in it has to start at zero: the GEMM of a
+// step writes every slot that the step's reduction then reads.  Calls that
+// overlap in time on one device (any handles, any threads) share the array
+// and race.
+static __device__ __align__(256) float am24_static_ws[AM24_STATIC_WS_BYTES / sizeof(float)];
+
+namespace {
+
+std::mutex g_static_ws_mu;
+std::unordered_map<int, float *> g_static_ws_ptr;  // device -> address of am24_static_ws
+
+// Address of am24_static_ws on `device`, looked up once per device with that
+// device current.
+am24_status static_ws_address(int device, float **out) {
+  std::lock_guard<std::mutex> lock(g_static_ws_mu);
+  auto it = g_static_ws_ptr.find(device);
+  if (it != g_static_ws_ptr.end()) {
+    *out = it->second;
+    return AM24_OK;
+  }
+  AM24_CUDA(cudaSetDevice(device));
+  float *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, am24_static_ws);
+  if (e != cudaSuccess || ptr == nullptr)
+    return fail(AM24_ERR_CUDA, std::string("cudaGetSymbolAddress(am24_static_ws): ") +
+                                   cudaGetErrorString(e));
+  g_static_ws_ptr[device] = ptr;
+  *out = ptr;
+  return AM24_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+am24_status am24_batch_iterate_static_ws(am24_handle h, am24_batch b, int32_t it0,
+                                         int32_t iterations, float *max_error) {
+  if (!h || !b) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  const size_t need =
+      ws_floats(b->d.splits1, b->d.m_tiles1, b->d.n_tiles1, b->d.bn1) * sizeof(float);
+  if (need > AM24_STATIC_WS_BYTES)
+    return fail(AM24_ERR_INVALID_ARG,
+                "split-K workspace of " + std::to_string(need) +
+                    " bytes exceeds the static workspace of " +
+                    std::to_string((size_t)AM24_STATIC_WS_BYTES) +
+                    " bytes; use am24_batch_iterate");
+  float *ws = nullptr;
+  AM24_TRY(static_ws_address(h->device, &ws));
+  AM24_CUDA(cudaSetDevice(h->device));
+  BatchDev d = b->d;
+  d.ws = ws;
+  for (int i = 0; i < iterations; i++) {
+    const StepParams p = step_params(b->s, it0 + i, 0);
+    AM24_CUDA(launch_am_step(b->mat->d, d, b->tm, p, h->stream, &b->launches));
+  }
+  if (max_error) {
+    AM24_CUDA(cudaMemcpyAsync(max_error, d.max_err, sizeof(float), cudaMemcpyDeviceToHost,
+                              h->stream));
+    AM24_CUDA(cudaStreamSynchronize(h->stream));
+    AM24_TRY(check_device_status(b));
+  }
+  return AM24_OK;
 }
 
 }  // extern "C"

@@ -177,6 +177,19 @@ am24_status am24_batch_iterate(am24_handle h, am24_batch b, int32_t it0, int32_t
  * number of non-zero loadings nnz. */
 am24_status am24_batch_read(am24_handle h, am24_batch b, float *V, float *val, float *err,
                             uint32_t *nnz);
+/* No counterpart in the reference.  The step of am24_batch_iterate, with the
+ * split-K partial sums of the dense Z = B V product kept in a file-scope device
+ * array of AM24_STATIC_WS_BYTES inside the library instead of the batch's own
+ * workspace; the call allocates no memory.  Batches whose workspace is larger
+ * (splits x ceil(m/128) x ceil(batch_size/bn) x bn x 128 floats, bn the GEMM
+ * N tile) are rejected with AM24_ERR_INVALID_ARG.  The array needs no
+ * initial contents.  There is one array per device: calls that overlap in time
+ * on one device, from any handle or thread, race on it.  The first call on a
+ * device looks up the array's address (set-up); make it before any stream
+ * capture. */
+#define AM24_STATIC_WS_BYTES (16u << 20)
+am24_status am24_batch_iterate_static_ws(am24_handle h, am24_batch b, int32_t it0,
+                                         int32_t iterations, float *max_error);
 /* Number of kernel launches one am24_batch_iterate step issues. */
 am24_status am24_batch_launches_per_step(am24_handle h, am24_batch b, int32_t *launches);
 /* Synchronizes the handle's stream. */
