@@ -441,6 +441,9 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   d.n_tiles2 = (k + d.bn2 - 1) / d.bn2;
   d.bk = BK_DEFAULT;
   if (const char *e = getenv("AM24_GEMM_BK")) d.bk = (atoi(e) == 16) ? 16 : 32;
+  // V = B^T Z on CTA pairs when its N tile is 256 (AM24_GEMM_PAIR=0 turns it off)
+  d.pair2 = d.bn2 == 256;
+  if (const char *e = getenv("AM24_GEMM_PAIR")) d.pair2 = d.pair2 && atoi(e) != 0;
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;
   choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
   const int parts = d.m_tiles2 * 4;
@@ -488,8 +491,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = make_map(h, &b->tm.b1_lo, d.V_lo, M.n, k, M.ldn, d.bn1, d.bk)) ||
       (st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM, d.bk)) ||
       (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM, d.bk)) ||
-      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.bn2, d.bk)) ||
-      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.bn2, d.bk))) {
+      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, d.bk)) ||
+      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, d.bk))) {
     delete b;
     return st;
   }

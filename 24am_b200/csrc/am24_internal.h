@@ -37,6 +37,7 @@ struct BatchDev {
   int splits1;    // split-K factor of Z = B V
   int kbps1;      // K blocks per split of Z = B V
   int m_tiles1, n_tiles1, m_tiles2, n_tiles2;
+  int pair2;      // V = B^T Z runs on CTA pairs (256-row tiles; B maps of bn2/2 rows)
   float *Vx;            // k x ldn loadings; entry i of a column is defined only
                         // where its vmask bit is set (zero elsewhere)
   float *V_hi, *V_lo;   // k x ldn dense TF32 hi/lo planes of V: the B operand of the

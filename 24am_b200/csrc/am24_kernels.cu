@@ -22,6 +22,7 @@
 
 #include "am24_internal.h"
 #include "gemm_tf32x3.cuh"
+#include "gemm_tf32x3_pair.cuh"
 
 namespace am24 {
 
@@ -1350,6 +1351,48 @@ cudaError_t run_gemm(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUt
 }
 
 // Stages per (N tile, K slab) fill ~192 KB of shared memory.
+// Co-resident clusters of two CTAs for a pair kernel (queried once per kernel).
+template <class K>
+cudaError_t pair_clusters(K kern, int smem, int *out) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * num_sms());
+  cfg.blockDim = dim3(GEMM_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  int n = 0;
+  cudaError_t e = cudaOccupancyMaxActiveClusters(&n, (void *)kern, &cfg);
+  if (e != cudaSuccess) return e;
+  if (n < 1) return cudaErrorInvalidConfiguration;
+  *out = n;
+  return cudaSuccess;
+}
+
+template <int BN, int BKT, int ST, class Epi>
+cudaError_t run_gemm_pair(const CUtensorMap &a_hi, const CUtensorMap &a_lo,
+                          const CUtensorMap &b_hi, const CUtensorMap &b_lo, const GemmShape &sh,
+                          const Epi &epi, cudaStream_t st) {
+  using L = PairSmem<BN, BKT, ST>;
+  auto kern = gemm_tf32x3_pair_kernel<BN, BKT, ST, GEMM_PROMO_K / BKT, Epi>;
+  static int clusters = 0;
+  if (clusters == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
+    if (e != cudaSuccess) return e;
+    if ((e = pair_clusters(kern, L::TOTAL, &clusters)) != cudaSuccess) return e;
+  }
+  const int pairs = sh.num_units < clusters ? sh.num_units : clusters;
+  kern<<<2 * pairs, GEMM_THREADS, L::TOTAL, st>>>(a_hi, a_lo, b_hi, b_lo, sh, epi);
+  return cudaGetLastError();
+}
+
+// V = B^T Z on CTA pairs (N tile 256).  sh.num_units counts pair tiles.
+template <class Epi>
+cudaError_t dispatch_gemm_pair(int bk, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
+                               const CUtensorMap &b_hi, const CUtensorMap &b_lo,
+                               const GemmShape &sh, const Epi &epi, cudaStream_t st) {
+  if (bk == 32) return run_gemm_pair<256, 32, 3>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+  if (bk == 16) return run_gemm_pair<256, 16, 6>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
+  return cudaErrorInvalidValue;
+}
+
 template <class Epi>
 cudaError_t dispatch_gemm(int bn, int bk, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
                           const CUtensorMap &b_hi, const CUtensorMap &b_lo, const GemmShape &sh,
@@ -1368,6 +1411,17 @@ cudaError_t dispatch_gemm(int bn, int bk, const CUtensorMap &a_hi, const CUtenso
     }
   }
   return cudaErrorInvalidValue;
+}
+
+template <class Epi>
+cudaError_t dispatch_gemm2(const BatchDev &b, const TensorMaps &tm, const GemmShape &sh,
+                           const Epi &epi, cudaStream_t st) {
+  if (b.pair2) {
+    GemmShape s2 = sh;
+    s2.num_units = s2.splits * ((s2.m_tiles + 1) / 2) * s2.n_tiles;
+    return dispatch_gemm_pair(b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, s2, epi, st);
+  }
+  return dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, sh, epi, st);
 }
 
 template <class F1, class F2>
@@ -1535,15 +1589,15 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if ((e = mark(2)) != cudaSuccess) return e;
   if (is_constrained(f)) {
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
-    e = dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, er, st);
+    e = dispatch_gemm2(b, tm, g2, er, st);
   } else if (is_l1_penalized(f)) {
     EpiPenalty<true> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts, p.penalty,
                         b.vmask};
-    e = dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
+    e = dispatch_gemm2(b, tm, g2, pe, st);
   } else {
     EpiPenalty<false> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
                          p.penalty, b.vmask};
-    e = dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, g2, pe, st);
+    e = dispatch_gemm2(b, tm, g2, pe, st);
   }
   if (e != cudaSuccess) return e;
   nl++;
