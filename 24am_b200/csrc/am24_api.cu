@@ -119,6 +119,42 @@ am24_status make_map(am24_handle h, CUtensorMap *map, const float *base, int K, 
   return AM24_OK;
 }
 
+// K-major BF16 operand [rows][ld] (ld in elements), loaded as 32 x box_rows
+// tiles (64-byte rows, 64-byte swizzle), as the BF16 pair GEMM reads them.
+am24_status make_map_bf16(am24_handle h, CUtensorMap *map, const uint16_t *base, int K, int rows,
+                          int ld, int box_rows) {
+  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(uint16_t)};
+  cuuint32_t box[2] = {(cuuint32_t)PAIR_BK_BF16, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = h->encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t *>(base),
+                         dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return fail(AM24_ERR_CUDA, "cuTensorMapEncodeTiled (BF16) failed with code " +
+                                   std::to_string((int)r));
+  return AM24_OK;
+}
+
+// The matrix's three BF16 planes of B (made once, on first use).
+am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat) {
+  MatrixDev &M = mat->d;
+  if (M.Bc_b3) return AM24_OK;
+  const size_t plane = (size_t)M.n * M.ldm;
+  uint16_t *p = nullptr;
+  AM24_TRY(mat->mem.get(&p, 3 * plane));
+  AM24_CUDA(cudaMemsetAsync(p, 0, sizeof(uint16_t) * 3 * plane, h->stream));
+  M.Bc_b3 = p;
+  cudaError_t e = launch_prep_bf16x3(M, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    M.Bc_b3 = nullptr;
+    return fail(AM24_ERR_CUDA, std::string("BF16 planes: ") + cudaGetErrorString(e));
+  }
+  return AM24_OK;
+}
+
 // Split-K factor for Z = B V: minimise rounds * (K blocks per unit + fixed
 // per-unit cost) over the persistent grid.
 void choose_splits(int tiles, int kb_total, int sms, int *splits, int *kbps) {
@@ -441,9 +477,14 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   d.n_tiles2 = (k + d.bn2 - 1) / d.bn2;
   d.bk = BK_DEFAULT;
   if (const char *e = getenv("AM24_GEMM_BK")) d.bk = (atoi(e) == 16) ? 16 : 32;
-  // V = B^T Z on CTA pairs when its N tile is 256 (AM24_GEMM_PAIR=0 turns it off)
+  // V = B^T Z on CTA pairs when its N tile is 256 (AM24_GEMM_PAIR=0 turns it off),
+  // with exact BF16 operands for the L1-variance forms (AM24_GEMM_BF16=0 turns
+  // that off)
   d.pair2 = d.bn2 == 256;
   if (const char *e = getenv("AM24_GEMM_PAIR")) d.pair2 = d.pair2 && atoi(e) != 0;
+  d.bf16_2 = d.pair2 && is_l1_variance(settings->formulation);
+  if (const char *e = getenv("AM24_GEMM_BF16")) d.bf16_2 = d.bf16_2 && atoi(e) != 0;
+  const int bk2 = d.pair2 ? PAIR_BK_TF32 : d.bk;  // K box of the TF32 maps of V = B^T Z
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;
   choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
   const int parts = d.m_tiles2 * 4;
@@ -460,7 +501,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.val, k)) || (st = A.get(&d.err, k)) || (st = A.get(&d.max_err, 1)) ||
       (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
       (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||
-      (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.sel_hint, k))) {
+      (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.sel_hint, k)) ||
+      (d.bf16_2 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat))))) {
     delete b;
     return st;
   }
@@ -478,6 +520,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.vmask, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
   if (!e) e = cudaMemsetAsync(d.max_nnz, 0xFF, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.sel_hint, 0, sizeof(float) * k, h->stream);
+  if (!e && d.Z_b) e = cudaMemsetAsync(d.Z_b, 0, sizeof(uint16_t) * kz, h->stream);
   if (!e) e = cudaMemsetAsync(d.iters, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaMemsetAsync(d.cards, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaStreamSynchronize(h->stream);
@@ -489,12 +532,22 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = make_map(h, &b->tm.a1_lo, M.Bt_lo, M.n, M.m, M.ldn, BM, d.bk)) ||
       (st = make_map(h, &b->tm.b1_hi, d.V_hi, M.n, k, M.ldn, d.bn1, d.bk)) ||
       (st = make_map(h, &b->tm.b1_lo, d.V_lo, M.n, k, M.ldn, d.bn1, d.bk)) ||
-      (st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM, d.bk)) ||
-      (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM, d.bk)) ||
-      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, d.bk)) ||
-      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, d.bk))) {
+      (st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM, bk2)) ||
+      (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM, bk2)) ||
+      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, bk2)) ||
+      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, bk2))) {
     delete b;
     return st;
+  }
+  if (d.bf16_2) {
+    const size_t plane = (size_t)M.n * M.ldm;
+    if ((st = make_map_bf16(h, &b->tm.a2_b0, M.Bc_b3, M.m, M.n, M.ldm, BM)) ||
+        (st = make_map_bf16(h, &b->tm.a2_b1, M.Bc_b3 + plane, M.m, M.n, M.ldm, BM)) ||
+        (st = make_map_bf16(h, &b->tm.a2_b2, M.Bc_b3 + 2 * plane, M.m, M.n, M.ldm, BM)) ||
+        (st = make_map_bf16(h, &b->tm.b2_b, d.Z_b, M.m, k, M.ldm, d.bn2 / 2))) {
+      delete b;
+      return st;
+    }
   }
   // a gather over V's non-zeros beats the dense product while they are few
   d.sparse_cap = (uint32_t)std::min(4096, M.n / 32);

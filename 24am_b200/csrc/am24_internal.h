@@ -12,6 +12,8 @@ constexpr int BM = 128;
 // K slab per pipeline stage: 32 (128-byte rows, 128B swizzle, fewer deeper
 // stages) or 16 (64-byte rows, 64B swizzle, twice the stages).
 constexpr int BK_DEFAULT = 16;
+constexpr int PAIR_BK_TF32 = 16;  // K elements per 64-byte row: TF32 pair scheme
+constexpr int PAIR_BK_BF16 = 32;  // and BF16 pair scheme
 
 // Formulation helpers (c++/src/class/optimization_settings.h:125-153).
 inline bool is_constrained(int f) { return f >= 0 && f <= 3; }
@@ -27,6 +29,10 @@ struct MatrixDev {
   int m, n, ldm, ldn;
   float *Bc_hi, *Bc_lo, *Bt_hi, *Bt_lo;
   float *Bc;  // plain FP32 B, n rows of ldm samples: the gather Z = B V reads it
+  // Three BF16 planes of Bc (plane p at Bc_b3 + p * n * ldm) with
+  // x = b0 + b1 + b2 exactly; made when a batch of an L1-variance form first
+  // needs them (null before).
+  uint16_t *Bc_b3;
 };
 
 // Per-batch device state for k starting points.
@@ -38,6 +44,8 @@ struct BatchDev {
   int kbps1;      // K blocks per split of Z = B V
   int m_tiles1, n_tiles1, m_tiles2, n_tiles2;
   int pair2;      // V = B^T Z runs on CTA pairs (256-row tiles; B maps of bn2/2 rows)
+  int bf16_2;     // ... with the exact BF16 operands of the L1-variance forms
+  uint16_t *Z_b;  // k x ldm BF16 sgn(B V) (L1-variance forms with bf16_2, else null)
   float *Vx;            // k x ldn loadings; entry i of a column is defined only
                         // where its vmask bit is set (zero elsewhere)
   float *V_hi, *V_lo;   // k x ldn dense TF32 hi/lo planes of V: the B operand of the
@@ -76,11 +84,14 @@ struct StepParams {
 struct TensorMaps {
   CUtensorMap a1_hi, a1_lo, b1_hi, b1_lo;  // Z = B V :  A = Bt, B = V
   CUtensorMap a2_hi, a2_lo, b2_hi, b2_lo;  // V = B^T Z: A = Bc, B = Z
+  CUtensorMap a2_b0, a2_b1, a2_b2, b2_b;   // V = B^T Z, BF16: A = Bc_b3, B = Z_b
 };
 
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
 int num_sms();
 cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st);
+// Fills M.Bc_b3 from M.Bc.
+cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st);
 // Loadings of `cols` columns from src (rows entries each) into dst and their
 // non-zero masks (mask + c * (ld_dst / 32) per column).
 cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols, float *dst,

@@ -17,12 +17,13 @@
 //
 // Every reduction has a fixed order, so a step is bitwise reproducible.
 #include <cfloat>
+#include <cuda_bf16.h>
 #include <climits>
 #include <cstdio>
 
 #include "am24_internal.h"
 #include "gemm_tf32x3.cuh"
-#include "gemm_tf32x3_pair.cuh"
+#include "gemm_pair.cuh"
 
 namespace am24 {
 
@@ -47,6 +48,10 @@ __device__ __forceinline__ void split_store(float x, float *hi, float *lo) {
 }
 // sgn with sgn(0) = 0 (c++/src/utils/various.h:44-46)
 __device__ __forceinline__ float sgnf(float v) { return (float)((v > 0.f) - (v < 0.f)); }
+// sgn(v) as BF16 bits: +1 0x3F80, -1 0xBF80, 0 (and NaN) 0.
+__device__ __forceinline__ uint16_t bf16_sign(float v) {
+  return v > 0.f ? (uint16_t)0x3F80u : (v < 0.f ? (uint16_t)0xBF80u : (uint16_t)0u);
+}
 __device__ __forceinline__ uint32_t abs_key(float v) { return __float_as_uint(v) & 0x7FFFFFFFu; }
 
 template <typename T>
@@ -193,6 +198,27 @@ __global__ void prep_copy_kernel(const float *__restrict__ B, int ldB, int m, fl
   }
 }
 
+// Three BF16 planes with x = b0 + b1 + b2 exactly: b0 = bf16_rn(x),
+// b1 = bf16_rn(x - b0), b2 = x - b0 - b1.  Each difference is exact in FP32
+// (its operands are within a factor of two), the first remainder has at most
+// 16 significant bits and the second at most 8, so b2 is a BF16 value.  (FP32
+// subnormals below 2^-126 aside, where a tensor core may flush b2.)
+__global__ void prep_bf16x3_kernel(const float *__restrict__ Bc, int ldm, int m, size_t plane,
+                                   uint16_t *__restrict__ out) {
+  const size_t c = blockIdx.x;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    const size_t o = c * ldm + r;
+    const float x = Bc[o];
+    const __nv_bfloat16 b0 = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(b0);
+    const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 b2 = __float2bfloat16_rn(r1 - __bfloat162float(b1));
+    out[o] = __bfloat16_as_ushort(b0);
+    out[plane + o] = __bfloat16_as_ushort(b1);
+    out[2 * plane + o] = __bfloat16_as_ushort(b2);
+  }
+}
+
 // Bt[r * ldn + c] = split(B[c * ldB + r]): 32 x 32 tiles through shared memory.
 __global__ void prep_transpose_kernel(const float *__restrict__ B, int ldB, int m, int n,
                                       float *__restrict__ hi, float *__restrict__ lo, int ldn) {
@@ -261,7 +287,8 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
                                                        float *__restrict__ Z_hi,
                                                        float *__restrict__ Z_lo, int ldm,
                                                        float *__restrict__ fz,
-                                                       const uint32_t *gate, uint32_t gate_max) {
+                                                       const uint32_t *gate, uint32_t gate_max,
+                                                       uint16_t *__restrict__ Zb) {
   __shared__ double red[32];
   if (*gate <= gate_max) return;  // the gather kernel produced Z this step
   const int j = blockIdx.x;
@@ -281,6 +308,7 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
       acc += (double)fabsf(y);
       zh[i] = sgnf(y);
       zl[i] = 0.f;
+      if (Zb) Zb[(size_t)j * ldm + i] = bf16_sign(y);
     } else {
       acc += (double)y * (double)y;
       split_store(y, zh + i, zl + i);
@@ -313,7 +341,8 @@ template <int MODE>
 __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
     const float *__restrict__ Bc, int ldm, int m, int ldn,
     const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
-    float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max) {
+    float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
+    uint16_t *__restrict__ Zb) {
   __shared__ int idx[GATHER_CAP];
   __shared__ float val[GATHER_CAP];
   __shared__ uint32_t wsum[GATHER_THREADS / 32];
@@ -383,6 +412,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
         acc += (double)fabsf(y[r]);
         zh[i] = sgnf(y[r]);
         zl[i] = 0.f;
+        if (Zb) Zb[(size_t)j * ldm + i] = bf16_sign(y[r]);
       } else {
         acc += (double)y[r] * (double)y[r];
         if (!(MODE == 2 && one_pass)) split_store(y[r], zh + i, zl + i);
@@ -1366,31 +1396,26 @@ cudaError_t pair_clusters(K kern, int smem, int *out) {
   return cudaSuccess;
 }
 
-template <int BN, int BKT, int ST, class Epi>
-cudaError_t run_gemm_pair(const CUtensorMap &a_hi, const CUtensorMap &a_lo,
-                          const CUtensorMap &b_hi, const CUtensorMap &b_lo, const GemmShape &sh,
-                          const Epi &epi, cudaStream_t st) {
-  using L = PairSmem<BN, BKT, ST>;
-  auto kern = gemm_tf32x3_pair_kernel<BN, BKT, ST, GEMM_PROMO_K / BKT, Epi>;
+template <class S, int BN, int ST, class Epi>
+cudaError_t run_gemm_pair(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &m2,
+                          const CUtensorMap &m3, const GemmShape &sh, const Epi &epi,
+                          cudaStream_t st) {
+  using L = PairSmem<S, BN, ST>;
+  auto kern = gemm_pair_kernel<S, BN, ST, GEMM_PROMO_K / S::BK, Epi>;
   static int clusters = 0;
   if (clusters == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
     if (e != cudaSuccess) return e;
     if ((e = pair_clusters(kern, L::TOTAL, &clusters)) != cudaSuccess) return e;
   }
-  const int pairs = sh.num_units < clusters ? sh.num_units : clusters;
-  kern<<<2 * pairs, GEMM_THREADS, L::TOTAL, st>>>(a_hi, a_lo, b_hi, b_lo, sh, epi);
+  GemmShape s2 = sh;  // K blocks of this scheme's BK; units are pair tiles
+  s2.kb_total = (sh.K + S::BK - 1) / S::BK;
+  s2.kb_per_split = s2.kb_total;
+  s2.splits = 1;
+  s2.num_units = ((sh.m_tiles + 1) / 2) * sh.n_tiles;
+  const int pairs = s2.num_units < clusters ? s2.num_units : clusters;
+  kern<<<2 * pairs, GEMM_THREADS, L::TOTAL, st>>>(m0, m1, m2, m3, s2, epi);
   return cudaGetLastError();
-}
-
-// V = B^T Z on CTA pairs (N tile 256).  sh.num_units counts pair tiles.
-template <class Epi>
-cudaError_t dispatch_gemm_pair(int bk, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
-                               const CUtensorMap &b_hi, const CUtensorMap &b_lo,
-                               const GemmShape &sh, const Epi &epi, cudaStream_t st) {
-  if (bk == 32) return run_gemm_pair<256, 32, 3>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
-  if (bk == 16) return run_gemm_pair<256, 16, 6>(a_hi, a_lo, b_hi, b_lo, sh, epi, st);
-  return cudaErrorInvalidValue;
 }
 
 template <class Epi>
@@ -1413,13 +1438,16 @@ cudaError_t dispatch_gemm(int bn, int bk, const CUtensorMap &a_hi, const CUtenso
   return cudaErrorInvalidValue;
 }
 
+// V = B^T Z: CTA pairs when the N tile is 256 (BF16 operands for the
+// L1-variance forms when prepared), else the one-CTA kernel.
 template <class Epi>
 cudaError_t dispatch_gemm2(const BatchDev &b, const TensorMaps &tm, const GemmShape &sh,
-                           const Epi &epi, cudaStream_t st) {
+                           const Epi &epi, bool l1_variance, cudaStream_t st) {
   if (b.pair2) {
-    GemmShape s2 = sh;
-    s2.num_units = s2.splits * ((s2.m_tiles + 1) / 2) * s2.n_tiles;
-    return dispatch_gemm_pair(b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, s2, epi, st);
+    if (b.bf16_2 && l1_variance)
+      return run_gemm_pair<PairBF16x3A, 256, 6>(tm.a2_b0, tm.a2_b1, tm.a2_b2, tm.b2_b, sh, epi,
+                                                st);
+    return run_gemm_pair<PairTF32x3, 256, 6>(tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, sh, epi, st);
   }
   return dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, sh, epi, st);
 }
@@ -1462,6 +1490,11 @@ int pick_bn(int k) { return k > 128 ? 256 : (k > 64 ? 128 : 64); }
 
 size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn) {
   return (size_t)splits * m_tiles * n_tiles * bn * BM;
+}
+
+cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st) {
+  prep_bf16x3_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, (size_t)M.n * M.ldm, M.Bc_b3);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st) {
@@ -1535,15 +1568,15 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (mode == 0)
     gather_bv_kernel<0><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b);
   else if (mode == 1)
     gather_bv_kernel<1><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b);
   else
     gather_bv_kernel<2><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   // 1b. dense V: TF32 hi/lo planes, tensor-core Z = B V (split-K partials) ...
@@ -1561,13 +1594,16 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if ((e = mark(1)) != cudaSuccess) return e;
   if (mode == 0)
     z_reduce_kernel<0><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
-                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap);
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
+                                             b.Z_b);
   else if (mode == 1)
     z_reduce_kernel<1><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
-                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap);
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
+                                             b.Z_b);
   else
     z_reduce_kernel<2><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
-                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap);
+                                             b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
+                                             b.Z_b);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   // 3. V = B^T Z
@@ -1589,15 +1625,15 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if ((e = mark(2)) != cudaSuccess) return e;
   if (is_constrained(f)) {
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
-    e = dispatch_gemm2(b, tm, g2, er, st);
+    e = dispatch_gemm2(b, tm, g2, er, is_l1_variance(f), st);
   } else if (is_l1_penalized(f)) {
     EpiPenalty<true> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts, p.penalty,
                         b.vmask};
-    e = dispatch_gemm2(b, tm, g2, pe, st);
+    e = dispatch_gemm2(b, tm, g2, pe, is_l1_variance(f), st);
   } else {
     EpiPenalty<false> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
                          p.penalty, b.vmask};
-    e = dispatch_gemm2(b, tm, g2, pe, st);
+    e = dispatch_gemm2(b, tm, g2, pe, is_l1_variance(f), st);
   }
   if (e != cudaSuccess) return e;
   nl++;

@@ -1,13 +1,29 @@
-// CTA-pair (cta_group::2) form of the 3xTF32 GEMM of gemm_tf32x3.cuh.
+// CTA-pair (cta_group::2) GEMM for V = B^T Z, FP32-accurate, in two operand
+// schemes (the Scheme template parameter):
+//
+//   PairTF32x3   both operands as TF32 hi/lo planes (x = hi + lo exactly);
+//                lo*hi + hi*lo + hi*hi per K step, as in gemm_tf32x3.cuh.
+//   PairBF16x3A  A as three BF16 planes with x = b0 + b1 + b2 exactly (each a
+//                round-to-nearest BF16 of the remainder of the previous ones),
+//                B as one BF16 plane that must hold B exactly -- the L1-variance
+//                forms, where Z = sgn(B V) has entries -1, 0, +1.  Every product
+//                b_i * z is exact; b2*z + b1*z + b0*z per K step.  Half the
+//                tensor-core time of PairTF32x3 (BF16 runs at twice the TF32
+//                rate and needs 3 instead of 6 MMAs per 16 K elements).
 //
 // A cluster of two CTAs, on two SMs, computes a 256 x BN tile of C.  CTA rank r
 // of the pair loads rows [r*128, r*128 + 128) of the tile's A rows and rows
 // [r*BN/2, r*BN/2 + BN/2) of its B rows; the leader CTA (rank 0) issues
 // tcgen05.mma.cta_group::2 with M = 256, which reads both CTAs' shared memory
 // and accumulates 128 rows x BN columns into each CTA's tensor memory.  The
-// tensor-core work per SM is that of the one-CTA kernel with a 128 x BN tile,
-// but each SM streams 128 + BN/2 operand rows per K slab instead of 128 + BN:
-// for BN = 256 a third fewer bytes from L2 for the same FLOPs.
+// tensor-core work per SM is that of a one-CTA kernel with a 128 x BN tile,
+// but each SM streams 128 + BN/2 operand rows per K slab instead of 128 + BN.
+// Shared-memory rows are 64 bytes of K (64-byte swizzle) in both schemes, so a
+// stage is 32 KB either way.
+//
+// The tensor-core FP32 accumulation does not round to nearest; as in
+// gemm_tf32x3.cuh each TMEM buffer takes PROMO K slabs (128 K elements) and the
+// epilogue warps add it into round-to-nearest FP32 registers.
 //
 // Roles are the one-CTA kernel's (warp 0 TMA, warp 1 MMA, warps 2..9
 // accumulate + epilogue), with the MMA warp active in the leader only.
@@ -45,32 +61,75 @@ __device__ __forceinline__ Unit decode_pair_unit(const GemmShape &s, int u, int 
   return r;
 }
 
-template <int BN, int BK, int STAGES>
+// Operand schemes.  NA + NB = 4 planes, passed as the kernel's four tensor maps
+// (A planes first); BK = K elements per 64-byte shared-memory row.
+struct PairTF32x3 {
+  static constexpr int NA = 2, NB = 2, BK = PAIR_BK_TF32;
+  // a[0] = hi, a[1] = lo; b[0] = hi, b[1] = lo.  One 16-element K block:
+  // two K = 8 steps of lo*hi + hi*lo + hi*hi.
+  template <uint32_t ID>
+  __device__ static void k_block(uint32_t d, const uint32_t (&a)[2], const uint32_t (&b)[2],
+                                 uint32_t sbo, bool first) {
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+      const uint32_t off = kk * 32;
+      const uint64_t dah = sdesc_kmajor(a[0] + off, sbo, 4u);
+      const uint64_t dal = sdesc_kmajor(a[1] + off, sbo, 4u);
+      const uint64_t dbh = sdesc_kmajor(b[0] + off, sbo, 4u);
+      const uint64_t dbl = sdesc_kmajor(b[1] + off, sbo, 4u);
+      mma_tf32_pair(d, dal, dbh, ID, (first && kk == 0) ? 0u : 1u);
+      mma_tf32_pair(d, dah, dbl, ID, 1u);
+      mma_tf32_pair(d, dah, dbh, ID, 1u);
+    }
+  }
+  static constexpr uint32_t FMT = 2u;
+};
+struct PairBF16x3A {
+  static constexpr int NA = 3, NB = 1, BK = PAIR_BK_BF16;
+  // a[0..2] = b0, b1, b2; b[0] = the exact BF16 operand.  One 32-element K
+  // block: two K = 16 steps of b2*z + b1*z + b0*z.
+  template <uint32_t ID>
+  __device__ static void k_block(uint32_t d, const uint32_t (&a)[3], const uint32_t (&b)[1],
+                                 uint32_t sbo, bool first) {
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+      const uint32_t off = kk * 32;
+      const uint64_t db = sdesc_kmajor(b[0] + off, sbo, 4u);
+      mma_bf16_pair(d, sdesc_kmajor(a[2] + off, sbo, 4u), db, ID, (first && kk == 0) ? 0u : 1u);
+      mma_bf16_pair(d, sdesc_kmajor(a[1] + off, sbo, 4u), db, ID, 1u);
+      mma_bf16_pair(d, sdesc_kmajor(a[0] + off, sbo, 4u), db, ID, 1u);
+    }
+  }
+  static constexpr uint32_t FMT = 1u;
+};
+
+template <class S, int BN, int STAGES>
 struct PairSmem {
-  static constexpr int A_BYTES = GEMM_BM * BK * 4;
-  static constexpr int B_BYTES = (BN / 2) * BK * 4;
-  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int ROW = 64;  // bytes of K per shared-memory row
+  static constexpr int A_BYTES = GEMM_BM * ROW;
+  static constexpr int B_BYTES = (BN / 2) * ROW;
+  static constexpr int STAGE_BYTES = S::NA * A_BYTES + S::NB * B_BYTES;
   static constexpr int BAR_BYTES = 256;
   static constexpr int TOTAL = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
 };
 
 constexpr int PAIR_EPI_WARPS = 2 * (GEMM_EPI_THREADS / 32);  // tempty arrivals per phase
 
-template <int BN, int BK, int STAGES, int PROMO, class Epi>
+template <class S, int BN, int STAGES, int PROMO, class Epi>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
-    gemm_tf32x3_pair_kernel(const __grid_constant__ CUtensorMap tmA_hi,
-                            const __grid_constant__ CUtensorMap tmA_lo,
-                            const __grid_constant__ CUtensorMap tmB_hi,
-                            const __grid_constant__ CUtensorMap tmB_lo, const GemmShape shape,
-                            Epi epi) {
-  using L = PairSmem<BN, BK, STAGES>;
-  static_assert(BK == 32 || BK == 16, "BK must be 32 (128B swizzle) or 16 (64B swizzle)");
+    gemm_pair_kernel(const __grid_constant__ CUtensorMap tm0,
+                     const __grid_constant__ CUtensorMap tm1,
+                     const __grid_constant__ CUtensorMap tm2,
+                     const __grid_constant__ CUtensorMap tm3, const GemmShape shape, Epi epi) {
+  using L = PairSmem<S, BN, STAGES>;
+  constexpr int BK = S::BK;
+  static_assert(S::NA + S::NB == 4, "four operand planes");
   static_assert(BN % 32 == 0 && BN >= 64 && BN <= 256, "BN must be a multiple of 32 in [64,256]");
-  constexpr uint32_t SWZ = (BK == 32) ? 2u : 4u;
-  constexpr uint32_t SBO = BK * 4 * 8;
+  constexpr uint32_t SBO = L::ROW * 8;  // bytes between 8-row core-matrix groups
   constexpr uint32_t TMEM_COLS = (2 * BN <= 128) ? 128 : (2 * BN <= 256) ? 256 : 512;
-  constexpr uint32_t IDESC = make_idesc(2 * GEMM_BM, BN, 2u, 2u);
+  constexpr uint32_t IDESC = make_idesc(2 * GEMM_BM, BN, S::FMT, S::FMT);
   constexpr uint16_t BOTH = 0x3;
+  const CUtensorMap *maps[4] = {&tm0, &tm1, &tm2, &tm3};
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -102,10 +161,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
     mbar_init(drain, 1);
     *abort = 0;
     fence_mbar_init();
-    tma_prefetch_desc(&tmA_hi);
-    tma_prefetch_desc(&tmA_lo);
-    tma_prefetch_desc(&tmB_hi);
-    tma_prefetch_desc(&tmB_lo);
+    for (int i = 0; i < 4; i++) tma_prefetch_desc(maps[i]);
   }
   if (warp == 0) {
     __syncwarp();
@@ -140,10 +196,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
           const uint32_t bar = mapa_shared(smem_u32(&full[stage]), 0);
           const int kx = kb * BK;
           const int yb = t.nt * BN + rank * (BN / 2);
-          tma_load_2d_pair(st, &tmA_hi, bar, kx, t.m0);
-          tma_load_2d_pair(st + L::A_BYTES, &tmA_lo, bar, kx, t.m0);
-          tma_load_2d_pair(st + 2 * L::A_BYTES, &tmB_hi, bar, kx, yb);
-          tma_load_2d_pair(st + 2 * L::A_BYTES + L::B_BYTES, &tmB_lo, bar, kx, yb);
+#pragma unroll
+          for (int i = 0; i < S::NA; i++)
+            tma_load_2d_pair(st + i * L::A_BYTES, maps[i], bar, kx, t.m0);
+#pragma unroll
+          for (int i = 0; i < S::NB; i++)
+            tma_load_2d_pair(st + S::NA * L::A_BYTES + i * L::B_BYTES, maps[S::NA + i], bar, kx,
+                             yb);
           if (++stage == STAGES) {
             stage = 0;
             phase ^= 1u;
@@ -192,21 +251,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
               break;
             }
             tc_fence_after();
-            const uint32_t a_hi = smem_u32(smem + stage * L::STAGE_BYTES);
-            const uint32_t a_lo = a_hi + L::A_BYTES;
-            const uint32_t b_hi = a_hi + 2 * L::A_BYTES;
-            const uint32_t b_lo = b_hi + L::B_BYTES;
+            const uint32_t base = smem_u32(smem + stage * L::STAGE_BYTES);
+            uint32_t a[S::NA], b[S::NB];
 #pragma unroll
-            for (int kk = 0; kk < BK / 8; kk++) {
-              const uint32_t off = kk * 32;
-              const uint64_t dah = sdesc_kmajor(a_hi + off, SBO, SWZ);
-              const uint64_t dal = sdesc_kmajor(a_lo + off, SBO, SWZ);
-              const uint64_t dbh = sdesc_kmajor(b_hi + off, SBO, SWZ);
-              const uint64_t dbl = sdesc_kmajor(b_lo + off, SBO, SWZ);
-              mma_tf32_pair(d_tmem, dal, dbh, IDESC, (kb > c0 || kk > 0) ? 1u : 0u);
-              mma_tf32_pair(d_tmem, dah, dbl, IDESC, 1u);
-              mma_tf32_pair(d_tmem, dah, dbh, IDESC, 1u);
-            }
+            for (int i = 0; i < S::NA; i++) a[i] = base + i * L::A_BYTES;
+#pragma unroll
+            for (int i = 0; i < S::NB; i++) b[i] = base + S::NA * L::A_BYTES + i * L::B_BYTES;
+            S::template k_block<IDESC>(d_tmem, a, b, SBO, kb == c0);
             mma_commit_pair(&empty[stage], BOTH);
             if (++stage == STAGES) {
               stage = 0;
