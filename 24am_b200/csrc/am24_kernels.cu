@@ -78,6 +78,21 @@ __device__ T block_sum(T v, T *red) {
   return r;
 }
 
+// Transposes the 32 x 32 bit matrix held by a warp: lane L passes bit j of
+// x = A[L][j]; lane j gets the word whose bit L is A[L][j].  Five butterfly
+// stages, each swapping the off-diagonal s x s blocks of every 2s x 2s block.
+__device__ __forceinline__ uint32_t bit_transpose32(uint32_t x, int lane) {
+  const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const int sft = 16 >> k;
+    const uint32_t m = masks[k];
+    const uint32_t y = __shfl_xor_sync(FULL, x, sft);
+    x = (lane & sft) ? ((x & ~m) | ((y >> sft) & m)) : ((x & m) | ((y << sft) & ~m));
+  }
+  return x;
+}
+
 // 32 lanes each hold v[0..31] (one per column); afterwards lane L returns the
 // sum over all lanes of v[L].  31 shuffles instead of 32 x 5.
 __device__ __forceinline__ float transpose_reduce32(float (&v)[32], int lane) {
@@ -127,18 +142,21 @@ struct EpiRaw {
 };
 
 // V = B^T Z with the penalty threshold fused (penalized forms).
-//   L1 (c++/src/gpower/sparse_PCA_thresholding.h:26-47): d = |v| - gamma (in
-//      double, gamma is a double there), x = sgn(v) d if d > 0, objective term d^2.
+//   L1 (c++/src/gpower/sparse_PCA_thresholding.h:26-47): d = |v| - gamma,
+//      x = sgn(v) d if d > 0, objective term d^2.
 //   L0 (:68-87): d = v^2 - gamma, x = v if d > 0, objective term d.
+// The reference subtracts a double gamma; here d is the FP32 difference with
+// gamma rounded to FP32 (they differ only where |v| or v^2 is within an ulp
+// of gamma, a decision that the FP32 products feeding it already leave open).
 // Writes the non-zero x and the non-zero bitmask and, per start and per
-// (m-tile, warp), the partial objective and non-zero count, summed in fixed
-// order by the finalize kernel.
+// (128-row block, warp), the partial objective and non-zero count, summed in
+// fixed order by the finalize kernel.
 template <bool L1>
 struct EpiPenalty {
   float *Vx;
   float *obj_part, *nnz_part;
   int ld, M, N, bn, parts;  // parts = m_tiles * 4
-  double gamma;
+  float gamma;
   uint32_t *vmask;  // non-zero bitmask words, ld / 32 per column
   __device__ void begin(const Unit &, int, int) {}
   __device__ void end(const Unit &, int, int) {}
@@ -150,38 +168,35 @@ struct EpiPenalty {
     const bool rv = gi < M;
     const int mb = t.m0 / BM;  // 128-row block
     const int c0 = t.nt * bn + col0;
-    float mycnt = 0.f;
-    uint32_t mymask = 0u;
+    const int ncols = rv ? min(32, N - c0) : 0;  // valid columns of this row
+    uint32_t bits = 0u;  // bit j: (row, column c0 + j) is a non-zero
 #pragma unroll
     for (int j = 0; j < 32; j++) {
       const float v = r[j];
-      float x, o;
+      const bool valid = j < ncols;
+      float d, o, x;
       if (L1) {
-        const float d = (float)((double)fabsf(v) - gamma);
-        const bool keep = d > 0.f;
-        x = keep ? d * sgnf(v) : 0.f;
-        o = keep ? __fmul_rn(d, d) : 0.f;
+        d = __fsub_rn(fabsf(v), gamma);
+        o = __fmul_rn(d, d);
+        x = v > 0.f ? d : -d;
       } else {
-        const float d = (float)((double)__fmul_rn(v, v) - gamma);
-        const bool keep = d > 0.f;
-        x = keep ? v : 0.f;
-        o = keep ? d : 0.f;
+        d = __fsub_rn(__fmul_rn(v, v), gamma);
+        o = d;
+        x = v;
       }
-      const bool valid = rv && (c0 + j < N);
-      r[j] = valid ? o : 0.f;
-      const unsigned nz = __ballot_sync(FULL, valid && x != 0.f);
-      if (lane == j) {
-        mycnt = (float)__popc(nz);
-        mymask = nz;
-      }
-      if (valid && x != 0.f) Vx[(size_t)(c0 + j) * ld + gi] = x;  // zeros live in the mask
+      const bool keep = valid && d > 0.f;
+      r[j] = keep ? o : 0.f;
+      const bool nz = keep && v != 0.f;
+      bits |= (uint32_t)nz << j;
+      if (nz) Vx[(size_t)(c0 + j) * ld + gi] = x;  // zeros live in the mask
     }
+    const uint32_t word = bit_transpose32(bits, lane);  // lane j: column c0 + j, bit = row
     const float so = transpose_reduce32(r, lane);
     const int col = c0 + lane;
     if (col < N) {
       obj_part[(size_t)col * parts + mb * 4 + q] = so;
-      nnz_part[(size_t)col * parts + mb * 4 + q] = mycnt;
-      if (mb * 4 + q < (ld >> 5)) vmask[(size_t)col * (ld >> 5) + mb * 4 + q] = mymask;
+      nnz_part[(size_t)col * parts + mb * 4 + q] = (float)__popc(word);
+      if (mb * 4 + q < (ld >> 5)) vmask[(size_t)col * (ld >> 5) + mb * 4 + q] = word;
     }
   }
 };
@@ -1401,7 +1416,7 @@ cudaError_t run_gemm_pair(const CUtensorMap &m0, const CUtensorMap &m1, const CU
                           const CUtensorMap &m3, const GemmShape &sh, const Epi &epi,
                           cudaStream_t st) {
   using L = PairSmem<S, BN, ST>;
-  auto kern = gemm_pair_kernel<S, BN, ST, GEMM_PROMO_K / S::BK, Epi>;
+  auto kern = gemm_pair_kernel<S, BN, ST, S::PROMO_K / S::BK, Epi>;
   static int clusters = 0;
   if (clusters == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
@@ -1627,12 +1642,13 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
     e = dispatch_gemm2(b, tm, g2, er, is_l1_variance(f), st);
   } else if (is_l1_penalized(f)) {
-    EpiPenalty<true> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts, p.penalty,
+    EpiPenalty<true> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
+                        (float)p.penalty,
                         b.vmask};
     e = dispatch_gemm2(b, tm, g2, pe, is_l1_variance(f), st);
   } else {
     EpiPenalty<false> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
-                         p.penalty, b.vmask};
+                         (float)p.penalty, b.vmask};
     e = dispatch_gemm2(b, tm, g2, pe, is_l1_variance(f), st);
   }
   if (e != cudaSuccess) return e;

@@ -22,8 +22,9 @@
 // stage is 32 KB either way.
 //
 // The tensor-core FP32 accumulation does not round to nearest; as in
-// gemm_tf32x3.cuh each TMEM buffer takes PROMO K slabs (128 K elements) and the
-// epilogue warps add it into round-to-nearest FP32 registers.
+// gemm_tf32x3.cuh each TMEM buffer takes PROMO K slabs (S::PROMO_K elements: 48
+// MMA accumulations in both schemes) and the epilogue warps add it into
+// round-to-nearest FP32 registers.
 //
 // Roles are the one-CTA kernel's (warp 0 TMA, warp 1 MMA, warps 2..9
 // accumulate + epilogue), with the MMA warp active in the leader only.
@@ -65,6 +66,9 @@ __device__ __forceinline__ Unit decode_pair_unit(const GemmShape &s, int u, int 
 // (A planes first); BK = K elements per 64-byte shared-memory row.
 struct PairTF32x3 {
   static constexpr int NA = 2, NB = 2, BK = PAIR_BK_TF32;
+  // K elements per TMEM chunk before the FP32 promotion: 48 MMAs accumulate
+  // into a chunk (16 K steps of 3)
+  static constexpr int PROMO_K = 128;
   // a[0] = hi, a[1] = lo; b[0] = hi, b[1] = lo.  One 16-element K block:
   // two K = 8 steps of lo*hi + hi*lo + hi*hi.
   template <uint32_t ID>
@@ -86,6 +90,8 @@ struct PairTF32x3 {
 };
 struct PairBF16x3A {
   static constexpr int NA = 3, NB = 1, BK = PAIR_BK_BF16;
+  // the same 48 MMA accumulations per chunk as PairTF32x3 (16 K steps of 3)
+  static constexpr int PROMO_K = 256;
   // a[0..2] = b0, b1, b2; b[0] = the exact BF16 operand.  One 32-element K
   // block: two K = 16 steps of b2*z + b1*z + b0*z.
   template <uint32_t ID>

@@ -5,8 +5,10 @@ Workload (one GPU): n = 2000 samples x p = 50000 features, low-rank (r = 50,
 256 non-zeros per loading) plus N(0, 0.1^2) noise, seeded and generated on
 the device; k = 1024 starting points U[-1, 1] normalised; all 8 formulations:
 s = 16 for the constraint forms, gamma = 0.1 x max column 2-norm (L2-variance
-penalties) or 0.1 x max column 1-norm (L1-variance penalties).  FP32 data,
-3xTF32 tensor-core products with FP32 accumulation.
+penalties) or 0.1 x max column 1-norm (L1-variance penalties).  FP32 data;
+tensor-core products FP32-accurate: 3xTF32 (L2-variance forms), or for the
+L1-variance forms, whose Z = sgn(B V) is exact in BF16, B split exactly into
+three BF16 planes; FP32 accumulation.
 
 A step is one AM iteration of every formulation over its k starts, i.e.
 8 x 1024 start-iterations.  `value` = start-iterations/s of the whole job with
@@ -208,6 +210,21 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------ GPU arm
+def kernel_label(kind, f):
+    """Bench name of a step kernel of formulation f: V = B^T Z by operand scheme
+    (BF16 for the L1-variance forms 1, 3, 5, 7 on CTA pairs, else 3xTF32) and
+    epilogue (raw for the constrained forms, fused penalty otherwise); the
+    select by constraint (top-s for 0, 1; L1 ball for 2, 3)."""
+    skipped = kind.endswith("(skipped)")
+    base = kind[:-len("(skipped)")] if skipped else kind
+    if base == "gemm_BtZ":
+        base = (f"gemm_BtZ_{'bf16x3' if f in (1, 3, 5, 7) and STARTS > 128 else 'tf32x3'}"
+                f"_{'raw' if f <= 3 else 'pen'}")
+    elif base == "select":
+        base = "select_top_s" if f in (0, 1) else "select_l1_ball"
+    return base + ("(skipped)" if skipped else "")
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -275,29 +292,39 @@ def run_ours(args):
     value = its_per_step * args.steps * world / (ms_max * 1e-3)
 
     # per-kernel CUDA events inside the same kind of steps
-    per_kind = {}
+    per_kind, per_form = {}, {}
     for i in range(max(1, min(args.steps, 5))):
         for f, b in zip(forms, batches):
             for kind, kms in b.step_timed(args.warmup + args.steps + i):
-                key = kind if kind not in ("gemm_BtZ", "select") else (
-                    f"{kind}_{'cons' if f <= 3 else 'pen'}")
+                key = kernel_label(kind, f)
                 per_kind.setdefault(key, []).append(kms)
+                pf = per_form.setdefault(f, {})
+                pf[key] = pf.get(key, 0.0) + kms
+    n_timed = max(1, min(args.steps, 5))
+    formulation_ms = {str(f): {"step_ms": sum(d.values()) / n_timed,
+                               "kernels": sorted(k for k in d if "skipped" not in k)}
+                      for f, d in per_form.items()}
     totals = {k: sum(v) for k, v in per_kind.items()}
     roof_kinds = {k: t for k, t in totals.items() if k.startswith(("gemm", "select"))
                   and "skipped" not in k}
     dom = max(roof_kinds, key=roof_kinds.get)
     pk, pk_kind = peaks()
-    tf32x3_peak = pk["bf16_tflops_sustained"] / 2.0 / 3.0
     avg_ms = statistics.mean(per_kind[dom])
     if dom.startswith("gemm"):
+        # FP32-equivalent rate: 2*n*p*k FLOPs per launch against the tensor
+        # rate of the scheme's passes (three TF32 MMAs, or three BF16 MMAs,
+        # per FP32 product)
+        bf16 = "bf16x3" in dom
+        peak = pk["bf16_tflops_sustained"] / (1.0 if bf16 else 2.0) / 3.0
         flops = 2.0 * N_SAMPLES * P_FEATURES * STARTS
         achieved = flops / (avg_ms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": tf32x3_peak, "unit": "TFLOP/s",
-                "frac": achieved / tf32x3_peak, "traffic": profiled_traffic(dom),
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": profiled_traffic(dom),
                 "kernel": dom, "avg_launch_ms": avg_ms,
-                "peak_note": f"{pk_kind} bf16 sustained {pk['bf16_tflops_sustained']} TF/s "
-                             "/2 (TF32 rate) /3 (three TF32 MMAs per FP32 product); "
-                             "achieved counts 2*n*p*k dense FLOPs per launch"}
+                "peak_note": f"{pk_kind} bf16 sustained {pk['bf16_tflops_sustained']} TF/s"
+                             + (" /3 (three BF16 MMAs per FP32 product)" if bf16 else
+                                " /2 (TF32 rate) /3 (three TF32 MMAs per FP32 product)")
+                             + "; achieved counts 2*n*p*k dense FLOPs per launch"}
     else:
         byts = 4.0 * P_FEATURES * STARTS * 3
         achieved = byts / (avg_ms * 1e-3) / 1e9
@@ -362,10 +389,11 @@ def run_ours(args):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": workload_name(), "n": N_SAMPLES, "p": P_FEATURES,
                            "starts_per_gpu": STARTS, "formulations": forms, "s": S_CONS,
-                           "gamma_factor": GAMMA_C, "precision": "3xTF32 products, FP32 accumulate",
+                           "gamma_factor": GAMMA_C, "precision": "FP32-accurate products (3xTF32; exact 3xBF16 split for the L1-variance forms), FP32 accumulate",
                            "l2": "inputs larger than L2 (B as 4 FP32 planes = 1.6 GB)",
                            "parallelism": f"start-sharded x{world}, no data-path collective"},
-                "roofline": roof, "kernels": breakdown, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "kernels": breakdown, "formulation_ms": formulation_ms,
+                "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
