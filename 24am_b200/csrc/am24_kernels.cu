@@ -731,126 +731,207 @@ __device__ void bitonic_desc(T *a, int len) {
 }
 
 // ------------------------------------------------------------ L0 constraint
-// k_hard_thresholding (c++/src/utils/thresh_functions.h:121-145): level = the
-// s-th largest |v| (with multiplicity, as the sorting variant :92-98 defines
-// it), keep |v| >= level, then x <- x / ||x|| (c++/src/gpower/gpower_commons.h:111).
-constexpr int HARD_CAND = 4096;  // candidates resolved in shared memory
-constexpr int HARD_THREADS = 1024;
-// fraction of the previous level used as the gather bound of the hinted search
+constexpr int HARD_THREADS = 256;
+constexpr int HARD_CAND = 2048;  // hinted (key, index) candidates resolved in shared memory
+// fraction of the previous level used as the gather bound of the hinted searches
 constexpr float HINT_FRACTION = 0.9f;
+
+// One streaming pass over a column in global memory (16-byte loads, four in
+// flight per thread): the entries with |v| key >= bound go to cand as
+// (key << 32 | ~index), the first `cap` of them in any order; returns how many
+// there are (it may exceed cap) and leaves in counter[1] the largest key below
+// the bound (0 if none).  Entries past n are not taken.
+__device__ uint32_t gather_pairs_above(const float *__restrict__ colg, int n, uint32_t bound,
+                                       uint64_t *cand, uint32_t cap, uint32_t *counter) {
+  if (threadIdx.x == 0) {
+    counter[0] = 0;
+    counter[1] = 0;
+  }
+  __syncthreads();
+  uint32_t below = 0;
+  const int lane = threadIdx.x & 31;
+  const int n4 = (n + 3) >> 2;
+  const float4 *c4 = reinterpret_cast<const float4 *>(colg);
+  constexpr int U = 4;
+  for (int base = (threadIdx.x & ~31); base < n4; base += U * blockDim.x) {
+    float4 v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = base + u * blockDim.x + lane;
+      v[u] = (i < n4) ? __ldg(c4 + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int e0 = 4 * (base + u * blockDim.x + lane);
+      const float x[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+      uint32_t take = 0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint32_t key = abs_key(x[q]);
+        const bool in = e0 + q < n;
+        take |= (uint32_t)(in && key >= bound) << q;
+        if (in && key < bound) below = max(below, key);
+      }
+      if (!__any_sync(FULL, take != 0)) continue;
+      const uint32_t mine = __popc(take);
+      uint32_t incl = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+      }
+      uint32_t wbase = 0;
+      if (lane == 31) wbase = atomicAdd(&counter[0], incl);
+      wbase = __shfl_sync(FULL, wbase, 31);
+      uint32_t pos = wbase + incl - mine;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (take & (1u << q)) {
+          if (pos < cap)
+            cand[pos] = ((uint64_t)abs_key(x[q]) << 32) | (uint32_t)~(uint32_t)(e0 + q);
+          pos++;
+        }
+    }
+  }
+  below = __reduce_max_sync(FULL, below);
+  if (lane == 0) atomicMax(&counter[1], below);
+  __syncthreads();
+  return counter[0];
+}
 
 // k_hard_thresholding (c++/src/utils/thresh_functions.h:121-145): level = the
 // s-th largest |v| (with multiplicity, as the sorting variant :92-98 defines
 // it), keep |v| >= level, then x <- x / ||x|| (c++/src/gpower/gpower_commons.h:111).
 //
-// The column is staged in shared memory by a bulk copy.  Level search:
-// (a) with the previous step's level as a hint, one pass gathers |v| >= hint/2;
-// when that holds s to HARD_CAND values, sorting them gives the exact level
-// and the norm; otherwise (b) a histogram of the top 11 bits of |v| finds the
-// bin holding rank s, keys above it are kept for sure, keys in it are gathered
-// and sorted; a bin too full for shared memory falls back to (c) the exact
-// three-level radix select.  Last, the non-zero loadings and the bitmask are
-// written.
-template <bool CACHED>
-__global__ void __launch_bounds__(HARD_THREADS, 1) hard_select_kernel(
+// One block per column, reading it from global memory.  (a) With the previous
+// step's level as a hint, a streaming pass gathers the entries with
+// |v| >= HINT_FRACTION * hint together with their indices; if fewer than s,
+// a second pass gathers down to the largest key below that bound (exactly
+// the kept set when one entry was missing).  When that holds s to HARD_CAND
+// entries, sorting them gives the exact level, the norm and the kept entries,
+// and the column is written sparsely (its mask words cleared, then the kept
+// entries' bits and values set).  Otherwise (b) a histogram of the top 11 bits
+// of |v| finds the bin holding rank s, keys above it are kept for sure, keys
+// in it are gathered and sorted; a bin too full for shared memory falls back
+// to (c) the exact three-level radix select; the column is then written by a
+// full pass.
+__global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
     float *__restrict__ hints) {
-  extern __shared__ __align__(16) uint8_t dsm[];
-  uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
-  uint32_t *cand = hist + 2048;
-  uint32_t *res = cand + HARD_CAND;
-  double *red = reinterpret_cast<double *>(res + 8);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(red + 32);
-  float *cache = reinterpret_cast<float *>(bar + 2);
+  __shared__ uint64_t cand[HARD_CAND];  // also 2 * HARD_CAND keys for (b)
+  __shared__ uint32_t hist[2048];
+  __shared__ uint32_t res[8];
+  __shared__ double red[32];
+  uint32_t *cand32 = reinterpret_cast<uint32_t *>(cand);
   const int j = blockIdx.x;
   const float *colg = Vraw + (size_t)j * ldv;
-  if (CACHED) stage_column(cache, colg, n, bar, status);
+  float *vx = Vx + (size_t)j * ldv;
+  uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
   uint32_t thr = 0;
   double ss = 0.0, cnt = 0.0;
-  // (a) the previous step's level: as the iterates settle the s-th largest
-  // moves little, so one pass gathering |v| >= HINT_FRACTION * level usually
-  // holds the exact answer (and few enough values to sort cheaply)
   bool done = false;
   const float hint = hints[j];
-  if (hint > 0.f) {
-    const uint32_t c = gather_keys_above<CACHED>(colg, cache, n, abs_key(HINT_FRACTION * hint),
-                                                 cand, HARD_CAND, res);
-    if (c >= s && c <= (uint32_t)HARD_CAND) {
+  uint32_t bound = max(1u, abs_key(HINT_FRACTION * hint));
+  for (int attempt = 0; attempt < 2 && hint > 0.f && !done; attempt++) {
+    const uint32_t c = gather_pairs_above(colg, n, bound, cand, HARD_CAND, &res[0]);
+    const uint32_t below = res[1];
+    if (c > (uint32_t)HARD_CAND) break;  // too many: the histogram path
+    if (c < s) {
+      // short by one: the s-th largest is the largest key below the bound, so
+      // gathering down to it takes exactly the kept entries; otherwise widen
+      bound = (s - c == 1) ? below : abs_key(HINT_FRACTION * __uint_as_float(below));
+      if (bound == 0) break;
+    } else {
       int len = 1;
       while (len < (int)c) len <<= 1;
-      for (int q = c + threadIdx.x; q < len; q += blockDim.x) cand[q] = 0u;
+      for (int q = c + threadIdx.x; q < len; q += blockDim.x) cand[q] = 0ull;
       __syncthreads();
       bitonic_desc(cand, len);
-      thr = cand[s - 1];
-      for (int q = threadIdx.x; q < (int)c; q += blockDim.x)
-        if (cand[q] >= thr) {
-          const double v = (double)__uint_as_float(cand[q]);
+      thr = (uint32_t)(cand[s - 1] >> 32);
+      // kept: the sorted prefix with key >= thr (ties with the s-th included)
+      if (threadIdx.x == 0) res[1] = 0;
+      __syncthreads();
+      for (int q = threadIdx.x; q < (int)c; q += blockDim.x) {
+        const uint32_t key = (uint32_t)(cand[q] >> 32);
+        if (key >= thr && (q + 1 == (int)c || (uint32_t)(cand[q + 1] >> 32) < thr))
+          res[1] = q + 1;
+        if (key >= thr) {
+          const double v = (double)__uint_as_float(key);
           ss += v * v;
-          cnt += 1.0;
         }
+      }
       done = true;
     }
     __syncthreads();
   }
-  // (b) histogram of the top 11 key bits, then the bin holding rank s
-  if (!done) {
-  key_histogram<CACHED>(colg, cache, n, hist);
-  find_rank_bin(hist, 2048, s, res);
-  const uint32_t b1 = res[0], above = res[1], in_bin = res[2];
-  __syncthreads();
-  if (in_bin <= (uint32_t)HARD_CAND) {
-    if (threadIdx.x == 0) res[3] = 0;
+  if (done) {
+    const uint32_t kept = res[1];
+    ss = block_sum(ss, red);
+    const float inv = 1.0f / (float)sqrt(ss);
+    for (int w = threadIdx.x; w < (ldv >> 5); w += blockDim.x) mk[w] = 0u;
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t key = col_key<CACHED>(colg, cache, i);
-      const uint32_t bin = key >> 20;
-      if (bin > b1) {
-        const double v = (double)__uint_as_float(key);
-        ss += v * v;
-        cnt += 1.0;
-      } else if (bin == b1) {
-        cand[atomicAdd(&res[3], 1u)] = key;
+    for (int q = threadIdx.x; q < (int)kept; q += blockDim.x) {
+      const uint32_t i = ~(uint32_t)cand[q];
+      vx[i] = __ldg(colg + i) * inv;
+      atomicOr(&mk[i >> 5], 1u << (i & 31));
+    }
+    cnt = (double)kept;
+  } else {
+    // (b) histogram of the top 11 key bits, then the bin holding rank s
+    key_histogram<false>(colg, nullptr, n, hist);
+    find_rank_bin(hist, 2048, s, res);
+    const uint32_t b1 = res[0], above = res[1], in_bin = res[2];
+    __syncthreads();
+    if (in_bin <= (uint32_t)(2 * HARD_CAND)) {
+      if (threadIdx.x == 0) res[3] = 0;
+      __syncthreads();
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t key = abs_key(colg[i]);
+        const uint32_t bin = key >> 20;
+        if (bin > b1) {
+          const double v = (double)__uint_as_float(key);
+          ss += v * v;
+          cnt += 1.0;
+        } else if (bin == b1) {
+          cand32[atomicAdd(&res[3], 1u)] = key;
+        }
+      }
+      __syncthreads();
+      const int nc = (int)res[3];
+      int len = 1;
+      while (len < nc) len <<= 1;
+      for (int q = nc + threadIdx.x; q < len; q += blockDim.x) cand32[q] = 0u;
+      __syncthreads();
+      bitonic_desc(cand32, len);
+      thr = cand32[s - above - 1];
+      for (int q = threadIdx.x; q < nc; q += blockDim.x)
+        if (cand32[q] >= thr) {
+          const double v = (double)__uint_as_float(cand32[q]);
+          ss += v * v;
+          cnt += 1.0;
+        }
+    } else {
+      // (c) exact radix select
+      thr = block_select<false>(colg, nullptr, n, s, hist, res).key;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float v = colg[i];
+        if (abs_key(v) >= thr) {
+          ss += (double)v * (double)v;
+          cnt += 1.0;
+        }
       }
     }
-    __syncthreads();
-    const int nc = (int)res[3];
-    int len = 1;
-    while (len < nc) len <<= 1;
-    for (int q = nc + threadIdx.x; q < len; q += blockDim.x) cand[q] = 0u;
-    __syncthreads();
-    bitonic_desc(cand, len);
-    thr = cand[s - above - 1];
-    for (int q = threadIdx.x; q < nc; q += blockDim.x)
-      if (cand[q] >= thr) {
-        const double v = (double)__uint_as_float(cand[q]);
-        ss += v * v;
-        cnt += 1.0;
-      }
-  } else {
-    thr = block_select<CACHED>(colg, cache, n, s, hist, res).key;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const float v = CACHED ? cache[i] : colg[i];
-      if (abs_key(v) >= thr) {
-        ss += (double)v * (double)v;
-        cnt += 1.0;
-      }
-    }
-  }
-  }
-  if (threadIdx.x == 0) hints[j] = __uint_as_float(thr);
-  ss = block_sum(ss, red);
-  cnt = block_sum(cnt, red);
-  const float inv = 1.0f / (float)sqrt(ss);
-  float *vx = Vx + (size_t)j * ldv;
-  uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
-  if (CACHED) {
-    write_column(cache, n, vx, mk, [=](float v) { return (abs_key(v) >= thr) ? v * inv : 0.f; });
-  } else {
+    ss = block_sum(ss, red);
+    cnt = block_sum(cnt, red);
+    const float inv = 1.0f / (float)sqrt(ss);
     write_column_global(colg, n, vx, mk,
                         [=](float v) { return (abs_key(v) >= thr) ? v * inv : 0.f; });
   }
-  if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
+  if (threadIdx.x == 0) {
+    hints[j] = __uint_as_float(thr);
+    nnz_out[j] = (uint32_t)cnt;
+  }
 }
 
 // ------------------------------------------------------------ L1 constraint
@@ -1486,7 +1567,6 @@ cudaError_t launch_select(bool cached, size_t smem_fixed, int n, int grid, int t
 }
 
 constexpr size_t SMEM_LIMIT = 227 * 1024;
-constexpr size_t HARD_FIXED = 2048 * 4 + HARD_CAND * 4 + 32 + 32 * 8 + 16;  // + mbarrier
 
 }  // namespace
 
@@ -1657,10 +1737,9 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (is_constrained(f)) {
     if ((e = mark(3)) != cudaSuccess) return e;
     if (!is_l1_constrained(f)) {
-      const bool cached = HARD_FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
-      e = launch_select(cached, HARD_FIXED, M.n, b.k, HARD_THREADS, hard_select_kernel<true>,
-                        hard_select_kernel<false>, st, b.Vraw, M.ldn, p.constraint, b.Vx, b.nnz,
-                        b.status, b.vmask, b.sel_hint);
+      hard_select_kernel<<<b.k, HARD_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint, b.Vx,
+                                                        b.nnz, b.status, b.vmask, b.sel_hint);
+      e = cudaGetLastError();
     } else {
       const bool cached = SoftSmem::FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
       if (p.l1_mode == 0)
