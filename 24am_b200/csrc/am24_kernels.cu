@@ -534,71 +534,10 @@ __device__ SelResult block_select(const float *__restrict__ colg, const float *c
   return SelResult{prefix, gt, eq};
 }
 
-// Stages col[0..n) (plus up to 3 floats of the 16-byte-rounded tail, which
-// lie in the column's padding) into shared memory with one bulk copy per
-// 32 KB.  If the copy does not land within the bound, raises *status and
-// falls back to plain loads.
-__device__ void stage_column(float *cache, const float *__restrict__ colg, int n, uint64_t *bar,
-                             int *status) {
-  const uint32_t bytes = ((uint32_t)n * 4u + 15u) & ~15u;
-  if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    mbar_arrive_expect_tx(bar, bytes);
-    for (uint32_t off = 0; off < bytes; off += 32768u)
-      bulk_load(reinterpret_cast<uint8_t *>(cache) + off,
-                reinterpret_cast<const uint8_t *>(colg) + off, min(32768u, bytes - off), bar);
-  }
-  const uint64_t t0 = global_timer_ns();
-  bool ok = true;
-  while (!mbar_try_wait(bar, 0)) {
-    if (global_timer_ns() - t0 > 2000000000ull) {
-      ok = false;
-      break;
-    }
-  }
-  if (!__syncthreads_and(ok)) {
-    if (threadIdx.x == 0) atomicCAS(status, 0, 0x201);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) cache[i] = colg[i];
-    __syncthreads();
-  }
-}
-
-// x_i = f(v_i) for a column staged in shared memory: the non-zero x_i are
-// stored (only they are defined; the bitmask says which) and the column's
-// non-zero bitmask is written.  Each warp covers 128 consecutive entries per
-// step (4 mask words); entries past n read the staged column's zero padding.
-template <class Fn>
-__device__ __forceinline__ void write_column(const float *cache, int n, float *vx, uint32_t *mask,
-                                             Fn fn) {
-  const int n4 = (n + 3) >> 2;
-  const int lane = threadIdx.x & 31;
-  const float4 *c4 = reinterpret_cast<const float4 *>(cache);
-  for (int base = threadIdx.x & ~31; base < n4; base += blockDim.x) {
-    const int i = base + lane;
-    uint32_t nib = 0;
-    if (i < n4) {
-      const float4 v = c4[i];
-      const float x0 = fn(v.x), x1 = fn(v.y), x2 = fn(v.z), x3 = fn(v.w);
-      if (x0 != 0.f) { vx[4 * i] = x0; nib |= 1u; }
-      if (x1 != 0.f) { vx[4 * i + 1] = x1; nib |= 2u; }
-      if (x2 != 0.f) { vx[4 * i + 2] = x2; nib |= 4u; }
-      if (x3 != 0.f) { vx[4 * i + 3] = x3; nib |= 8u; }
-    }
-    // 8 lanes x 4 entries -> one 32-bit mask word
-    uint32_t word = nib << (4 * (lane & 7));
-    word |= __shfl_xor_sync(FULL, word, 1);
-    word |= __shfl_xor_sync(FULL, word, 2);
-    word |= __shfl_xor_sync(FULL, word, 4);
-    if ((lane & 7) == 0 && 4 * i < ((n + 31) & ~31)) mask[(4 * i) >> 5] = word;
-  }
-}
-
-// Same as write_column, reading the column from global memory (entries up to
-// the next multiple of 32 are read; they lie in the column's zero padding).
+// x_i = f(v_i) for a column in global memory: the non-zero x_i are stored
+// (only they are defined; the bitmask says which) and the column's non-zero
+// bitmask is written.  Entries up to the next multiple of 32 are read; they lie
+// in the column's zero padding.
 template <class Fn>
 __device__ __forceinline__ void write_column_global(const float *__restrict__ colg, int n,
                                                     float *vx, uint32_t *mask, Fn fn) {
@@ -670,43 +609,6 @@ __device__ void key_histogram(const float *__restrict__ colg, const float *cols,
     if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], __popc(peers));
   }
   __syncthreads();
-}
-
-// Block-wide: the keys >= bound go to cand (the first `cap` of them, in any
-// order) and the count of all of them is returned (it may exceed cap);
-// res[1] gets the largest key below the bound.  res[0..1] are scratch.
-template <bool CACHED>
-__device__ uint32_t gather_keys_above(const float *__restrict__ colg, const float *cols, int n,
-                                      uint32_t bound, uint32_t *cand, uint32_t cap,
-                                      uint32_t *res) {
-  if (threadIdx.x == 0) {
-    res[0] = 0;
-    res[1] = 0;
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  uint32_t below = 0;
-  for (int base = threadIdx.x & ~31; base < n; base += blockDim.x) {
-    const int i = base + lane;
-    const uint32_t key = (i < n) ? col_key<CACHED>(colg, cols, i) : 0u;
-    const bool take = (i < n) && key >= bound;
-    if (!take) below = max(below, key);
-    const unsigned bal = __ballot_sync(FULL, take);
-    if (bal) {
-      uint32_t wbase = 0;
-      if (lane == 0) wbase = atomicAdd(&res[0], (uint32_t)__popc(bal));
-      wbase = __shfl_sync(FULL, wbase, 0);
-      if (take) {
-        const uint32_t pos = wbase + __popc(bal & ((1u << lane) - 1u));
-        if (pos < cap) cand[pos] = key;
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) below = max(below, __shfl_xor_sync(FULL, below, o));
-  if (lane == 0) atomicMax(&res[1], below);
-  __syncthreads();
-  return res[0];
 }
 
 // Descending bitonic sort of a[0..len), len a power of two.
@@ -936,13 +838,7 @@ __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
 
 // ------------------------------------------------------------ L1 constraint
 constexpr int SOFT_C = 1024;  // sorted-candidate chunk (power of two for the bitonic sort)
-constexpr int SOFT_THREADS = 512;
-
-struct SoftSmem {
-  static constexpr size_t HIST = 2048 * 4, RES = 128, RED = 32 * 8, CAND = SOFT_C * 4,
-                          P = SOFT_C * 8;
-  static constexpr size_t FIXED = HIST + RES + RED + CAND + 2 * P + 64 + 16;  // + mbarrier
-};
+constexpr int SOFT_THREADS = 256;
 
 // Unfused double arithmetic (no FMA contraction), as host C++ evaluates it.
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
@@ -1132,26 +1028,24 @@ __device__ uint32_t resolve_stop(uint32_t best, double bw, uint32_t *res,
 // EXACT: stop at the first segment whose lower knot already gives
 // ||.||_1/||.||_2 >= sqrt(s) and take the root inside it -- the exact
 // L1-ball / unit-sphere projection.
-template <bool CACHED, bool EXACT>
-__global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
+template <bool EXACT>
+__global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
     float *__restrict__ hints) {
-  extern __shared__ __align__(16) uint8_t dsm[];
-  uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
-  uint32_t *res = hist + 2048;
-  double *red = reinterpret_cast<double *>(dsm + SoftSmem::HIST + SoftSmem::RES);
-  float *cand = reinterpret_cast<float *>(dsm + SoftSmem::HIST + SoftSmem::RES + SoftSmem::RED);
-  double *p1 = reinterpret_cast<double *>(reinterpret_cast<uint8_t *>(cand) + SoftSmem::CAND);
-  double *p2 = p1 + SOFT_C;
-  volatile uint32_t *misc = reinterpret_cast<volatile uint32_t *>(p2 + SOFT_C);  // 16 words
-  double *w_sh = reinterpret_cast<double *>(const_cast<uint32_t *>(misc) + 8);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(dsm + SoftSmem::FIXED - 16);
-  float *cache = reinterpret_cast<float *>(dsm + SoftSmem::FIXED);
+  __shared__ uint64_t pairs[SOFT_C];  // hinted (key, index) candidates
+  __shared__ float cand[SOFT_C];
+  __shared__ double p1[SOFT_C], p2[SOFT_C];
+  __shared__ uint32_t hist[2048];
+  __shared__ uint32_t res[32];
+  __shared__ double red[32];
+  __shared__ uint32_t misc_raw[16];
+  __shared__ double w_shared;
+  volatile uint32_t *misc = misc_raw;
+  double *w_sh = &w_shared;
 
   const int j = blockIdx.x;
   const float *colg = Vraw + (size_t)j * ldv;
-  if (CACHED) stage_column(cache, colg, n, bar, status);
   // sqrt(s), sqrt(s)^2 as the double-precision reference forms them
   const double sq = __dsqrt_rn((double)s);
   const double sq2 = __dmul_rn(sq, sq);
@@ -1159,22 +1053,27 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
 
   double w = 0.0;
   uint32_t brk = NONE;
-  bool have_norm = false;
+  bool have_norm = false;  // ss and cnt already summed over the gathered values
+  bool sparse = false;     // ... and the gathered pairs hold every kept entry
+  uint32_t c_pairs = 0;
   double ss = 0.0, cnt = 0.0;
-  // ---- hinted path: gather |v| >= HINT_FRACTION * (previous step's level)
+  // ---- hinted path: gather (key, index) with |v| >= HINT_FRACTION * (previous level)
   const float hint = hints[j];
   if (hint > 0.f) {
-    const uint32_t c = gather_keys_above<CACHED>(colg, cache, n, abs_key(HINT_FRACTION * hint),
-                                                 reinterpret_cast<uint32_t *>(cand), SOFT_C, res);
+    const uint32_t c =
+        gather_pairs_above(colg, n, max(1u, abs_key(HINT_FRACTION * hint)), pairs, SOFT_C, res);
     const uint32_t below_key = res[1];
     __syncthreads();
     if (c > 0 && c <= (uint32_t)SOFT_C) {
       int len = 1;
       while (len < (int)c) len <<= 1;
-      for (uint32_t q = c + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
+      for (int q = c + threadIdx.x; q < len; q += blockDim.x) pairs[q] = 0ull;
+      __syncthreads();
+      bitonic_desc(pairs, len);
+      for (uint32_t q = threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x)
+        cand[q] = (q < c) ? __uint_as_float((uint32_t)(pairs[q] >> 32)) : -1.f;
       __syncthreads();
       const double lo_after = (c == (uint32_t)n) ? 0.0 : (double)__uint_as_float(below_key);
-      bitonic_desc(cand, len);
       block_scan2(cand, (int)c, 0.0, 0.0, p1, p2, red);
       const double lim = __dsub_rn((double)cand[0], 0.000001);  // ||v||_inf - 1e-6
       uint32_t best = NONE;
@@ -1191,6 +1090,7 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
         __syncthreads();
       }
       if (brk != NONE) {
+        // the level lies at or above every value outside the gathered set
         for (uint32_t q = threadIdx.x; q < c; q += blockDim.x) {
           const double d = (double)cand[q] - w;
           if (d > 0.0) {
@@ -1200,6 +1100,8 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
           }
         }
         have_norm = true;
+        sparse = true;
+        c_pairs = c;
       }
     }
     __syncthreads();
@@ -1208,7 +1110,7 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
   // ---- fast path: the highest bins holding at most SOFT_C values
   uint32_t c = 0, bstar = 0;
   if (brk == NONE) {
-    key_histogram<CACHED>(colg, cache, n, hist);
+    key_histogram<false>(colg, nullptr, n, hist);
     find_rank_bin(hist, 2048, (uint32_t)SOFT_C + 1u, res);
     const bool whole = (uint32_t)n <= (uint32_t)SOFT_C;
     bstar = whole ? 0u : res[0] + 1u;  // gather bins >= bstar
@@ -1223,7 +1125,7 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
     __syncthreads();
     uint32_t below = 0;  // largest key under the gathered bins
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t key = col_key<CACHED>(colg, cache, i);
+      const uint32_t key = abs_key(colg[i]);
       if ((key >> 20) >= bstar) cand[atomicAdd((uint32_t *)&misc[0], 1u)] = __uint_as_float(key);
       else below = max(below, key);
     }
@@ -1267,14 +1169,14 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
 
   // ---- exact walk, a chunk of SOFT_C ranks at a time
   if (brk == NONE) {
-    const SelResult top = block_select<CACHED>(colg, cache, n, 1u, hist, res);
+    const SelResult top = block_select<false>(colg, nullptr, n, 1u, hist, res);
     const double lim = __dsub_rn((double)__uint_as_float(top.key), 0.000001);
     uint32_t consumed = 0, khi = NONE, ge_hi = 0;
     double S1 = 0.0, S2 = 0.0;
     while (true) {
       const uint32_t R = min(consumed + (uint32_t)SOFT_C, (uint32_t)n);
       const uint32_t total = R - consumed;
-      const SelResult lo = block_select<CACHED>(colg, cache, n, R, hist, res);
+      const SelResult lo = block_select<false>(colg, nullptr, n, R, hist, res);
       if (threadIdx.x == 0) misc[0] = 0;
       __syncthreads();
       if (lo.key == khi) {
@@ -1282,7 +1184,7 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
         for (uint32_t q = threadIdx.x; q < total; q += blockDim.x) cand[q] = v;
       } else {
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-          const uint32_t key = col_key<CACHED>(colg, cache, i);
+          const uint32_t key = abs_key(colg[i]);
           if (key > lo.key && key < khi)
             cand[atomicAdd((uint32_t *)&misc[0], 1u)] = __uint_as_float(key);
         }
@@ -1329,7 +1231,7 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
   // reference's double arithmetic.
   if (!have_norm) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const float v = CACHED ? cache[i] : colg[i];
+      const float v = colg[i];
       const double d = (double)fabsf(v) - w;
       if (d > 0.0) {
         const double x = (double)(float)d;
@@ -1347,8 +1249,18 @@ __global__ void __launch_bounds__(SOFT_THREADS, 1) soft_select_kernel(
     return ((d > 0.0) ? (float)d * sgnf(v) : 0.f) * inv;
   };
   uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
-  if (CACHED) {
-    write_column(cache, n, vx, mk, soft);
+  if (sparse) {
+    // every kept entry is a gathered pair: clear the mask, then set the kept
+    for (int wd = threadIdx.x; wd < (ldv >> 5); wd += blockDim.x) mk[wd] = 0u;
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < c_pairs; q += blockDim.x) {
+      const uint32_t i = ~(uint32_t)pairs[q];
+      const float x = soft(__ldg(colg + i));
+      if (x != 0.f) {
+        vx[i] = x;
+        atomicOr(&mk[i >> 5], 1u << (i & 31));
+      }
+    }
   } else {
     write_column_global(colg, n, vx, mk, soft);
   }
@@ -1548,25 +1460,6 @@ cudaError_t dispatch_gemm2(const BatchDev &b, const TensorMaps &tm, const GemmSh
   return dispatch_gemm(b.bn2, b.bk, tm.a2_hi, tm.a2_lo, tm.b2_hi, tm.b2_lo, sh, epi, st);
 }
 
-template <class F1, class F2>
-cudaError_t launch_select(bool cached, size_t smem_fixed, int n, int grid, int threads, F1 kc, F2 kg,
-                          cudaStream_t st, const float *Vraw, int ld, unsigned s, float *vx,
-                          uint32_t *nnz, int *status, uint32_t *vmask, float *hints) {
-  if (cached) {
-    const size_t smem = smem_fixed + ((size_t)n * 4 + 15) / 16 * 16;
-    cudaError_t e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kc<<<grid, threads, smem, st>>>(Vraw, ld, n, s, vx, nnz, status, vmask, hints);
-  } else {
-    cudaError_t e =
-        cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fixed);
-    if (e != cudaSuccess) return e;
-    kg<<<grid, threads, smem_fixed, st>>>(Vraw, ld, n, s, vx, nnz, status, vmask, hints);
-  }
-  return cudaGetLastError();
-}
-
-constexpr size_t SMEM_LIMIT = 227 * 1024;
 
 }  // namespace
 
@@ -1741,15 +1634,15 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
                                                         b.nnz, b.status, b.vmask, b.sel_hint);
       e = cudaGetLastError();
     } else {
-      const bool cached = SoftSmem::FIXED + (size_t)M.n * 4 <= SMEM_LIMIT;
       if (p.l1_mode == 0)
-        e = launch_select(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
-                          soft_select_kernel<true, false>, soft_select_kernel<false, false>, st,
-                          b.Vraw, M.ldn, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint);
+        soft_select_kernel<false><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
+                                                                b.Vx, b.nnz, b.status, b.vmask,
+                                                                b.sel_hint);
       else
-        e = launch_select(cached, SoftSmem::FIXED, M.n, b.k, SOFT_THREADS,
-                          soft_select_kernel<true, true>, soft_select_kernel<false, true>, st,
-                          b.Vraw, M.ldn, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint);
+        soft_select_kernel<true><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
+                                                               b.Vx, b.nnz, b.status, b.vmask,
+                                                               b.sel_hint);
+      e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
     nl++;
