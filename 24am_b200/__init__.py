@@ -40,6 +40,7 @@ FORMULATIONS = {
 
 START_REFERENCE, START_INJECTED = 0, 1
 L1_REFERENCE_SCAN, L1_EXACT = 0, 1
+PRECISION_FP32, PRECISION_MIXED = 0, 1
 
 STATUS = {0: "AM24_OK", 1: "AM24_ERR_INVALID_ARG", 2: "AM24_ERR_OOM", 3: "AM24_ERR_CUDA",
           4: "AM24_ERR_DEVICE_TIMEOUT", 5: "AM24_ERR_UNSUPPORTED", 6: "AM24_ERR_DEGENERATE"}
@@ -58,7 +59,7 @@ class am24_settings(C.Structure):
         ("batch_size", C.c_int32), ("use_otf", C.c_int32), ("use_sort_hard", C.c_int32),
         ("store_all", C.c_int32), ("total_batches", C.c_uint32), ("verbose", C.c_int32),
         ("start_mode", C.c_int32), ("l1_mode", C.c_int32), ("timeout_ms", C.c_uint32),
-        ("reserved", C.c_uint32 * 7),
+        ("precision", C.c_int32), ("stable_iterations", C.c_uint32), ("reserved", C.c_uint32 * 5),
     ]
 
 
@@ -70,7 +71,8 @@ class am24_statistics(C.Structure):
         ("values", C.POINTER(C.c_double)), ("iters", C.POINTER(C.c_int32)),
         ("cardinalities", C.POINTER(C.c_int32)), ("per_start_capacity", C.c_uint32),
         ("explained_variance", C.c_double), ("start_iterations", C.c_uint64),
-        ("degenerate_starts", C.c_int32), ("reserved", C.c_uint32 * 7),
+        ("degenerate_starts", C.c_int32), ("low_precision_iterations", C.c_uint32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 
@@ -104,12 +106,14 @@ _SIGS = {
                                                C.POINTER(C.c_float)]),
     "am24_batch_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "am24_batch_launches_per_step": (C.c_int, [_VP, _VP, C.POINTER(C.c_int32)]),
+    "am24_batch_phase": (C.c_int, [_VP, _VP, C.POINTER(C.c_int32)]),
     "am24_sync": (C.c_int, [_VP]),
     "am24_stream": (C.c_void_p, [_VP]),
     "am24_batch_step_timed": (C.c_int, [_VP, _VP, C.c_int32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
 }
-KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV", "densify"]
+KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV", "densify",
+                "gemm_BtZ_bf16", "support"]
 
 _lib = None
 
@@ -145,7 +149,8 @@ def _ptr(a):
 class OptimizationSettings:
     """Mirror of SolverStructures::OptimizationSettings (reference field names
     and defaults, c++/src/class/optimization_settings.h:71-123), plus the
-    extensions startMode / l1Mode / timeoutMs of this library."""
+    extensions startMode / l1Mode / timeoutMs / precision / stableIterations of
+    this library."""
 
     def __init__(self, **kw):
         self.formulation = L0_constrained_L2_PCA
@@ -163,6 +168,8 @@ class OptimizationSettings:
         self.startMode = START_REFERENCE
         self.l1Mode = L1_REFERENCE_SCAN
         self.timeoutMs = 5000
+        self.precision = PRECISION_FP32
+        self.stableIterations = 5
         for k, v in kw.items():
             if not hasattr(self, k):
                 raise AttributeError(f"OptimizationSettings has no field {k}")
@@ -200,6 +207,8 @@ class OptimizationSettings:
         s.start_mode = int(self.startMode)
         s.l1_mode = int(self.l1Mode)
         s.timeout_ms = int(self.timeoutMs)
+        s.precision = int(self.precision)
+        s.stable_iterations = int(self.stableIterations)
         return s
 
     def from_c(self, s):
@@ -229,6 +238,7 @@ class OptimizationStatistics:
         self.explainedVariance = 0.0
         self.startIterations = 0
         self.degenerateStarts = 0
+        self.lowPrecisionIterations = 0
 
 
 class Solver:
@@ -296,6 +306,7 @@ class Solver:
         stats.explainedVariance = st.explained_variance
         stats.startIterations = st.start_iterations
         stats.degenerateStarts = st.degenerate_starts
+        stats.lowPrecisionIterations = st.low_precision_iterations
         if settings.storeIterationsForAllPoints:
             k = settings.totalStartingPoints
             stats.values = values[:k].tolist()
@@ -429,6 +440,13 @@ class Batch:
             name = KERNEL_KINDS[k & 0xFF] + ("(skipped)" if k & 0x100 else "")
             out.append((name, ms[i]))
         return out
+
+    def refining(self):
+        """False while a MIXED batch steps with BF16 operands, True after it
+        switched to the FP32-accurate products (and always for FP32 batches)."""
+        v = C.c_int32()
+        check(lib().am24_batch_phase(self.matrix.solver.h, self.bh, C.byref(v)))
+        return bool(v.value)
 
     def launches_per_step(self):
         v = C.c_int32()

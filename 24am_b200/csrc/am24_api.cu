@@ -155,6 +155,14 @@ am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat) {
   return AM24_OK;
 }
 
+// MIXED: back to the BF16 phase with no start counted stable (a new batch).
+cudaError_t reset_mixed(const BatchDev &d, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d.stable, 0, sizeof(uint32_t) * d.k, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d.phase, 0, sizeof(uint32_t) * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d.phase + 1, 0xFF, sizeof(uint32_t), st);
+  return e;
+}
+
 // Split-K factor for Z = B V: minimise rounds * (K blocks per unit + fixed
 // per-unit cost) over the persistent grid.
 void choose_splits(int tiles, int kb_total, int sms, int *splits, int *kbps) {
@@ -190,6 +198,8 @@ am24_status validate_settings(const am24_settings *s) {
     return fail(AM24_ERR_INVALID_ARG, "unknown start_mode");
   if (s->l1_mode != AM24_L1_REFERENCE_SCAN && s->l1_mode != AM24_L1_EXACT)
     return fail(AM24_ERR_INVALID_ARG, "unknown l1_mode");
+  if (s->precision != AM24_PRECISION_FP32 && s->precision != AM24_PRECISION_MIXED)
+    return fail(AM24_ERR_INVALID_ARG, "unknown precision");
   return AM24_OK;
 }
 
@@ -317,6 +327,8 @@ void am24_default_settings(am24_settings *s) {
   s->start_mode = AM24_START_REFERENCE;
   s->l1_mode = AM24_L1_REFERENCE_SCAN;
   s->timeout_ms = 5000;
+  s->precision = AM24_PRECISION_FP32;
+  s->stable_iterations = 5;
 }
 
 // chceckInputAndModifyIt (c++/src/class/optimization_settings.h:156-168).
@@ -484,6 +496,10 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (const char *e = getenv("AM24_GEMM_PAIR")) d.pair2 = d.pair2 && atoi(e) != 0;
   d.bf16_2 = d.pair2 && is_l1_variance(settings->formulation);
   if (const char *e = getenv("AM24_GEMM_BF16")) d.bf16_2 = d.bf16_2 && atoi(e) != 0;
+  // MIXED runs its BF16 phase on CTA-pair tiles; narrower batches stay FP32
+  d.mixed = settings->precision == AM24_PRECISION_MIXED && d.pair2;
+  d.k_stable = settings->stable_iterations;
+  const bool need_bf16 = d.bf16_2 || d.mixed;
   const int bk2 = d.pair2 ? PAIR_BK_TF32 : d.bk;  // K box of the TF32 maps of V = B^T Z
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;
   choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
@@ -502,7 +518,9 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
       (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||
       (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.sel_hint, k)) ||
-      (d.bf16_2 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat))))) {
+      (need_bf16 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat)))) ||
+      (d.mixed && ((st = A.get(&d.vmask_prev, (size_t)k * (M.ldn / 32))) ||
+                   (st = A.get(&d.stable, k)) || (st = A.get(&d.phase, 4))))) {
     delete b;
     return st;
   }
@@ -521,6 +539,9 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.max_nnz, 0xFF, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.sel_hint, 0, sizeof(float) * k, h->stream);
   if (!e && d.Z_b) e = cudaMemsetAsync(d.Z_b, 0, sizeof(uint16_t) * kz, h->stream);
+  if (!e && d.mixed)
+    e = cudaMemsetAsync(d.vmask_prev, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
+  if (!e && d.mixed) e = reset_mixed(d, h->stream);
   if (!e) e = cudaMemsetAsync(d.iters, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaMemsetAsync(d.cards, 0xFF, sizeof(int) * d.log_capacity, h->stream);
   if (!e) e = cudaStreamSynchronize(h->stream);
@@ -539,7 +560,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
     delete b;
     return st;
   }
-  if (d.bf16_2) {
+  if (need_bf16) {
     const size_t plane = (size_t)M.n * M.ldm;
     if ((st = make_map_bf16(h, &b->tm.a2_b0, M.Bc_b3, M.m, M.n, M.ldm, BM)) ||
         (st = make_map_bf16(h, &b->tm.a2_b1, M.Bc_b3 + plane, M.m, M.n, M.ldm, BM)) ||
@@ -551,7 +572,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   }
   // a gather over V's non-zeros beats the dense product while they are few
   d.sparse_cap = (uint32_t)std::min(4096, M.n / 32);
-  b->launches = is_constrained(settings->formulation) ? 7 : 6;
+  b->launches = (is_constrained(settings->formulation) ? 7 : 6) + (d.mixed ? 2 : 0);
   *out = b;
   return AM24_OK;
 }
@@ -583,6 +604,7 @@ am24_status am24_batch_load(am24_handle h, am24_batch b, const float *V, int32_t
   // ValueCoordinateHolder::reset (c++/src/utils/various.h:33-38)
   AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
   AM24_CUDA(cudaMemsetAsync(b->d.err, 0, sizeof(float) * k, h->stream));
+  if (b->d.mixed) AM24_CUDA(reset_mixed(b->d, h->stream));
   return AM24_OK;
 }
 
@@ -652,10 +674,12 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
       break;
     }
   int nl = 0, kk[17] = {0};
-  uint32_t gate = 0;
+  uint32_t gate = 0, phase = 1;
   if (st == AM24_OK &&
       cudaMemcpyAsync(&gate, b->d.max_nnz, sizeof gate, cudaMemcpyDeviceToHost, h->stream) ==
           cudaSuccess &&
+      (!b->d.mixed || cudaMemcpyAsync(&phase, b->d.phase, sizeof phase, cudaMemcpyDeviceToHost,
+                                      h->stream) == cudaSuccess) &&
       cudaStreamSynchronize(h->stream) == cudaSuccess) {
     const StepParams p = step_params(b->s, it, 0);
     cudaError_t e = launch_am_step(b->mat->d, b->d, b->tm, p, h->stream, &nl, ev, kk);
@@ -665,12 +689,16 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
   }
   for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
   if (st != AM24_OK) return st;
-  // mark the Z = B V kernels that the gate turned into no-ops
+  // mark the kernels that a gate turned into no-ops: the Z = B V path the
+  // step does not take, and (MIXED) the V = B^T Z of the other phase
   const bool sparse = gate <= b->d.sparse_cap;
   for (int i = 0; i < nl; i++) {
-    const bool skipped = sparse ? (kk[i] == AM24_KERNEL_GEMM_BV || kk[i] == AM24_KERNEL_Z_REDUCE ||
-                                   kk[i] == AM24_KERNEL_DENSIFY)
-                                : (kk[i] == AM24_KERNEL_GATHER_BV);
+    bool skipped = sparse ? (kk[i] == AM24_KERNEL_GEMM_BV || kk[i] == AM24_KERNEL_Z_REDUCE ||
+                             kk[i] == AM24_KERNEL_DENSIFY)
+                          : (kk[i] == AM24_KERNEL_GATHER_BV);
+    if (b->d.mixed)
+      skipped = skipped || (phase == 0 ? kk[i] == AM24_KERNEL_GEMM_BTZ
+                                       : kk[i] == AM24_KERNEL_GEMM_BTZ_BF16);
     kinds[i] = kk[i] | (skipped ? AM24_KERNEL_SKIPPED : 0);
   }
   *count = nl;
@@ -678,6 +706,18 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
 }
 
 void *am24_stream(am24_handle h) { return h ? static_cast<void *>(h->stream) : nullptr; }
+
+am24_status am24_batch_phase(am24_handle h, am24_batch b, int32_t *refining) {
+  if (!h || !b || !refining) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  uint32_t phase = 1;
+  if (b->d.mixed) {
+    AM24_CUDA(cudaMemcpyAsync(&phase, b->d.phase, sizeof phase, cudaMemcpyDeviceToHost,
+                              h->stream));
+    AM24_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  *refining = phase != 0 ? 1 : 0;
+  return AM24_OK;
+}
 
 am24_status am24_batch_launches_per_step(am24_handle h, am24_batch b, int32_t *launches) {
   if (!h || !b || !launches) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
@@ -736,6 +776,7 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
   float best = -1.f;
   uint32_t total_it = 0;
   uint64_t start_its = 0;
+  uint32_t low_its = 0;  // batch iterations in the BF16 phase (MIXED)
   double compute_s = 0.0;
   float last_max_err = 0.f;
   int degenerate = 0;
@@ -757,18 +798,26 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
       host_starts(s, n, start_points, gidx.data(), bs, staging);
       AM24_TRY(upload_columns(h, b, staging.data(), bs, slots.data()));
       AM24_CUDA(cudaMemsetAsync(d.val, 0, sizeof(float) * bs, h->stream));
+      if (d.mixed) AM24_CUDA(reset_mixed(d, h->stream));
+      uint32_t phase = d.mixed ? 0u : 1u;  // the phase the next step runs in
       AM24_CUDA(cudaEventRecord(e0, h->stream));
       int it = 0;
       for (; it < s.max_iter; it++) {
         total_it++;
+        const bool refined = phase != 0;
+        low_its += refined ? 0 : 1;
         const StepParams p = step_params(s, it, (int)shift);
         AM24_CUDA(launch_am_step(M, b->d, b->tm, p, h->stream, &b->launches));
         AM24_CUDA(cudaMemcpyAsync(&last_max_err, d.max_err, sizeof(float), cudaMemcpyDeviceToHost,
                                   h->stream));
+        if (d.mixed)
+          AM24_CUDA(cudaMemcpyAsync(&phase, d.phase, sizeof phase, cudaMemcpyDeviceToHost,
+                                    h->stream));
         AM24_CUDA(cudaStreamSynchronize(h->stream));
         AM24_TRY(check_device_status(b));
         start_its += (uint64_t)bs;
-        if (it > 0 && (double)last_max_err < s.tolerance) break;
+        // MIXED: the tolerance test applies to refinement steps only
+        if (it > 0 && refined && (double)last_max_err < s.tolerance) break;
       }
       AM24_CUDA(cudaEventRecord(e1, h->stream));
       AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * bs, cudaMemcpyDeviceToHost,
@@ -809,15 +858,24 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
     AM24_CUDA(cudaMemsetAsync(d.val, 0, sizeof(float) * bs, h->stream));
     unsigned generated = (unsigned)bs;
     bool go = true;
+    // MIXED: one BF16 phase for the whole run (starts refilled after the switch
+    // run refinement steps only); the tolerance test applies to refinement steps
+    if (d.mixed) AM24_CUDA(reset_mixed(d, h->stream));
+    uint32_t phase = d.mixed ? 0u : 1u;
     AM24_CUDA(cudaEventRecord(e0, h->stream));
     while (go) {
       total_it++;
+      const bool refined = phase != 0;
+      low_its += refined ? 0 : 1;
       const StepParams p = step_params(s, 0, 0);
       AM24_CUDA(launch_am_step(M, b->d, b->tm, p, h->stream, &b->launches));
       AM24_CUDA(cudaMemcpyAsync(err.data(), d.err, sizeof(float) * bs, cudaMemcpyDeviceToHost,
                                 h->stream));
       AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * bs, cudaMemcpyDeviceToHost,
                                 h->stream));
+      if (d.mixed)
+        AM24_CUDA(cudaMemcpyAsync(&phase, d.phase, sizeof phase, cudaMemcpyDeviceToHost,
+                                  h->stream));
       AM24_CUDA(cudaStreamSynchronize(h->stream));
       AM24_TRY(check_device_status(b));
       start_its += (uint64_t)bs;
@@ -825,7 +883,8 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
       int nref = 0;
       for (int i = 0; i < bs; i++) {
         cur[i]++;
-        const bool conv = (double)err[i] < s.tolerance;  // termination_criteria with it = cur > 0
+        // termination_criteria with it = cur > 0
+        const bool conv = refined && (double)err[i] < s.tolerance;
         if (conv || cur[i] >= (unsigned)s.max_iter) {
           if (best < val[i]) {
             best = val[i];
@@ -876,6 +935,7 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
     stats->explained_variance = ev;
     stats->start_iterations = start_its;
     stats->degenerate_starts = degenerate;
+    stats->low_precision_iterations = low_its;
     if (s.store_all && stats->per_start_capacity > 0) {
       const int cap = std::min<int>((int)stats->per_start_capacity, d.log_capacity);
       if (stats->iters)

@@ -45,7 +45,14 @@ struct BatchDev {
   int m_tiles1, n_tiles1, m_tiles2, n_tiles2;
   int pair2;      // V = B^T Z runs on CTA pairs (256-row tiles; B maps of bn2/2 rows)
   int bf16_2;     // ... with the exact BF16 operands of the L1-variance forms
-  uint16_t *Z_b;  // k x ldm BF16 sgn(B V) (L1-variance forms with bf16_2, else null)
+  uint16_t *Z_b;  // k x ldm BF16 Z: sgn(B V) exactly (L1-variance forms with bf16_2),
+                  // or Z rounded to BF16 (MIXED); else null
+  int mixed;             // MIXED precision: single-pass BF16 V = B^T Z until supports settle
+  uint32_t k_stable;     // steps of unchanged support every start needs before refining
+  uint32_t *vmask_prev;  // k x (ldn/32): the previous step's non-zero masks (MIXED)
+  uint32_t *stable;      // per start: consecutive steps with an unchanged support (MIXED)
+  uint32_t *phase;       // [0] 0 = BF16 phase, 1 = refinement (sticky); [1] the step's
+                         // minimum of `stable`; [2] blocks done (MIXED)
   float *Vx;            // k x ldn loadings; entry i of a column is defined only
                         // where its vmask bit is set (zero elsewhere)
   float *V_hi, *V_lo;   // k x ldn dense TF32 hi/lo planes of V: the B operand of the

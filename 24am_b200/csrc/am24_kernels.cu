@@ -48,6 +48,10 @@ __device__ __forceinline__ void split_store(float x, float *hi, float *lo) {
 }
 // sgn with sgn(0) = 0 (c++/src/utils/various.h:44-46)
 __device__ __forceinline__ float sgnf(float v) { return (float)((v > 0.f) - (v < 0.f)); }
+// x rounded to the nearest BF16, as bits.
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
 // sgn(v) as BF16 bits: +1 0x3F80, -1 0xBF80, 0 (and NaN) 0.
 __device__ __forceinline__ uint16_t bf16_sign(float v) {
   return v > 0.f ? (uint16_t)0x3F80u : (v < 0.f ? (uint16_t)0xBF80u : (uint16_t)0u);
@@ -327,6 +331,7 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
     } else {
       acc += (double)y * (double)y;
       split_store(y, zh + i, zl + i);
+      if (MODE == 0 && Zb) Zb[(size_t)j * ldm + i] = bf16_bits(y);
     }
   }
   const double tot = block_sum(acc, red);
@@ -335,6 +340,7 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       const float y = zh[i] + zl[i];  // exact: this thread wrote both planes
       split_store(y * inv, zh + i, zl + i);
+      if (Zb) Zb[(size_t)j * ldm + i] = bf16_bits(y * inv);
     }
   } else if (threadIdx.x == 0) {
     fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
@@ -345,6 +351,34 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
 constexpr int GATHER_THREADS = 256;
 constexpr int GATHER_ROWS = 8;  // samples per thread per pass
 constexpr int GATHER_CAP = 4096;
+
+// MIXED precision bookkeeping, after the step's non-zero masks are written:
+// per start, the number of consecutive steps whose support (non-zero mask)
+// equals the previous step's.  When every start of the batch has kept its
+// support for k_stable steps, phase[0] switches to refinement for good; the
+// last block to finish decides and resets the step's scratch words.
+__global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict__ vmask,
+                                                      const uint32_t *__restrict__ prev, int words,
+                                                      uint32_t *stable, uint32_t *phase,
+                                                      uint32_t k_stable) {
+  const int j = blockIdx.x;
+  const uint32_t *a = vmask + (size_t)j * words, *b = prev + (size_t)j * words;
+  int diff = 0;
+  for (int w = threadIdx.x; w < words; w += blockDim.x) diff |= (a[w] != b[w]);
+  diff = __syncthreads_or(diff);
+  if (threadIdx.x == 0) {
+    const uint32_t st = diff ? 0u : min(stable[j] + 1u, 0x7FFFFFFFu);
+    stable[j] = st;
+    atomicMin(&phase[1], st);
+    __threadfence();
+    if (atomicAdd(&phase[2], 1u) == gridDim.x - 1) {
+      __threadfence();
+      const uint32_t least = atomicExch(&phase[1], 0xFFFFFFFFu);
+      if (least >= k_stable) phase[0] = 1u;
+      phase[2] = 0u;
+    }
+  }
+}
 
 // Z = B V for one start when V's column has few non-zeros: runs instead of
 // gemm1 + z_reduce when the previous step left at most gate_max non-zeros in
@@ -431,6 +465,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
       } else {
         acc += (double)y[r] * (double)y[r];
         if (!(MODE == 2 && one_pass)) split_store(y[r], zh + i, zl + i);
+        if (MODE == 0 && Zb) Zb[(size_t)j * ldm + i] = bf16_bits(y[r]);
       }
     }
   }
@@ -441,12 +476,16 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
 #pragma unroll
       for (int r = 0; r < GATHER_ROWS; r++) {
         const int i = r * GATHER_THREADS + threadIdx.x;
-        if (i < m) split_store(y[r] * inv, zh + i, zl + i);
+        if (i < m) {
+          split_store(y[r] * inv, zh + i, zl + i);
+          if (Zb) Zb[(size_t)j * ldm + i] = bf16_bits(y[r] * inv);
+        }
       }
     } else {
       for (int i = threadIdx.x; i < m; i += GATHER_THREADS) {
         const float v = zh[i] + zl[i];
         split_store(v * inv, zh + i, zl + i);
+        if (Zb) Zb[(size_t)j * ldm + i] = bf16_bits(v * inv);
       }
     }
   } else if (threadIdx.x == 0) {
@@ -1535,6 +1574,10 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     return ev ? cudaEventRecord(ev[nl], st) : cudaSuccess;
   };
   if ((e = cudaMemsetAsync(b.max_err, 0, sizeof(float), st)) != cudaSuccess) return e;
+  if (b.mixed &&  // the support this step starts from, for the stability count
+      (e = cudaMemcpyAsync(b.vmask_prev, b.vmask, sizeof(uint32_t) * (size_t)b.k * (M.ldn / 32),
+                           cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+    return e;
   // 1. Z = B V (split-K partials)
   GemmShape g1;
   g1.M = M.m;
@@ -1548,8 +1591,9 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g1.num_units = g1.splits * g1.m_tiles * g1.n_tiles;
   g1.timeout_ns = p.timeout_ns;
   g1.status = b.status;
-  g1.gate = b.max_nnz;
-  g1.gate_max = b.sparse_cap;
+  g1.gate = b.max_nnz;  // dense steps only
+  g1.gate_min = b.sparse_cap + 1;
+  g1.gate_max = 0xFFFFFFFFu;
   const int mode = is_l1_variance(f) ? 1 : (is_constrained(f) ? 0 : 2);
   // 1a. sparse V (every column <= sparse_cap non-zeros last step): gather
   if ((e = mark(5)) != cudaSuccess) return e;
@@ -1608,24 +1652,45 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g2.timeout_ns = p.timeout_ns;
   g2.status = b.status;
   g2.gate = nullptr;
+  g2.gate_min = 0;
   g2.gate_max = 0;
   const int parts = b.m_tiles2 * 4;
-  if ((e = mark(2)) != cudaSuccess) return e;
+  // MIXED: the single-pass BF16 product runs while phase[0] == 0, the
+  // FP32-accurate one from then on; each launch returns at once in the other phase
+  auto gemm2 = [&](const auto &epi) -> cudaError_t {
+    cudaError_t e2;
+    if (b.mixed) {
+      GemmShape gl = g2;
+      gl.gate = b.phase;
+      gl.gate_min = 0;
+      gl.gate_max = 0;
+      if ((e2 = mark(7)) != cudaSuccess) return e2;
+      if ((e2 = run_gemm_pair<PairBF16x1, 256, 12>(tm.a2_b0, tm.b2_b, tm.a2_b0, tm.b2_b, gl, epi,
+                                                   st)) != cudaSuccess)
+        return e2;
+      nl++;
+      g2.gate = b.phase;
+      g2.gate_min = 1;
+      g2.gate_max = 0xFFFFFFFFu;
+    }
+    if ((e2 = mark(2)) != cudaSuccess) return e2;
+    if ((e2 = dispatch_gemm2(b, tm, g2, epi, is_l1_variance(f), st)) != cudaSuccess) return e2;
+    nl++;
+    return cudaSuccess;
+  };
   if (is_constrained(f)) {
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
-    e = dispatch_gemm2(b, tm, g2, er, is_l1_variance(f), st);
+    e = gemm2(er);
   } else if (is_l1_penalized(f)) {
     EpiPenalty<true> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
-                        (float)p.penalty,
-                        b.vmask};
-    e = dispatch_gemm2(b, tm, g2, pe, is_l1_variance(f), st);
+                        (float)p.penalty, b.vmask};
+    e = gemm2(pe);
   } else {
     EpiPenalty<false> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
                          (float)p.penalty, b.vmask};
-    e = dispatch_gemm2(b, tm, g2, pe, is_l1_variance(f), st);
+    e = gemm2(pe);
   }
   if (e != cudaSuccess) return e;
-  nl++;
   // 4. constrained: selection / projection + normalisation
   if (is_constrained(f)) {
     if ((e = mark(3)) != cudaSuccess) return e;
@@ -1645,6 +1710,14 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
+    nl++;
+  }
+  // 4b. MIXED: support stability and the phase switch
+  if (b.mixed) {
+    if ((e = mark(8)) != cudaSuccess) return e;
+    support_kernel<<<b.k, 256, 0, st>>>(b.vmask, b.vmask_prev, M.ldn / 32, b.stable, b.phase,
+                                        b.k_stable);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     nl++;
   }
   // 5. finalize

@@ -62,8 +62,9 @@ __device__ __forceinline__ Unit decode_pair_unit(const GemmShape &s, int u, int 
   return r;
 }
 
-// Operand schemes.  NA + NB = 4 planes, passed as the kernel's four tensor maps
-// (A planes first); BK = K elements per 64-byte shared-memory row.
+// Operand schemes.  NA + NB <= 4 planes, passed as the kernel's first tensor
+// maps (A planes first; the others are not read); BK = K elements per 64-byte
+// shared-memory row.
 struct PairTF32x3 {
   static constexpr int NA = 2, NB = 2, BK = PAIR_BK_TF32;
   // K elements per TMEM chunk before the FP32 promotion: 48 MMAs accumulate
@@ -109,6 +110,25 @@ struct PairBF16x3A {
   static constexpr uint32_t FMT = 1u;
 };
 
+// Single-pass BF16 operands (A = b0 of the split, B = Z rounded to BF16) for
+// the low-precision phase of the mixed mode: one MMA per 16 K elements, a
+// work unit accumulated whole in tensor memory (no intermediate promotion).
+struct PairBF16x1 {
+  static constexpr int NA = 1, NB = 1, BK = PAIR_BK_BF16;
+  static constexpr int PROMO_K = 1 << 20;
+  template <uint32_t ID>
+  __device__ static void k_block(uint32_t d, const uint32_t (&a)[1], const uint32_t (&b)[1],
+                                 uint32_t sbo, bool first) {
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+      const uint32_t off = kk * 32;
+      mma_bf16_pair(d, sdesc_kmajor(a[0] + off, sbo, 4u), sdesc_kmajor(b[0] + off, sbo, 4u), ID,
+                    (first && kk == 0) ? 0u : 1u);
+    }
+  }
+  static constexpr uint32_t FMT = 1u;
+};
+
 template <class S, int BN, int STAGES>
 struct PairSmem {
   static constexpr int ROW = 64;  // bytes of K per shared-memory row
@@ -129,7 +149,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
                      const __grid_constant__ CUtensorMap tm3, const GemmShape shape, Epi epi) {
   using L = PairSmem<S, BN, STAGES>;
   constexpr int BK = S::BK;
-  static_assert(S::NA + S::NB == 4, "four operand planes");
+  static_assert(S::NA + S::NB <= 4, "at most four operand planes");
   static_assert(BN % 32 == 0 && BN >= 64 && BN <= 256, "BN must be a multiple of 32 in [64,256]");
   constexpr uint32_t SBO = L::ROW * 8;  // bytes between 8-row core-matrix groups
   constexpr uint32_t TMEM_COLS = (2 * BN <= 128) ? 128 : (2 * BN <= 256) ? 256 : 512;
@@ -150,7 +170,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  if (shape.gate && *shape.gate <= shape.gate_max) return;  // uniform over the grid
+  if (shape.gate && (*shape.gate < shape.gate_min || *shape.gate > shape.gate_max))
+    return;  // uniform over the grid
   const int rank = static_cast<int>(cluster_ctarank());
   const int pair = blockIdx.x >> 1;
   const int pairs = gridDim.x >> 1;

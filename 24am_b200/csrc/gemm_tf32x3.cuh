@@ -55,10 +55,10 @@ struct GemmShape {
   int num_units;     // splits * m_tiles * n_tiles
   unsigned long long timeout_ns;
   int *status;
-  // Optional gate: when gate != nullptr and *gate <= gate_max the launch does
-  // nothing (another kernel of the step covers the work).
+  // Optional gate: when gate != nullptr the launch does its work only if
+  // gate_min <= *gate <= gate_max (otherwise another kernel of the step covers it).
   const uint32_t *gate;
-  uint32_t gate_max;
+  uint32_t gate_min, gate_max;
 };
 
 // One work unit as an epilogue sees it: rows [m0, m0 + 128) of C (this CTA's
@@ -129,7 +129,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  if (shape.gate && *shape.gate <= shape.gate_max) return;  // uniform over the grid
+  if (shape.gate && (*shape.gate < shape.gate_min || *shape.gate > shape.gate_max))
+    return;  // uniform over the grid
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {

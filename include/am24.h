@@ -55,6 +55,16 @@ typedef enum {
   AM24_L1_PENALIZED_L1_PCA = 7
 } am24_formulation;
 
+/* Arithmetic of the two products (an extension: the reference computes in F).
+ * FP32: FP32-accurate products every iteration (3xTF32, or an exact BF16 split
+ * where the operand allows).  MIXED: single-pass BF16 operands with FP32
+ * accumulation while the supports settle, then the FP32-accurate products from
+ * the first iteration after which every start of the batch has kept the same
+ * support for stable_iterations iterations; the tolerance test applies only from
+ * then on.  MIXED needs batches of more than 128 starts (CTA-pair tiles); smaller
+ * batches run FP32 throughout. */
+typedef enum { AM24_PRECISION_FP32 = 0, AM24_PRECISION_MIXED = 1 } am24_precision;
+
 /* How starting points are produced. */
 typedef enum {
   AM24_START_REFERENCE = 0, /* the reference generator: rand_r seeded with the global
@@ -90,7 +100,11 @@ typedef struct {
   int32_t start_mode;      /* am24_start_mode (default AM24_START_REFERENCE) */
   int32_t l1_mode;         /* am24_l1_mode (default AM24_L1_REFERENCE_SCAN) */
   uint32_t timeout_ms;     /* bound on any device-side wait (default 5000) */
-  uint32_t reserved[7];
+  int32_t precision;       /* am24_precision (default AM24_PRECISION_FP32) */
+  uint32_t stable_iterations; /* AM24_PRECISION_MIXED: iterations every start's
+                                 support must stay unchanged before refinement
+                                 (default 5) */
+  uint32_t reserved[5];
 } am24_settings;
 
 /* Mirror of OptimizationStatistics (c++/src/class/optimization_statistics.h:27-46).
@@ -113,7 +127,8 @@ typedef struct {
   double explained_variance;  /* ||B x||_2^2 of the returned x, FP64 on the device */
   uint64_t start_iterations;  /* AM steps summed over starting points */
   int32_t degenerate_starts;  /* starts whose final objective was NaN */
-  uint32_t reserved[7];
+  uint32_t low_precision_iterations; /* batch iterations run with BF16 operands */
+  uint32_t reserved[6];
 } am24_statistics;
 
 typedef struct am24_handle_s *am24_handle;
@@ -190,6 +205,10 @@ am24_status am24_batch_read(am24_handle h, am24_batch b, float *V, float *val, f
 #define AM24_STATIC_WS_BYTES (16u << 20)
 am24_status am24_batch_iterate_static_ws(am24_handle h, am24_batch b, int32_t it0,
                                          int32_t iterations, float *max_error);
+/* AM24_PRECISION_MIXED batches: *refining = 1 once the batch has switched to
+ * the FP32-accurate products (0 while its steps use BF16 operands); FP32
+ * batches report 1.  Synchronizes the handle's stream. */
+am24_status am24_batch_phase(am24_handle h, am24_batch b, int32_t *refining);
 /* Number of kernel launches one am24_batch_iterate step issues. */
 am24_status am24_batch_launches_per_step(am24_handle h, am24_batch b, int32_t *launches);
 /* Synchronizes the handle's stream. */
@@ -207,6 +226,8 @@ typedef enum {
   AM24_KERNEL_FINALIZE = 4,  /* per-start objective, change, logs, batch maximum */
   AM24_KERNEL_GATHER_BV = 5, /* Z = B V as a gather over V's non-zeros (sparse steps) */
   AM24_KERNEL_DENSIFY = 6,   /* dense TF32 hi/lo planes of V for the tensor-core Z = B V */
+  AM24_KERNEL_GEMM_BTZ_BF16 = 7, /* V = B^T Z with single-pass BF16 operands (MIXED) */
+  AM24_KERNEL_SUPPORT = 8,   /* support-stability count and phase switch (MIXED) */
   AM24_KERNEL_SKIPPED = 0x100 /* or-ed into a kind: the launch returned at once */
 } am24_kernel_kind;
 /* One AM step like am24_batch_iterate(h, b, it, 1, NULL), with a CUDA event

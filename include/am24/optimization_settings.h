@@ -3,7 +3,8 @@
  * reference's member names, types and defaults
  * (c++/src/class/optimization_settings.h:27-170), so code written against the
  * reference compiles unchanged.  Extra members (startMode, l1Mode, timeoutMs,
- * device) select this library's options and default to reference behaviour.
+ * precision, stableIterations, device) select this library's options and
+ * default to reference behaviour.
  */
 #ifndef AM24_OPTIMIZATION_SETTINGS_H
 #define AM24_OPTIMIZATION_SETTINGS_H
@@ -62,6 +63,8 @@ class OptimizationSettings {
   int startMode;       // 0: reference generator (rand_r per start index), 1: injected
   int l1Mode;          // 0: the reference's L1-ball scan, 1: exact projection
   unsigned timeoutMs;  // bound on any device-side wait
+  int precision;       // 0: FP32-accurate products, 1: BF16 until supports settle, then FP32
+  unsigned stableIterations;  // precision 1: iterations of unchanged supports before refining
   int device;          // CUDA device of the default handle
 
   OptimizationSettings()
@@ -73,6 +76,7 @@ class OptimizationSettings {
         storeIterationsForAllPoints(false), maximumIterations(20), totalStartingPoints(64),
         batchSize(64), totalBatches(0), useOTF(false), doColumnMean(true), doRowMean(false),
         L2RowNormalization(true), tfidf(true), startMode(0), l1Mode(0), timeoutMs(5000),
+        precision(0), stableIterations(5),
         device(0) {}
 
   bool isConstrainedProblem() const { return (int)formulation <= 3; }

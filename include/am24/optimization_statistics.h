@@ -24,9 +24,11 @@ class OptimizationStatistics {
   double explainedVariance;          // ||B x||^2 of the returned x, FP64
   unsigned long long startIterations;
   int degenerateStarts;
+  unsigned lowPrecisionIterations;  // batch iterations with BF16 operands (precision 1)
   OptimizationStatistics()
       : it(0), fval(0), error(0), totalTrueComputationTime(0), totalElapsedTime(0), n(0),
-        totalThreadsUsed(1), explainedVariance(0), startIterations(0), degenerateStarts(0) {}
+        totalThreadsUsed(1), explainedVariance(0), startIterations(0), degenerateStarts(0),
+        lowPrecisionIterations(0) {}
 };
 }  // namespace SolverStructures
 #endif

@@ -52,6 +52,8 @@ inline void to_c(const SolverStructures::OptimizationSettings &o, am24_settings 
   s->start_mode = o.startMode;
   s->l1_mode = o.l1Mode;
   s->timeout_ms = o.timeoutMs;
+  s->precision = o.precision;
+  s->stable_iterations = o.stableIterations;
 }
 
 inline void from_c(const am24_settings &s, SolverStructures::OptimizationSettings *o) {
@@ -105,6 +107,7 @@ inline float solve_f32(const float *B, int ldB, float *x, unsigned m, unsigned n
   st->explainedVariance = cs.explained_variance;
   st->startIterations = cs.start_iterations;
   st->degenerateStarts = cs.degenerate_starts;
+  st->lowPrecisionIterations = cs.low_precision_iterations;
   return f;
 }
 
