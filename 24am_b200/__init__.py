@@ -59,7 +59,8 @@ class am24_settings(C.Structure):
         ("batch_size", C.c_int32), ("use_otf", C.c_int32), ("use_sort_hard", C.c_int32),
         ("store_all", C.c_int32), ("total_batches", C.c_uint32), ("verbose", C.c_int32),
         ("start_mode", C.c_int32), ("l1_mode", C.c_int32), ("timeout_ms", C.c_uint32),
-        ("precision", C.c_int32), ("stable_iterations", C.c_uint32), ("reserved", C.c_uint32 * 5),
+        ("precision", C.c_int32), ("stable_iterations", C.c_uint32), ("stable_share", C.c_float),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 
@@ -149,8 +150,8 @@ def _ptr(a):
 class OptimizationSettings:
     """Mirror of SolverStructures::OptimizationSettings (reference field names
     and defaults, c++/src/class/optimization_settings.h:71-123), plus the
-    extensions startMode / l1Mode / timeoutMs / precision / stableIterations of
-    this library."""
+    extensions startMode / l1Mode / timeoutMs / precision / stableIterations /
+    stableShare of this library."""
 
     def __init__(self, **kw):
         self.formulation = L0_constrained_L2_PCA
@@ -170,6 +171,7 @@ class OptimizationSettings:
         self.timeoutMs = 5000
         self.precision = PRECISION_FP32
         self.stableIterations = 5
+        self.stableShare = 1.0
         for k, v in kw.items():
             if not hasattr(self, k):
                 raise AttributeError(f"OptimizationSettings has no field {k}")
@@ -209,6 +211,7 @@ class OptimizationSettings:
         s.timeout_ms = int(self.timeoutMs)
         s.precision = int(self.precision)
         s.stable_iterations = int(self.stableIterations)
+        s.stable_share = float(self.stableShare)
         return s
 
     def from_c(self, s):

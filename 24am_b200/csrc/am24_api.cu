@@ -159,7 +159,6 @@ am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat) {
 cudaError_t reset_mixed(const BatchDev &d, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(d.stable, 0, sizeof(uint32_t) * d.k, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d.phase, 0, sizeof(uint32_t) * 4, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d.phase + 1, 0xFF, sizeof(uint32_t), st);
   return e;
 }
 
@@ -200,6 +199,8 @@ am24_status validate_settings(const am24_settings *s) {
     return fail(AM24_ERR_INVALID_ARG, "unknown l1_mode");
   if (s->precision != AM24_PRECISION_FP32 && s->precision != AM24_PRECISION_MIXED)
     return fail(AM24_ERR_INVALID_ARG, "unknown precision");
+  if (s->precision == AM24_PRECISION_MIXED && !(s->stable_share > 0.f && s->stable_share <= 1.f))
+    return fail(AM24_ERR_INVALID_ARG, "stable_share must be in (0, 1]");
   return AM24_OK;
 }
 
@@ -329,6 +330,7 @@ void am24_default_settings(am24_settings *s) {
   s->timeout_ms = 5000;
   s->precision = AM24_PRECISION_FP32;
   s->stable_iterations = 5;
+  s->stable_share = 1.0f;
 }
 
 // chceckInputAndModifyIt (c++/src/class/optimization_settings.h:156-168).
@@ -499,6 +501,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   // MIXED runs its BF16 phase on CTA-pair tiles; narrower batches stay FP32
   d.mixed = settings->precision == AM24_PRECISION_MIXED && d.pair2;
   d.k_stable = settings->stable_iterations;
+  d.need_stable = (uint32_t)std::max(1.0, std::ceil((double)settings->stable_share * k - 1e-9));
+  d.need_stable = std::min(d.need_stable, (uint32_t)k);
   const bool need_bf16 = d.bf16_2 || d.mixed;
   const int bk2 = d.pair2 ? PAIR_BK_TF32 : d.bk;  // K box of the TF32 maps of V = B^T Z
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;

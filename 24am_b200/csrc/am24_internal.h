@@ -48,11 +48,12 @@ struct BatchDev {
   uint16_t *Z_b;  // k x ldm BF16 Z: sgn(B V) exactly (L1-variance forms with bf16_2),
                   // or Z rounded to BF16 (MIXED); else null
   int mixed;             // MIXED precision: single-pass BF16 V = B^T Z until supports settle
-  uint32_t k_stable;     // steps of unchanged support every start needs before refining
+  uint32_t k_stable;     // steps of unchanged support a start needs ...
+  uint32_t need_stable;  // ... in this many starts before the batch refines
   uint32_t *vmask_prev;  // k x (ldn/32): the previous step's non-zero masks (MIXED)
   uint32_t *stable;      // per start: consecutive steps with an unchanged support (MIXED)
   uint32_t *phase;       // [0] 0 = BF16 phase, 1 = refinement (sticky); [1] the step's
-                         // minimum of `stable`; [2] blocks done (MIXED)
+                         // count of stable starts; [2] blocks done (MIXED)
   float *Vx;            // k x ldn loadings; entry i of a column is defined only
                         // where its vmask bit is set (zero elsewhere)
   float *V_hi, *V_lo;   // k x ldn dense TF32 hi/lo planes of V: the B operand of the

@@ -354,13 +354,13 @@ constexpr int GATHER_CAP = 4096;
 
 // MIXED precision bookkeeping, after the step's non-zero masks are written:
 // per start, the number of consecutive steps whose support (non-zero mask)
-// equals the previous step's.  When every start of the batch has kept its
-// support for k_stable steps, phase[0] switches to refinement for good; the
-// last block to finish decides and resets the step's scratch words.
+// equals the previous step's.  When at least `need` starts of the batch have
+// kept their support for k_stable steps, phase[0] switches to refinement for
+// good; the last block to finish decides and resets the step's scratch words.
 __global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict__ vmask,
                                                       const uint32_t *__restrict__ prev, int words,
                                                       uint32_t *stable, uint32_t *phase,
-                                                      uint32_t k_stable) {
+                                                      uint32_t k_stable, uint32_t need) {
   const int j = blockIdx.x;
   const uint32_t *a = vmask + (size_t)j * words, *b = prev + (size_t)j * words;
   int diff = 0;
@@ -369,12 +369,12 @@ __global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict
   if (threadIdx.x == 0) {
     const uint32_t st = diff ? 0u : min(stable[j] + 1u, 0x7FFFFFFFu);
     stable[j] = st;
-    atomicMin(&phase[1], st);
+    if (st >= k_stable) atomicAdd(&phase[1], 1u);
     __threadfence();
     if (atomicAdd(&phase[2], 1u) == gridDim.x - 1) {
       __threadfence();
-      const uint32_t least = atomicExch(&phase[1], 0xFFFFFFFFu);
-      if (least >= k_stable) phase[0] = 1u;
+      const uint32_t count = atomicExch(&phase[1], 0u);
+      if (count >= need) phase[0] = 1u;
       phase[2] = 0u;
     }
   }
@@ -1716,7 +1716,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (b.mixed) {
     if ((e = mark(8)) != cudaSuccess) return e;
     support_kernel<<<b.k, 256, 0, st>>>(b.vmask, b.vmask_prev, M.ldn / 32, b.stable, b.phase,
-                                        b.k_stable);
+                                        b.k_stable, b.need_stable);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     nl++;
   }

@@ -44,7 +44,13 @@ SIZES = {  # (n samples, p features, rank, nnz per loading, starts)
     "config1": (2000, 50000, 50, 256, 1024),
     # profiling case: same kernels, B planes 262 MB (> L2), a few GB on the device
     "small": (2000, 8192, 50, 256, 1024),
+    # mixed-precision workload (whole solves, --mode solve): s = 128
+    "config2": (8192, 65536, 100, 512, 4096),
 }
+SIZE_S = {"config1": 16, "small": 16, "config2": 128}
+# gamma = factor x the largest column norm: at n = 8192 samples, 0.1 x the
+# largest column 1-norm lies above every loading and empties every support
+SIZE_GAMMA = {"config1": 0.1, "small": 0.1, "config2": 0.025}
 N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = SIZES["config1"]
 S_CONS, GAMMA_C, SEED = 16, 0.1, 1
 E2E_MAX_IT, E2E_TOL = 200, 1e-6
@@ -210,6 +216,67 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------ GPU arm
+def run_solves(args):
+    """Whole solves on one GPU (resident matrix, injected seeded starts, one batch
+    of all starts, maxIter 200, tol 1e-6), each formulation in FP32 and in MIXED
+    precision.  start-iterations/s from the library's CUDA-event time of the
+    iterations; the best explained variance ||B x||^2 is evaluated in FP64 on the
+    device, and the line gives MIXED's relative difference from FP32's."""
+    import numpy as np
+    import torch
+    am = importlib.import_module("24am_b200")
+    wl = am.workloads
+    solver = am.Solver(0)
+    Dt = wl.low_rank_data_torch(N_SAMPLES, P_FEATURES, RANK, NNZ_V, SEED)
+    col2 = float(Dt.double().norm(dim=1).max())
+    col1 = float(Dt.double().abs().sum(dim=1).max())
+    gam = wl.penalty_gammas(col2, col1, GAMMA_C)
+    torch.cuda.synchronize()
+    M = am.Matrix(solver, None, on_device_ptr=Dt.data_ptr(), m=N_SAMPLES, n=P_FEATURES,
+                  ldB=N_SAMPLES)
+    forms = [int(x) for x in args.formulations.split(",")]
+    res = {}
+    tot = {"fp32": [0, 0.0], "mixed": [0, 0.0]}
+    for f in forms:
+        V = wl.uniform_starts_torch(P_FEATURES, STARTS, seed=1000 + SEED + f).cpu().numpy()
+        V = np.asfortranarray(V.T)  # p x k column-major
+        row = {}
+        for name, prec in (("fp32", am.PRECISION_FP32), ("mixed", am.PRECISION_MIXED)):
+            st = am.OptimizationSettings(formulation=f, constraintParameter=S_CONS,
+                                         penaltyParameter=gam.get(f, 0.0), tolerance=E2E_TOL,
+                                         maximumIterations=E2E_MAX_IT, totalStartingPoints=STARTS,
+                                         batchSize=STARTS, startMode=am.START_INJECTED,
+                                         precision=prec)
+            _, fval, s = M.solve(st, start_points=V)
+            row[name] = {"start_it_per_s": s.start_iterations / s.total_true_computation_time,
+                         "iterations": int(s.it), "bf16_iterations": int(s.low_precision_iterations),
+                         "seconds": s.total_true_computation_time, "fval": fval,
+                         "explained_variance": s.explained_variance}
+            tot[name][0] += int(s.start_iterations)
+            tot[name][1] += s.total_true_computation_time
+        ev32, evmx = row["fp32"]["explained_variance"], row["mixed"]["explained_variance"]
+        row["ev_rel_diff"] = abs(evmx - ev32) / ev32
+        res[str(f)] = row
+    v32 = tot["fp32"][0] / tot["fp32"][1]
+    vmx = tot["mixed"][0] / tot["mixed"][1]
+    line = {"metric": "start-iterations/s (whole solves to tol)", "value": vmx,
+            "unit": "start-it/s", "n_gpus": 1, "higher_is_better": True, "dtype": "bf16+f32",
+            "data": "synthetic",
+            "config": {"workload": f"mixed precision solves: n={N_SAMPLES} x p={P_FEATURES} "
+                                   f"(r={RANK}, {NNZ_V} nnz/loading), k={STARTS} starts, "
+                                   f"s={S_CONS}, gamma {GAMMA_C} x max column norm, "
+                                   f"formulations {forms}, maxIter {E2E_MAX_IT}, tol {E2E_TOL}",
+                       "precision": "MIXED: single-pass BF16 V = B^T Z until every start's "
+                                    "support is unchanged for 5 iterations, then FP32-accurate"},
+            "fp32_value": v32, "speedup_vs_fp32": vmx / v32,
+            "max_ev_rel_diff": max(r["ev_rel_diff"] for r in res.values()),
+            "formulations": res}
+    print(json.dumps(line), flush=True)
+    M.close()
+    solver.close()
+    return 0
+
+
 def kernel_label(kind, f):
     """Bench name of a step kernel of formulation f: V = B^T Z by operand scheme
     (BF16 for the L1-variance forms 1, 3, 5, 7 on CTA pairs, else 3xTF32) and
@@ -417,15 +484,25 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--size", default="config1", choices=sorted(SIZES))
-    ap.add_argument("--formulations", default="0,1,2,3,4,5,6,7",
-                    help="subset for profiling runs; the headline uses all 8")
+    ap.add_argument("--formulations", default=None,
+                    help="subset for profiling runs; the headline uses all 8 "
+                         "(config2: 0 and 7, its two forms)")
+    ap.add_argument("--mode", default="step", choices=["step", "solve"],
+                    help="step: the AM-step throughput line; solve: whole solves to tol, "
+                         "FP32 and MIXED precision from the same starts")
     args = ap.parse_args()
-    global N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS
+    global N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS, S_CONS, GAMMA_C
     N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = SIZES[args.size]
+    S_CONS = SIZE_S[args.size]
+    GAMMA_C = SIZE_GAMMA[args.size]
+    if args.formulations is None:
+        args.formulations = "0,7" if args.size == "config2" else "0,1,2,3,4,5,6,7"
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.mode == "solve":
+        return run_solves(args)
     return run_ours(args)
 
 

@@ -59,10 +59,10 @@ typedef enum {
  * FP32: FP32-accurate products every iteration (3xTF32, or an exact BF16 split
  * where the operand allows).  MIXED: single-pass BF16 operands with FP32
  * accumulation while the supports settle, then the FP32-accurate products from
- * the first iteration after which every start of the batch has kept the same
- * support for stable_iterations iterations; the tolerance test applies only from
- * then on.  MIXED needs batches of more than 128 starts (CTA-pair tiles); smaller
- * batches run FP32 throughout. */
+ * the first iteration after which a share stable_share of the batch's starts
+ * has kept the same support for stable_iterations iterations; the tolerance
+ * test applies only from then on.  MIXED needs batches of more than 128 starts
+ * (CTA-pair tiles); smaller batches run FP32 throughout. */
 typedef enum { AM24_PRECISION_FP32 = 0, AM24_PRECISION_MIXED = 1 } am24_precision;
 
 /* How starting points are produced. */
@@ -101,10 +101,11 @@ typedef struct {
   int32_t l1_mode;         /* am24_l1_mode (default AM24_L1_REFERENCE_SCAN) */
   uint32_t timeout_ms;     /* bound on any device-side wait (default 5000) */
   int32_t precision;       /* am24_precision (default AM24_PRECISION_FP32) */
-  uint32_t stable_iterations; /* AM24_PRECISION_MIXED: iterations every start's
-                                 support must stay unchanged before refinement
-                                 (default 5) */
-  uint32_t reserved[5];
+  uint32_t stable_iterations; /* AM24_PRECISION_MIXED: iterations a start's
+                                 support must stay unchanged (default 5) ... */
+  float stable_share;         /* ... in this share of the batch's starts before the
+                                 batch refines (default 1: every start) */
+  uint32_t reserved[4];
 } am24_settings;
 
 /* Mirror of OptimizationStatistics (c++/src/class/optimization_statistics.h:27-46).

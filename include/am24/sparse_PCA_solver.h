@@ -54,6 +54,7 @@ inline void to_c(const SolverStructures::OptimizationSettings &o, am24_settings 
   s->timeout_ms = o.timeoutMs;
   s->precision = o.precision;
   s->stable_iterations = o.stableIterations;
+  s->stable_share = o.stableShare;
 }
 
 inline void from_c(const am24_settings &s, SolverStructures::OptimizationSettings *o) {

@@ -71,3 +71,29 @@ def test_no_gpu_fails_loudly(am):
         pytest.skip("a GPU is present")
     with pytest.raises(am.Am24Error):
         am.Solver(0)
+
+
+def test_struct_layouts_match_the_header(am, tmp_path):
+    """The ctypes mirrors of am24_settings / am24_statistics have the C layout
+    (offsets of every field, and the size), compiled from include/am24.h."""
+    import ctypes as C
+    import os
+    import subprocess
+    structs = {"am24_settings": am.am24_settings, "am24_statistics": am.am24_statistics}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "am24.h"', 'int main(void) {']
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-I", inc, "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in out.splitlines():
+        cname, field, value = line.split()
+        py = structs[cname]
+        got = C.sizeof(py) if field == "size" else getattr(py, field).offset
+        assert got == int(value), (cname, field, got, value)
