@@ -286,6 +286,7 @@ am24_status upload_columns(am24_handle h, am24_batch b, const float *host, int c
   }
   // new starts are dense: the next Z = B V runs on the tensor cores
   AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));
+  AM24_CUDA(cudaMemsetAsync(b->d.planes_nnz, 0, sizeof(uint32_t), h->stream));  // stale planes
   return AM24_OK;
 }
 
@@ -521,7 +522,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.val, k)) || (st = A.get(&d.err, k)) || (st = A.get(&d.max_err, 1)) ||
       (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
       (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||
-      (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.sel_hint, k)) ||
+      (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.planes_nnz, 1)) ||
+      (st = A.get(&d.sel_hint, k)) ||
       (need_bf16 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat)))) ||
       (d.mixed && ((st = A.get(&d.vmask_prev, (size_t)k * (M.ldn / 32))) ||
                    (st = A.get(&d.stable, k)) || (st = A.get(&d.phase, 4))))) {
@@ -541,6 +543,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.status, 0, sizeof(int), h->stream);
   if (!e) e = cudaMemsetAsync(d.vmask, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
   if (!e) e = cudaMemsetAsync(d.max_nnz, 0xFF, sizeof(uint32_t), h->stream);
+  if (!e) e = cudaMemsetAsync(d.planes_nnz, 0, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.sel_hint, 0, sizeof(float) * k, h->stream);
   if (!e && d.Z_b) e = cudaMemsetAsync(d.Z_b, 0, sizeof(uint16_t) * kz, h->stream);
   if (!e && d.mixed)
@@ -604,6 +607,7 @@ am24_status am24_batch_load(am24_handle h, am24_batch b, const float *V, int32_t
   }
   AM24_CUDA(launch_load_columns(b->d.Vraw, M.ldn, M.n, k, b->d.Vx, M.ldn, b->d.vmask, h->stream));
   AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));  // dense starts
+  AM24_CUDA(cudaMemsetAsync(b->d.planes_nnz, 0, sizeof(uint32_t), h->stream));  // stale planes
   AM24_CUDA(cudaMemsetAsync(b->d.sel_hint, 0, sizeof(float) * k, h->stream));      // no hints
   // ValueCoordinateHolder::reset (c++/src/utils/various.h:33-38)
   AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
@@ -678,10 +682,12 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
       break;
     }
   int nl = 0, kk[17] = {0};
-  uint32_t gate = 0, phase = 1;
+  uint32_t gate = 0, phase = 1, planes = 0;
   if (st == AM24_OK &&
       cudaMemcpyAsync(&gate, b->d.max_nnz, sizeof gate, cudaMemcpyDeviceToHost, h->stream) ==
           cudaSuccess &&
+      cudaMemcpyAsync(&planes, b->d.planes_nnz, sizeof planes, cudaMemcpyDeviceToHost,
+                      h->stream) == cudaSuccess &&
       (!b->d.mixed || cudaMemcpyAsync(&phase, b->d.phase, sizeof phase, cudaMemcpyDeviceToHost,
                                       h->stream) == cudaSuccess) &&
       cudaStreamSynchronize(h->stream) == cudaSuccess) {
@@ -699,7 +705,8 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
   for (int i = 0; i < nl; i++) {
     bool skipped = sparse ? (kk[i] == AM24_KERNEL_GEMM_BV || kk[i] == AM24_KERNEL_Z_REDUCE ||
                              kk[i] == AM24_KERNEL_DENSIFY)
-                          : (kk[i] == AM24_KERNEL_GATHER_BV);
+                          : (kk[i] == AM24_KERNEL_GATHER_BV ||
+                             (kk[i] == AM24_KERNEL_DENSIFY && planes > b->d.sparse_cap));
     if (b->d.mixed)
       skipped = skipped || (phase == 0 ? kk[i] == AM24_KERNEL_GEMM_BTZ
                                        : kk[i] == AM24_KERNEL_GEMM_BTZ_BF16);

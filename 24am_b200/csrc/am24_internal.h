@@ -69,6 +69,9 @@ struct BatchDev {
   uint32_t *vmask;      // k x (ldn/32): bit r of word w set iff V[32w + r] != 0
   uint32_t *max_nnz;    // largest non-zero count of the last step (0xFFFFFFFF: dense V)
   uint32_t sparse_cap;  // Z = B V runs as a gather when max_nnz <= sparse_cap
+  uint32_t *planes_nnz; // the max_nnz the previous step's penalty epilogue saw: above
+                        // sparse_cap it wrote V_hi / V_lo (0 for constrained forms
+                        // and after starts are loaded)
   float *val, *err;     // ValueCoordinateHolder val / current_error
   float *max_err;       // batch maximum relative change (1 float)
   int *iters, *cards;   // storeIterationsForAllPoints logs (total_starts each)

@@ -118,8 +118,7 @@ __device__ __forceinline__ float transpose_reduce32(float (&v)[32], int lane) {
 struct EpiPartial {
   float *ws;
   int bn, m_tiles, n_tiles;  // m_tiles: 128-row blocks of C
-  __device__ void begin(const Unit &, int, int) {}
-  __device__ void end(const Unit &, int, int) {}
+  __device__ void setup() {}
   __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
     if (t.m0 >= m_tiles * BM) return;  // a 2-CTA tile's second half can lie past the last block
     const size_t slot = ((size_t)t.split * m_tiles + t.m0 / BM) * n_tiles + t.nt;
@@ -133,8 +132,7 @@ struct EpiPartial {
 struct EpiRaw {
   float *out;
   int ld, M, N, bn;
-  __device__ void begin(const Unit &, int, int) {}
-  __device__ void end(const Unit &, int, int) {}
+  __device__ void setup() {}
   __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
     const int gi = t.m0 + row;
     if (gi >= M) return;
@@ -154,7 +152,10 @@ struct EpiRaw {
 // of gamma, a decision that the FP32 products feeding it already leave open).
 // Writes the non-zero x and the non-zero bitmask and, per start and per
 // (128-row block, warp), the partial objective and non-zero count, summed in
-// fixed order by the finalize kernel.
+// fixed order by the finalize kernel.  When the previous step was dense
+// (*max_nnz > cap), the next step most likely is too, so the epilogue also
+// writes x as the TF32 hi/lo planes the tensor-core Z = B V reads (zeros
+// included), which spares that step the densify pass.
 template <bool L1>
 struct EpiPenalty {
   float *Vx;
@@ -162,11 +163,21 @@ struct EpiPenalty {
   int ld, M, N, bn, parts;  // parts = m_tiles * 4
   float gamma;
   uint32_t *vmask;  // non-zero bitmask words, ld / 32 per column
-  __device__ void begin(const Unit &, int, int) {}
-  __device__ void end(const Unit &, int, int) {}
+  float *V_hi, *V_lo;
+  const uint32_t *max_nnz;  // the previous step's largest non-zero count
+  uint32_t cap;             // ... above which Z = B V runs dense
+  bool planes = false;      // this launch writes V_hi / V_lo (set by setup)
+  __device__ void setup() { planes = *max_nnz > cap; }
   // r holds this thread's 32 values (row `row`, columns col0..col0+31) and is
   // overwritten with the objective terms.
   __device__ void chunk(const Unit &t, int q, int lane, int row, int col0, float (&r)[32]) {
+    if (planes)
+      body<true>(t, q, lane, row, col0, r);
+    else
+      body<false>(t, q, lane, row, col0, r);
+  }
+  template <bool PLANES>
+  __device__ void body(const Unit &t, int q, int lane, int row, int col0, float (&r)[32]) {
     if (t.m0 >= M) return;  // a 2-CTA tile's second half can lie past the last row
     const int gi = t.m0 + row;
     const bool rv = gi < M;
@@ -193,6 +204,10 @@ struct EpiPenalty {
       const bool nz = keep && v != 0.f;
       bits |= (uint32_t)nz << j;
       if (nz) Vx[(size_t)(c0 + j) * ld + gi] = x;  // zeros live in the mask
+      if (PLANES && valid) {
+        const size_t o = (size_t)(c0 + j) * ld + gi;
+        split_store(nz ? x : 0.f, V_hi + o, V_lo + o);
+      }
     }
     const uint32_t word = bit_transpose32(bits, lane);  // lane j: column c0 + j, bit = row
     const float so = transpose_reduce32(r, lane);
@@ -283,12 +298,14 @@ __global__ void masked_copy_kernel(const float *__restrict__ Vx, const uint32_t 
 }
 
 // Dense TF32 hi/lo planes of V for the tensor-core Z = B V; does nothing on
-// steps where the gather kernel takes Z = B V (*gate <= gate_max).
+// steps where the gather kernel takes Z = B V (*gate <= gate_max), and on
+// dense steps whose planes the previous step's penalty epilogue already wrote
+// (*planes > gate_max: the count that epilogue saw).
 __global__ void densify_kernel(const float *__restrict__ Vx, const uint32_t *__restrict__ mask,
                                int ld, int rows, float *__restrict__ V_hi,
                                float *__restrict__ V_lo, const uint32_t *gate,
-                               uint32_t gate_max) {
-  if (*gate <= gate_max) return;
+                               const uint32_t *planes, uint32_t gate_max) {
+  if (*gate <= gate_max || *planes > gate_max) return;
   const size_t c = blockIdx.x;
   for (int r = threadIdx.x; r < ld; r += blockDim.x) {
     const bool on = r < rows && ((mask[c * (ld >> 5) + (r >> 5)] >> (r & 31)) & 1u);
@@ -1614,7 +1631,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   // 1b. dense V: TF32 hi/lo planes, tensor-core Z = B V (split-K partials) ...
   if ((e = mark(6)) != cudaSuccess) return e;
   densify_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_hi, b.V_lo, b.max_nnz,
-                                      b.sparse_cap);
+                                      b.planes_nnz, b.sparse_cap);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   EpiPartial ep{b.ws, b.bn1, b.m_tiles1, b.n_tiles1};
@@ -1682,12 +1699,14 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
     e = gemm2(er);
   } else if (is_l1_penalized(f)) {
-    EpiPenalty<true> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
-                        (float)p.penalty, b.vmask};
+    EpiPenalty<true> pe{b.Vx,       b.obj_part, b.nnz_part, M.ldn,    M.n,
+                        b.k,        b.bn2,      parts,      (float)p.penalty,
+                        b.vmask,    b.V_hi,     b.V_lo,     b.max_nnz, b.sparse_cap};
     e = gemm2(pe);
   } else {
-    EpiPenalty<false> pe{b.Vx, b.obj_part, b.nnz_part, M.ldn, M.n, b.k, b.bn2, parts,
-                         (float)p.penalty, b.vmask};
+    EpiPenalty<false> pe{b.Vx,       b.obj_part, b.nnz_part, M.ldn,    M.n,
+                         b.k,        b.bn2,      parts,      (float)p.penalty,
+                         b.vmask,    b.V_hi,     b.V_lo,     b.max_nnz, b.sparse_cap};
     e = gemm2(pe);
   }
   if (e != cudaSuccess) return e;
@@ -1741,6 +1760,12 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   fa.cards = b.cards;
   fa.max_nnz = b.max_nnz;
   // Z = B V of this step has read max_nnz; finalize sets it for the next step
+  // penalized forms: the count this step's epilogue saw (whether it wrote the
+  // dense planes), for the next step's densify gate
+  if (!is_constrained(f) &&
+      (e = cudaMemcpyAsync(b.planes_nnz, b.max_nnz, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                           st)) != cudaSuccess)
+    return e;
   if ((e = cudaMemsetAsync(b.max_nnz, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
   if ((e = mark(4)) != cudaSuccess) return e;
   finalize_kernel<<<(b.k + 7) / 8, 256, 0, st>>>(fa);

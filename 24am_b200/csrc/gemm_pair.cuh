@@ -312,6 +312,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
     const int q = warp & 3;
     const int half = (warp - 2) >> 2;
     const int row = q * 32 + lane;
+    Epi ep = epi;  // per-launch state the epilogue reads once
+    ep.setup();
     int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true;
@@ -347,12 +349,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
         }
       }
       if (!ok) break;
-      epi.begin(t, q, lane);
 #pragma unroll
       for (int c = 0; c < HALF / 32; c++)
-        epi.chunk(t, q, lane, row, half * HALF + c * 32,
+        ep.chunk(t, q, lane, row, half * HALF + c * 32,
                   *reinterpret_cast<float(*)[32]>(sum + c * 32));
-      epi.end(t, q, lane);
     }
   }
 

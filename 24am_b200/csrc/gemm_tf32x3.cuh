@@ -268,6 +268,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     const int q = warp & 3;          // TMEM lanes [32q, 32q+32) are the ones this warp may read
     const int half = (warp - 2) >> 2;  // column half [half*HALF, half*HALF + HALF)
     const int row = q * 32 + lane;
+    Epi ep = epi;  // per-launch state the epilogue reads once
+    ep.setup();
     int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true;
@@ -302,12 +304,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         }
       }
       if (!ok) break;
-      epi.begin(t, q, lane);
 #pragma unroll
       for (int c = 0; c < HALF / 32; c++)
-        epi.chunk(t, q, lane, row, half * HALF + c * 32,
+        ep.chunk(t, q, lane, row, half * HALF + c * 32,
                   *reinterpret_cast<float(*)[32]>(sum + c * 32));
-      epi.end(t, q, lane);
     }
   }
 

@@ -142,3 +142,43 @@ def test_steps_through_sparse_gather_match_oracle(solver, po, formulation):
     assert ok >= 0.9 * k, f"{ok} of {k} starts agree after 3 steps"
     b.close()
     M.close()
+
+
+@pytest.mark.parametrize("k", [96, 256])  # one-CTA and CTA-pair tiles
+@pytest.mark.parametrize("formulation", [4, 5, 6, 7])
+def test_dense_penalized_steps_reuse_epilogue_planes(solver, po, formulation, k):
+    """Penalties small enough to keep V dense step after step: from the second
+    step on, Z = B V reads the TF32 planes the previous step's penalty epilogue
+    wrote (densify returns at once); the loadings stay with the oracle's."""
+    import importlib
+    am = importlib.import_module("24am_b200")
+    m, n = 300, 2048
+    B = po.low_rank_data(m, n, 8, 30, seed=91, dtype=np.float32)
+    B64 = B.astype(np.float64)
+    V0 = po.uniform_starts(n, k, seed=92, dtype=np.float32)
+    g = {4: 1e-4, 5: 1e-2, 6: 1e-3, 7: 1e-2}[formulation]
+    st = am.OptimizationSettings(formulation=formulation, penaltyParameter=g, tolerance=1e-6,
+                                 maximumIterations=10, totalStartingPoints=k, batchSize=k)
+    M = solver.matrix(B)
+    b = M.batch(st, k)
+    b.load(V0)
+    os_ = po.make_settings(formulation, penalty=g, tolerance=1e-6, max_iter=10, total_starts=k,
+                           batch_size=k)
+    Vo, val_o = V0.astype(np.float64), np.zeros(k)
+    kinds = []
+    for it in range(4):
+        kinds.append([name for name, _ in b.step_timed(it)])
+        Vo, _, val_o, _, _ = po.oracle_iteration(B64, Vo, os_, val_o, it=it)
+    V, val, err, nnz = b.read()
+    assert np.count_nonzero(Vo, axis=0).max() > n // 32  # dense every step
+    assert "densify" in kinds[0]
+    for ks in kinds[1:]:
+        assert "densify(skipped)" in ks and "gemm_BV" in ks, ks
+    ok = 0
+    for j in range(k):
+        same = np.array_equal(V[:, j] != 0, Vo[:, j] != 0)
+        close = np.abs(V[:, j] - Vo[:, j]).max() <= 1e-4 * max(np.abs(Vo[:, j]).max(), 1e-30)
+        ok += same and close and abs(val[j] - val_o[j]) <= 1e-4 * abs(val_o[j]) + 1e-20
+    assert ok >= 0.9 * k, f"{ok} of {k} starts agree after 4 steps"
+    b.close()
+    M.close()
