@@ -452,57 +452,97 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
     }
   }
   __syncthreads();
+  // Each thread accumulates 2 x 4 consecutive samples per pass (16-byte loads);
+  // the rows of four non-zeros are loaded before their FMAs, which still run in
+  // index order per sample.  Samples in [m, ldm) read B's zero padding.
+  constexpr int G4 = GATHER_ROWS / 4;
   double acc = 0.0;
-  float y[GATHER_ROWS];
+  float4 y[G4];
   float *zh = Z_hi + (size_t)j * ldm;
   float *zl = Z_lo + (size_t)j * ldm;
+  uint16_t *zb = Zb ? Zb + (size_t)j * ldm : nullptr;
   const int chunk = GATHER_THREADS * GATHER_ROWS;
+  const int ld4 = ldm >> 2;
   const bool one_pass = m <= chunk;
+  auto sample = [&](int base, int r) { return base + 4 * (r * GATHER_THREADS + (int)threadIdx.x); };
+  auto fma4 = [](float v, const float4 &b, float4 &acc4) {
+    acc4.x = fmaf(v, b.x, acc4.x);
+    acc4.y = fmaf(v, b.y, acc4.y);
+    acc4.z = fmaf(v, b.z, acc4.z);
+    acc4.w = fmaf(v, b.w, acc4.w);
+  };
+  // the final value of sample i (c of the float4), stored as Z needs it
+  auto emit = [&](int i, float yv) {
+    if (MODE == 1) {
+      acc += (double)fabsf(yv);
+      zh[i] = sgnf(yv);
+      zl[i] = 0.f;
+      if (zb) zb[i] = bf16_sign(yv);
+    } else {
+      acc += (double)yv * (double)yv;
+      if (!(MODE == 2 && one_pass)) split_store(yv, zh + i, zl + i);
+      if (MODE == 0 && zb) zb[i] = bf16_bits(yv);
+    }
+  };
   for (int base = 0; base < m; base += chunk) {
+    int i4[G4];
+    bool ok[G4];
 #pragma unroll
-    for (int r = 0; r < GATHER_ROWS; r++) y[r] = 0.f;
-    for (uint32_t q = 0; q < total; q++) {
-      const float v = val[q];
-      const size_t row = (size_t)idx[q] * ldm;
+    for (int r = 0; r < G4; r++) {
+      y[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+      i4[r] = sample(base, r) >> 2;
+      ok[r] = i4[r] < ld4;
+    }
+    uint32_t q = 0;
+    for (; q + 4 <= total; q += 4) {
+      float4 bq[4][G4];
 #pragma unroll
-      for (int r = 0; r < GATHER_ROWS; r++) {
-        const int i = base + r * GATHER_THREADS + threadIdx.x;
-        if (i < m) y[r] = fmaf(v, Bc[row + i], y[r]);
+      for (int u = 0; u < 4; u++) {
+        const float4 *row4 = reinterpret_cast<const float4 *>(Bc + (size_t)idx[q + u] * ldm);
+#pragma unroll
+        for (int r = 0; r < G4; r++)
+          bq[u][r] = ok[r] ? __ldg(row4 + i4[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const float v = val[q + u];
+#pragma unroll
+        for (int r = 0; r < G4; r++) fma4(v, bq[u][r], y[r]);
       }
     }
+    for (; q < total; q++) {
+      const float4 *row4 = reinterpret_cast<const float4 *>(Bc + (size_t)idx[q] * ldm);
+      const float v = val[q];
 #pragma unroll
-    for (int r = 0; r < GATHER_ROWS; r++) {
-      const int i = base + r * GATHER_THREADS + threadIdx.x;
-      if (i >= m) continue;
-      if (MODE == 1) {
-        acc += (double)fabsf(y[r]);
-        zh[i] = sgnf(y[r]);
-        zl[i] = 0.f;
-        if (Zb) Zb[(size_t)j * ldm + i] = bf16_sign(y[r]);
-      } else {
-        acc += (double)y[r] * (double)y[r];
-        if (!(MODE == 2 && one_pass)) split_store(y[r], zh + i, zl + i);
-        if (MODE == 0 && Zb) Zb[(size_t)j * ldm + i] = bf16_bits(y[r]);
-      }
+      for (int r = 0; r < G4; r++)
+        if (ok[r]) fma4(v, __ldg(row4 + i4[r]), y[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < G4; r++) {
+      const int i = sample(base, r);
+      const float e[4] = {y[r].x, y[r].y, y[r].z, y[r].w};
+#pragma unroll
+      for (int c = 0; c < 4; c++)
+        if (i + c < m) emit(i + c, e[c]);
     }
   }
   const double tot = block_sum(acc, red);
   if (MODE == 2) {
     const float inv = 1.0f / (float)sqrt(tot);
-    if (one_pass) {
+    for (int base = 0; base < m; base += chunk) {
 #pragma unroll
-      for (int r = 0; r < GATHER_ROWS; r++) {
-        const int i = r * GATHER_THREADS + threadIdx.x;
-        if (i < m) {
-          split_store(y[r] * inv, zh + i, zl + i);
-          if (Zb) Zb[(size_t)j * ldm + i] = bf16_bits(y[r] * inv);
+      for (int r = 0; r < G4; r++) {
+        const int i = sample(base, r);
+        const float e[4] = {y[r].x, y[r].y, y[r].z, y[r].w};
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          if (i + c >= m) continue;
+          // one pass: the sums are still in registers; else re-read what this
+          // thread wrote (hi + lo is exact)
+          const float v = one_pass ? e[c] : zh[i + c] + zl[i + c];
+          split_store(v * inv, zh + i + c, zl + i + c);
+          if (zb) zb[i + c] = bf16_bits(v * inv);
         }
-      }
-    } else {
-      for (int i = threadIdx.x; i < m; i += GATHER_THREADS) {
-        const float v = zh[i] + zl[i];
-        split_store(v * inv, zh + i, zl + i);
-        if (Zb) Zb[(size_t)j * ldm + i] = bf16_bits(v * inv);
       }
     }
   } else if (threadIdx.x == 0) {
