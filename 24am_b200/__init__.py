@@ -108,6 +108,19 @@ _SIGS = {
     "am24_batch_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "am24_batch_launches_per_step": (C.c_int, [_VP, _VP, C.POINTER(C.c_int32)]),
     "am24_batch_phase": (C.c_int, [_VP, _VP, C.POINTER(C.c_int32)]),
+    "am24_solve_dense_f64": (C.c_int, [_VP, _VP, C.c_int32, _VP, C.c_uint32, C.c_uint32,
+                                       C.POINTER(am24_settings), C.POINTER(am24_statistics), _VP,
+                                       C.POINTER(C.c_double)]),
+    "am24_server_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_VP)]),
+    "am24_server_destroy": (C.c_int, [_VP]),
+    "am24_server_add_matrix_f32": (C.c_int, [_VP, _VP, C.c_int32, C.c_uint32, C.c_uint32,
+                                             C.c_int32, C.POINTER(C.c_uint32)]),
+    "am24_server_remove_matrix": (C.c_int, [_VP, C.c_uint32]),
+    "am24_submit": (C.c_int, [_VP, C.c_uint32, C.POINTER(am24_settings), _VP,
+                              C.POINTER(C.c_uint64)]),
+    "am24_poll": (C.c_int, [_VP, C.c_uint64, _VP, C.POINTER(am24_statistics),
+                            C.POINTER(C.c_int32)]),
+    "am24_wait": (C.c_int, [_VP, C.c_uint64, _VP, C.POINTER(am24_statistics)]),
     "am24_sync": (C.c_int, [_VP]),
     "am24_stream": (C.c_void_p, [_VP]),
     "am24_batch_step_timed": (C.c_int, [_VP, _VP, C.c_int32, C.POINTER(C.c_float),
@@ -455,6 +468,67 @@ class Batch:
         v = C.c_int32()
         check(lib().am24_batch_launches_per_step(self.matrix.solver.h, self.bh, C.byref(v)))
         return v.value
+
+
+class Server:
+    """A serving loop (am24_server_*): resident matrices under an HBM budget,
+    queued solves batched on arrival by a worker thread."""
+
+    def __init__(self, device=0, hbm_budget_bytes=150 << 30):
+        sh = C.c_void_p()
+        check(lib().am24_server_create(int(device), int(hbm_budget_bytes), C.byref(sh)))
+        self.sh = sh
+        self.shapes = {}
+
+    def close(self):
+        if self.sh:
+            lib().am24_server_destroy(self.sh)
+            self.sh = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_matrix(self, B=None, on_device_ptr=None, m=None, n=None, ldB=None):
+        mid = C.c_uint32()
+        if on_device_ptr is None:
+            B = np.asfortranarray(B, np.float32)
+            m, n = B.shape
+            check(lib().am24_server_add_matrix_f32(self.sh, _ptr(B), m, m, n, 0, C.byref(mid)))
+        else:
+            check(lib().am24_server_add_matrix_f32(self.sh, C.c_void_p(on_device_ptr), ldB or m,
+                                                   m, n, 1, C.byref(mid)))
+        self.shapes[mid.value] = (m, n)
+        return mid.value
+
+    def remove_matrix(self, matrix_id):
+        check(lib().am24_server_remove_matrix(self.sh, int(matrix_id)))
+        self.shapes.pop(matrix_id, None)
+
+    def submit(self, matrix_id, settings, start_points=None):
+        s = settings.to_c()
+        sp = None if start_points is None else np.asfortranarray(start_points, np.float32)
+        t = C.c_uint64()
+        check(lib().am24_submit(self.sh, int(matrix_id), C.byref(s), _ptr(sp), C.byref(t)))
+        return (t.value, matrix_id)
+
+    def poll(self, ticket):
+        """(done, x, stats); x and stats are None while the request runs."""
+        t, mid = ticket
+        x = np.zeros(self.shapes[mid][1], np.float32)
+        st = am24_statistics()
+        done = C.c_int32()
+        check(lib().am24_poll(self.sh, t, _ptr(x), C.byref(st), C.byref(done)))
+        return (True, x, st) if done.value else (False, None, None)
+
+    def wait(self, ticket):
+        t, mid = ticket
+        x = np.zeros(self.shapes[mid][1], np.float32)
+        st = am24_statistics()
+        check(lib().am24_wait(self.sh, t, _ptr(x), C.byref(st)))
+        return x, st
 
 
 def header_symbols():

@@ -12,7 +12,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -308,6 +313,7 @@ const char *am24_status_string(am24_status s) {
     case AM24_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
     case AM24_ERR_UNSUPPORTED: return "unsupported";
     case AM24_ERR_DEGENERATE: return "degenerate start (NaN objective)";
+    case AM24_ERR_ADMISSION_REJECTED: return "admission rejected (HBM budget)";
   }
   return "unknown status";
 }
@@ -1058,6 +1064,450 @@ am24_status am24_batch_iterate_static_ws(am24_handle h, am24_batch b, int32_t it
     AM24_TRY(check_device_status(b));
   }
   return AM24_OK;
+}
+
+}  // extern "C"
+
+// ---- FP64 host data --------------------------------------------------------
+extern "C" {
+
+am24_status am24_solve_dense_f64(am24_handle h, const double *B, int32_t ldB, double *x,
+                                 uint32_t m, uint32_t n, am24_settings *settings,
+                                 am24_statistics *stats, const double *start_points,
+                                 double *fval_out) {
+  if (!h || !B || !x || !settings) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  if (ldB < (int32_t)m) return fail(AM24_ERR_INVALID_ARG, "ldB must be >= m");
+  std::vector<float> Bf((size_t)m * n), xf(n), sp;
+  for (uint32_t c = 0; c < n; c++)
+    for (uint32_t r = 0; r < m; r++) Bf[(size_t)c * m + r] = (float)B[(size_t)c * ldB + r];
+  for (uint32_t i = 0; i < n; i++) xf[i] = (float)x[i];
+  if (settings->start_mode == AM24_START_INJECTED && start_points) {
+    am24_settings probe = *settings;
+    AM24_TRY(am24_check_input(&probe, n));
+    sp.resize((size_t)n * probe.total_starts);
+    for (size_t i = 0; i < sp.size(); i++) sp[i] = (float)start_points[i];
+  }
+  float f = 0.f;
+  AM24_TRY(am24_solve_dense_f32(h, Bf.data(), (int32_t)m, xf.data(), m, n, settings, stats,
+                                sp.empty() ? nullptr : sp.data(), &f));
+  for (uint32_t i = 0; i < n; i++) x[i] = xf[i];
+  if (fval_out) *fval_out = f;
+  return AM24_OK;
+}
+
+}  // extern "C"
+
+// ---- serving ---------------------------------------------------------------
+namespace {
+
+struct ServeRequest {
+  uint64_t ticket = 0;
+  uint32_t matrix_id = 0;
+  am24_settings s{};          // after am24_check_input, one batch of all starts
+  std::vector<float> starts;  // n x total_starts (injected starts only)
+  std::chrono::steady_clock::time_point submitted;
+  bool done = false;
+  am24_status status = AM24_OK;
+  std::string error;
+  std::vector<float> x;
+  am24_statistics stats{};
+};
+using RequestPtr = std::shared_ptr<ServeRequest>;
+
+// Requests that may share one batch: same matrix, same step.
+bool same_step(const ServeRequest &a, const ServeRequest &b) {
+  return a.matrix_id == b.matrix_id && a.s.formulation == b.s.formulation &&
+         a.s.constraint == b.s.constraint && a.s.penalty == b.s.penalty &&
+         a.s.tolerance == b.s.tolerance && a.s.max_iter == b.s.max_iter &&
+         a.s.l1_mode == b.s.l1_mode && a.s.precision == b.s.precision &&
+         a.s.stable_iterations == b.s.stable_iterations &&
+         a.s.stable_share == b.s.stable_share && a.s.timeout_ms == b.s.timeout_ms;
+}
+
+// Device bytes of a matrix's layouts (the BF16 planes included: batches of the
+// L1-variance forms and MIXED ones add them on first use).
+uint64_t matrix_bytes(uint32_t m, uint32_t n) {
+  const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
+  return 4ull * (2 * n * ldm + 2 * m * ldn + n * ldm) + 2ull * 3 * n * ldm;
+}
+
+// Device bytes of a batch of k starts on an m x n matrix (an upper estimate).
+uint64_t batch_bytes(uint32_t m, uint32_t n, uint32_t k) {
+  const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
+  const uint64_t kv = (uint64_t)k * ldn, kz = (uint64_t)k * ldm;
+  const uint64_t ws = 2ull * ((m + 127) / 128) * ((k + 63) / 64 + 3) * 256 * 128 * 4 * 8;
+  return 4 * kv * 4 + 2 * kz * 4 + kz * 2 + 2 * (kv / 32) * 4 + ws + (uint64_t)k * 256 +
+         (4ull << 20);
+}
+
+}  // namespace
+
+struct am24_server_s {
+  am24_handle worker_h = nullptr;  // used by the worker thread only
+  am24_handle upload_h = nullptr;  // matrix uploads from callers' threads
+  std::mutex upload_mu;
+  uint64_t budget = 0;
+  std::mutex mu;  // everything below
+  std::condition_variable cv_work, cv_done;
+  struct Resident {
+    am24_matrix mat;
+    uint64_t bytes;
+    uint32_t m, n;
+    int pending;
+  };
+  std::map<uint32_t, Resident> matrices;
+  uint64_t resident = 0;
+  uint32_t next_matrix = 1;
+  uint64_t next_ticket = 1;
+  std::deque<RequestPtr> queue;
+  std::map<uint64_t, RequestPtr> tickets;
+  bool stop = false;
+  uint32_t max_batch = 8192;
+  std::thread worker;
+  // the worker's cached batch (reused while the shape and step stay the same)
+  am24_batch cached = nullptr;
+  uint32_t cached_matrix = 0, cached_k = 0;
+  am24_settings cached_s{};
+};
+
+namespace {
+
+// Runs one batch made of the requests' starts (worker thread).
+am24_status run_group(am24_server s, am24_matrix mat, uint32_t matrix_id,
+                      std::vector<RequestPtr> &group) {
+  am24_handle h = s->worker_h;
+  const MatrixDev &M = mat->d;
+  const unsigned n = (unsigned)M.n;
+  uint32_t K = 0;
+  for (auto &r : group) K += (uint32_t)r->s.total_starts;
+  am24_settings bs = group[0]->s;
+  bs.total_starts = (int32_t)K;
+  bs.batch_size = (int32_t)K;
+  bs.total_batches = 1;
+  bs.use_otf = 0;
+  bs.store_all = 0;
+  if (!(s->cached && s->cached_matrix == matrix_id && s->cached_k == K &&
+        s->cached_s.formulation == bs.formulation && s->cached_s.precision == bs.precision &&
+        s->cached_s.stable_iterations == bs.stable_iterations &&
+        s->cached_s.stable_share == bs.stable_share)) {
+    if (s->cached) am24_batch_destroy(h, s->cached);
+    s->cached = nullptr;
+    AM24_TRY(am24_batch_create(h, mat, &bs, K, &s->cached));
+    s->cached_matrix = matrix_id;
+    s->cached_k = K;
+    s->cached_s = bs;
+  }
+  am24_batch b = s->cached;
+  b->s = bs;  // the step parameters of this group (penalty, tolerance, ...)
+  const BatchDev &d = b->d;
+  // starts: each request's own (injected, or the reference generator by its
+  // own start index), one segment after the other
+  std::vector<float> staging((size_t)n * K), seg;
+  uint32_t off = 0;
+  for (auto &r : group) {
+    const uint32_t k = (uint32_t)r->s.total_starts;
+    std::vector<unsigned> gidx(k);
+    for (uint32_t i = 0; i < k; i++) gidx[i] = i;
+    host_starts(r->s, n, r->starts.empty() ? nullptr : r->starts.data(), gidx.data(), (int)k,
+                seg);
+    std::memcpy(&staging[(size_t)off * n], seg.data(), sizeof(float) * seg.size());
+    off += k;
+  }
+  AM24_TRY(am24_batch_load(h, b, staging.data(), 0));
+  cudaEvent_t e0, e1;
+  AM24_CUDA(cudaEventCreate(&e0));
+  AM24_CUDA(cudaEventCreate(&e1));
+  struct EvGuard {
+    cudaEvent_t a, c;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(c);
+    }
+  } evg{e0, e1};
+  AM24_CUDA(cudaEventRecord(e0, h->stream));
+  uint32_t phase = d.mixed ? 0u : 1u, low_its = 0;
+  float max_err = 0.f;
+  int it = 0;
+  for (; it < bs.max_iter; it++) {
+    const bool refined = phase != 0;
+    low_its += refined ? 0 : 1;
+    const StepParams p = step_params(bs, it, 0);
+    AM24_CUDA(launch_am_step(M, b->d, b->tm, p, h->stream, &b->launches));
+    AM24_CUDA(cudaMemcpyAsync(&max_err, d.max_err, sizeof(float), cudaMemcpyDeviceToHost,
+                              h->stream));
+    if (d.mixed)
+      AM24_CUDA(cudaMemcpyAsync(&phase, d.phase, sizeof phase, cudaMemcpyDeviceToHost, h->stream));
+    AM24_CUDA(cudaStreamSynchronize(h->stream));
+    AM24_TRY(check_device_status(b));
+    if (it > 0 && refined && (double)max_err < bs.tolerance) {
+      it++;
+      break;
+    }
+  }
+  AM24_CUDA(cudaEventRecord(e1, h->stream));
+  std::vector<float> val(K);
+  AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * K, cudaMemcpyDeviceToHost,
+                            h->stream));
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  float ms = 0.f;
+  AM24_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  // per request: the best of its own starts, normalised, and its ||B x||^2
+  Allocs local;
+  float *xb = nullptr, *x_dev = nullptr;
+  double *ev_rows = nullptr;
+  AM24_TRY(local.get(&xb, n));
+  AM24_TRY(local.get(&x_dev, n));
+  AM24_TRY(local.get(&ev_rows, (size_t)M.m));
+  off = 0;
+  for (auto &r : group) {
+    const uint32_t k = (uint32_t)r->s.total_starts;
+    uint32_t sel = 0;
+    float bv = val[off];
+    int degenerate = std::isnan(val[off]) ? 1 : 0;
+    for (uint32_t i = 1; i < k; i++) {
+      degenerate += std::isnan(val[off + i]) ? 1 : 0;
+      if (val[off + i] > bv) {
+        bv = val[off + i];
+        sel = i;
+      }
+    }
+    const uint32_t j = off + sel;
+    AM24_CUDA(launch_masked_copy(d.Vx + (size_t)j * M.ldn, d.vmask + (size_t)j * (M.ldn / 32),
+                                 M.ldn, (int)n, 1, xb, (int)n, h->stream));
+    AM24_CUDA(launch_finalize_x(xb, (int)n, x_dev, h->stream));
+    AM24_CUDA(launch_explained_variance(M, x_dev, ev_rows, h->ev_out, h->stream));
+    r->x.resize(n);
+    double ev = 0.0;
+    AM24_CUDA(cudaMemcpyAsync(r->x.data(), x_dev, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                              h->stream));
+    AM24_CUDA(cudaMemcpyAsync(&ev, h->ev_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    AM24_CUDA(cudaStreamSynchronize(h->stream));
+    am24_statistics &st = r->stats;
+    st = am24_statistics{};
+    st.it = (uint32_t)it;
+    st.fval = bv;
+    st.error = max_err;
+    st.total_true_computation_time = ms * 1e-3;
+    st.n = n;
+    st.total_threads_used = 1;
+    st.explained_variance = ev;
+    st.start_iterations = (uint64_t)k * (uint64_t)it;
+    st.degenerate_starts = degenerate;
+    st.low_precision_iterations = low_its;
+    off += k;
+  }
+  return AM24_OK;
+}
+
+void worker_loop(am24_server s) {
+  cudaSetDevice(s->worker_h->device);
+  for (;;) {
+    std::vector<RequestPtr> take;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+      if (s->queue.empty()) return;  // stopping, nothing left
+      take.assign(s->queue.begin(), s->queue.end());
+      s->queue.clear();
+    }
+    while (!take.empty()) {
+      // the oldest request and every later one that shares its step, while
+      // the batch stays within the server's limits
+      std::vector<RequestPtr> group{take.front()};
+      std::vector<RequestPtr> rest;
+      am24_matrix mat = nullptr;
+      uint64_t room = 0;
+      uint32_t m = 0, n = 0;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto &res = s->matrices.at(take.front()->matrix_id);
+        mat = res.mat;
+        m = res.m;
+        n = res.n;
+        room = s->budget > s->resident ? s->budget - s->resident : 0;
+      }
+      uint32_t K = (uint32_t)group[0]->s.total_starts;
+      for (size_t i = 1; i < take.size(); i++) {
+        const uint32_t k = (uint32_t)take[i]->s.total_starts;
+        if (same_step(*group[0], *take[i]) && K + k <= s->max_batch &&
+            batch_bytes(m, n, K + k) <= room) {
+          group.push_back(take[i]);
+          K += k;
+        } else {
+          rest.push_back(take[i]);
+        }
+      }
+      take.swap(rest);
+      const am24_status st = run_group(s, mat, group[0]->matrix_id, group);
+      const std::string err = st == AM24_OK ? std::string() : g_last_error;
+      if (st != AM24_OK && s->cached) {  // do not reuse a batch left in an unknown state
+        am24_batch_destroy(s->worker_h, s->cached);
+        s->cached = nullptr;
+      }
+      const auto now = std::chrono::steady_clock::now();
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto &r : group) {
+          r->status = st;
+          r->error = err;
+          r->stats.total_elapsed_time = std::chrono::duration<double>(now - r->submitted).count();
+          r->done = true;
+          s->matrices.at(r->matrix_id).pending--;
+        }
+      }
+      s->cv_done.notify_all();
+    }
+  }
+}
+
+am24_status finish_ticket(am24_server s, const RequestPtr &r, float *x, am24_statistics *stats) {
+  // caller holds s->mu; the request is done
+  if (x && !r->x.empty()) std::memcpy(x, r->x.data(), sizeof(float) * r->x.size());
+  if (stats) *stats = r->stats;
+  s->tickets.erase(r->ticket);
+  if (r->status != AM24_OK) return fail(r->status, r->error);
+  return AM24_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+am24_status am24_server_create(int device, uint64_t hbm_budget_bytes, am24_server *out) {
+  if (!out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  auto *s = new am24_server_s();
+  s->budget = hbm_budget_bytes;
+  am24_status st;
+  if ((st = am24_create(&s->worker_h, device)) != AM24_OK ||
+      (st = am24_create(&s->upload_h, device)) != AM24_OK) {
+    if (s->worker_h) am24_destroy(s->worker_h);
+    delete s;
+    return st;
+  }
+  s->worker = std::thread(worker_loop, s);
+  *out = s;
+  return AM24_OK;
+}
+
+am24_status am24_server_destroy(am24_server s) {
+  if (!s) return AM24_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  if (s->cached) am24_batch_destroy(s->worker_h, s->cached);
+  for (auto &kv : s->matrices) am24_matrix_destroy(s->upload_h, kv.second.mat);
+  am24_destroy(s->worker_h);
+  am24_destroy(s->upload_h);
+  delete s;
+  return AM24_OK;
+}
+
+am24_status am24_server_add_matrix_f32(am24_server s, const float *B, int32_t ldB, uint32_t m,
+                                       uint32_t n, int32_t on_device, uint32_t *matrix_id) {
+  if (!s || !B || !matrix_id) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  const uint64_t bytes = matrix_bytes(m, n);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->resident + bytes > s->budget)
+      return fail(AM24_ERR_ADMISSION_REJECTED,
+                  "matrix needs " + std::to_string(bytes) + " bytes, " +
+                      std::to_string(s->budget - std::min(s->budget, s->resident)) +
+                      " left in the budget");
+    s->resident += bytes;  // reserved while uploading
+  }
+  am24_matrix mat = nullptr;
+  am24_status st;
+  {
+    std::lock_guard<std::mutex> lk(s->upload_mu);
+    st = am24_matrix_create_f32(s->upload_h, B, ldB, m, n, on_device, &mat);
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (st != AM24_OK) {
+    s->resident -= bytes;
+    return st;
+  }
+  const uint32_t id = s->next_matrix++;
+  s->matrices[id] = am24_server_s::Resident{mat, bytes, m, n, 0};
+  *matrix_id = id;
+  return AM24_OK;
+}
+
+am24_status am24_server_remove_matrix(am24_server s, uint32_t matrix_id) {
+  if (!s) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  am24_matrix mat = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->matrices.find(matrix_id);
+    if (it == s->matrices.end()) return fail(AM24_ERR_INVALID_ARG, "unknown matrix id");
+    if (it->second.pending > 0)
+      return fail(AM24_ERR_INVALID_ARG, "requests for this matrix are pending");
+    if (s->cached && s->cached_matrix == matrix_id)
+      return fail(AM24_ERR_INVALID_ARG, "the matrix is in use");
+    mat = it->second.mat;
+    s->resident -= it->second.bytes;
+    s->matrices.erase(it);
+  }
+  std::lock_guard<std::mutex> lk(s->upload_mu);
+  return am24_matrix_destroy(s->upload_h, mat);
+}
+
+am24_status am24_submit(am24_server s, uint32_t matrix_id, const am24_settings *settings,
+                        const float *start_points, uint64_t *ticket) {
+  if (!s || !settings || !ticket) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  AM24_TRY(validate_settings(settings));
+  if (settings->use_otf || settings->store_all)
+    return fail(AM24_ERR_INVALID_ARG, "the server supports neither use_otf nor store_all");
+  if (settings->start_mode == AM24_START_INJECTED && !start_points)
+    return fail(AM24_ERR_INVALID_ARG, "start_mode INJECTED needs start_points");
+  auto r = std::make_shared<ServeRequest>();
+  r->s = *settings;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->matrices.find(matrix_id);
+  if (it == s->matrices.end()) return fail(AM24_ERR_INVALID_ARG, "unknown matrix id");
+  const uint32_t n = it->second.n, m = it->second.m;
+  AM24_TRY(am24_check_input(&r->s, n));
+  r->s.batch_size = r->s.total_starts;
+  r->s.total_batches = 1;
+  if ((uint32_t)r->s.total_starts > s->max_batch)
+    return fail(AM24_ERR_ADMISSION_REJECTED, "more starts than the server's largest batch");
+  if (s->resident + batch_bytes(m, n, (uint32_t)r->s.total_starts) > s->budget)
+    return fail(AM24_ERR_ADMISSION_REJECTED, "the request's batch does not fit the budget");
+  if (r->s.start_mode == AM24_START_INJECTED)
+    r->starts.assign(start_points, start_points + (size_t)n * r->s.total_starts);
+  r->matrix_id = matrix_id;
+  r->ticket = s->next_ticket++;
+  r->submitted = std::chrono::steady_clock::now();
+  it->second.pending++;
+  s->tickets[r->ticket] = r;
+  s->queue.push_back(r);
+  *ticket = r->ticket;
+  s->cv_work.notify_one();
+  return AM24_OK;
+}
+
+am24_status am24_poll(am24_server s, uint64_t ticket, float *x, am24_statistics *stats,
+                      int32_t *done) {
+  if (!s || !done) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return fail(AM24_ERR_INVALID_ARG, "unknown ticket");
+  *done = it->second->done ? 1 : 0;
+  if (!*done) return AM24_OK;
+  return finish_ticket(s, it->second, x, stats);
+}
+
+am24_status am24_wait(am24_server s, uint64_t ticket, float *x, am24_statistics *stats) {
+  if (!s) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return fail(AM24_ERR_INVALID_ARG, "unknown ticket");
+  RequestPtr r = it->second;
+  s->cv_done.wait(lk, [&] { return r->done; });
+  return finish_ticket(s, r, x, stats);
 }
 
 }  // extern "C"

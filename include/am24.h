@@ -40,7 +40,8 @@ typedef enum {
   AM24_ERR_CUDA = 3,           /* CUDA runtime/driver error */
   AM24_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait gave up */
   AM24_ERR_UNSUPPORTED = 5,    /* device is not sm_100 or feature not built */
-  AM24_ERR_DEGENERATE = 6      /* informational: some start produced a NaN objective */
+  AM24_ERR_DEGENERATE = 6,     /* informational: some start produced a NaN objective */
+  AM24_ERR_ADMISSION_REJECTED = 7 /* a server's HBM budget cannot hold the matrix or request */
 } am24_status;
 
 /* SPCA_Formulation (c++/src/class/optimization_settings.h:27-37), same values. */
@@ -164,6 +165,14 @@ am24_status am24_solve_device_f32(am24_handle h, const float *d_B, int32_t ldB, 
                                   am24_statistics *stats, const float *start_points,
                                   float *fval_out);
 
+/* FP64 host data (the reference's denseDataSolver<double> call): B and the
+ * injected starts are rounded to FP32 and solved as am24_solve_dense_f32 does;
+ * x and *fval_out are returned in double. */
+am24_status am24_solve_dense_f64(am24_handle h, const double *B, int32_t ldB, double *x,
+                                 uint32_t m, uint32_t n, am24_settings *settings,
+                                 am24_statistics *stats, const double *start_points,
+                                 double *fval_out);
+
 /* ---- resident data matrices ---------------------------------------------- */
 /* Copies B (host, or device when on_device != 0) into the handle's layout and
  * keeps it until am24_matrix_destroy. */
@@ -217,6 +226,42 @@ am24_status am24_sync(am24_handle h);
 /* The handle's CUDA stream (a cudaStream_t), for callers that record their own
  * events around library work. */
 void *am24_stream(am24_handle h);
+
+/* ---- serving: resident matrices, queued solves, batching on arrival ------- */
+/* A server owns its own handles on `device` and one worker thread.  Matrices
+ * are admitted while their device layouts fit hbm_budget_bytes (the budget
+ * also bounds the largest request batch).  Queued requests that share a
+ * matrix and the settings that shape the AM step (formulation, constraint,
+ * penalty, tolerance, max_iter, l1_mode, precision and its stability rule) run
+ * together as one batch of starting points; each request still gets the best
+ * of its own starts, its own x and its own statistics.  Each request's starts
+ * form one segment of that batch (batchSize = totalStartingPoints), and the
+ * batch stops on its batch-wide maximum change as a reference batch does.
+ * settings->use_otf and store_all are not supported by the server. */
+typedef struct am24_server_s *am24_server;
+am24_status am24_server_create(int device, uint64_t hbm_budget_bytes, am24_server *out);
+/* Finishes queued requests, then frees everything the server holds. */
+am24_status am24_server_destroy(am24_server s);
+/* Copies B (host, or device when on_device != 0) into a resident matrix;
+ * AM24_ERR_ADMISSION_REJECTED when its layouts do not fit the budget left. */
+am24_status am24_server_add_matrix_f32(am24_server s, const float *B, int32_t ldB, uint32_t m,
+                                       uint32_t n, int32_t on_device, uint32_t *matrix_id);
+/* Frees a resident matrix; AM24_ERR_INVALID_ARG while requests for it are pending. */
+am24_status am24_server_remove_matrix(am24_server s, uint32_t matrix_id);
+/* Queues a solve of `settings` (copied, after am24_check_input) on a resident
+ * matrix; start_points (n x total_starts, copied) is read for
+ * AM24_START_INJECTED.  AM24_ERR_ADMISSION_REJECTED when the request's batch
+ * can never fit the budget.  Returns at once with a ticket. */
+am24_status am24_submit(am24_server s, uint32_t matrix_id, const am24_settings *settings,
+                        const float *start_points, uint64_t *ticket);
+/* Non-blocking: *done = 1 once the request finished, then x (n floats) and
+ * stats (may be NULL) are filled, the ticket is released and the request's own
+ * status is returned; *done = 0 otherwise.  stats->total_elapsed_time is the
+ * time from submission to completion. */
+am24_status am24_poll(am24_server s, uint64_t ticket, float *x, am24_statistics *stats,
+                      int32_t *done);
+/* Blocking form of am24_poll. */
+am24_status am24_wait(am24_server s, uint64_t ticket, float *x, am24_statistics *stats);
 
 /* Kernel kinds reported by am24_batch_step_timed. */
 typedef enum {

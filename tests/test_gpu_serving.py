@@ -1,0 +1,114 @@
+"""The serving layer (am24_server_*, am24_submit / am24_poll / am24_wait) and
+the FP64 host entry point."""
+import ctypes as C
+import importlib
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _am():
+    return importlib.import_module("24am_b200")
+
+
+def test_merged_requests_match_solo_solves(solver, po):
+    """Requests that share a matrix and a step run as one batch; each gets the
+    best of its own starts.  The batch stops when every start of every request
+    has converged, so each result is compared with a solo solve of the same
+    starts within the solver tolerance of the tests."""
+    am = _am()
+    m, n, k = 300, 2000, 64
+    B = po.low_rank_data(m, n, 8, 30, seed=41, dtype=np.float32)
+    B64 = B.astype(np.float64)
+    big = po.low_rank_data(1000, 20000, 8, 30, seed=42, dtype=np.float32)
+    srv = am.Server(0, 40 << 30)
+    mid = srv.add_matrix(B)
+    mbig = srv.add_matrix(big)
+    # a long request on the other matrix keeps the worker busy meanwhile
+    hold = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=0.0,
+                                   maximumIterations=150, totalStartingPoints=512, batchSize=512)
+    t_hold = srv.submit(mbig, hold)
+    time.sleep(0.05)
+    starts = [po.uniform_starts(n, k, seed=50 + i, dtype=np.float32) for i in range(3)]
+    st = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=1e-6,
+                                 maximumIterations=100, totalStartingPoints=k, batchSize=k,
+                                 startMode=am.START_INJECTED)
+    tickets = [srv.submit(mid, st, start_points=V) for V in starts]
+    st4 = am.OptimizationSettings(formulation=4, penaltyParameter=0.3, tolerance=1e-6,
+                                  maximumIterations=100, totalStartingPoints=k, batchSize=k,
+                                  startMode=am.START_INJECTED)
+    t4 = srv.submit(mid, st4, start_points=starts[0])
+    done, _, _ = srv.poll(tickets[0])
+    assert not done  # still queued behind the long request
+    results = [srv.wait(t) for t in tickets]
+    x4, s4 = srv.wait(t4)
+    srv.wait(t_hold)
+    # the three merged requests ran as one batch: same iteration count
+    its = {r[1].it for r in results}
+    assert len(its) == 1, its
+    for (x, s), V in zip(results, starts):
+        assert s.start_iterations == k * s.it
+        assert s.total_elapsed_time >= s.total_true_computation_time
+        M = solver.matrix(B)
+        xs, fs, ss = M.solve(am.OptimizationSettings(
+            formulation=0, constraintParameter=16, tolerance=1e-6, maximumIterations=100,
+            totalStartingPoints=k, batchSize=k, startMode=am.START_INJECTED), start_points=V)
+        M.close()
+        ev = float(np.linalg.norm(B64 @ x.astype(np.float64)) ** 2)
+        ev_solo = float(np.linalg.norm(B64 @ xs.astype(np.float64)) ** 2)
+        assert abs(ev - ev_solo) <= 1e-4 * ev_solo
+        assert abs(s.fval - fs) <= 1e-4 * abs(fs)
+        assert abs(s.explained_variance - ev) <= 1e-6 * ev
+    ev4 = float(np.linalg.norm(B64 @ x4.astype(np.float64)) ** 2)
+    assert np.isfinite(ev4) and ev4 > 0
+    srv.remove_matrix(mbig)
+    srv.close()
+
+
+def test_admission_by_hbm_budget(po):
+    am = _am()
+    B = po.low_rank_data(300, 2000, 8, 30, seed=43, dtype=np.float32)
+    srv = am.Server(0, 8 << 20)  # 8 MiB: less than the matrix's layouts
+    with pytest.raises(am.Am24Error) as ex:
+        srv.add_matrix(B)
+    assert ex.value.status == 7
+    srv.close()
+    srv = am.Server(0, 64 << 20)  # the matrix fits, a large batch does not
+    mid = srv.add_matrix(B)
+    st = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=1e-6,
+                                 maximumIterations=10, totalStartingPoints=4096,
+                                 batchSize=4096)
+    with pytest.raises(am.Am24Error) as ex:
+        srv.submit(mid, st)
+    assert ex.value.status == 7
+    small = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=1e-6,
+                                    maximumIterations=10, totalStartingPoints=32, batchSize=32)
+    x, s = srv.wait(srv.submit(mid, small))
+    assert s.it > 0 and np.isfinite(x).all()
+    srv.close()
+
+
+def test_f64_entry_matches_f32_on_float_data(solver, po):
+    """FP64 host data rounds to FP32 and solves as the FP32 entry point does:
+    on data that are FP32 values, x is the same bit for bit."""
+    am = _am()
+    m, n = 200, 1500
+    B = po.low_rank_data(m, n, 6, 20, seed=44, dtype=np.float32)
+    st32 = am.OptimizationSettings(formulation=2, constraintParameter=12, tolerance=1e-6,
+                                   maximumIterations=50, totalStartingPoints=64, batchSize=32)
+    x32, f32, _ = solver.solve(B, st32)
+    B64 = np.asfortranarray(B.astype(np.float64))
+    x64 = np.zeros(n, np.float64)
+    s = am.OptimizationSettings(formulation=2, constraintParameter=12, tolerance=1e-6,
+                                maximumIterations=50, totalStartingPoints=64,
+                                batchSize=32).to_c()
+    stc = am.am24_statistics()
+    f = C.c_double()
+    am.check(am.lib().am24_solve_dense_f64(solver.h, B64.ctypes.data_as(C.c_void_p), m,
+                                           x64.ctypes.data_as(C.c_void_p), m, n, C.byref(s),
+                                           C.byref(stc), None, C.byref(f)))
+    assert np.array_equal(x64.astype(np.float32), x32)
+    assert f.value == pytest.approx(f32, rel=0, abs=0)
