@@ -38,7 +38,7 @@ FORMULATIONS = {
     "L2var_L0pen": 4, "L1var_L0pen": 5, "L2var_L1pen": 6, "L1var_L1pen": 7,
 }
 
-START_REFERENCE, START_INJECTED = 0, 1
+START_REFERENCE, START_INJECTED, START_DEVICE_UNIFORM = 0, 1, 2
 L1_REFERENCE_SCAN, L1_EXACT = 0, 1
 PRECISION_FP32, PRECISION_MIXED = 0, 1
 

@@ -167,6 +167,26 @@ cudaError_t reset_mixed(const BatchDev &d, cudaStream_t st) {
   return e;
 }
 
+}  // namespace
+
+// The starting points staged in b's Vraw (all batch_size columns) become the
+// batch's loadings: values and masks, dense-step gate, no select hints, and
+// ValueCoordinateHolder::reset (c++/src/utils/various.h:33-38).
+static am24_status load_from_vraw(am24_handle h, am24_batch b) {
+  const MatrixDev &M = b->mat->d;
+  const int k = b->d.k;
+  AM24_CUDA(launch_load_columns(b->d.Vraw, M.ldn, M.n, k, b->d.Vx, M.ldn, b->d.vmask, h->stream));
+  AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));  // dense starts
+  AM24_CUDA(cudaMemsetAsync(b->d.planes_nnz, 0, sizeof(uint32_t), h->stream));  // stale planes
+  AM24_CUDA(cudaMemsetAsync(b->d.sel_hint, 0, sizeof(float) * k, h->stream));      // no hints
+  AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
+  AM24_CUDA(cudaMemsetAsync(b->d.err, 0, sizeof(float) * k, h->stream));
+  if (b->d.mixed) AM24_CUDA(reset_mixed(b->d, h->stream));
+  return AM24_OK;
+}
+
+namespace {
+
 // Split-K factor for Z = B V: minimise rounds * (K blocks per unit + fixed
 // per-unit cost) over the persistent grid.
 void choose_splits(int tiles, int kb_total, int sms, int *splits, int *kbps) {
@@ -198,8 +218,11 @@ am24_status validate_settings(const am24_settings *s) {
   if (s->batch_size < 0) return fail(AM24_ERR_INVALID_ARG, "batch_size must be >= 0");
   if (is_constrained(s->formulation) && s->constraint < 1)
     return fail(AM24_ERR_INVALID_ARG, "constraint (s) must be >= 1 for constrained formulations");
-  if (s->start_mode != AM24_START_REFERENCE && s->start_mode != AM24_START_INJECTED)
+  if (s->start_mode != AM24_START_REFERENCE && s->start_mode != AM24_START_INJECTED &&
+      s->start_mode != AM24_START_DEVICE_UNIFORM)
     return fail(AM24_ERR_INVALID_ARG, "unknown start_mode");
+  if (s->start_mode == AM24_START_DEVICE_UNIFORM && s->use_otf)
+    return fail(AM24_ERR_INVALID_ARG, "device starts need batch mode (use_otf = 0)");
   if (s->l1_mode != AM24_L1_REFERENCE_SCAN && s->l1_mode != AM24_L1_EXACT)
     return fail(AM24_ERR_INVALID_ARG, "unknown l1_mode");
   if (s->precision != AM24_PRECISION_FP32 && s->precision != AM24_PRECISION_MIXED)
@@ -611,15 +634,7 @@ am24_status am24_batch_load(am24_handle h, am24_batch b, const float *V, int32_t
     AM24_CUDA(cudaMemcpy2DAsync(b->d.Vraw, sizeof(float) * M.ldn, V, sizeof(float) * M.n,
                                 sizeof(float) * M.n, k, cudaMemcpyHostToDevice, h->stream));
   }
-  AM24_CUDA(launch_load_columns(b->d.Vraw, M.ldn, M.n, k, b->d.Vx, M.ldn, b->d.vmask, h->stream));
-  AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));  // dense starts
-  AM24_CUDA(cudaMemsetAsync(b->d.planes_nnz, 0, sizeof(uint32_t), h->stream));  // stale planes
-  AM24_CUDA(cudaMemsetAsync(b->d.sel_hint, 0, sizeof(float) * k, h->stream));      // no hints
-  // ValueCoordinateHolder::reset (c++/src/utils/various.h:33-38)
-  AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
-  AM24_CUDA(cudaMemsetAsync(b->d.err, 0, sizeof(float) * k, h->stream));
-  if (b->d.mixed) AM24_CUDA(reset_mixed(b->d, h->stream));
-  return AM24_OK;
+  return load_from_vraw(h, b);
 }
 
 am24_status am24_batch_iterate(am24_handle h, am24_batch b, int32_t it0, int32_t iterations,
@@ -812,9 +827,14 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
         gidx[j] = shift + j;
         slots[j] = j;
       }
-      host_starts(s, n, start_points, gidx.data(), bs, staging);
-      AM24_TRY(upload_columns(h, b, staging.data(), bs, slots.data()));
-      AM24_CUDA(cudaMemsetAsync(d.val, 0, sizeof(float) * bs, h->stream));
+      if (s.start_mode == AM24_START_DEVICE_UNIFORM) {
+        AM24_CUDA(launch_uniform_starts(d.Vraw, M.ldn, (int)n, bs, shift, h->stream));
+        AM24_TRY(load_from_vraw(h, b));
+      } else {
+        host_starts(s, n, start_points, gidx.data(), bs, staging);
+        AM24_TRY(upload_columns(h, b, staging.data(), bs, slots.data()));
+        AM24_CUDA(cudaMemsetAsync(d.val, 0, sizeof(float) * bs, h->stream));
+      }
       if (d.mixed) AM24_CUDA(reset_mixed(d, h->stream));
       uint32_t phase = d.mixed ? 0u : 1u;  // the phase the next step runs in
       AM24_CUDA(cudaEventRecord(e0, h->stream));
@@ -1200,20 +1220,28 @@ am24_status run_group(am24_server s, am24_matrix mat, uint32_t matrix_id,
   am24_batch b = s->cached;
   b->s = bs;  // the step parameters of this group (penalty, tolerance, ...)
   const BatchDev &d = b->d;
-  // starts: each request's own (injected, or the reference generator by its
-  // own start index), one segment after the other
-  std::vector<float> staging((size_t)n * K), seg;
+  // starts: each request's own (injected, the reference generator or the
+  // device generator, by the request's own start indices), one segment after
+  // the other in the batch's staging plane
+  std::vector<float> seg;
   uint32_t off = 0;
   for (auto &r : group) {
     const uint32_t k = (uint32_t)r->s.total_starts;
-    std::vector<unsigned> gidx(k);
-    for (uint32_t i = 0; i < k; i++) gidx[i] = i;
-    host_starts(r->s, n, r->starts.empty() ? nullptr : r->starts.data(), gidx.data(), (int)k,
-                seg);
-    std::memcpy(&staging[(size_t)off * n], seg.data(), sizeof(float) * seg.size());
+    float *dst = d.Vraw + (size_t)off * M.ldn;
+    if (r->s.start_mode == AM24_START_DEVICE_UNIFORM) {
+      AM24_CUDA(launch_uniform_starts(dst, M.ldn, (int)n, (int)k, 0, h->stream));
+    } else {
+      std::vector<unsigned> gidx(k);
+      for (uint32_t i = 0; i < k; i++) gidx[i] = i;
+      host_starts(r->s, n, r->starts.empty() ? nullptr : r->starts.data(), gidx.data(), (int)k,
+                  seg);
+      AM24_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * M.ldn, seg.data(), sizeof(float) * n,
+                                  sizeof(float) * n, k, cudaMemcpyHostToDevice, h->stream));
+      AM24_CUDA(cudaStreamSynchronize(h->stream));  // `seg` is reused
+    }
     off += k;
   }
-  AM24_TRY(am24_batch_load(h, b, staging.data(), 0));
+  AM24_TRY(load_from_vraw(h, b));
   cudaEvent_t e0, e1;
   AM24_CUDA(cudaEventCreate(&e0));
   AM24_CUDA(cudaEventCreate(&e1));

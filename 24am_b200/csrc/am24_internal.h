@@ -108,6 +108,10 @@ cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st);
 cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols, float *dst,
                                 int ld_dst, uint32_t *mask, cudaStream_t st);
 // dst[c][i] = mask bit i of column c ? Vx[c][i] : 0 for i < rows.
+// Columns [0, cols) of V (leading dimension ld): device uniform starts for the
+// global start indices first, first + 1, ... (AM24_START_DEVICE_UNIFORM).
+cudaError_t launch_uniform_starts(float *V, int ld, int rows, int cols, uint32_t first,
+                                  cudaStream_t st);
 cudaError_t launch_masked_copy(const float *Vx, const uint32_t *mask, int ld, int rows, int cols,
                                float *dst, int ld_dst, cudaStream_t st);
 // ev (optional, >= 17 events): ev[i] is recorded before launch i and

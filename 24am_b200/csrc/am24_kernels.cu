@@ -1597,6 +1597,41 @@ cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols
   return cudaGetLastError();
 }
 
+// splitmix64's output mixer (Steele, Lea and Flood, "Fast splittable
+// pseudorandom number generators", OOPSLA 2014): a bijection on 64-bit words.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Column c: U[-1, 1) from the top 24 bits of splitmix64((first + c) << 32 | i)
+// for row i < rows, then scaled to unit 2-norm.
+__global__ void __launch_bounds__(256) uniform_starts_kernel(float *__restrict__ V, int ld,
+                                                             int rows, uint32_t first) {
+  __shared__ double red[32];
+  const size_t c = blockIdx.x;
+  float *v = V + c * ld;
+  const uint64_t key = (uint64_t)(first + (uint32_t)c) << 32;
+  double ss = 0.0;
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+    const float u = (float)(splitmix64(key | (uint32_t)i) >> 40) * (2.0f / 16777216.0f) - 1.0f;
+    v[i] = u;
+    ss += (double)u * (double)u;
+  }
+  ss = block_sum(ss, red);
+  const float inv = (float)(1.0 / sqrt(ss));
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) v[i] *= inv;
+}
+
+cudaError_t launch_uniform_starts(float *V, int ld, int rows, int cols, uint32_t first,
+                                  cudaStream_t st) {
+  if (cols <= 0) return cudaSuccess;
+  uniform_starts_kernel<<<cols, 256, 0, st>>>(V, ld, rows, first);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_masked_copy(const float *Vx, const uint32_t *mask, int ld, int rows, int cols,
                                float *dst, int ld_dst, cudaStream_t st) {
   if (cols <= 0) return cudaSuccess;

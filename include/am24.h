@@ -70,7 +70,10 @@ typedef enum { AM24_PRECISION_FP32 = 0, AM24_PRECISION_MIXED = 1 } am24_precisio
 typedef enum {
   AM24_START_REFERENCE = 0, /* the reference generator: rand_r seeded with the global
                                start index (c++/src/gpower/gpower_commons.h:22-47) */
-  AM24_START_INJECTED = 1   /* caller-supplied n x total_starts matrix */
+  AM24_START_INJECTED = 1,  /* caller-supplied n x total_starts matrix */
+  AM24_START_DEVICE_UNIFORM = 2 /* generated on the device: U[-1, 1] per entry from
+                                   the splitmix64 mixer of (global start index, row),
+                                   column normalised (batch mode only) */
 } am24_start_mode;
 
 /* L1-constraint projection (the soft-thresholding level w). */

@@ -2,7 +2,6 @@
 the FP64 host entry point."""
 import ctypes as C
 import importlib
-import time
 
 import numpy as np
 import pytest
@@ -23,16 +22,17 @@ def test_merged_requests_match_solo_solves(solver, po):
     m, n, k = 300, 2000, 64
     B = po.low_rank_data(m, n, 8, 30, seed=41, dtype=np.float32)
     B64 = B.astype(np.float64)
-    big = po.low_rank_data(1000, 20000, 8, 30, seed=42, dtype=np.float32)
+    big = po.low_rank_data(1500, 40000, 8, 30, seed=42, dtype=np.float32)
     srv = am.Server(0, 40 << 30)
     mid = srv.add_matrix(B)
     mbig = srv.add_matrix(big)
-    # a long request on the other matrix keeps the worker busy meanwhile
-    hold = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=0.0,
-                                   maximumIterations=150, totalStartingPoints=512, batchSize=512)
-    t_hold = srv.submit(mbig, hold)
-    time.sleep(0.05)
     starts = [po.uniform_starts(n, k, seed=50 + i, dtype=np.float32) for i in range(3)]
+    # a long request on the other matrix (tolerance 0: all 300 iterations, some
+    # 0.3 s) keeps the worker busy while the others queue
+    hold = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=0.0,
+                                   maximumIterations=300, totalStartingPoints=1024,
+                                   batchSize=1024)
+    t_hold = srv.submit(mbig, hold)
     st = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=1e-6,
                                  maximumIterations=100, totalStartingPoints=k, batchSize=k,
                                  startMode=am.START_INJECTED)
@@ -112,3 +112,34 @@ def test_f64_entry_matches_f32_on_float_data(solver, po):
                                            C.byref(stc), None, C.byref(f)))
     assert np.array_equal(x64.astype(np.float32), x32)
     assert f.value == pytest.approx(f32, rel=0, abs=0)
+
+
+def splitmix64(x):
+    """The splitmix64 output mixer on uint64 arrays (wrapping arithmetic)."""
+    x = (x + np.uint64(0x9E3779B97F4A7C15))
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def test_device_starts_follow_their_definition(solver, po):
+    """AM24_START_DEVICE_UNIFORM: entry i of start c is U[-1, 1) from the top 24
+    bits of splitmix64((c << 32) | i), then the column is normalised.  A solve
+    from device starts and one from the same starts computed here agree."""
+    am = _am()
+    m, n, k = 200, 1500, 64
+    B = po.low_rank_data(m, n, 6, 20, seed=45, dtype=np.float32)
+    with np.errstate(over="ignore"):
+        key = (np.arange(k, dtype=np.uint64)[None, :] << np.uint64(32)) | \
+            np.arange(n, dtype=np.uint64)[:, None]
+        z = splitmix64(key)
+    U = (z >> np.uint64(40)).astype(np.float64) * (2.0 / 16777216.0) - 1.0
+    V = (U / np.linalg.norm(U, axis=0)).astype(np.float32)
+    common = dict(formulation=0, constraintParameter=12, tolerance=1e-6, maximumIterations=60,
+                  totalStartingPoints=k, batchSize=k)
+    xd, fd, sd = solver.solve(B, am.OptimizationSettings(startMode=am.START_DEVICE_UNIFORM,
+                                                         **common))
+    xi, fi, si = solver.solve(B, am.OptimizationSettings(startMode=am.START_INJECTED, **common),
+                              start_points=V)
+    assert abs(fd - fi) <= 1e-5 * abs(fi)
+    assert abs(sd.explainedVariance - si.explainedVariance) <= 1e-5 * si.explainedVariance
