@@ -58,20 +58,33 @@ am24_status fail(am24_status s, const std::string &msg) {
 
 int round_up(int v, int a) { return (v + a - 1) / a * a; }
 
-// Scoped device allocations of one object.
+// Scoped device allocations of one object.  With a stream, stream-ordered
+// (cudaMallocAsync / cudaFreeAsync on it, for memory only that stream uses):
+// freeing then waits for no other stream, which matters when several handles
+// work on one device at once.
 struct Allocs {
   std::vector<void *> ptrs;
+  cudaStream_t stream = nullptr;
+  bool ordered = false;
+  Allocs() = default;
+  explicit Allocs(cudaStream_t st) : stream(st), ordered(true) {}
   ~Allocs() {
-    for (void *p : ptrs) cudaFree(p);
+    for (void *p : ptrs) {
+      if (ordered)
+        cudaFreeAsync(p, stream);
+      else
+        cudaFree(p);
+    }
   }
   template <typename T>
   am24_status get(T **out, size_t count) {
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = ordered ? cudaMallocAsync(&p, bytes, stream) : cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return fail(e == cudaErrorMemoryAllocation ? AM24_ERR_OOM : AM24_ERR_CUDA,
-                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+                  std::string("device allocation: ") + cudaGetErrorString(e));
     }
     ptrs.push_back(p);
     *out = static_cast<T *>(p);
@@ -507,6 +520,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
     return fail(AM24_ERR_INVALID_ARG, "constraint exceeds n (run am24_check_input first)");
   AM24_CUDA(cudaSetDevice(h->device));
   auto *b = new am24_batch_s();
+  b->mem.stream = h->stream;  // used on this handle's stream only
+  b->mem.ordered = true;
   b->mat = mat;
   b->s = *settings;
   const MatrixDev &M = mat->d;
@@ -783,7 +798,7 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
 
   // best loading so far, kept as hi/lo planes; starts as the caller's x, which
   // the reference returns normalised when no start ever improves on -1
-  Allocs local;
+  Allocs local(h->stream);
   float *xb = nullptr, *x_dev = nullptr;
   double *ev_rows = nullptr;
   AM24_TRY(local.get(&xb, n));
@@ -1162,10 +1177,21 @@ uint64_t batch_bytes(uint32_t m, uint32_t n, uint32_t k) {
 
 }  // namespace
 
+// One worker thread: its own handle (stream) and its last batch, reused while
+// the matrix, the batch size and the batch-shaping settings stay the same.
+struct ServeWorker {
+  am24_handle h = nullptr;
+  std::thread thread;
+  am24_batch cached = nullptr;
+  uint32_t cached_matrix = 0, cached_k = 0;
+  am24_settings cached_s{};
+};
+
 struct am24_server_s {
-  am24_handle worker_h = nullptr;  // used by the worker thread only
-  am24_handle upload_h = nullptr;  // matrix uploads from callers' threads
+  std::vector<ServeWorker> workers;  // each used by its own thread only
+  am24_handle upload_h = nullptr;    // matrix uploads from callers' threads
   std::mutex upload_mu;
+  std::mutex create_mu;  // batch creation (it may add BF16 planes to a shared matrix)
   uint64_t budget = 0;
   std::mutex mu;  // everything below
   std::condition_variable cv_work, cv_done;
@@ -1181,21 +1207,17 @@ struct am24_server_s {
   uint64_t next_ticket = 1;
   std::deque<RequestPtr> queue;
   std::map<uint64_t, RequestPtr> tickets;
+  uint64_t inflight = 0;  // device bytes of the batches the workers are running
   bool stop = false;
   uint32_t max_batch = 8192;
-  std::thread worker;
-  // the worker's cached batch (reused while the shape and step stay the same)
-  am24_batch cached = nullptr;
-  uint32_t cached_matrix = 0, cached_k = 0;
-  am24_settings cached_s{};
 };
 
 namespace {
 
 // Runs one batch made of the requests' starts (worker thread).
-am24_status run_group(am24_server s, am24_matrix mat, uint32_t matrix_id,
+am24_status run_group(am24_server s, ServeWorker &w, am24_matrix mat, uint32_t matrix_id,
                       std::vector<RequestPtr> &group) {
-  am24_handle h = s->worker_h;
+  am24_handle h = w.h;
   const MatrixDev &M = mat->d;
   const unsigned n = (unsigned)M.n;
   uint32_t K = 0;
@@ -1206,18 +1228,19 @@ am24_status run_group(am24_server s, am24_matrix mat, uint32_t matrix_id,
   bs.total_batches = 1;
   bs.use_otf = 0;
   bs.store_all = 0;
-  if (!(s->cached && s->cached_matrix == matrix_id && s->cached_k == K &&
-        s->cached_s.formulation == bs.formulation && s->cached_s.precision == bs.precision &&
-        s->cached_s.stable_iterations == bs.stable_iterations &&
-        s->cached_s.stable_share == bs.stable_share)) {
-    if (s->cached) am24_batch_destroy(h, s->cached);
-    s->cached = nullptr;
-    AM24_TRY(am24_batch_create(h, mat, &bs, K, &s->cached));
-    s->cached_matrix = matrix_id;
-    s->cached_k = K;
-    s->cached_s = bs;
+  if (!(w.cached && w.cached_matrix == matrix_id && w.cached_k == K &&
+        w.cached_s.formulation == bs.formulation && w.cached_s.precision == bs.precision &&
+        w.cached_s.stable_iterations == bs.stable_iterations &&
+        w.cached_s.stable_share == bs.stable_share)) {
+    if (w.cached) am24_batch_destroy(h, w.cached);
+    w.cached = nullptr;
+    std::lock_guard<std::mutex> lk(s->create_mu);
+    AM24_TRY(am24_batch_create(h, mat, &bs, K, &w.cached));
+    w.cached_matrix = matrix_id;
+    w.cached_k = K;
+    w.cached_s = bs;
   }
-  am24_batch b = s->cached;
+  am24_batch b = w.cached;
   b->s = bs;  // the step parameters of this group (penalty, tolerance, ...)
   const BatchDev &d = b->d;
   // starts: each request's own (injected, the reference generator or the
@@ -1280,7 +1303,7 @@ am24_status run_group(am24_server s, am24_matrix mat, uint32_t matrix_id,
   float ms = 0.f;
   AM24_CUDA(cudaEventElapsedTime(&ms, e0, e1));
   // per request: the best of its own starts, normalised, and its ||B x||^2
-  Allocs local;
+  Allocs local(h->stream);
   float *xb = nullptr, *x_dev = nullptr;
   double *ev_rows = nullptr;
   AM24_TRY(local.get(&xb, n));
@@ -1327,64 +1350,80 @@ am24_status run_group(am24_server s, am24_matrix mat, uint32_t matrix_id,
   return AM24_OK;
 }
 
-void worker_loop(am24_server s) {
-  cudaSetDevice(s->worker_h->device);
+void worker_loop(am24_server s, size_t wi) {
+  ServeWorker &w = s->workers[wi];
+  cudaSetDevice(w.h->device);
   for (;;) {
-    std::vector<RequestPtr> take;
+    // the oldest queued request and every later one that shares its step, while
+    // the batch fits the largest batch size and the budget left beside the
+    // resident matrices and the other workers' batches
+    std::vector<RequestPtr> group;
+    am24_matrix mat = nullptr;
+    uint64_t bytes = 0;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-      if (s->queue.empty()) return;  // stopping, nothing left
-      take.assign(s->queue.begin(), s->queue.end());
-      s->queue.clear();
-    }
-    while (!take.empty()) {
-      // the oldest request and every later one that shares its step, while
-      // the batch stays within the server's limits
-      std::vector<RequestPtr> group{take.front()};
-      std::vector<RequestPtr> rest;
-      am24_matrix mat = nullptr;
-      uint64_t room = 0;
-      uint32_t m = 0, n = 0;
-      {
-        std::lock_guard<std::mutex> lk(s->mu);
-        auto &res = s->matrices.at(take.front()->matrix_id);
+      for (;;) {
+        s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+        if (s->queue.empty()) return;  // stopping, nothing left
+        const RequestPtr head = s->queue.front();
+        const auto &res = s->matrices.at(head->matrix_id);
+        const uint64_t used = s->resident + s->inflight;
+        const uint64_t room = s->budget > used ? s->budget - used : 0;
+        uint32_t K = (uint32_t)head->s.total_starts;
+        if (batch_bytes(res.m, res.n, K) > room) {
+          if (s->inflight > 0) {  // wait for another worker's batch to finish
+            s->cv_work.wait(lk);
+            continue;
+          }
+          // the matrices admitted since this request was queued leave no room
+          s->queue.pop_front();
+          head->status = AM24_ERR_ADMISSION_REJECTED;
+          head->error = "the request's batch no longer fits the budget";
+          head->done = true;
+          s->matrices.at(head->matrix_id).pending--;
+          s->cv_done.notify_all();
+          continue;
+        }
+        group.push_back(head);
+        std::deque<RequestPtr> rest;
+        for (size_t i = 1; i < s->queue.size(); i++) {
+          const RequestPtr &r = s->queue[i];
+          const uint32_t k = (uint32_t)r->s.total_starts;
+          if (same_step(*head, *r) && K + k <= s->max_batch &&
+              batch_bytes(res.m, res.n, K + k) <= room) {
+            group.push_back(r);
+            K += k;
+          } else {
+            rest.push_back(r);
+          }
+        }
+        s->queue.swap(rest);
+        bytes = batch_bytes(res.m, res.n, K);
+        s->inflight += bytes;
         mat = res.mat;
-        m = res.m;
-        n = res.n;
-        room = s->budget > s->resident ? s->budget - s->resident : 0;
+        break;
       }
-      uint32_t K = (uint32_t)group[0]->s.total_starts;
-      for (size_t i = 1; i < take.size(); i++) {
-        const uint32_t k = (uint32_t)take[i]->s.total_starts;
-        if (same_step(*group[0], *take[i]) && K + k <= s->max_batch &&
-            batch_bytes(m, n, K + k) <= room) {
-          group.push_back(take[i]);
-          K += k;
-        } else {
-          rest.push_back(take[i]);
-        }
-      }
-      take.swap(rest);
-      const am24_status st = run_group(s, mat, group[0]->matrix_id, group);
-      const std::string err = st == AM24_OK ? std::string() : g_last_error;
-      if (st != AM24_OK && s->cached) {  // do not reuse a batch left in an unknown state
-        am24_batch_destroy(s->worker_h, s->cached);
-        s->cached = nullptr;
-      }
-      const auto now = std::chrono::steady_clock::now();
-      {
-        std::lock_guard<std::mutex> lk(s->mu);
-        for (auto &r : group) {
-          r->status = st;
-          r->error = err;
-          r->stats.total_elapsed_time = std::chrono::duration<double>(now - r->submitted).count();
-          r->done = true;
-          s->matrices.at(r->matrix_id).pending--;
-        }
-      }
-      s->cv_done.notify_all();
     }
+    const am24_status st = run_group(s, w, mat, group[0]->matrix_id, group);
+    const std::string err = st == AM24_OK ? std::string() : g_last_error;
+    if (st != AM24_OK && w.cached) {  // do not reuse a batch left in an unknown state
+      am24_batch_destroy(w.h, w.cached);
+      w.cached = nullptr;
+    }
+    const auto now = std::chrono::steady_clock::now();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->inflight -= bytes;
+      for (auto &r : group) {
+        r->status = st;
+        r->error = err;
+        r->stats.total_elapsed_time = std::chrono::duration<double>(now - r->submitted).count();
+        r->done = true;
+        s->matrices.at(r->matrix_id).pending--;
+      }
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();  // budget freed
   }
 }
 
@@ -1406,14 +1445,19 @@ am24_status am24_server_create(int device, uint64_t hbm_budget_bytes, am24_serve
   *out = nullptr;
   auto *s = new am24_server_s();
   s->budget = hbm_budget_bytes;
-  am24_status st;
-  if ((st = am24_create(&s->worker_h, device)) != AM24_OK ||
-      (st = am24_create(&s->upload_h, device)) != AM24_OK) {
-    if (s->worker_h) am24_destroy(s->worker_h);
+  s->workers.resize(AM24_SERVER_WORKERS);
+  am24_status st = am24_create(&s->upload_h, device);
+  for (size_t i = 0; st == AM24_OK && i < s->workers.size(); i++)
+    st = am24_create(&s->workers[i].h, device);
+  if (st != AM24_OK) {
+    for (auto &w : s->workers)
+      if (w.h) am24_destroy(w.h);
+    if (s->upload_h) am24_destroy(s->upload_h);
     delete s;
     return st;
   }
-  s->worker = std::thread(worker_loop, s);
+  for (size_t i = 0; i < s->workers.size(); i++)
+    s->workers[i].thread = std::thread(worker_loop, s, i);
   *out = s;
   return AM24_OK;
 }
@@ -1425,10 +1469,13 @@ am24_status am24_server_destroy(am24_server s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
-  if (s->worker.joinable()) s->worker.join();
-  if (s->cached) am24_batch_destroy(s->worker_h, s->cached);
+  for (auto &w : s->workers)
+    if (w.thread.joinable()) w.thread.join();
+  for (auto &w : s->workers) {
+    if (w.cached) am24_batch_destroy(w.h, w.cached);
+    am24_destroy(w.h);
+  }
   for (auto &kv : s->matrices) am24_matrix_destroy(s->upload_h, kv.second.mat);
-  am24_destroy(s->worker_h);
   am24_destroy(s->upload_h);
   delete s;
   return AM24_OK;
@@ -1471,10 +1518,9 @@ am24_status am24_server_remove_matrix(am24_server s, uint32_t matrix_id) {
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->matrices.find(matrix_id);
     if (it == s->matrices.end()) return fail(AM24_ERR_INVALID_ARG, "unknown matrix id");
+    // (a worker's cached batch of this matrix is never reused: ids are not reused)
     if (it->second.pending > 0)
       return fail(AM24_ERR_INVALID_ARG, "requests for this matrix are pending");
-    if (s->cached && s->cached_matrix == matrix_id)
-      return fail(AM24_ERR_INVALID_ARG, "the matrix is in use");
     mat = it->second.mat;
     s->resident -= it->second.bytes;
     s->matrices.erase(it);

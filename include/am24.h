@@ -231,7 +231,8 @@ am24_status am24_sync(am24_handle h);
 void *am24_stream(am24_handle h);
 
 /* ---- serving: resident matrices, queued solves, batching on arrival ------- */
-/* A server owns its own handles on `device` and one worker thread.  Matrices
+/* A server owns its own handles on `device` and AM24_SERVER_WORKERS worker
+ * threads, each with its own stream, which run different batches at once.  Matrices
  * are admitted while their device layouts fit hbm_budget_bytes (the budget
  * also bounds the largest request batch).  Queued requests that share a
  * matrix and the settings that shape the AM step (formulation, constraint,
@@ -241,6 +242,7 @@ void *am24_stream(am24_handle h);
  * form one segment of that batch (batchSize = totalStartingPoints), and the
  * batch stops on its batch-wide maximum change as a reference batch does.
  * settings->use_otf and store_all are not supported by the server. */
+#define AM24_SERVER_WORKERS 4 /* worker threads (streams) per server */
 typedef struct am24_server_s *am24_server;
 am24_status am24_server_create(int device, uint64_t hbm_budget_bytes, am24_server *out);
 /* Finishes queued requests, then frees everything the server holds. */

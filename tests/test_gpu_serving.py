@@ -27,12 +27,12 @@ def test_merged_requests_match_solo_solves(solver, po):
     mid = srv.add_matrix(B)
     mbig = srv.add_matrix(big)
     starts = [po.uniform_starts(n, k, seed=50 + i, dtype=np.float32) for i in range(3)]
-    # a long request on the other matrix (tolerance 0: all 300 iterations, some
-    # 0.3 s) keeps the worker busy while the others queue
-    hold = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=0.0,
-                                   maximumIterations=300, totalStartingPoints=1024,
-                                   batchSize=1024)
-    t_hold = srv.submit(mbig, hold)
+    # long requests on the other matrix (tolerance 0: all 300 iterations, some
+    # 0.3 s each; different s, so they do not merge) keep every worker busy
+    # while the others queue
+    holds = [srv.submit(mbig, am.OptimizationSettings(
+        formulation=0, constraintParameter=16 + i, tolerance=0.0, maximumIterations=300,
+        totalStartingPoints=1024, batchSize=1024)) for i in range(4)]
     st = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=1e-6,
                                  maximumIterations=100, totalStartingPoints=k, batchSize=k,
                                  startMode=am.START_INJECTED)
@@ -45,7 +45,8 @@ def test_merged_requests_match_solo_solves(solver, po):
     assert not done  # still queued behind the long request
     results = [srv.wait(t) for t in tickets]
     x4, s4 = srv.wait(t4)
-    srv.wait(t_hold)
+    for t in holds:
+        srv.wait(t)
     # the three merged requests ran as one batch: same iteration count
     its = {r[1].it for r in results}
     assert len(its) == 1, its
