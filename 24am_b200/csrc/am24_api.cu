@@ -402,6 +402,14 @@ am24_status am24_create(am24_handle *out, int device) {
   if (prop.major != 10)
     return fail(AM24_ERR_UNSUPPORTED, std::string("needs an sm_100 (B200-class) GPU, found ") +
                                           prop.name);
+  // Stream-ordered allocations (batches, one-call matrices, temporaries) come
+  // from the device's default pool; keep what they free there for reuse
+  // instead of returning it to the driver at every synchronization, which makes
+  // the next allocation map the memory again.
+  cudaMemPool_t pool;
+  AM24_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t keep = UINT64_MAX;
+  AM24_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   auto *h = new am24_handle_s();
   h->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
@@ -444,8 +452,12 @@ am24_status am24_sync(am24_handle h) {
 }
 
 // ============================================================== matrices
-am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, uint32_t m,
-                                   uint32_t n, int32_t on_device, am24_matrix *out) {
+}  // extern "C"
+
+// `ordered`: the matrix is private to the handle's stream (the one-call
+// solves), so its memory is stream-ordered too.
+static am24_status create_matrix(am24_handle h, const float *B, int32_t ldB, uint32_t m,
+                                 uint32_t n, int32_t on_device, bool ordered, am24_matrix *out) {
   if (!h || !B || !out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
   *out = nullptr;
   if (m == 0 || n == 0) return fail(AM24_ERR_INVALID_ARG, "m and n must be positive");
@@ -453,6 +465,10 @@ am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, u
   if (m > (1u << 30) || n > (1u << 30)) return fail(AM24_ERR_INVALID_ARG, "matrix too large");
   AM24_CUDA(cudaSetDevice(h->device));
   auto *mat = new am24_matrix_s();
+  if (ordered) {
+    mat->mem.stream = h->stream;
+    mat->mem.ordered = true;
+  }
   MatrixDev &M = mat->d;
   M.m = (int)m;
   M.n = (int)n;
@@ -496,6 +512,13 @@ am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, u
   }
   *out = mat;
   return AM24_OK;
+}
+
+extern "C" {
+
+am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, uint32_t m,
+                                   uint32_t n, int32_t on_device, am24_matrix *out) {
+  return create_matrix(h, B, ldB, m, n, on_device, false, out);
 }
 
 am24_status am24_matrix_destroy(am24_handle h, am24_matrix mat) {
@@ -842,14 +865,19 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
         gidx[j] = shift + j;
         slots[j] = j;
       }
+      // the batch's starts, staged in Vraw by one copy (or generated there)
       if (s.start_mode == AM24_START_DEVICE_UNIFORM) {
         AM24_CUDA(launch_uniform_starts(d.Vraw, M.ldn, (int)n, bs, shift, h->stream));
-        AM24_TRY(load_from_vraw(h, b));
       } else {
-        host_starts(s, n, start_points, gidx.data(), bs, staging);
-        AM24_TRY(upload_columns(h, b, staging.data(), bs, slots.data()));
-        AM24_CUDA(cudaMemsetAsync(d.val, 0, sizeof(float) * bs, h->stream));
+        const float *src = start_points + (size_t)shift * n;  // injected: read in place
+        if (s.start_mode != AM24_START_INJECTED) {
+          host_starts(s, n, start_points, gidx.data(), bs, staging);
+          src = staging.data();
+        }
+        AM24_CUDA(cudaMemcpy2DAsync(d.Vraw, sizeof(float) * M.ldn, src, sizeof(float) * n,
+                                    sizeof(float) * n, bs, cudaMemcpyHostToDevice, h->stream));
       }
+      AM24_TRY(load_from_vraw(h, b));
       if (d.mixed) AM24_CUDA(reset_mixed(d, h->stream));
       uint32_t phase = d.mixed ? 0u : 1u;  // the phase the next step runs in
       AM24_CUDA(cudaEventRecord(e0, h->stream));
@@ -1008,7 +1036,7 @@ am24_status am24_solve_dense_f32(am24_handle h, const float *B, int32_t ldB, flo
                                  const float *start_points, float *fval_out) {
   const auto t0 = std::chrono::steady_clock::now();
   am24_matrix mat = nullptr;
-  AM24_TRY(am24_matrix_create_f32(h, B, ldB, m, n, 0, &mat));
+  AM24_TRY(create_matrix(h, B, ldB, m, n, 0, true, &mat));
   am24_status st = am24_solve_resident_f32(h, mat, x, settings, stats, start_points, fval_out);
   am24_matrix_destroy(h, mat);
   if (st == AM24_OK && stats)
@@ -1023,7 +1051,7 @@ am24_status am24_solve_device_f32(am24_handle h, const float *d_B, int32_t ldB, 
                                   float *fval_out) {
   const auto t0 = std::chrono::steady_clock::now();
   am24_matrix mat = nullptr;
-  AM24_TRY(am24_matrix_create_f32(h, d_B, ldB, m, n, 1, &mat));
+  AM24_TRY(create_matrix(h, d_B, ldB, m, n, 1, true, &mat));
   am24_status st = am24_solve_resident_f32(h, mat, x, settings, stats, start_points, fval_out);
   am24_matrix_destroy(h, mat);
   if (st == AM24_OK && stats)
