@@ -43,7 +43,8 @@ L1_REFERENCE_SCAN, L1_EXACT = 0, 1
 PRECISION_FP32, PRECISION_MIXED = 0, 1
 
 STATUS = {0: "AM24_OK", 1: "AM24_ERR_INVALID_ARG", 2: "AM24_ERR_OOM", 3: "AM24_ERR_CUDA",
-          4: "AM24_ERR_DEVICE_TIMEOUT", 5: "AM24_ERR_UNSUPPORTED", 6: "AM24_ERR_DEGENERATE"}
+          4: "AM24_ERR_DEVICE_TIMEOUT", 5: "AM24_ERR_UNSUPPORTED", 6: "AM24_ERR_DEGENERATE",
+          7: "AM24_ERR_ADMISSION_REJECTED"}
 
 
 class Am24Error(RuntimeError):
@@ -122,6 +123,7 @@ _SIGS = {
                             C.POINTER(C.c_int32)]),
     "am24_wait": (C.c_int, [_VP, C.c_uint64, _VP, C.POINTER(am24_statistics)]),
     "am24_sync": (C.c_int, [_VP]),
+    "am24_selftest_bounded_wait": (C.c_int, [_VP, C.c_uint32]),
     "am24_stream": (C.c_void_p, [_VP]),
     "am24_batch_step_timed": (C.c_int, [_VP, _VP, C.c_int32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),

@@ -445,6 +445,26 @@ am24_status am24_destroy(am24_handle h) {
   return AM24_OK;
 }
 
+am24_status am24_selftest_bounded_wait(am24_handle h, uint32_t timeout_us) {
+  if (!h) return fail(AM24_ERR_INVALID_ARG, "NULL handle");
+  AM24_CUDA(cudaSetDevice(h->device));
+  int *status = nullptr;
+  Allocs local(h->stream);
+  AM24_TRY(local.get(&status, 1));
+  AM24_CUDA(cudaMemsetAsync(status, 0, sizeof(int), h->stream));
+  AM24_CUDA(launch_bounded_wait_probe((unsigned long long)timeout_us * 1000ull, status,
+                                      h->stream));
+  int code = 0;
+  AM24_CUDA(cudaMemcpyAsync(&code, status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  if (code != 0) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "device-side wait timed out (code 0x%x)", code);
+    return fail(AM24_ERR_DEVICE_TIMEOUT, buf);
+  }
+  return fail(AM24_ERR_CUDA, "the bounded-wait probe returned without giving up");
+}
+
 am24_status am24_sync(am24_handle h) {
   if (!h) return fail(AM24_ERR_INVALID_ARG, "handle is NULL");
   AM24_CUDA(cudaStreamSynchronize(h->stream));

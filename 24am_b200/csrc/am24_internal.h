@@ -120,6 +120,10 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
                            const StepParams &p, cudaStream_t st, int *launches,
                            cudaEvent_t *ev = nullptr, int *kinds = nullptr);
 cudaError_t launch_finalize_x(const float *v, int n, float *x, cudaStream_t st);
+// A wait that nothing satisfies, bounded by timeout_ns; records the probe's
+// timeout code in *status.
+cudaError_t launch_bounded_wait_probe(unsigned long long timeout_ns, int *status,
+                                      cudaStream_t st);
 cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double *partial,
                                       double *out, cudaStream_t st);
 int pick_bn(int k);

@@ -557,17 +557,12 @@ struct SelResult {
   uint32_t eq;   // number of keys equal
 };
 
-template <bool CACHED>
-__device__ __forceinline__ uint32_t col_key(const float *__restrict__ g, const float *s, int i) {
-  return abs_key(CACHED ? s[i] : g[i]);
-}
 
 // Key of descending rank `rank` (1 = largest) among |col[0..n)|, by three
 // histogram passes over 11, 11 and 9 key bits.  All threads of the block
 // call it; hist has 2048 entries, res 4.
-template <bool CACHED>
-__device__ SelResult block_select(const float *__restrict__ colg, const float *cols, int n,
-                                  uint32_t rank, uint32_t *hist, uint32_t *res) {
+__device__ SelResult block_select(const float *__restrict__ colg, int n, uint32_t rank,
+                                  uint32_t *hist, uint32_t *res) {
   uint32_t prefix = 0, pmask = 0, gt = 0, need = rank, eq = 0;
 #pragma unroll 1
   for (int lvl = 0; lvl < 3; lvl++) {
@@ -577,7 +572,7 @@ __device__ SelResult block_select(const float *__restrict__ colg, const float *c
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t key = col_key<CACHED>(colg, cols, i);
+      const uint32_t key = abs_key(colg[i]);
       if ((key & pmask) == prefix) {
         const uint32_t bin = (key >> sh) & bmask;
         const unsigned peers = __match_any_sync(__activemask(), bin);
@@ -694,13 +689,11 @@ __device__ void find_rank_bin(const uint32_t *hist, int nb, uint32_t need, uint3
 }
 
 // Top-11-bit histogram of |col| keys into hist[2048] (warp-aggregated adds).
-template <bool CACHED>
-__device__ void key_histogram(const float *__restrict__ colg, const float *cols, int n,
-                              uint32_t *hist) {
+__device__ void key_histogram(const float *__restrict__ colg, int n, uint32_t *hist) {
   for (int b = threadIdx.x; b < 2048; b += blockDim.x) hist[b] = 0;
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const uint32_t bin = col_key<CACHED>(colg, cols, i) >> 20;
+    const uint32_t bin = abs_key(colg[i]) >> 20;
     const unsigned peers = __match_any_sync(__activemask(), bin);
     if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], __popc(peers));
   }
@@ -877,7 +870,7 @@ __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
     cnt = (double)kept;
   } else {
     // (b) histogram of the top 11 key bits, then the bin holding rank s
-    key_histogram<false>(colg, nullptr, n, hist);
+    key_histogram(colg, n, hist);
     find_rank_bin(hist, 2048, s, res);
     const uint32_t b1 = res[0], above = res[1], in_bin = res[2];
     __syncthreads();
@@ -911,7 +904,7 @@ __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
         }
     } else {
       // (c) exact radix select
-      thr = block_select<false>(colg, nullptr, n, s, hist, res).key;
+      thr = block_select(colg, n, s, hist, res).key;
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const float v = colg[i];
         if (abs_key(v) >= thr) {
@@ -1206,7 +1199,7 @@ __global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
   // ---- fast path: the highest bins holding at most SOFT_C values
   uint32_t c = 0, bstar = 0;
   if (brk == NONE) {
-    key_histogram<false>(colg, nullptr, n, hist);
+    key_histogram(colg, n, hist);
     find_rank_bin(hist, 2048, (uint32_t)SOFT_C + 1u, res);
     const bool whole = (uint32_t)n <= (uint32_t)SOFT_C;
     bstar = whole ? 0u : res[0] + 1u;  // gather bins >= bstar
@@ -1265,14 +1258,14 @@ __global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
 
   // ---- exact walk, a chunk of SOFT_C ranks at a time
   if (brk == NONE) {
-    const SelResult top = block_select<false>(colg, nullptr, n, 1u, hist, res);
+    const SelResult top = block_select(colg, n, 1u, hist, res);
     const double lim = __dsub_rn((double)__uint_as_float(top.key), 0.000001);
     uint32_t consumed = 0, khi = NONE, ge_hi = 0;
     double S1 = 0.0, S2 = 0.0;
     while (true) {
       const uint32_t R = min(consumed + (uint32_t)SOFT_C, (uint32_t)n);
       const uint32_t total = R - consumed;
-      const SelResult lo = block_select<false>(colg, nullptr, n, R, hist, res);
+      const SelResult lo = block_select(colg, n, R, hist, res);
       if (threadIdx.x == 0) misc[0] = 0;
       __syncthreads();
       if (lo.key == khi) {
@@ -1636,6 +1629,28 @@ cudaError_t launch_masked_copy(const float *Vx, const uint32_t *mask, int ld, in
                                float *dst, int ld_dst, cudaStream_t st) {
   if (cols <= 0) return cudaSuccess;
   masked_copy_kernel<<<cols, 256, 0, st>>>(Vx, mask, ld, rows, dst, ld_dst);
+  return cudaGetLastError();
+}
+
+// One warp waits, bounded by timeout_ns, on an mbarrier that nothing arrives
+// on: the wait gives up, records DEV_ERR_TIMEOUT_PROBE in *status and the
+// kernel returns, as every kernel's waits do when a partner never comes.
+__global__ void bounded_wait_probe_kernel(unsigned long long timeout_ns, int *status) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  mbar_wait_bounded(&bar, 0, &abort_flag, status, DEV_ERR_TIMEOUT_PROBE, timeout_ns);
+  __syncwarp();
+}
+
+cudaError_t launch_bounded_wait_probe(unsigned long long timeout_ns, int *status,
+                                      cudaStream_t st) {
+  bounded_wait_probe_kernel<<<1, 32, 0, st>>>(timeout_ns, status);
   return cudaGetLastError();
 }
 

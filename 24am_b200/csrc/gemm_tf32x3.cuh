@@ -44,6 +44,7 @@ enum DeviceError : int {
   DEV_ERR_TIMEOUT_MMA_SMEM = 0x102,
   DEV_ERR_TIMEOUT_MMA_TMEM = 0x103,
   DEV_ERR_TIMEOUT_EPILOGUE = 0x104,
+  DEV_ERR_TIMEOUT_PROBE = 0x1FF,  // the bounded-wait self-test (expected)
 };
 
 struct GemmShape {

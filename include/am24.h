@@ -224,6 +224,11 @@ am24_status am24_batch_iterate_static_ws(am24_handle h, am24_batch b, int32_t it
 am24_status am24_batch_phase(am24_handle h, am24_batch b, int32_t *refining);
 /* Number of kernel launches one am24_batch_iterate step issues. */
 am24_status am24_batch_launches_per_step(am24_handle h, am24_batch b, int32_t *launches);
+/* Diagnostic of the device-side timeouts: runs a kernel whose wait nothing
+ * satisfies, bounded by timeout_us.  It gives up, reports as a timed-out solve
+ * does (returns AM24_ERR_DEVICE_TIMEOUT, the expected outcome) and leaves the
+ * handle usable.  Synchronizes the handle's stream. */
+am24_status am24_selftest_bounded_wait(am24_handle h, uint32_t timeout_us);
 /* Synchronizes the handle's stream. */
 am24_status am24_sync(am24_handle h);
 /* The handle's CUDA stream (a cudaStream_t), for callers that record their own

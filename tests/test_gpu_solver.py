@@ -95,3 +95,21 @@ def test_large_gamma_is_degenerate_like_reference(solver, po):
     r = po.oracle_solve(B.astype(np.float64), po.make_settings(6, penalty=1e6, max_iter=5,
                                                                 total_starts=8, batch_size=8))
     assert np.isnan(r["x"]).all() == np.isnan(x).all()
+
+
+def test_device_wait_gives_up_and_handle_stays_usable(solver, po):
+    """A wait that nothing satisfies ends after its limit with the timeout
+    status (no trap, no hang); the same handle then solves normally."""
+    import time
+    am = _am()
+    t0 = time.perf_counter()
+    status = am.lib().am24_selftest_bounded_wait(solver.h, 20000)  # 20 ms
+    elapsed = time.perf_counter() - t0
+    assert status == 4, am.last_error()  # AM24_ERR_DEVICE_TIMEOUT
+    assert "timed out" in am.last_error()
+    assert 0.015 <= elapsed < 2.0
+    B = po.low_rank_data(120, 700, 6, 20, seed=3, dtype=np.float32)
+    st = am.OptimizationSettings(formulation=0, constraintParameter=12, tolerance=1e-6,
+                                 maximumIterations=30, totalStartingPoints=32, batchSize=32)
+    x, f, stats = solver.solve(B, st)
+    assert np.isfinite(f) and stats.it > 0
