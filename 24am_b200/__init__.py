@@ -15,6 +15,7 @@ The package directory name starts with a digit, so import it with
 """
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -260,15 +261,20 @@ class OptimizationStatistics:
 
 
 class Solver:
-    """One device handle (am24_create / am24_destroy)."""
+    """One device handle (am24_create / am24_destroy).  Closing it closes the
+    matrices (and their batches) still open on it first: the C API wants every
+    batch and matrix destroyed before their handle."""
 
     def __init__(self, device=0):
         h = C.c_void_p()
         check(lib().am24_create(C.byref(h), int(device)))
         self.h = h
+        self._matrices = weakref.WeakSet()
 
     def close(self):
         if self.h:
+            for m in list(self._matrices):
+                m.close()
             lib().am24_destroy(self.h)
             self.h = None
 
@@ -361,9 +367,14 @@ class Matrix:
                                                n, 1, C.byref(mh)))
         self.m, self.n = m, n
         self.mh = mh
+        self._batches = weakref.WeakSet()
+        solver._matrices.add(self)
 
     def close(self):
+        """Destroys the matrix, after any batch still open on it."""
         if self.mh:
+            for b in list(self._batches):
+                b.close()
             lib().am24_matrix_destroy(self.solver.h, self.mh)
             self.mh = None
 
@@ -400,6 +411,7 @@ class Batch:
         check(lib().am24_batch_create(matrix.solver.h, matrix.mh, C.byref(s), self.k,
                                       C.byref(bh)))
         self.bh = bh
+        matrix._batches.add(self)
 
     def close(self):
         if self.bh:

@@ -137,15 +137,17 @@ am24_status make_map(am24_handle h, CUtensorMap *map, const float *base, int K, 
   return AM24_OK;
 }
 
-// K-major BF16 operand [rows][ld] (ld in elements), loaded as 32 x box_rows
-// tiles (64-byte rows, 64-byte swizzle), as the BF16 pair GEMM reads them.
+// K-major 16-bit operand [rows][ld] (ld in elements; BF16, or FP16 when
+// fp16), loaded as 32 x box_rows tiles (64-byte rows, 64-byte swizzle), as the
+// 16-bit pair GEMMs read them.
 am24_status make_map_bf16(am24_handle h, CUtensorMap *map, const uint16_t *base, int K, int rows,
-                          int ld, int box_rows) {
+                          int ld, int box_rows, bool fp16 = false) {
   cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(uint16_t)};
   cuuint32_t box[2] = {(cuuint32_t)PAIR_BK_BF16, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = h->encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t *>(base),
+  CUresult r = h->encode(map, fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16,
+                         2, const_cast<uint16_t *>(base),
                          dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -169,6 +171,29 @@ am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat) {
   if (e != cudaSuccess) {
     M.Bc_b3 = nullptr;
     return fail(AM24_ERR_CUDA, std::string("BF16 planes: ") + cudaGetErrorString(e));
+  }
+  return AM24_OK;
+}
+
+// The matrix's two scaled FP16 planes of B and their row scales (made once, on
+// first use).
+am24_status ensure_fp16_planes(am24_handle h, am24_matrix mat) {
+  MatrixDev &M = mat->d;
+  if (M.Bc_h2) return AM24_OK;
+  const size_t plane = (size_t)M.n * M.ldm;
+  uint16_t *p = nullptr;
+  float *rs = nullptr;
+  AM24_TRY(mat->mem.get(&p, 2 * plane));
+  AM24_TRY(mat->mem.get(&rs, (size_t)M.n));
+  AM24_CUDA(cudaMemsetAsync(p, 0, sizeof(uint16_t) * 2 * plane, h->stream));
+  M.Bc_h2 = p;
+  M.row_scale = rs;
+  cudaError_t e = launch_prep_fp16x2(M, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    M.Bc_h2 = nullptr;
+    M.row_scale = nullptr;
+    return fail(AM24_ERR_CUDA, std::string("FP16 planes: ") + cudaGetErrorString(e));
   }
   return AM24_OK;
 }
@@ -580,11 +605,14 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   d.bk = BK_DEFAULT;
   if (const char *e = getenv("AM24_GEMM_BK")) d.bk = (atoi(e) == 16) ? 16 : 32;
   // V = B^T Z on CTA pairs when its N tile is 256 (AM24_GEMM_PAIR=0 turns it off),
-  // with exact BF16 operands for the L1-variance forms (AM24_GEMM_BF16=0 turns
-  // that off)
+  // with split FP16 operands (AM24_GEMM_FP16=0 turns that off), else with exact
+  // BF16 operands for the L1-variance forms (AM24_GEMM_BF16=0 turns that off)
+  // or TF32 hi/lo planes
   d.pair2 = d.bn2 == 256;
   if (const char *e = getenv("AM24_GEMM_PAIR")) d.pair2 = d.pair2 && atoi(e) != 0;
-  d.bf16_2 = d.pair2 && is_l1_variance(settings->formulation);
+  d.fp16_2 = d.pair2;
+  if (const char *e = getenv("AM24_GEMM_FP16")) d.fp16_2 = d.fp16_2 && atoi(e) != 0;
+  d.bf16_2 = d.pair2 && !d.fp16_2 && is_l1_variance(settings->formulation);
   if (const char *e = getenv("AM24_GEMM_BF16")) d.bf16_2 = d.bf16_2 && atoi(e) != 0;
   // MIXED runs its BF16 phase on CTA-pair tiles; narrower batches stay FP32
   d.mixed = settings->precision == AM24_PRECISION_MIXED && d.pair2;
@@ -592,6 +620,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   d.need_stable = (uint32_t)std::max(1.0, std::ceil((double)settings->stable_share * k - 1e-9));
   d.need_stable = std::min(d.need_stable, (uint32_t)k);
   const bool need_bf16 = d.bf16_2 || d.mixed;
+  const size_t zh_planes = is_l1_variance(settings->formulation) ? 1 : 2;
   const int bk2 = d.pair2 ? PAIR_BK_TF32 : d.bk;  // K box of the TF32 maps of V = B^T Z
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;
   choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
@@ -612,6 +641,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.planes_nnz, 1)) ||
       (st = A.get(&d.sel_hint, k)) ||
       (need_bf16 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat)))) ||
+      (d.fp16_2 && ((st = A.get(&d.Z_h, zh_planes * kz)) || (st = A.get(&d.z_scale, k)) ||
+                    (st = ensure_fp16_planes(h, mat)))) ||
       (d.mixed && ((st = A.get(&d.vmask_prev, (size_t)k * (M.ldn / 32))) ||
                    (st = A.get(&d.stable, k)) || (st = A.get(&d.phase, 4))))) {
     delete b;
@@ -633,6 +664,9 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.planes_nnz, 0, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.sel_hint, 0, sizeof(float) * k, h->stream);
   if (!e && d.Z_b) e = cudaMemsetAsync(d.Z_b, 0, sizeof(uint16_t) * kz, h->stream);
+  if (!e && d.Z_h) e = cudaMemsetAsync(d.Z_h, 0, sizeof(uint16_t) * zh_planes * kz, h->stream);
+  if (!e && d.z_scale) e = cudaMemsetAsync(d.z_scale, 0, sizeof(float) * k, h->stream);
+  d.row_scale = M.row_scale;
   if (!e && d.mixed)
     e = cudaMemsetAsync(d.vmask_prev, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
   if (!e && d.mixed) e = reset_mixed(d, h->stream);
@@ -660,6 +694,17 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
         (st = make_map_bf16(h, &b->tm.a2_b1, M.Bc_b3 + plane, M.m, M.n, M.ldm, BM)) ||
         (st = make_map_bf16(h, &b->tm.a2_b2, M.Bc_b3 + 2 * plane, M.m, M.n, M.ldm, BM)) ||
         (st = make_map_bf16(h, &b->tm.b2_b, d.Z_b, M.m, k, M.ldm, d.bn2 / 2))) {
+      delete b;
+      return st;
+    }
+  }
+  if (d.fp16_2) {
+    const size_t plane = (size_t)M.n * M.ldm;
+    if ((st = make_map_bf16(h, &b->tm.a2_h0, M.Bc_h2, M.m, M.n, M.ldm, BM, true)) ||
+        (st = make_map_bf16(h, &b->tm.a2_h1, M.Bc_h2 + plane, M.m, M.n, M.ldm, BM, true)) ||
+        (st = make_map_bf16(h, &b->tm.b2_h0, d.Z_h, M.m, k, M.ldm, d.bn2 / 2, true)) ||
+        (zh_planes == 2 &&
+         (st = make_map_bf16(h, &b->tm.b2_h1, d.Z_h + kz, M.m, k, M.ldm, d.bn2 / 2, true)))) {
       delete b;
       return st;
     }
@@ -1207,11 +1252,12 @@ bool same_step(const ServeRequest &a, const ServeRequest &b) {
          a.s.stable_share == b.s.stable_share && a.s.timeout_ms == b.s.timeout_ms;
 }
 
-// Device bytes of a matrix's layouts (the BF16 planes included: batches of the
-// L1-variance forms and MIXED ones add them on first use).
+// Device bytes of a matrix's layouts (the BF16 and FP16 planes included:
+// batches add them on first use).
 uint64_t matrix_bytes(uint32_t m, uint32_t n) {
   const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
-  return 4ull * (2 * n * ldm + 2 * m * ldn + n * ldm) + 2ull * 3 * n * ldm;
+  return 4ull * (2 * n * ldm + 2 * m * ldn + n * ldm) + 2ull * 3 * n * ldm +
+         2ull * 2 * n * ldm + 4ull * n;
 }
 
 // Device bytes of a batch of k starts on an m x n matrix (an upper estimate).
@@ -1219,8 +1265,8 @@ uint64_t batch_bytes(uint32_t m, uint32_t n, uint32_t k) {
   const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
   const uint64_t kv = (uint64_t)k * ldn, kz = (uint64_t)k * ldm;
   const uint64_t ws = 2ull * ((m + 127) / 128) * ((k + 63) / 64 + 3) * 256 * 128 * 4 * 8;
-  return 4 * kv * 4 + 2 * kz * 4 + kz * 2 + 2 * (kv / 32) * 4 + ws + (uint64_t)k * 256 +
-         (4ull << 20);
+  return 4 * kv * 4 + 2 * kz * 4 + kz * 2 + 2 * kz * 2 + 2 * (kv / 32) * 4 + ws +
+         (uint64_t)k * 256 + (4ull << 20);
 }
 
 }  // namespace

@@ -33,6 +33,11 @@ struct MatrixDev {
   // x = b0 + b1 + b2 exactly; made when a batch of an L1-variance form first
   // needs them (null before).
   uint16_t *Bc_b3;
+  // Two FP16 planes of Bc scaled per feature (plane p at Bc_h2 + p * n * ldm):
+  // x * 2^s_c = h0 + h1 (+ under 2^-22 |x|), row_scale[c] = 2^-s_c; made when a
+  // batch first runs V = B^T Z on FP16 operands (null before).
+  uint16_t *Bc_h2;
+  float *row_scale;
 };
 
 // Per-batch device state for k starting points.
@@ -45,6 +50,11 @@ struct BatchDev {
   int m_tiles1, n_tiles1, m_tiles2, n_tiles2;
   int pair2;      // V = B^T Z runs on CTA pairs (256-row tiles; B maps of bn2/2 rows)
   int bf16_2;     // ... with the exact BF16 operands of the L1-variance forms
+  int fp16_2;     // ... with the split FP16 operands (preferred over bf16_2 and TF32)
+  uint16_t *Z_h;  // FP16 Z for fp16_2: sgn(B V) exactly (one k x ldm plane, L1-variance
+                  // forms), or two planes (second at Z_h + k * ldm) of z * 2^s_j
+  float *z_scale;    // per start 2^-s_j (L2-variance forms with fp16_2)
+  const float *row_scale;  // the matrix's FP16 row scales (fp16_2)
   uint16_t *Z_b;  // k x ldm BF16 Z: sgn(B V) exactly (L1-variance forms with bf16_2),
                   // or Z rounded to BF16 (MIXED); else null
   int mixed;             // MIXED precision: single-pass BF16 V = B^T Z until supports settle
@@ -96,6 +106,7 @@ struct TensorMaps {
   CUtensorMap a1_hi, a1_lo, b1_hi, b1_lo;  // Z = B V :  A = Bt, B = V
   CUtensorMap a2_hi, a2_lo, b2_hi, b2_lo;  // V = B^T Z: A = Bc, B = Z
   CUtensorMap a2_b0, a2_b1, a2_b2, b2_b;   // V = B^T Z, BF16: A = Bc_b3, B = Z_b
+  CUtensorMap a2_h0, a2_h1, b2_h0, b2_h1;  // V = B^T Z, FP16: A = Bc_h2, B = Z_h
 };
 
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
@@ -103,6 +114,8 @@ int num_sms();
 cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st);
 // Fills M.Bc_b3 from M.Bc.
 cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st);
+// Fills M.Bc_h2 and M.row_scale from M.Bc.
+cudaError_t launch_prep_fp16x2(const MatrixDev &M, cudaStream_t st);
 // Loadings of `cols` columns from src (rows entries each) into dst and their
 // non-zero masks (mask + c * (ld_dst / 32) per column).
 cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols, float *dst,

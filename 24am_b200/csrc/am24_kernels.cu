@@ -18,6 +18,7 @@
 // Every reduction has a fixed order, so a step is bitwise reproducible.
 #include <cfloat>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <climits>
 #include <cstdio>
 
@@ -57,6 +58,29 @@ __device__ __forceinline__ uint16_t bf16_sign(float v) {
   return v > 0.f ? (uint16_t)0x3F80u : (v < 0.f ? (uint16_t)0xBF80u : (uint16_t)0u);
 }
 __device__ __forceinline__ uint32_t abs_key(float v) { return __float_as_uint(v) & 0x7FFFFFFFu; }
+// sgn(v) as FP16 bits: +1 0x3C00, -1 0xBC00, 0 (and NaN) 0.
+__device__ __forceinline__ uint16_t f16_sign(float v) {
+  return v > 0.f ? (uint16_t)0x3C00u : (v < 0.f ? (uint16_t)0xBC00u : (uint16_t)0u);
+}
+// 2^e for e in [-126, 127], exactly.
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+// The shift s in [-113, 126] that puts a positive bound on |x| into
+// [2^14, 2^15) (bounds below 2^-112 stay below that range); 0 for zero, NaN or
+// infinite bounds.  x * 2^s then splits into FP16 planes without overflow
+// (FP16's largest finite value is 65504).
+__device__ __forceinline__ int fp16_shift(float bound) {
+  const uint32_t eb = (__float_as_uint(bound) >> 23) & 0xFFu;
+  if (!(bound > 0.f) || eb == 0xFFu) return 0;
+  const int e = max((int)eb, 1) - 127;  // floor(log2(bound)) for normal bounds
+  return min(14 - e, 126);
+}
+// x = h0 + h1 + r: h0 = fp16_rn(x), h1 = fp16_rn(x - h0) (the difference is
+// exact in FP32), |r| <= 2^-11 |x - h0| for FP16-normal x - h0, else <= 2^-25.
+__device__ __forceinline__ void fp16_split(float x, uint16_t *h0, uint16_t *h1) {
+  const __half a = __float2half_rn(x);
+  *h0 = __half_as_ushort(a);
+  *h1 = __half_as_ushort(__float2half_rn(x - __half2float(a)));
+}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -253,6 +277,32 @@ __global__ void prep_bf16x3_kernel(const float *__restrict__ Bc, int ldm, int m,
   }
 }
 
+// Two FP16 planes of each feature of B with a power-of-two scale per feature:
+// x * 2^s = h0 + h1 (fp16_split), s from the feature's largest |x| so that it
+// lands in [2^14, 2^15); row_scale[c] = 2^-s undoes it in the GEMM epilogue.
+__global__ void __launch_bounds__(256) prep_fp16x2_kernel(const float *__restrict__ Bc, int ldm,
+                                                          int m, size_t plane,
+                                                          uint16_t *__restrict__ out,
+                                                          float *__restrict__ row_scale) {
+  __shared__ uint32_t red[8];
+  const size_t c = blockIdx.x;
+  uint32_t mx = 0;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) mx = max(mx, abs_key(Bc[c * ldm + r]));
+  mx = __reduce_max_sync(FULL, mx);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  mx = 0;
+#pragma unroll
+  for (int w = 0; w < 8; w++) mx = max(mx, red[w]);
+  const int s = fp16_shift(__uint_as_float(mx));
+  const float sc = pow2f(s);
+  if (threadIdx.x == 0) row_scale[c] = pow2f(-s);
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    const size_t o = c * ldm + r;
+    fp16_split(Bc[o] * sc, out + o, out + plane + o);
+  }
+}
+
 // Bt[r * ldn + c] = split(B[c * ldB + r]): 32 x 32 tiles through shared memory.
 __global__ void prep_transpose_kernel(const float *__restrict__ B, int ldB, int m, int n,
                                       float *__restrict__ hi, float *__restrict__ lo, int ldn) {
@@ -324,7 +374,9 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
                                                        float *__restrict__ Z_lo, int ldm,
                                                        float *__restrict__ fz,
                                                        const uint32_t *gate, uint32_t gate_max,
-                                                       uint16_t *__restrict__ Zb) {
+                                                       uint16_t *__restrict__ Zb,
+                                                       uint16_t *__restrict__ Zh, size_t zplane,
+                                                       float *__restrict__ zscale) {
   __shared__ double red[32];
   if (*gate <= gate_max) return;  // the gather kernel produced Z this step
   const int j = blockIdx.x;
@@ -345,6 +397,7 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
       zh[i] = sgnf(y);
       zl[i] = 0.f;
       if (Zb) Zb[(size_t)j * ldm + i] = bf16_sign(y);
+      if (Zh) Zh[(size_t)j * ldm + i] = f16_sign(y);
     } else {
       acc += (double)y * (double)y;
       split_store(y, zh + i, zl + i);
@@ -352,16 +405,24 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
     }
   }
   const double tot = block_sum(acc, red);
-  if (MODE == 2) {
-    const float inv = 1.0f / (float)sqrt(tot);
+  if (MODE == 2 || (MODE == 0 && Zh)) {
+    // second pass: MODE 2 normalises; both write the FP16 planes of z * 2^s,
+    // s from a bound on |z| (||y||_2, or 1 for the normalised z)
+    const float inv = MODE == 2 ? 1.0f / (float)sqrt(tot) : 1.0f;
+    const int s = fp16_shift(MODE == 2 ? 1.0f : (float)sqrt(tot));
+    const float sc = pow2f(s);
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       const float y = zh[i] + zl[i];  // exact: this thread wrote both planes
-      split_store(y * inv, zh + i, zl + i);
-      if (Zb) Zb[(size_t)j * ldm + i] = bf16_bits(y * inv);
+      const float z = MODE == 2 ? y * inv : y;
+      if (MODE == 2) {
+        split_store(z, zh + i, zl + i);
+        if (Zb) Zb[(size_t)j * ldm + i] = bf16_bits(z);
+      }
+      if (Zh) fp16_split(z * sc, Zh + (size_t)j * ldm + i, Zh + zplane + (size_t)j * ldm + i);
     }
-  } else if (threadIdx.x == 0) {
-    fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
+    if (Zh && threadIdx.x == 0) zscale[j] = pow2f(-s);
   }
+  if (MODE != 2 && threadIdx.x == 0) fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
 }
 
 // ------------------------------------------------------------ sparse Z = B V
@@ -408,7 +469,8 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
     const float *__restrict__ Bc, int ldm, int m, int ldn,
     const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
     float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
-    uint16_t *__restrict__ Zb) {
+    uint16_t *__restrict__ Zb, uint16_t *__restrict__ Zh, size_t zplane,
+    float *__restrict__ zscale) {
   __shared__ int idx[GATHER_CAP];
   __shared__ float val[GATHER_CAP];
   __shared__ uint32_t wsum[GATHER_THREADS / 32];
@@ -461,6 +523,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
   float *zh = Z_hi + (size_t)j * ldm;
   float *zl = Z_lo + (size_t)j * ldm;
   uint16_t *zb = Zb ? Zb + (size_t)j * ldm : nullptr;
+  uint16_t *zh0 = Zh ? Zh + (size_t)j * ldm : nullptr;
   const int chunk = GATHER_THREADS * GATHER_ROWS;
   const int ld4 = ldm >> 2;
   const bool one_pass = m <= chunk;
@@ -478,6 +541,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
       zh[i] = sgnf(yv);
       zl[i] = 0.f;
       if (zb) zb[i] = bf16_sign(yv);
+      if (zh0) zh0[i] = f16_sign(yv);
     } else {
       acc += (double)yv * (double)yv;
       if (!(MODE == 2 && one_pass)) split_store(yv, zh + i, zl + i);
@@ -527,8 +591,11 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
     }
   }
   const double tot = block_sum(acc, red);
-  if (MODE == 2) {
-    const float inv = 1.0f / (float)sqrt(tot);
+  if (MODE == 2 || (MODE == 0 && zh0)) {
+    // as in z_reduce_kernel: MODE 2 normalises, both write the FP16 planes
+    const float inv = MODE == 2 ? 1.0f / (float)sqrt(tot) : 1.0f;
+    const int s = fp16_shift(MODE == 2 ? 1.0f : (float)sqrt(tot));
+    const float sc = pow2f(s);
     for (int base = 0; base < m; base += chunk) {
 #pragma unroll
       for (int r = 0; r < G4; r++) {
@@ -540,14 +607,18 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
           // one pass: the sums are still in registers; else re-read what this
           // thread wrote (hi + lo is exact)
           const float v = one_pass ? e[c] : zh[i + c] + zl[i + c];
-          split_store(v * inv, zh + i + c, zl + i + c);
-          if (zb) zb[i + c] = bf16_bits(v * inv);
+          const float z = MODE == 2 ? v * inv : v;
+          if (MODE == 2) {
+            split_store(z, zh + i + c, zl + i + c);
+            if (zb) zb[i + c] = bf16_bits(z);
+          }
+          if (zh0) fp16_split(z * sc, zh0 + i + c, zh0 + zplane + i + c);
         }
       }
     }
-  } else if (threadIdx.x == 0) {
-    fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
+    if (zh0 && threadIdx.x == 0) zscale[j] = pow2f(-s);
   }
+  if (MODE != 2 && threadIdx.x == 0) fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
 }
 
 // ------------------------------------------------------------ radix select
@@ -1541,6 +1612,16 @@ template <class Epi>
 cudaError_t dispatch_gemm2(const BatchDev &b, const TensorMaps &tm, const GemmShape &sh,
                            const Epi &epi, bool l1_variance, cudaStream_t st) {
   if (b.pair2) {
+    if (b.fp16_2) {
+      GemmShape s2 = sh;
+      s2.row_scale = b.row_scale;
+      if (l1_variance)  // B = sgn(z), exact
+        return run_gemm_pair<PairFP16x2A, 256, 8>(tm.a2_h0, tm.a2_h1, tm.b2_h0, tm.b2_h0, s2, epi,
+                                                  st);
+      s2.col_scale = b.z_scale;
+      return run_gemm_pair<PairFP16x3, 256, 6>(tm.a2_h0, tm.a2_h1, tm.b2_h0, tm.b2_h1, s2, epi,
+                                               st);
+    }
     if (b.bf16_2 && l1_variance)
       return run_gemm_pair<PairBF16x3A, 256, 6>(tm.a2_b0, tm.a2_b1, tm.a2_b2, tm.b2_b, sh, epi,
                                                 st);
@@ -1571,6 +1652,12 @@ size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn) {
 
 cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st) {
   prep_bf16x3_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, (size_t)M.n * M.ldm, M.Bc_b3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep_fp16x2(const MatrixDev &M, cudaStream_t st) {
+  prep_fp16x2_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, (size_t)M.n * M.ldm, M.Bc_h2,
+                                          M.row_scale);
   return cudaGetLastError();
 }
 
@@ -1702,20 +1789,21 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g1.gate_min = b.sparse_cap + 1;
   g1.gate_max = 0xFFFFFFFFu;
   const int mode = is_l1_variance(f) ? 1 : (is_constrained(f) ? 0 : 2);
+  const size_t zplane = (size_t)b.k * M.ldm;  // second FP16 plane of Z
   // 1a. sparse V (every column <= sparse_cap non-zeros last step): gather
   if ((e = mark(5)) != cudaSuccess) return e;
   if (mode == 0)
     gather_bv_kernel<0><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap, b.Z_b);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale);
   else if (mode == 1)
     gather_bv_kernel<1><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap, b.Z_b);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale);
   else
     gather_bv_kernel<2><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap, b.Z_b);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   // 1b. dense V: TF32 hi/lo planes, tensor-core Z = B V (split-K partials) ...
@@ -1734,15 +1822,15 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (mode == 0)
     z_reduce_kernel<0><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
-                                             b.Z_b);
+                                             b.Z_b, b.Z_h, zplane, b.z_scale);
   else if (mode == 1)
     z_reduce_kernel<1><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
-                                             b.Z_b);
+                                             b.Z_b, b.Z_h, zplane, b.z_scale);
   else
     z_reduce_kernel<2><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
-                                             b.Z_b);
+                                             b.Z_b, b.Z_h, zplane, b.z_scale);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   // 3. V = B^T Z

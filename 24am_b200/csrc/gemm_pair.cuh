@@ -110,6 +110,50 @@ struct PairBF16x3A {
   static constexpr uint32_t FMT = 1u;
 };
 
+// FP16 operands, each split in two: x = h0 + h1 (+ a residual under 2^-22 |x|),
+// h0 = fp16_rn(x), h1 = fp16_rn(x - h0), after a power-of-two scaling that puts
+// the operand's largest magnitude just under 2^14 (FP16's range is narrow; the
+// epilogue multiplies the scaling back out exactly).  h1*g0 + h0*g1 + h0*g0 per
+// K step: the accuracy class of PairTF32x3 (FP16 holds TF32's 11 significant
+// bits) at half its tensor time (FP16 runs at twice the TF32 rate, 3 instead of
+// 6 MMAs per 16 K elements).
+struct PairFP16x3 {
+  static constexpr int NA = 2, NB = 2, BK = PAIR_BK_BF16;
+  static constexpr int PROMO_K = 256;  // 48 MMA accumulations per chunk
+  template <uint32_t ID>
+  __device__ static void k_block(uint32_t d, const uint32_t (&a)[2], const uint32_t (&b)[2],
+                                 uint32_t sbo, bool first) {
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+      const uint32_t off = kk * 32;
+      const uint64_t da0 = sdesc_kmajor(a[0] + off, sbo, 4u);
+      const uint64_t db0 = sdesc_kmajor(b[0] + off, sbo, 4u);
+      mma_f16_pair(d, sdesc_kmajor(a[1] + off, sbo, 4u), db0, ID, (first && kk == 0) ? 0u : 1u);
+      mma_f16_pair(d, da0, sdesc_kmajor(b[1] + off, sbo, 4u), ID, 1u);
+      mma_f16_pair(d, da0, db0, ID, 1u);
+    }
+  }
+  static constexpr uint32_t FMT = 0u;  // F16
+};
+// As PairFP16x3 with B exact in one FP16 plane (the L1-variance forms' sgn):
+// h1*z + h0*z per K step, 2 MMAs per 16 K elements.
+struct PairFP16x2A {
+  static constexpr int NA = 2, NB = 1, BK = PAIR_BK_BF16;
+  static constexpr int PROMO_K = 384;  // 48 MMA accumulations per chunk
+  template <uint32_t ID>
+  __device__ static void k_block(uint32_t d, const uint32_t (&a)[2], const uint32_t (&b)[1],
+                                 uint32_t sbo, bool first) {
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+      const uint32_t off = kk * 32;
+      const uint64_t db = sdesc_kmajor(b[0] + off, sbo, 4u);
+      mma_f16_pair(d, sdesc_kmajor(a[1] + off, sbo, 4u), db, ID, (first && kk == 0) ? 0u : 1u);
+      mma_f16_pair(d, sdesc_kmajor(a[0] + off, sbo, 4u), db, ID, 1u);
+    }
+  }
+  static constexpr uint32_t FMT = 0u;
+};
+
 // Single-pass BF16 operands (A = b0 of the split, B = Z rounded to BF16) for
 // the low-precision phase of the mixed mode: one MMA per 16 K elements, a
 // work unit accumulated whole in tensor memory (no intermediate promotion).
@@ -349,6 +393,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
         }
       }
       if (!ok) break;
+      if (shape.row_scale) {  // exact: powers of two
+        const float rs = __ldg(shape.row_scale + min(t.m0 + row, shape.M - 1));
+#pragma unroll
+        for (int i = 0; i < HALF; i++) sum[i] *= rs;
+      }
+      if (shape.col_scale) {
+#pragma unroll
+        for (int i = 0; i < HALF; i++)
+          sum[i] *= __ldg(shape.col_scale + min(t.nt * BN + half * HALF + i, shape.N - 1));
+      }
 #pragma unroll
       for (int c = 0; c < HALF / 32; c++)
         ep.chunk(t, q, lane, row, half * HALF + c * 32,

@@ -60,6 +60,11 @@ struct GemmShape {
   // gate_min <= *gate <= gate_max (otherwise another kernel of the step covers it).
   const uint32_t *gate;
   uint32_t gate_min, gate_max;
+  // Optional output scaling (FP16 schemes): C[i][j] is multiplied by
+  // row_scale[i] * col_scale[j] (either may be absent), powers of two that undo
+  // the operands' range scaling exactly.
+  const float *row_scale = nullptr;
+  const float *col_scale = nullptr;
 };
 
 // One work unit as an epilogue sees it: rows [m0, m0 + 128) of C (this CTA's

@@ -390,16 +390,32 @@ def run_serving(args):
     return 0
 
 
+PRECISION_NOTE = ("FP32-accurate products, FP32 accumulate: V = B^T Z on split FP16 operands "
+                  "with power-of-two scales (h0 + h1 per operand, 22 significant bits; Z of the "
+                  "L1-variance forms an exact sign), Z = B V on 3xTF32 or an FP32 gather")
+
+
+def gemm_scheme(f):
+    """Operand scheme of V = B^T Z for formulation f: on CTA pairs (more than
+    128 starts) split FP16 (two MMAs per product for the L1-variance forms 1, 3,
+    5, 7, whose Z is an exact sign; three for the others), or with
+    AM24_GEMM_FP16=0 three BF16 MMAs for the L1-variance forms; else 3xTF32."""
+    pair = STARTS > 128 and os.environ.get("AM24_GEMM_PAIR", "1") != "0"
+    if pair and os.environ.get("AM24_GEMM_FP16", "1") != "0":
+        return "fp16x2" if f in (1, 3, 5, 7) else "fp16x3"
+    if pair and f in (1, 3, 5, 7) and os.environ.get("AM24_GEMM_BF16", "1") != "0":
+        return "bf16x3"
+    return "tf32x3"
+
+
 def kernel_label(kind, f):
     """Bench name of a step kernel of formulation f: V = B^T Z by operand scheme
-    (BF16 for the L1-variance forms 1, 3, 5, 7 on CTA pairs, else 3xTF32) and
-    epilogue (raw for the constrained forms, fused penalty otherwise); the
-    select by constraint (top-s for 0, 1; L1 ball for 2, 3)."""
+    (gemm_scheme) and epilogue (raw for the constrained forms, fused penalty
+    otherwise); the select by constraint (top-s for 0, 1; L1 ball for 2, 3)."""
     skipped = kind.endswith("(skipped)")
     base = kind[:-len("(skipped)")] if skipped else kind
     if base == "gemm_BtZ":
-        base = (f"gemm_BtZ_{'bf16x3' if f in (1, 3, 5, 7) and STARTS > 128 else 'tf32x3'}"
-                f"_{'raw' if f <= 3 else 'pen'}")
+        base = f"gemm_BtZ_{gemm_scheme(f)}_{'raw' if f <= 3 else 'pen'}"
     elif base == "select":
         base = "select_top_s" if f in (0, 1) else "select_l1_ball"
     return base + ("(skipped)" if skipped else "")
@@ -492,10 +508,11 @@ def run_ours(args):
     avg_ms = statistics.mean(per_kind[dom])
     if dom.startswith("gemm"):
         # FP32-equivalent rate: 2*n*p*k FLOPs per launch against the tensor
-        # rate of the scheme's passes (three TF32 MMAs, or three BF16 MMAs,
-        # per FP32 product)
-        bf16 = "bf16x3" in dom
-        div = (1.0 if bf16 else 2.0) * 3.0
+        # rate of the scheme's passes (three TF32 MMAs at half the 16-bit
+        # rate, or three or two BF16 / FP16 MMAs, per FP32 product)
+        passes = {"fp16x2": 2.0, "fp16x3": 3.0, "bf16x3": 3.0, "tf32x3": 6.0}
+        scheme = next(s for s in passes if s in dom)
+        div = passes[scheme]
         peak = pk["bf16_tflops_sustained"] / div
         flops = 2.0 * N_SAMPLES * P_FEATURES * STARTS
         achieved = flops / (avg_ms * 1e-3) / 1e12
@@ -508,8 +525,11 @@ def run_ours(args):
                 # burst figure is given beside it
                 "frac_of_burst": achieved / (pk["bf16_tflops"] / div),
                 "peak_note": f"{pk_kind} bf16 sustained {pk['bf16_tflops_sustained']} TF/s"
-                             + (" /3 (three BF16 MMAs per FP32 product)" if bf16 else
-                                " /2 (TF32 rate) /3 (three TF32 MMAs per FP32 product)")
+                             + {"fp16x2": " /2 (two FP16 MMAs per FP32 product)",
+                                "fp16x3": " /3 (three FP16 MMAs per FP32 product)",
+                                "bf16x3": " /3 (three BF16 MMAs per FP32 product)",
+                                "tf32x3": " /2 (TF32 rate) /3 (three TF32 MMAs per FP32 "
+                                          "product)"}[scheme]
                              + "; achieved counts 2*n*p*k dense FLOPs per launch"}
     else:
         byts = 4.0 * P_FEATURES * STARTS * 3
@@ -575,7 +595,7 @@ def run_ours(args):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": workload_name(), "n": N_SAMPLES, "p": P_FEATURES,
                            "starts_per_gpu": STARTS, "formulations": forms, "s": S_CONS,
-                           "gamma_factor": GAMMA_C, "precision": "FP32-accurate products (3xTF32; exact 3xBF16 split for the L1-variance forms), FP32 accumulate",
+                           "gamma_factor": GAMMA_C, "precision": PRECISION_NOTE,
                            "l2": "inputs larger than L2 (B as 4 FP32 planes = 1.6 GB)",
                            "parallelism": f"start-sharded x{world}, no data-path collective"},
                 "roofline": roof, "kernels": breakdown, "formulation_ms": formulation_ms,

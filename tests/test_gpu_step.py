@@ -22,7 +22,43 @@ def gammas(B):
 @pytest.mark.parametrize("formulation", range(8))
 def test_step_matches_oracle(solver, po, shape, formulation):
     m, n, k = shape
-    B = po.low_rank_data(m, n, 8, 30, seed=m + n, dtype=np.float32)
+    check_step(solver, po, po.low_rank_data(m, n, 8, 30, seed=m + n, dtype=np.float32), k,
+               formulation)
+
+
+@pytest.mark.parametrize("formulation,spread", [(0, 6), (1, 6), (2, 0.5), (3, 0.5), (4, 6),
+                                                (5, 6), (6, 6), (7, 6)])
+def test_step_with_feature_scales_far_apart(solver, po, formulation, spread):
+    """Features scaled from 10^-spread to 10^spread (and one all zero): the
+    FP16 operands of V = B^T Z carry a power-of-two scale per feature, so every
+    feature keeps its relative accuracy.  (The L1-ball forms 2 and 3 take a
+    narrow spread: with a wide one the projection keeps only the largest
+    feature, the tie case the parity check sets aside.)"""
+    m, n, k = 300, 2000, 256
+    B = po.low_rank_data(m, n, 8, 30, seed=11, dtype=np.float64)
+    B *= 10.0 ** np.random.default_rng(12).uniform(-spread, spread, n)
+    B[:, 7] = 0.0
+    check_step(solver, po, B.astype(np.float32), k, formulation)
+
+
+@pytest.mark.parametrize("scheme", ["tf32_bf16", "tf32"])
+@pytest.mark.parametrize("shape", [(1000, 5000, 256), (129, 4097, 257)],
+                         ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("formulation", range(8))
+def test_step_matches_oracle_other_pair_schemes(solver, po, shape, formulation, scheme,
+                                                monkeypatch):
+    """The CTA-pair V = B^T Z without the FP16 operands: 3xTF32 for every
+    formulation, or with exact BF16 operands for the L1-variance forms."""
+    monkeypatch.setenv("AM24_GEMM_FP16", "0")
+    if scheme == "tf32":
+        monkeypatch.setenv("AM24_GEMM_BF16", "0")
+    m, n, k = shape
+    check_step(solver, po, po.low_rank_data(m, n, 8, 30, seed=m + n, dtype=np.float32), k,
+               formulation)
+
+
+def check_step(solver, po, B, k, formulation):
+    m, n = B.shape
     B64 = B.astype(np.float64)
     V0 = po.uniform_starts(n, k, seed=n, dtype=np.float32)
     s = min(16, n)
