@@ -198,6 +198,29 @@ am24_status ensure_fp16_planes(am24_handle h, am24_matrix mat) {
   return AM24_OK;
 }
 
+// The matrix's two scaled FP16 planes of B^T and their row scales (made once,
+// on first use).
+am24_status ensure_bt_fp16_planes(am24_handle h, am24_matrix mat) {
+  MatrixDev &M = mat->d;
+  if (M.Bt_h2) return AM24_OK;
+  const size_t plane = (size_t)M.m * M.ldn;
+  uint16_t *p = nullptr;
+  float *rs = nullptr;
+  AM24_TRY(mat->mem.get(&p, 2 * plane));
+  AM24_TRY(mat->mem.get(&rs, (size_t)M.m));
+  AM24_CUDA(cudaMemsetAsync(p, 0, sizeof(uint16_t) * 2 * plane, h->stream));
+  M.Bt_h2 = p;
+  M.bt_row_scale = rs;
+  cudaError_t e = launch_prep_bt_fp16x2(M, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    M.Bt_h2 = nullptr;
+    M.bt_row_scale = nullptr;
+    return fail(AM24_ERR_CUDA, std::string("FP16 planes of B^T: ") + cudaGetErrorString(e));
+  }
+  return AM24_OK;
+}
+
 // MIXED: back to the BF16 phase with no start counted stable (a new batch).
 cudaError_t reset_mixed(const BatchDev &d, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(d.stable, 0, sizeof(uint32_t) * d.k, st);
@@ -612,6 +635,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (const char *e = getenv("AM24_GEMM_PAIR")) d.pair2 = d.pair2 && atoi(e) != 0;
   d.fp16_2 = d.pair2;
   if (const char *e = getenv("AM24_GEMM_FP16")) d.fp16_2 = d.fp16_2 && atoi(e) != 0;
+  // Z = B V on FP16 CTA pairs under the same switches, when its N tile is 256
+  d.fp16_1 = d.fp16_2 && d.bn1 == 256;
   d.bf16_2 = d.pair2 && !d.fp16_2 && is_l1_variance(settings->formulation);
   if (const char *e = getenv("AM24_GEMM_BF16")) d.bf16_2 = d.bf16_2 && atoi(e) != 0;
   // MIXED runs its BF16 phase on CTA-pair tiles; narrower batches stay FP32
@@ -624,6 +649,13 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   const int bk2 = d.pair2 ? PAIR_BK_TF32 : d.bk;  // K box of the TF32 maps of V = B^T Z
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;
   choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
+  d.ws_len = ws_floats(d.splits1, d.m_tiles1, d.n_tiles1, d.bn1);
+  if (d.fp16_1) {  // pair tiles of 256 rows, K blocks of 32, one unit per cluster (2 SMs)
+    int kbps = 0;
+    choose_splits(((d.m_tiles1 + 1) / 2) * d.n_tiles1, (M.n + PAIR_BK_BF16 - 1) / PAIR_BK_BF16,
+                  std::max(1, num_sms() / 2), &d.splits1p, &kbps);
+    d.ws_len = std::max(d.ws_len, ws_floats(d.splits1p, d.m_tiles1, d.n_tiles1, d.bn1));
+  }
   const int parts = d.m_tiles2 * 4;
   d.log_capacity = std::max(settings->total_starts, k);
   am24_status st;
@@ -632,7 +664,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if ((st = A.get(&d.Vx, kv)) || (st = A.get(&d.V_hi, kv)) || (st = A.get(&d.V_lo, kv)) ||
       (st = A.get(&d.Vraw, kv)) ||
       (st = A.get(&d.Z_hi, kz)) || (st = A.get(&d.Z_lo, kz)) ||
-      (st = A.get(&d.ws, ws_floats(d.splits1, d.m_tiles1, d.n_tiles1, d.bn1))) ||
+      (st = A.get(&d.ws, d.ws_len)) ||
       (st = A.get(&d.fz, k)) || (st = A.get(&d.obj_part, (size_t)k * parts)) ||
       (st = A.get(&d.nnz_part, (size_t)k * parts)) || (st = A.get(&d.nnz, k)) ||
       (st = A.get(&d.val, k)) || (st = A.get(&d.err, k)) || (st = A.get(&d.max_err, 1)) ||
@@ -643,6 +675,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (need_bf16 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat)))) ||
       (d.fp16_2 && ((st = A.get(&d.Z_h, zh_planes * kz)) || (st = A.get(&d.z_scale, k)) ||
                     (st = ensure_fp16_planes(h, mat)))) ||
+      (d.fp16_1 && ((st = A.get(&d.V_h, 2 * kv)) || (st = A.get(&d.v_scale, k)) ||
+                    (st = ensure_bt_fp16_planes(h, mat)))) ||
       (d.mixed && ((st = A.get(&d.vmask_prev, (size_t)k * (M.ldn / 32))) ||
                    (st = A.get(&d.stable, k)) || (st = A.get(&d.phase, 4))))) {
     delete b;
@@ -666,7 +700,10 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e && d.Z_b) e = cudaMemsetAsync(d.Z_b, 0, sizeof(uint16_t) * kz, h->stream);
   if (!e && d.Z_h) e = cudaMemsetAsync(d.Z_h, 0, sizeof(uint16_t) * zh_planes * kz, h->stream);
   if (!e && d.z_scale) e = cudaMemsetAsync(d.z_scale, 0, sizeof(float) * k, h->stream);
+  if (!e && d.V_h) e = cudaMemsetAsync(d.V_h, 0, sizeof(uint16_t) * 2 * kv, h->stream);
+  if (!e && d.v_scale) e = cudaMemsetAsync(d.v_scale, 0, sizeof(float) * k, h->stream);
   d.row_scale = M.row_scale;
+  d.bt_row_scale = M.bt_row_scale;
   if (!e && d.mixed)
     e = cudaMemsetAsync(d.vmask_prev, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
   if (!e && d.mixed) e = reset_mixed(d, h->stream);
@@ -705,6 +742,16 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
         (st = make_map_bf16(h, &b->tm.b2_h0, d.Z_h, M.m, k, M.ldm, d.bn2 / 2, true)) ||
         (zh_planes == 2 &&
          (st = make_map_bf16(h, &b->tm.b2_h1, d.Z_h + kz, M.m, k, M.ldm, d.bn2 / 2, true)))) {
+      delete b;
+      return st;
+    }
+  }
+  if (d.fp16_1) {
+    const size_t plane = (size_t)M.m * M.ldn;
+    if ((st = make_map_bf16(h, &b->tm.a1_h0, M.Bt_h2, M.n, M.m, M.ldn, BM, true)) ||
+        (st = make_map_bf16(h, &b->tm.a1_h1, M.Bt_h2 + plane, M.n, M.m, M.ldn, BM, true)) ||
+        (st = make_map_bf16(h, &b->tm.b1_h0, d.V_h, M.n, k, M.ldn, d.bn1 / 2, true)) ||
+        (st = make_map_bf16(h, &b->tm.b1_h1, d.V_h + kv, M.n, k, M.ldn, d.bn1 / 2, true))) {
       delete b;
       return st;
     }
@@ -1168,8 +1215,7 @@ extern "C" {
 am24_status am24_batch_iterate_static_ws(am24_handle h, am24_batch b, int32_t it0,
                                          int32_t iterations, float *max_error) {
   if (!h || !b) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  const size_t need =
-      ws_floats(b->d.splits1, b->d.m_tiles1, b->d.n_tiles1, b->d.bn1) * sizeof(float);
+  const size_t need = b->d.ws_len * sizeof(float);
   if (need > AM24_STATIC_WS_BYTES)
     return fail(AM24_ERR_INVALID_ARG,
                 "split-K workspace of " + std::to_string(need) +
@@ -1257,7 +1303,7 @@ bool same_step(const ServeRequest &a, const ServeRequest &b) {
 uint64_t matrix_bytes(uint32_t m, uint32_t n) {
   const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
   return 4ull * (2 * n * ldm + 2 * m * ldn + n * ldm) + 2ull * 3 * n * ldm +
-         2ull * 2 * n * ldm + 4ull * n;
+         2ull * 2 * n * ldm + 4ull * n + 2ull * 2 * m * ldn + 4ull * m;
 }
 
 // Device bytes of a batch of k starts on an m x n matrix (an upper estimate).
@@ -1265,7 +1311,7 @@ uint64_t batch_bytes(uint32_t m, uint32_t n, uint32_t k) {
   const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
   const uint64_t kv = (uint64_t)k * ldn, kz = (uint64_t)k * ldm;
   const uint64_t ws = 2ull * ((m + 127) / 128) * ((k + 63) / 64 + 3) * 256 * 128 * 4 * 8;
-  return 4 * kv * 4 + 2 * kz * 4 + kz * 2 + 2 * kz * 2 + 2 * (kv / 32) * 4 + ws +
+  return 4 * kv * 4 + 2 * kv * 2 + 2 * kz * 4 + kz * 2 + 2 * kz * 2 + 2 * (kv / 32) * 4 + ws +
          (uint64_t)k * 256 + (4ull << 20);
 }
 

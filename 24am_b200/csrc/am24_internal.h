@@ -38,6 +38,10 @@ struct MatrixDev {
   // batch first runs V = B^T Z on FP16 operands (null before).
   uint16_t *Bc_h2;
   float *row_scale;
+  // The same for B^T (Z = B V): two FP16 planes of each sample's row of Bt,
+  // scaled per sample (plane p at Bt_h2 + p * m * ldn), bt_row_scale[i] = 2^-s_i.
+  uint16_t *Bt_h2;
+  float *bt_row_scale;
 };
 
 // Per-batch device state for k starting points.
@@ -51,6 +55,13 @@ struct BatchDev {
   int pair2;      // V = B^T Z runs on CTA pairs (256-row tiles; B maps of bn2/2 rows)
   int bf16_2;     // ... with the exact BF16 operands of the L1-variance forms
   int fp16_2;     // ... with the split FP16 operands (preferred over bf16_2 and TF32)
+  int fp16_1;     // Z = B V on CTA pairs with split FP16 operands (split-K, splits1p)
+  int splits1p;   // its split-K factor
+  uint16_t *V_h;  // its B operand: two k x ldn FP16 planes (second at V_h + k * ldn)
+                  // of v * 2^s_j, written by densify_fp16_kernel
+  float *v_scale;            // per start 2^-s_j
+  const float *bt_row_scale;  // the matrix's FP16 row scales of B^T
+  size_t ws_len;  // floats in ws (the larger split-K layout)
   uint16_t *Z_h;  // FP16 Z for fp16_2: sgn(B V) exactly (one k x ldm plane, L1-variance
                   // forms), or two planes (second at Z_h + k * ldm) of z * 2^s_j
   float *z_scale;    // per start 2^-s_j (L2-variance forms with fp16_2)
@@ -107,6 +118,7 @@ struct TensorMaps {
   CUtensorMap a2_hi, a2_lo, b2_hi, b2_lo;  // V = B^T Z: A = Bc, B = Z
   CUtensorMap a2_b0, a2_b1, a2_b2, b2_b;   // V = B^T Z, BF16: A = Bc_b3, B = Z_b
   CUtensorMap a2_h0, a2_h1, b2_h0, b2_h1;  // V = B^T Z, FP16: A = Bc_h2, B = Z_h
+  CUtensorMap a1_h0, a1_h1, b1_h0, b1_h1;  // Z = B V, FP16: A = Bt_h2, B = V_h
 };
 
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
@@ -116,6 +128,8 @@ cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream
 cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st);
 // Fills M.Bc_h2 and M.row_scale from M.Bc.
 cudaError_t launch_prep_fp16x2(const MatrixDev &M, cudaStream_t st);
+// Fills M.Bt_h2 and M.bt_row_scale from M.Bt_hi + M.Bt_lo.
+cudaError_t launch_prep_bt_fp16x2(const MatrixDev &M, cudaStream_t st);
 // Loadings of `cols` columns from src (rows entries each) into dst and their
 // non-zero masks (mask + c * (ld_dst / 32) per column).
 cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols, float *dst,

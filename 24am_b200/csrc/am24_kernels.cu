@@ -191,7 +191,7 @@ struct EpiPenalty {
   const uint32_t *max_nnz;  // the previous step's largest non-zero count
   uint32_t cap;             // ... above which Z = B V runs dense
   bool planes = false;      // this launch writes V_hi / V_lo (set by setup)
-  __device__ void setup() { planes = *max_nnz > cap; }
+  __device__ void setup() { planes = V_hi != nullptr && *max_nnz > cap; }
   // r holds this thread's 32 values (row `row`, columns col0..col0+31) and is
   // overwritten with the objective terms.
   __device__ void chunk(const Unit &t, int q, int lane, int row, int col0, float (&r)[32]) {
@@ -303,6 +303,30 @@ __global__ void __launch_bounds__(256) prep_fp16x2_kernel(const float *__restric
   }
 }
 
+// As prep_fp16x2_kernel for the rows of B^T (one block per sample), whose
+// values are Bt_hi + Bt_lo (exact).
+__global__ void __launch_bounds__(256) prep_bt_fp16x2_kernel(const float *__restrict__ hi,
+                                                             const float *__restrict__ lo,
+                                                             int ldn, int n, size_t plane,
+                                                             uint16_t *__restrict__ out,
+                                                             float *__restrict__ row_scale) {
+  __shared__ uint32_t red[8];
+  const size_t r0 = (size_t)blockIdx.x * ldn;
+  uint32_t mx = 0;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) mx = max(mx, abs_key(hi[r0 + c] + lo[r0 + c]));
+  mx = __reduce_max_sync(FULL, mx);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  mx = 0;
+#pragma unroll
+  for (int w = 0; w < 8; w++) mx = max(mx, red[w]);
+  const int s = fp16_shift(__uint_as_float(mx));
+  const float sc = pow2f(s);
+  if (threadIdx.x == 0) row_scale[blockIdx.x] = pow2f(-s);
+  for (int c = threadIdx.x; c < n; c += blockDim.x)
+    fp16_split((hi[r0 + c] + lo[r0 + c]) * sc, out + r0 + c, out + plane + r0 + c);
+}
+
 // Bt[r * ldn + c] = split(B[c * ldB + r]): 32 x 32 tiles through shared memory.
 __global__ void prep_transpose_kernel(const float *__restrict__ B, int ldB, int m, int n,
                                       float *__restrict__ hi, float *__restrict__ lo, int ldn) {
@@ -360,6 +384,60 @@ __global__ void densify_kernel(const float *__restrict__ Vx, const uint32_t *__r
   for (int r = threadIdx.x; r < ld; r += blockDim.x) {
     const bool on = r < rows && ((mask[c * (ld >> 5) + (r >> 5)] >> (r & 31)) & 1u);
     split_store(on ? Vx[c * ld + r] : 0.f, V_hi + c * ld + r, V_lo + c * ld + r);
+  }
+}
+
+// Dense FP16 planes of V for the CTA-pair Z = B V (split FP16 operands): on
+// dense steps only (*gate > gate_max), one block per start, v * 2^s = h0 + h1
+// with s from the column's largest |v|, v_scale[c] = 2^-s.
+__global__ void __launch_bounds__(256) densify_fp16_kernel(const float *__restrict__ Vx,
+                                                           const uint32_t *__restrict__ mask,
+                                                           int ld, int rows,
+                                                           uint16_t *__restrict__ Vh, size_t plane,
+                                                           float *__restrict__ v_scale,
+                                                           const uint32_t *gate, uint32_t gate_max) {
+  __shared__ uint32_t red[8];
+  if (*gate <= gate_max) return;
+  const size_t c = blockIdx.x;
+  const uint32_t *mk = mask + c * (ld >> 5);
+  const float4 *vx4 = reinterpret_cast<const float4 *>(Vx + c * ld);
+  // four consecutive rows per thread and pass (ld is a multiple of 32)
+  auto quad = [&](int q, float (&v)[4]) {
+    const float4 x = vx4[q];
+    const uint32_t bits = mk[q >> 3] >> ((4 * q) & 31);
+    v[0] = ((bits & 1u) && 4 * q < rows) ? x.x : 0.f;
+    v[1] = ((bits & 2u) && 4 * q + 1 < rows) ? x.y : 0.f;
+    v[2] = ((bits & 4u) && 4 * q + 2 < rows) ? x.z : 0.f;
+    v[3] = ((bits & 8u) && 4 * q + 3 < rows) ? x.w : 0.f;
+  };
+  const int quads = ld >> 2;
+  uint32_t mx = 0;
+#pragma unroll 4
+  for (int q = threadIdx.x; q < quads; q += blockDim.x) {
+    float v[4];
+    quad(q, v);
+    mx = max(mx, max(max(abs_key(v[0]), abs_key(v[1])), max(abs_key(v[2]), abs_key(v[3]))));
+  }
+  mx = __reduce_max_sync(FULL, mx);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  mx = 0;
+#pragma unroll
+  for (int w = 0; w < 8; w++) mx = max(mx, red[w]);
+  const int s = fp16_shift(__uint_as_float(mx));
+  const float sc = pow2f(s);
+  if (threadIdx.x == 0) v_scale[c] = pow2f(-s);
+  uint2 *h0 = reinterpret_cast<uint2 *>(Vh + c * ld);
+  uint2 *h1 = reinterpret_cast<uint2 *>(Vh + plane + c * ld);
+#pragma unroll 4
+  for (int q = threadIdx.x; q < quads; q += blockDim.x) {
+    float v[4];
+    quad(q, v);
+    uint16_t a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) fp16_split(v[i] * sc, &a[i], &b[i]);
+    h0[q] = make_uint2(a[0] | ((uint32_t)a[1] << 16), a[2] | ((uint32_t)a[3] << 16));
+    h1[q] = make_uint2(b[0] | ((uint32_t)b[1] << 16), b[2] | ((uint32_t)b[3] << 16));
   }
 }
 
@@ -1567,7 +1645,7 @@ cudaError_t pair_clusters(K kern, int smem, int *out) {
 template <class S, int BN, int ST, class Epi>
 cudaError_t run_gemm_pair(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &m2,
                           const CUtensorMap &m3, const GemmShape &sh, const Epi &epi,
-                          cudaStream_t st) {
+                          cudaStream_t st, int splits = 1) {
   using L = PairSmem<S, BN, ST>;
   auto kern = gemm_pair_kernel<S, BN, ST, S::PROMO_K / S::BK, Epi>;
   static int clusters = 0;
@@ -1576,11 +1654,11 @@ cudaError_t run_gemm_pair(const CUtensorMap &m0, const CUtensorMap &m1, const CU
     if (e != cudaSuccess) return e;
     if ((e = pair_clusters(kern, L::TOTAL, &clusters)) != cudaSuccess) return e;
   }
-  GemmShape s2 = sh;  // K blocks of this scheme's BK; units are pair tiles
+  GemmShape s2 = sh;  // K blocks of this scheme's BK; units are pair tiles x splits
   s2.kb_total = (sh.K + S::BK - 1) / S::BK;
-  s2.kb_per_split = s2.kb_total;
-  s2.splits = 1;
-  s2.num_units = ((sh.m_tiles + 1) / 2) * sh.n_tiles;
+  s2.kb_per_split = (s2.kb_total + splits - 1) / splits;
+  s2.splits = (s2.kb_total + s2.kb_per_split - 1) / s2.kb_per_split;
+  s2.num_units = s2.splits * ((sh.m_tiles + 1) / 2) * sh.n_tiles;
   const int pairs = s2.num_units < clusters ? s2.num_units : clusters;
   kern<<<2 * pairs, GEMM_THREADS, L::TOTAL, st>>>(m0, m1, m2, m3, s2, epi);
   return cudaGetLastError();
@@ -1658,6 +1736,12 @@ cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st) {
 cudaError_t launch_prep_fp16x2(const MatrixDev &M, cudaStream_t st) {
   prep_fp16x2_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, (size_t)M.n * M.ldm, M.Bc_h2,
                                           M.row_scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep_bt_fp16x2(const MatrixDev &M, cudaStream_t st) {
+  prep_bt_fp16x2_kernel<<<M.m, 256, 0, st>>>(M.Bt_hi, M.Bt_lo, M.ldn, M.n, (size_t)M.m * M.ldn,
+                                             M.Bt_h2, M.bt_row_scale);
   return cudaGetLastError();
 }
 
@@ -1808,27 +1892,41 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   nl++;
   // 1b. dense V: TF32 hi/lo planes, tensor-core Z = B V (split-K partials) ...
   if ((e = mark(6)) != cudaSuccess) return e;
-  densify_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_hi, b.V_lo, b.max_nnz,
-                                      b.planes_nnz, b.sparse_cap);
+  if (b.fp16_1)
+    densify_fp16_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_h,
+                                             (size_t)b.k * M.ldn, b.v_scale, b.max_nnz,
+                                             b.sparse_cap);
+  else
+    densify_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_hi, b.V_lo, b.max_nnz,
+                                        b.planes_nnz, b.sparse_cap);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   EpiPartial ep{b.ws, b.bn1, b.m_tiles1, b.n_tiles1};
   if ((e = mark(0)) != cudaSuccess) return e;
-  e = dispatch_gemm(b.bn1, b.bk, tm.a1_hi, tm.a1_lo, tm.b1_hi, tm.b1_lo, g1, ep, st);
+  if (b.fp16_1) {
+    GemmShape gp = g1;
+    gp.row_scale = b.bt_row_scale;
+    gp.col_scale = b.v_scale;
+    e = run_gemm_pair<PairFP16x3, 256, 6>(tm.a1_h0, tm.a1_h1, tm.b1_h0, tm.b1_h1, gp, ep, st,
+                                          b.splits1p);
+  } else {
+    e = dispatch_gemm(b.bn1, b.bk, tm.a1_hi, tm.a1_lo, tm.b1_hi, tm.b1_lo, g1, ep, st);
+  }
   if (e != cudaSuccess) return e;
   nl++;
   // 2. ... then reduce + sign / normalise
+  const int splits1 = b.fp16_1 ? b.splits1p : b.splits1;
   if ((e = mark(1)) != cudaSuccess) return e;
   if (mode == 0)
-    z_reduce_kernel<0><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
+    z_reduce_kernel<0><<<b.k, 256, 0, st>>>(b.ws, splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
                                              b.Z_b, b.Z_h, zplane, b.z_scale);
   else if (mode == 1)
-    z_reduce_kernel<1><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
+    z_reduce_kernel<1><<<b.k, 256, 0, st>>>(b.ws, splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
                                              b.Z_b, b.Z_h, zplane, b.z_scale);
   else
-    z_reduce_kernel<2><<<b.k, 256, 0, st>>>(b.ws, b.splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
+    z_reduce_kernel<2><<<b.k, 256, 0, st>>>(b.ws, splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
                                              b.Z_b, b.Z_h, zplane, b.z_scale);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1873,18 +1971,21 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     nl++;
     return cudaSuccess;
   };
+  // the penalty epilogue writes the next dense step's TF32 planes of V
+  // (unless that step's Z = B V takes FP16 planes from densify_fp16_kernel)
+  float *vhi = b.fp16_1 ? nullptr : b.V_hi;
   if (is_constrained(f)) {
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
     e = gemm2(er);
   } else if (is_l1_penalized(f)) {
     EpiPenalty<true> pe{b.Vx,       b.obj_part, b.nnz_part, M.ldn,    M.n,
                         b.k,        b.bn2,      parts,      (float)p.penalty,
-                        b.vmask,    b.V_hi,     b.V_lo,     b.max_nnz, b.sparse_cap};
+                        b.vmask,    vhi,        b.V_lo,     b.max_nnz, b.sparse_cap};
     e = gemm2(pe);
   } else {
     EpiPenalty<false> pe{b.Vx,       b.obj_part, b.nnz_part, M.ldn,    M.n,
                          b.k,        b.bn2,      parts,      (float)p.penalty,
-                         b.vmask,    b.V_hi,     b.V_lo,     b.max_nnz, b.sparse_cap};
+                         b.vmask,    vhi,        b.V_lo,     b.max_nnz, b.sparse_cap};
     e = gemm2(pe);
   }
   if (e != cudaSuccess) return e;
@@ -1940,7 +2041,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   // Z = B V of this step has read max_nnz; finalize sets it for the next step
   // penalized forms: the count this step's epilogue saw (whether it wrote the
   // dense planes), for the next step's densify gate
-  if (!is_constrained(f) &&
+  if (!is_constrained(f) && !b.fp16_1 &&
       (e = cudaMemcpyAsync(b.planes_nnz, b.max_nnz, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                            st)) != cudaSuccess)
     return e;

@@ -180,14 +180,20 @@ def test_steps_through_sparse_gather_match_oracle(solver, po, formulation):
     M.close()
 
 
-@pytest.mark.parametrize("k", [96, 256])  # one-CTA and CTA-pair tiles
+@pytest.mark.parametrize("k,fp16", [(96, True), (256, False), (256, True)])
 @pytest.mark.parametrize("formulation", [4, 5, 6, 7])
-def test_dense_penalized_steps_reuse_epilogue_planes(solver, po, formulation, k):
-    """Penalties small enough to keep V dense step after step: from the second
-    step on, Z = B V reads the TF32 planes the previous step's penalty epilogue
-    wrote (densify returns at once); the loadings stay with the oracle's."""
+def test_dense_penalized_steps(solver, po, formulation, k, fp16, monkeypatch):
+    """Penalties small enough to keep V dense step after step.  On one-CTA
+    tiles (k = 96), and on CTA pairs without FP16 operands, from the second step
+    on Z = B V reads the TF32 planes the previous step's penalty epilogue wrote
+    (densify returns at once); on CTA pairs with FP16 operands densify writes
+    V's scaled FP16 planes every dense step.  The loadings stay with the
+    oracle's."""
     import importlib
     am = importlib.import_module("24am_b200")
+    if not fp16:
+        monkeypatch.setenv("AM24_GEMM_FP16", "0")
+    reuse = k <= 128 or not fp16
     m, n = 300, 2048
     B = po.low_rank_data(m, n, 8, 30, seed=91, dtype=np.float32)
     B64 = B.astype(np.float64)
@@ -209,7 +215,7 @@ def test_dense_penalized_steps_reuse_epilogue_planes(solver, po, formulation, k)
     assert np.count_nonzero(Vo, axis=0).max() > n // 32  # dense every step
     assert "densify" in kinds[0]
     for ks in kinds[1:]:
-        assert "densify(skipped)" in ks and "gemm_BV" in ks, ks
+        assert ("densify(skipped)" if reuse else "densify") in ks and "gemm_BV" in ks, ks
     ok = 0
     for j in range(k):
         same = np.array_equal(V[:, j] != 0, Vo[:, j] != 0)
