@@ -97,10 +97,9 @@ struct Allocs {
 struct am24_handle_s {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy = nullptr;  // host-to-device copies that overlap work on `stream`
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   Allocs scratch;  // small per-handle buffers
-  double *ev_rows = nullptr;
-  size_t ev_rows_cap = 0;
   double *ev_out = nullptr;
 };
 
@@ -175,6 +174,31 @@ am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat) {
   return AM24_OK;
 }
 
+// The matrix's TF32 hi/lo planes of B and B^T (made once, on first use).
+am24_status ensure_tf32_planes(am24_handle h, am24_matrix mat) {
+  MatrixDev &M = mat->d;
+  if (M.Bc_hi) return AM24_OK;
+  const size_t c_elems = (size_t)M.n * M.ldm, t_elems = (size_t)M.m * M.ldn;
+  float *p[4] = {nullptr, nullptr, nullptr, nullptr};
+  AM24_TRY(mat->mem.get(&p[0], c_elems));
+  AM24_TRY(mat->mem.get(&p[1], c_elems));
+  AM24_TRY(mat->mem.get(&p[2], t_elems));
+  AM24_TRY(mat->mem.get(&p[3], t_elems));
+  for (int i = 0; i < 4; i++)
+    AM24_CUDA(cudaMemsetAsync(p[i], 0, sizeof(float) * (i < 2 ? c_elems : t_elems), h->stream));
+  M.Bc_hi = p[0];
+  M.Bc_lo = p[1];
+  M.Bt_hi = p[2];
+  M.Bt_lo = p[3];
+  cudaError_t e = launch_prep_tf32_planes(M, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    M.Bc_hi = M.Bc_lo = M.Bt_hi = M.Bt_lo = nullptr;
+    return fail(AM24_ERR_CUDA, std::string("TF32 planes: ") + cudaGetErrorString(e));
+  }
+  return AM24_OK;
+}
+
 // The matrix's two scaled FP16 planes of B and their row scales (made once, on
 // first use).
 am24_status ensure_fp16_planes(am24_handle h, am24_matrix mat) {
@@ -185,7 +209,9 @@ am24_status ensure_fp16_planes(am24_handle h, am24_matrix mat) {
   float *rs = nullptr;
   AM24_TRY(mat->mem.get(&p, 2 * plane));
   AM24_TRY(mat->mem.get(&rs, (size_t)M.n));
-  AM24_CUDA(cudaMemsetAsync(p, 0, sizeof(uint16_t) * 2 * plane, h->stream));
+  if (M.ldm > M.m)  // the pad rows of both planes (2n columns)
+    AM24_CUDA(cudaMemset2DAsync(p + M.m, sizeof(uint16_t) * M.ldm, 0,
+                                sizeof(uint16_t) * (M.ldm - M.m), 2 * (size_t)M.n, h->stream));
   M.Bc_h2 = p;
   M.row_scale = rs;
   cudaError_t e = launch_prep_fp16x2(M, h->stream);
@@ -206,12 +232,16 @@ am24_status ensure_bt_fp16_planes(am24_handle h, am24_matrix mat) {
   const size_t plane = (size_t)M.m * M.ldn;
   uint16_t *p = nullptr;
   float *rs = nullptr;
+  uint32_t *key = nullptr;
   AM24_TRY(mat->mem.get(&p, 2 * plane));
   AM24_TRY(mat->mem.get(&rs, (size_t)M.m));
-  AM24_CUDA(cudaMemsetAsync(p, 0, sizeof(uint16_t) * 2 * plane, h->stream));
+  AM24_TRY(mat->mem.get(&key, (size_t)M.m));
+  if (M.ldn > M.n)  // the pad columns of both planes (2m rows)
+    AM24_CUDA(cudaMemset2DAsync(p + M.n, sizeof(uint16_t) * M.ldn, 0,
+                                sizeof(uint16_t) * (M.ldn - M.n), 2 * (size_t)M.m, h->stream));
   M.Bt_h2 = p;
   M.bt_row_scale = rs;
-  cudaError_t e = launch_prep_bt_fp16x2(M, h->stream);
+  cudaError_t e = launch_prep_bt_fp16x2(M, key, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     M.Bt_h2 = nullptr;
@@ -461,6 +491,10 @@ am24_status am24_create(am24_handle *out, int device) {
   auto *h = new am24_handle_s();
   h->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    e = cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking);
+    if (e != cudaSuccess) cudaStreamDestroy(h->stream);
+  }
   if (e != cudaSuccess) {
     delete h;
     return fail(AM24_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
@@ -470,6 +504,7 @@ am24_status am24_create(am24_handle *out, int device) {
   e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
   if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
     cudaStreamDestroy(h->stream);
+    cudaStreamDestroy(h->copy);
     delete h;
     return fail(AM24_ERR_CUDA, "cuTensorMapEncodeTiled entry point not available");
   }
@@ -477,6 +512,7 @@ am24_status am24_create(am24_handle *out, int device) {
   am24_status st = h->scratch.get(&h->ev_out, 1);
   if (st != AM24_OK) {
     cudaStreamDestroy(h->stream);
+    cudaStreamDestroy(h->copy);
     delete h;
     return st;
   }
@@ -487,7 +523,9 @@ am24_status am24_create(am24_handle *out, int device) {
 am24_status am24_destroy(am24_handle h) {
   if (!h) return AM24_OK;
   cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->copy);
   cudaStreamSynchronize(h->stream);
+  cudaStreamDestroy(h->copy);
   cudaStreamDestroy(h->stream);
   delete h;
   return AM24_OK;
@@ -543,35 +581,22 @@ static am24_status create_matrix(am24_handle h, const float *B, int32_t ldB, uin
   M.ldm = round_up((int)m, 32);
   M.ldn = round_up((int)n, 32);
   am24_status st;
-  const size_t c_elems = (size_t)n * M.ldm, t_elems = (size_t)m * M.ldn;
-  if ((st = mat->mem.get(&M.Bc_hi, c_elems)) != AM24_OK ||
-      (st = mat->mem.get(&M.Bc_lo, c_elems)) != AM24_OK ||
-      (st = mat->mem.get(&M.Bt_hi, t_elems)) != AM24_OK ||
-      (st = mat->mem.get(&M.Bt_lo, t_elems)) != AM24_OK ||
-      (st = mat->mem.get(&M.Bc, c_elems)) != AM24_OK) {
+  const size_t c_elems = (size_t)n * M.ldm;
+  if ((st = mat->mem.get(&M.Bc, c_elems)) != AM24_OK) {
     delete mat;
     return st;
   }
-  const float *src = B;
-  int ld_src = ldB;
-  float *staging = nullptr;
+  // one 2-D copy straight into Bc's layout (host or device source), pad rows
+  // zeroed; the other layouts are made from Bc when a batch first needs them
   cudaError_t e = cudaSuccess;
-  if (!on_device) {
-    e = cudaMallocAsync(reinterpret_cast<void **>(&staging), sizeof(float) * (size_t)m * n,
-                        h->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpy2DAsync(staging, sizeof(float) * m, B, sizeof(float) * (size_t)ldB,
-                            sizeof(float) * m, n, cudaMemcpyHostToDevice, h->stream);
-    src = staging;
-    ld_src = (int)m;
-  }
-  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bc_hi, 0, sizeof(float) * c_elems, h->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bc_lo, 0, sizeof(float) * c_elems, h->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bt_hi, 0, sizeof(float) * t_elems, h->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bt_lo, 0, sizeof(float) * t_elems, h->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(M.Bc, 0, sizeof(float) * c_elems, h->stream);
-  if (e == cudaSuccess) e = launch_prep_matrix(src, ld_src, M, h->stream);
-  if (staging) cudaFreeAsync(staging, h->stream);
+  if (M.ldm > (int)m)
+    e = cudaMemset2DAsync(M.Bc + m, sizeof(float) * M.ldm, 0, sizeof(float) * (M.ldm - m), n,
+                          h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(M.Bc, sizeof(float) * M.ldm, B, sizeof(float) * (size_t)ldB,
+                          sizeof(float) * m, n,
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                          h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     delete mat;
@@ -645,6 +670,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   d.need_stable = (uint32_t)std::max(1.0, std::ceil((double)settings->stable_share * k - 1e-9));
   d.need_stable = std::min(d.need_stable, (uint32_t)k);
   const bool need_bf16 = d.bf16_2 || d.mixed;
+  // TF32 planes: Z = B V off the FP16 pairs; V = B^T Z with neither FP16 nor BF16 operands
+  const bool tf32_1 = !d.fp16_1, tf32_2 = !d.fp16_2 && !d.bf16_2;
   const size_t zh_planes = is_l1_variance(settings->formulation) ? 1 : 2;
   const int bk2 = d.pair2 ? PAIR_BK_TF32 : d.bk;  // K box of the TF32 maps of V = B^T Z
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;
@@ -661,7 +688,9 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   am24_status st;
   auto &A = b->mem;
   const size_t kv = (size_t)k * M.ldn, kz = (size_t)k * M.ldm;
-  if ((st = A.get(&d.Vx, kv)) || (st = A.get(&d.V_hi, kv)) || (st = A.get(&d.V_lo, kv)) ||
+  if ((st = A.get(&d.Vx, kv)) ||
+      (tf32_1 && ((st = A.get(&d.V_hi, kv)) || (st = A.get(&d.V_lo, kv)))) ||
+      ((tf32_1 || tf32_2) && (st = ensure_tf32_planes(h, mat))) ||
       (st = A.get(&d.Vraw, kv)) ||
       (st = A.get(&d.Z_hi, kz)) || (st = A.get(&d.Z_lo, kz)) ||
       (st = A.get(&d.ws, d.ws_len)) ||
@@ -683,8 +712,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
     return st;
   }
   cudaError_t e = cudaMemsetAsync(d.Vx, 0, sizeof(float) * kv, h->stream);
-  if (!e) e = cudaMemsetAsync(d.V_hi, 0, sizeof(float) * kv, h->stream);
-  if (!e) e = cudaMemsetAsync(d.V_lo, 0, sizeof(float) * kv, h->stream);
+  if (!e && d.V_hi) e = cudaMemsetAsync(d.V_hi, 0, sizeof(float) * kv, h->stream);
+  if (!e && d.V_lo) e = cudaMemsetAsync(d.V_lo, 0, sizeof(float) * kv, h->stream);
   if (!e) e = cudaMemsetAsync(d.Vraw, 0, sizeof(float) * kv, h->stream);
   if (!e) e = cudaMemsetAsync(d.Z_hi, 0, sizeof(float) * kz, h->stream);
   if (!e) e = cudaMemsetAsync(d.Z_lo, 0, sizeof(float) * kz, h->stream);
@@ -714,14 +743,17 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
     delete b;
     return fail(AM24_ERR_CUDA, std::string("batch init: ") + cudaGetErrorString(e));
   }
-  if ((st = make_map(h, &b->tm.a1_hi, M.Bt_hi, M.n, M.m, M.ldn, BM, d.bk)) ||
-      (st = make_map(h, &b->tm.a1_lo, M.Bt_lo, M.n, M.m, M.ldn, BM, d.bk)) ||
-      (st = make_map(h, &b->tm.b1_hi, d.V_hi, M.n, k, M.ldn, d.bn1, d.bk)) ||
-      (st = make_map(h, &b->tm.b1_lo, d.V_lo, M.n, k, M.ldn, d.bn1, d.bk)) ||
-      (st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM, bk2)) ||
-      (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM, bk2)) ||
-      (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, bk2)) ||
-      (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2, bk2))) {
+  if ((tf32_1 && ((st = make_map(h, &b->tm.a1_hi, M.Bt_hi, M.n, M.m, M.ldn, BM, d.bk)) ||
+                  (st = make_map(h, &b->tm.a1_lo, M.Bt_lo, M.n, M.m, M.ldn, BM, d.bk)) ||
+                  (st = make_map(h, &b->tm.b1_hi, d.V_hi, M.n, k, M.ldn, d.bn1, d.bk)) ||
+                  (st = make_map(h, &b->tm.b1_lo, d.V_lo, M.n, k, M.ldn, d.bn1, d.bk)))) ||
+      (tf32_2 &&
+       ((st = make_map(h, &b->tm.a2_hi, M.Bc_hi, M.m, M.n, M.ldm, BM, bk2)) ||
+        (st = make_map(h, &b->tm.a2_lo, M.Bc_lo, M.m, M.n, M.ldm, BM, bk2)) ||
+        (st = make_map(h, &b->tm.b2_hi, d.Z_hi, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2,
+                       bk2)) ||
+        (st = make_map(h, &b->tm.b2_lo, d.Z_lo, M.m, k, M.ldm, d.pair2 ? d.bn2 / 2 : d.bn2,
+                       bk2))))) {
     delete b;
     return st;
   }
@@ -922,6 +954,38 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
   AM24_TRY(am24_check_input(settings, n));
   am24_settings &s = *settings;
   const int bs = s.batch_size;
+  Allocs local(h->stream);
+
+  // The first batch's injected starts cross to the device on the copy stream
+  // while the batch and the matrix layouts it needs are prepared on the main
+  // stream; the main stream waits for them before its first load.
+  float *pre = nullptr;
+  cudaEvent_t pre_ready = nullptr, pre_done = nullptr;
+  struct PreGuard {
+    cudaEvent_t *a, *c;
+    ~PreGuard() {
+      if (*a) cudaEventDestroy(*a);
+      if (*c) cudaEventDestroy(*c);
+    }
+  } preg{&pre_ready, &pre_done};
+  if (s.start_mode == AM24_START_INJECTED && !s.use_otf) {
+    AM24_TRY(local.get(&pre, (size_t)n * bs));
+    AM24_CUDA(cudaEventCreateWithFlags(&pre_ready, cudaEventDisableTiming));
+    AM24_CUDA(cudaEventCreateWithFlags(&pre_done, cudaEventDisableTiming));
+    AM24_CUDA(cudaEventRecord(pre_ready, h->stream));  // `pre` is allocated from here on
+    AM24_CUDA(cudaStreamWaitEvent(h->copy, pre_ready, 0));
+    AM24_CUDA(cudaMemcpyAsync(pre, start_points, sizeof(float) * (size_t)n * bs,
+                              cudaMemcpyHostToDevice, h->copy));
+    AM24_CUDA(cudaEventRecord(pre_done, h->copy));
+  }
+  // the main stream never runs ahead of the copy's completion past this scope
+  struct CopyJoin {
+    am24_handle h;
+    cudaEvent_t *done;
+    ~CopyJoin() {
+      if (*done) cudaStreamWaitEvent(h->stream, *done, 0);
+    }
+  } join{h, &pre_done};
 
   am24_batch b = nullptr;
   AM24_TRY(am24_batch_create(h, mat, &s, (uint32_t)bs, &b));
@@ -933,12 +997,11 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
 
   // best loading so far, kept as hi/lo planes; starts as the caller's x, which
   // the reference returns normalised when no start ever improves on -1
-  Allocs local(h->stream);
   float *xb = nullptr, *x_dev = nullptr;
   double *ev_rows = nullptr;
   AM24_TRY(local.get(&xb, n));
   AM24_TRY(local.get(&x_dev, n));
-  AM24_TRY(local.get(&ev_rows, (size_t)M.m));
+  AM24_TRY(local.get(&ev_rows, ev_partial_len(M)));
   AM24_CUDA(cudaMemcpyAsync(xb, x, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
 
   cudaEvent_t e0, e1;
@@ -980,6 +1043,10 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
       // the batch's starts, staged in Vraw by one copy (or generated there)
       if (s.start_mode == AM24_START_DEVICE_UNIFORM) {
         AM24_CUDA(launch_uniform_starts(d.Vraw, M.ldn, (int)n, bs, shift, h->stream));
+      } else if (batch == 0 && pre) {  // already on the device
+        AM24_CUDA(cudaStreamWaitEvent(h->stream, pre_done, 0));
+        AM24_CUDA(cudaMemcpy2DAsync(d.Vraw, sizeof(float) * M.ldn, pre, sizeof(float) * n,
+                                    sizeof(float) * n, bs, cudaMemcpyDeviceToDevice, h->stream));
       } else {
         const float *src = start_points + (size_t)shift * n;  // injected: read in place
         if (s.start_mode != AM24_START_INJECTED) {
@@ -1448,7 +1515,7 @@ am24_status run_group(am24_server s, ServeWorker &w, am24_matrix mat, uint32_t m
   double *ev_rows = nullptr;
   AM24_TRY(local.get(&xb, n));
   AM24_TRY(local.get(&x_dev, n));
-  AM24_TRY(local.get(&ev_rows, (size_t)M.m));
+  AM24_TRY(local.get(&ev_rows, ev_partial_len(M)));
   off = 0;
   for (auto &r : group) {
     const uint32_t k = (uint32_t)r->s.total_starts;

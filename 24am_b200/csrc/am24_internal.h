@@ -27,8 +27,11 @@ inline bool is_l1_penalized(int f) { return f == 6 || f == 7; }
 //   Bt: m rows (samples) of n features, leading dimension ldn  -> A of Z = B V
 struct MatrixDev {
   int m, n, ldm, ldn;
+  // TF32 hi/lo planes of Bc and Bt for the 3xTF32 products; made when a batch
+  // first needs them (null before)
   float *Bc_hi, *Bc_lo, *Bt_hi, *Bt_lo;
-  float *Bc;  // plain FP32 B, n rows of ldm samples: the gather Z = B V reads it
+  float *Bc;  // plain FP32 B, n rows of ldm samples (pad rows zero): the gather
+              // Z = B V, the explained variance and every other layout read it
   // Three BF16 planes of Bc (plane p at Bc_b3 + p * n * ldm) with
   // x = b0 + b1 + b2 exactly; made when a batch of an L1-variance form first
   // needs them (null before).
@@ -123,13 +126,14 @@ struct TensorMaps {
 
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
 int num_sms();
-cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st);
+// Fills M's TF32 planes (Bc_hi/lo, Bt_hi/lo) from M.Bc.
+cudaError_t launch_prep_tf32_planes(MatrixDev &M, cudaStream_t st);
 // Fills M.Bc_b3 from M.Bc.
 cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st);
 // Fills M.Bc_h2 and M.row_scale from M.Bc.
 cudaError_t launch_prep_fp16x2(const MatrixDev &M, cudaStream_t st);
-// Fills M.Bt_h2 and M.bt_row_scale from M.Bt_hi + M.Bt_lo.
-cudaError_t launch_prep_bt_fp16x2(const MatrixDev &M, cudaStream_t st);
+// Fills M.Bt_h2 and M.bt_row_scale from M.Bc; key: m words of scratch.
+cudaError_t launch_prep_bt_fp16x2(const MatrixDev &M, uint32_t *key, cudaStream_t st);
 // Loadings of `cols` columns from src (rows entries each) into dst and their
 // non-zero masks (mask + c * (ld_dst / 32) per column).
 cudaError_t launch_load_columns(const float *src, int ld_src, int rows, int cols, float *dst,
@@ -151,8 +155,13 @@ cudaError_t launch_finalize_x(const float *v, int n, float *x, cudaStream_t st);
 // timeout code in *status.
 cudaError_t launch_bounded_wait_probe(unsigned long long timeout_ns, int *status,
                                       cudaStream_t st);
+// ||B x||^2 in FP64 into *out; partial: ev_partial_len(M) doubles of scratch.
 cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double *partial,
                                       double *out, cudaStream_t st);
+constexpr int EV_CHUNK = 512;  // features per partial sum of the explained variance
+inline size_t ev_partial_len(const MatrixDev &M) {
+  return (size_t)((M.n + EV_CHUNK - 1) / EV_CHUNK) * M.m;
+}
 int pick_bn(int k);
 size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn);
 

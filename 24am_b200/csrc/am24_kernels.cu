@@ -252,7 +252,7 @@ __global__ void prep_copy_kernel(const float *__restrict__ B, int ldB, int m, fl
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
     const float v = B[c * ldB + r];
     split_store(v, hi + c * ldm + r, lo + c * ldm + r);
-    full[c * ldm + r] = v;
+    if (full) full[c * ldm + r] = v;
   }
 }
 
@@ -303,28 +303,43 @@ __global__ void __launch_bounds__(256) prep_fp16x2_kernel(const float *__restric
   }
 }
 
-// As prep_fp16x2_kernel for the rows of B^T (one block per sample), whose
-// values are Bt_hi + Bt_lo (exact).
-__global__ void __launch_bounds__(256) prep_bt_fp16x2_kernel(const float *__restrict__ hi,
-                                                             const float *__restrict__ lo,
-                                                             int ldn, int n, size_t plane,
-                                                             uint16_t *__restrict__ out,
-                                                             float *__restrict__ row_scale) {
-  __shared__ uint32_t red[8];
-  const size_t r0 = (size_t)blockIdx.x * ldn;
+// Per sample i, the largest |B[i, c]| over the features as a key, for the
+// FP16 planes of B^T: blocks of SAMPLE_MAX_CHUNK features, threads over samples
+// (coalesced reads of B's columns), atomicMax into key[i] (zeroed before).
+constexpr int SAMPLE_MAX_CHUNK = 64;
+__global__ void __launch_bounds__(256) sample_max_kernel(const float *__restrict__ Bc, int ldm,
+                                                         int m, int n, uint32_t *__restrict__ key) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int c0 = blockIdx.y * SAMPLE_MAX_CHUNK, c1 = min(n, c0 + SAMPLE_MAX_CHUNK);
   uint32_t mx = 0;
-  for (int c = threadIdx.x; c < n; c += blockDim.x) mx = max(mx, abs_key(hi[r0 + c] + lo[r0 + c]));
-  mx = __reduce_max_sync(FULL, mx);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  for (int c = c0; c < c1; c++) mx = max(mx, abs_key(Bc[(size_t)c * ldm + i]));
+  atomicMax(key + i, mx);
+}
+
+// As prep_fp16x2_kernel for the rows of B^T: out[i * ldn + c] (second plane at
+// out + plane) split from B[i, c] * 2^s_i, s_i from key[i]; row_scale[i] = 2^-s_i.
+// 32 x 32 tiles through shared memory; columns [n, ldn) are left as they are.
+__global__ void prep_bt_fp16x2_kernel(const float *__restrict__ Bc, int ldm, int m, int n,
+                                      const uint32_t *__restrict__ key, int ldn, size_t plane,
+                                      uint16_t *__restrict__ out, float *__restrict__ row_scale) {
+  __shared__ float tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;  // features, samples
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int c = c0 + y, r = r0 + threadIdx.x;
+    tile[y][threadIdx.x] = (c < n && r < m) ? Bc[(size_t)c * ldm + r] : 0.f;
+  }
   __syncthreads();
-  mx = 0;
-#pragma unroll
-  for (int w = 0; w < 8; w++) mx = max(mx, red[w]);
-  const int s = fp16_shift(__uint_as_float(mx));
-  const float sc = pow2f(s);
-  if (threadIdx.x == 0) row_scale[blockIdx.x] = pow2f(-s);
-  for (int c = threadIdx.x; c < n; c += blockDim.x)
-    fp16_split((hi[r0 + c] + lo[r0 + c]) * sc, out + r0 + c, out + plane + r0 + c);
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int r = r0 + y, c = c0 + threadIdx.x;
+    if (r >= m) continue;
+    const int s = fp16_shift(__uint_as_float(key[r]));
+    if (c < n) {
+      const size_t o = (size_t)r * ldn + c;
+      fp16_split(tile[threadIdx.x][y] * pow2f(s), out + o, out + plane + o);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) row_scale[r] = pow2f(-s);
+  }
 }
 
 // Bt[r * ldn + c] = split(B[c * ldB + r]): 32 x 32 tiles through shared memory.
@@ -1581,25 +1596,33 @@ __global__ void finalize_x_kernel(const float *__restrict__ v, int n, float *__r
   for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = v[i] * inv;
 }
 
-// y_r = sum_c B[r, c] x_c in FP64, one warp per sample row of Bt (hi + lo = B exactly).
-__global__ void ev_rows_kernel(const float *__restrict__ hi, const float *__restrict__ lo, int ld,
-                               int m, int n, const float *__restrict__ x,
-                               double *__restrict__ y) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= m) return;
-  const float *h = hi + (size_t)warp * ld;
-  const float *l = lo + (size_t)warp * ld;
+// Partial sums of y_i = sum_c B[i, c] x_c in FP64 over chunks of EV_CHUNK
+// features: partial[chunk * m + i], threads over samples (coalesced reads of
+// B's columns), features with x_c = 0 skipped, a fixed order per chunk.
+__global__ void __launch_bounds__(256) ev_partial_kernel(const float *__restrict__ Bc, int ldm,
+                                                         int m, int n, const float *__restrict__ x,
+                                                         double *__restrict__ partial) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int c0 = blockIdx.y * EV_CHUNK, c1 = min(n, c0 + EV_CHUNK);
   double acc = 0.0;
-  for (int c = lane; c < n; c += 32) acc += ((double)h[c] + (double)l[c]) * (double)x[c];
-  acc = warp_sum(acc);
-  if (lane == 0) y[warp] = acc;
+  for (int c = c0; c < c1; c++) {
+    const float xc = x[c];
+    if (xc != 0.f) acc += (double)Bc[(size_t)c * ldm + i] * (double)xc;
+  }
+  partial[(size_t)blockIdx.y * m + i] = acc;
 }
 
-__global__ void ev_sum_kernel(const double *__restrict__ y, int m, double *__restrict__ out) {
+// ||y||^2 with y_i the sum of its chunks' partials (in chunk order).
+__global__ void ev_sum_kernel(const double *__restrict__ partial, int chunks, int m,
+                              double *__restrict__ out) {
   __shared__ double red[32];
   double acc = 0.0;
-  for (int i = threadIdx.x; i < m; i += blockDim.x) acc += y[i] * y[i];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    double y = 0.0;
+    for (int c = 0; c < chunks; c++) y += partial[(size_t)c * m + i];
+    acc += y * y;
+  }
   acc = block_sum(acc, red);
   if (threadIdx.x == 0) *out = acc;
 }
@@ -1739,18 +1762,24 @@ cudaError_t launch_prep_fp16x2(const MatrixDev &M, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_prep_bt_fp16x2(const MatrixDev &M, cudaStream_t st) {
-  prep_bt_fp16x2_kernel<<<M.m, 256, 0, st>>>(M.Bt_hi, M.Bt_lo, M.ldn, M.n, (size_t)M.m * M.ldn,
-                                             M.Bt_h2, M.bt_row_scale);
+cudaError_t launch_prep_bt_fp16x2(const MatrixDev &M, uint32_t *key, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(key, 0, sizeof(uint32_t) * M.m, st);
+  if (e != cudaSuccess) return e;
+  sample_max_kernel<<<dim3((M.m + 255) / 256, (M.n + SAMPLE_MAX_CHUNK - 1) / SAMPLE_MAX_CHUNK),
+                      256, 0, st>>>(M.Bc, M.ldm, M.m, M.n, key);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  prep_bt_fp16x2_kernel<<<dim3((M.n + 31) / 32, (M.m + 31) / 32), dim3(32, 8), 0, st>>>(
+      M.Bc, M.ldm, M.m, M.n, key, M.ldn, (size_t)M.m * M.ldn, M.Bt_h2, M.bt_row_scale);
   return cudaGetLastError();
 }
 
-cudaError_t launch_prep_matrix(const float *B, int ldB, MatrixDev &M, cudaStream_t st) {
-  prep_copy_kernel<<<M.n, 256, 0, st>>>(B, ldB, M.m, M.Bc_hi, M.Bc_lo, M.Bc, M.ldm);
+cudaError_t launch_prep_tf32_planes(MatrixDev &M, cudaStream_t st) {
+  prep_copy_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, M.Bc_hi, M.Bc_lo, nullptr, M.ldm);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   dim3 grid((M.n + 31) / 32, (M.m + 31) / 32);
-  prep_transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(B, ldB, M.m, M.n, M.Bt_hi, M.Bt_lo, M.ldn);
+  prep_transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(M.Bc, M.ldm, M.m, M.n, M.Bt_hi, M.Bt_lo,
+                                                      M.ldn);
   return cudaGetLastError();
 }
 
@@ -1832,12 +1861,12 @@ cudaError_t launch_finalize_x(const float *v, int n, float *x, cudaStream_t st) 
 
 cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double *partial,
                                       double *out, cudaStream_t st) {
-  const int threads = 256;
-  const int blocks = (M.m * 32 + threads - 1) / threads;
-  ev_rows_kernel<<<blocks, threads, 0, st>>>(M.Bt_hi, M.Bt_lo, M.ldn, M.m, M.n, x, partial);
+  const int chunks = (M.n + EV_CHUNK - 1) / EV_CHUNK;
+  ev_partial_kernel<<<dim3((M.m + 255) / 256, chunks), 256, 0, st>>>(M.Bc, M.ldm, M.m, M.n, x,
+                                                                     partial);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  ev_sum_kernel<<<1, 1024, 0, st>>>(partial, M.m, out);
+  ev_sum_kernel<<<1, 1024, 0, st>>>(partial, chunks, M.m, out);
   return cudaGetLastError();
 }
 
