@@ -98,6 +98,11 @@ struct am24_handle_s {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy = nullptr;  // host-to-device copies that overlap work on `stream`
+  // run-ahead batch loops: the stop word of each queued step lands in pinned
+  // host memory, an event per slot
+  static constexpr int AHEAD = 4;
+  uint32_t *flags = nullptr;
+  cudaEvent_t run_ev[AHEAD] = {};
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   Allocs scratch;  // small per-handle buffers
   double *ev_out = nullptr;
@@ -272,6 +277,7 @@ static am24_status load_from_vraw(am24_handle h, am24_batch b) {
   AM24_CUDA(cudaMemsetAsync(b->d.sel_hint, 0, sizeof(float) * k, h->stream));      // no hints
   AM24_CUDA(cudaMemsetAsync(b->d.val, 0, sizeof(float) * k, h->stream));
   AM24_CUDA(cudaMemsetAsync(b->d.err, 0, sizeof(float) * k, h->stream));
+  AM24_CUDA(cudaMemsetAsync(b->d.ctl, 0, sizeof(uint32_t) * CTL_WORDS, h->stream));
   if (b->d.mixed) AM24_CUDA(reset_mixed(b->d, h->stream));
   return AM24_OK;
 }
@@ -346,6 +352,47 @@ am24_status check_device_status(am24_batch b) {
     snprintf(buf, sizeof buf, "device-side wait timed out (code 0x%x)", st);
     return fail(AM24_ERR_DEVICE_TIMEOUT, buf);
   }
+  return AM24_OK;
+}
+
+// What a batch loop ran: its steps, how many of them in the BF16 phase
+// (MIXED), and the last step's largest change.
+struct BatchRun {
+  int steps = 0;
+  uint32_t low_steps = 0;
+  float max_err = 0.f;
+};
+
+// The reference's batch loop (sparse_PCA_solver.h:192-212) over the loaded
+// batch: steps it = 0, 1, ... until one with it > 0, in the refinement phase,
+// leaves the batch's largest change below the tolerance, or max_iter steps.
+// The test runs on the device at the end of each step (finalize), which then
+// sets the batch's stop word; steps stay queued up to AHEAD ahead of the
+// host's look at that word, and the ones queued past the stop return at once.
+am24_status run_batch_steps(am24_handle h, am24_batch b, const am24_settings &s, int shift,
+                            BatchRun *out) {
+  constexpr int AHEAD = am24_handle_s::AHEAD;
+  const BatchDev &d = b->d;
+  for (int it = 0; it < s.max_iter; it++) {
+    StepParams p = step_params(s, it, shift);
+    p.stop_check = 1;
+    AM24_CUDA(launch_am_step(b->mat->d, b->d, b->tm, p, h->stream, &b->launches));
+    AM24_CUDA(cudaMemcpyAsync(&h->flags[it % AHEAD], d.ctl + CTL_STOP, sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, h->stream));
+    AM24_CUDA(cudaEventRecord(h->run_ev[it % AHEAD], h->stream));
+    const int probe = it - (AHEAD - 1);  // the oldest step still unread
+    if (probe >= 0) {
+      AM24_CUDA(cudaEventSynchronize(h->run_ev[probe % AHEAD]));
+      if (h->flags[probe % AHEAD]) break;
+    }
+  }
+  uint32_t c[CTL_WORDS];
+  AM24_CUDA(cudaMemcpyAsync(c, d.ctl, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  AM24_TRY(check_device_status(b));
+  out->steps = (int)c[CTL_STEPS];
+  out->low_steps = c[CTL_LOW_STEPS];
+  memcpy(&out->max_err, &c[CTL_MAX_ERR], sizeof(float));
   return AM24_OK;
 }
 
@@ -510,7 +557,16 @@ am24_status am24_create(am24_handle *out, int device) {
   }
   h->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   am24_status st = h->scratch.get(&h->ev_out, 1);
+  if (st == AM24_OK && cudaMallocHost(reinterpret_cast<void **>(&h->flags),
+                                      sizeof(uint32_t) * am24_handle_s::AHEAD) != cudaSuccess)
+    st = fail(AM24_ERR_CUDA, "cudaMallocHost failed");
+  for (int i = 0; st == AM24_OK && i < am24_handle_s::AHEAD; i++)
+    if (cudaEventCreateWithFlags(&h->run_ev[i], cudaEventDisableTiming) != cudaSuccess)
+      st = fail(AM24_ERR_CUDA, "cudaEventCreate failed");
   if (st != AM24_OK) {
+    for (int i = 0; i < am24_handle_s::AHEAD; i++)
+      if (h->run_ev[i]) cudaEventDestroy(h->run_ev[i]);
+    if (h->flags) cudaFreeHost(h->flags);
     cudaStreamDestroy(h->stream);
     cudaStreamDestroy(h->copy);
     delete h;
@@ -525,6 +581,8 @@ am24_status am24_destroy(am24_handle h) {
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->copy);
   cudaStreamSynchronize(h->stream);
+  for (int i = 0; i < am24_handle_s::AHEAD; i++) cudaEventDestroy(h->run_ev[i]);
+  cudaFreeHost(h->flags);
   cudaStreamDestroy(h->copy);
   cudaStreamDestroy(h->stream);
   delete h;
@@ -700,7 +758,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
       (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||
       (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.planes_nnz, 1)) ||
-      (st = A.get(&d.sel_hint, k)) ||
+      (st = A.get(&d.sel_hint, k)) || (st = A.get(&d.ctl, (size_t)CTL_WORDS)) ||
       (need_bf16 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat)))) ||
       (d.fp16_2 && ((st = A.get(&d.Z_h, zh_planes * kz)) || (st = A.get(&d.z_scale, k)) ||
                     (st = ensure_fp16_planes(h, mat)))) ||
@@ -726,6 +784,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.max_nnz, 0xFF, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.planes_nnz, 0, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.sel_hint, 0, sizeof(float) * k, h->stream);
+  if (!e) e = cudaMemsetAsync(d.ctl, 0, sizeof(uint32_t) * CTL_WORDS, h->stream);
   if (!e && d.Z_b) e = cudaMemsetAsync(d.Z_b, 0, sizeof(uint16_t) * kz, h->stream);
   if (!e && d.Z_h) e = cudaMemsetAsync(d.Z_h, 0, sizeof(uint16_t) * zh_planes * kz, h->stream);
   if (!e && d.z_scale) e = cudaMemsetAsync(d.z_scale, 0, sizeof(float) * k, h->stream);
@@ -1058,27 +1117,14 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
       }
       AM24_TRY(load_from_vraw(h, b));
       if (d.mixed) AM24_CUDA(reset_mixed(d, h->stream));
-      uint32_t phase = d.mixed ? 0u : 1u;  // the phase the next step runs in
       AM24_CUDA(cudaEventRecord(e0, h->stream));
-      int it = 0;
-      for (; it < s.max_iter; it++) {
-        total_it++;
-        const bool refined = phase != 0;
-        low_its += refined ? 0 : 1;
-        const StepParams p = step_params(s, it, (int)shift);
-        AM24_CUDA(launch_am_step(M, b->d, b->tm, p, h->stream, &b->launches));
-        AM24_CUDA(cudaMemcpyAsync(&last_max_err, d.max_err, sizeof(float), cudaMemcpyDeviceToHost,
-                                  h->stream));
-        if (d.mixed)
-          AM24_CUDA(cudaMemcpyAsync(&phase, d.phase, sizeof phase, cudaMemcpyDeviceToHost,
-                                    h->stream));
-        AM24_CUDA(cudaStreamSynchronize(h->stream));
-        AM24_TRY(check_device_status(b));
-        start_its += (uint64_t)bs;
-        // MIXED: the tolerance test applies to refinement steps only
-        if (it > 0 && refined && (double)last_max_err < s.tolerance) break;
-      }
+      BatchRun run;
+      AM24_TRY(run_batch_steps(h, b, s, (int)shift, &run));
       AM24_CUDA(cudaEventRecord(e1, h->stream));
+      total_it += (uint32_t)run.steps;
+      low_its += run.low_steps;
+      start_its += (uint64_t)run.steps * (uint64_t)bs;
+      last_max_err = run.max_err;
       AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * bs, cudaMemcpyDeviceToHost,
                                 h->stream));
       AM24_CUDA(cudaStreamSynchronize(h->stream));
@@ -1483,26 +1529,12 @@ am24_status run_group(am24_server s, ServeWorker &w, am24_matrix mat, uint32_t m
     }
   } evg{e0, e1};
   AM24_CUDA(cudaEventRecord(e0, h->stream));
-  uint32_t phase = d.mixed ? 0u : 1u, low_its = 0;
-  float max_err = 0.f;
-  int it = 0;
-  for (; it < bs.max_iter; it++) {
-    const bool refined = phase != 0;
-    low_its += refined ? 0 : 1;
-    const StepParams p = step_params(bs, it, 0);
-    AM24_CUDA(launch_am_step(M, b->d, b->tm, p, h->stream, &b->launches));
-    AM24_CUDA(cudaMemcpyAsync(&max_err, d.max_err, sizeof(float), cudaMemcpyDeviceToHost,
-                              h->stream));
-    if (d.mixed)
-      AM24_CUDA(cudaMemcpyAsync(&phase, d.phase, sizeof phase, cudaMemcpyDeviceToHost, h->stream));
-    AM24_CUDA(cudaStreamSynchronize(h->stream));
-    AM24_TRY(check_device_status(b));
-    if (it > 0 && refined && (double)max_err < bs.tolerance) {
-      it++;
-      break;
-    }
-  }
+  BatchRun run;
+  AM24_TRY(run_batch_steps(h, b, bs, 0, &run));
   AM24_CUDA(cudaEventRecord(e1, h->stream));
+  const int it = run.steps;
+  const uint32_t low_its = run.low_steps;
+  const float max_err = run.max_err;
   std::vector<float> val(K);
   AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * K, cudaMemcpyDeviceToHost,
                             h->stream));

@@ -65,6 +65,7 @@ struct BatchDev {
   float *v_scale;            // per start 2^-s_j
   const float *bt_row_scale;  // the matrix's FP16 row scales of B^T
   size_t ws_len;  // floats in ws (the larger split-K layout)
+  uint32_t *ctl;  // CTL_WORDS run-ahead control words
   uint16_t *Z_h;  // FP16 Z for fp16_2: sgn(B V) exactly (one k x ldm plane, L1-variance
                   // forms), or two planes (second at Z_h + k * ldm) of z * 2^s_j
   float *z_scale;    // per start 2^-s_j (L2-variance forms with fp16_2)
@@ -114,6 +115,19 @@ struct StepParams {
   int it;             // iteration index within the batch (termination_criteria)
   int log_shift;      // batch shift of the per-start logs
   unsigned long long timeout_ns;
+  int stop_check = 0;  // the step sets the stop word when the batch loop would end
+};
+
+// Run-ahead control words of a batch (BatchDev::ctl).  Every step kernel
+// returns at once while ctl[CTL_STOP] is set, so a driver can queue steps
+// ahead of the convergence test; a load clears the words.
+enum : int {
+  CTL_STOP = 0,       // set by the step that ends the batch loop (or a device timeout)
+  CTL_STEPS = 1,      // steps executed since the load
+  CTL_LOW_STEPS = 2,  // ... of them in the BF16 phase (MIXED)
+  CTL_MAX_ERR = 3,    // the last executed step's largest change (float bits)
+  CTL_BLOCKS = 4,     // finalize's block counter (scratch)
+  CTL_WORDS = 8
 };
 
 struct TensorMaps {

@@ -393,8 +393,9 @@ __global__ void masked_copy_kernel(const float *__restrict__ Vx, const uint32_t 
 __global__ void densify_kernel(const float *__restrict__ Vx, const uint32_t *__restrict__ mask,
                                int ld, int rows, float *__restrict__ V_hi,
                                float *__restrict__ V_lo, const uint32_t *gate,
-                               const uint32_t *planes, uint32_t gate_max) {
-  if (*gate <= gate_max || *planes > gate_max) return;
+                               const uint32_t *planes, uint32_t gate_max,
+                               const uint32_t *stop) {
+  if (*stop || *gate <= gate_max || *planes > gate_max) return;
   const size_t c = blockIdx.x;
   for (int r = threadIdx.x; r < ld; r += blockDim.x) {
     const bool on = r < rows && ((mask[c * (ld >> 5) + (r >> 5)] >> (r & 31)) & 1u);
@@ -410,9 +411,10 @@ __global__ void __launch_bounds__(256) densify_fp16_kernel(const float *__restri
                                                            int ld, int rows,
                                                            uint16_t *__restrict__ Vh, size_t plane,
                                                            float *__restrict__ v_scale,
-                                                           const uint32_t *gate, uint32_t gate_max) {
+                                                           const uint32_t *gate, uint32_t gate_max,
+                                                           const uint32_t *stop) {
   __shared__ uint32_t red[8];
-  if (*gate <= gate_max) return;
+  if (*stop || *gate <= gate_max) return;
   const size_t c = blockIdx.x;
   const uint32_t *mk = mask + c * (ld >> 5);
   const float4 *vx4 = reinterpret_cast<const float4 *>(Vx + c * ld);
@@ -469,9 +471,10 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
                                                        const uint32_t *gate, uint32_t gate_max,
                                                        uint16_t *__restrict__ Zb,
                                                        uint16_t *__restrict__ Zh, size_t zplane,
-                                                       float *__restrict__ zscale) {
+                                                       float *__restrict__ zscale,
+                                                       const uint32_t *stop) {
   __shared__ double red[32];
-  if (*gate <= gate_max) return;  // the gather kernel produced Z this step
+  if (*stop || *gate <= gate_max) return;  // the gather kernel produced Z this step
   const int j = blockIdx.x;
   const int nt = j / bn, c = j - nt * bn;
   const size_t unit_stride = (size_t)bn * BM;
@@ -527,11 +530,14 @@ constexpr int GATHER_CAP = 4096;
 // per start, the number of consecutive steps whose support (non-zero mask)
 // equals the previous step's.  When at least `need` starts of the batch have
 // kept their support for k_stable steps, phase[0] switches to refinement for
-// good; the last block to finish decides and resets the step's scratch words.
+// good; the last block to finish decides, keeps the phase the step ran in as
+// phase[3] and resets the step's scratch words.
 __global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict__ vmask,
                                                       const uint32_t *__restrict__ prev, int words,
                                                       uint32_t *stable, uint32_t *phase,
-                                                      uint32_t k_stable, uint32_t need) {
+                                                      uint32_t k_stable, uint32_t need,
+                                                      const uint32_t *stop) {
+  if (*stop) return;
   const int j = blockIdx.x;
   const uint32_t *a = vmask + (size_t)j * words, *b = prev + (size_t)j * words;
   int diff = 0;
@@ -545,6 +551,7 @@ __global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict
     if (atomicAdd(&phase[2], 1u) == gridDim.x - 1) {
       __threadfence();
       const uint32_t count = atomicExch(&phase[1], 0u);
+      phase[3] = phase[0];
       if (count >= need) phase[0] = 1u;
       phase[2] = 0u;
     }
@@ -563,12 +570,12 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
     const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
     float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
     uint16_t *__restrict__ Zb, uint16_t *__restrict__ Zh, size_t zplane,
-    float *__restrict__ zscale) {
+    float *__restrict__ zscale, const uint32_t *stop) {
   __shared__ int idx[GATHER_CAP];
   __shared__ float val[GATHER_CAP];
   __shared__ uint32_t wsum[GATHER_THREADS / 32];
   __shared__ double red[32];
-  if (*gate > gate_max) return;  // dense V: gemm1 + z_reduce handle this step
+  if (*stop || *gate > gate_max) return;  // dense V: gemm1 + z_reduce handle this step
   const int j = blockIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int words = ldn >> 5;
@@ -973,7 +980,8 @@ __device__ uint32_t gather_pairs_above(const float *__restrict__ colg, int n, ui
 __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
-    float *__restrict__ hints) {
+    float *__restrict__ hints, const uint32_t *stop) {
+  if (*stop) return;
   __shared__ uint64_t cand[HARD_CAND];  // also 2 * HARD_CAND keys for (b)
   __shared__ uint32_t hist[2048];
   __shared__ uint32_t res[8];
@@ -1285,7 +1293,8 @@ template <bool EXACT>
 __global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
-    float *__restrict__ hints) {
+    float *__restrict__ hints, const uint32_t *stop) {
+  if (*stop) return;
   __shared__ uint64_t pairs[SOFT_C];  // hinted (key, index) candidates
   __shared__ float cand[SOFT_C];
   __shared__ double p1[SOFT_C], p2[SOFT_C];
@@ -1534,15 +1543,48 @@ struct FinalizeArgs {
   float *val, *err, *max_err;
   uint32_t *max_nnz;
   int *iters, *cards;
+  // run-ahead control (StepCtl words); stop_check: this step may stop the batch
+  uint32_t *ctl;
+  const uint32_t *phase;  // MIXED: phase[3] is the phase the step ran in; else null
+  const int *status;
+  int stop_check;
 };
 
 // One warp per start; the batch maximum is an atomicMax on the bit pattern
 // of the (non-negative, non-NaN) changes, zeroed before the step -- max is
 // order-independent, so the result is deterministic.
+__device__ void finalize_start(const FinalizeArgs &a, int j, int lane);
+
+// The last block to finish also closes the step for the run-ahead driver: it
+// counts the step (and, MIXED, whether it ran in the BF16 phase), keeps the
+// batch's largest change, and sets the stop word when the reference's batch
+// loop would end here (it > 0, a refinement step, max change < tolerance) or
+// a device-side wait gave up.
 __global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs a) {
+  if (a.ctl[CTL_STOP]) return;
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (j >= a.k) return;
+  if (j < a.k) finalize_start(a, j, lane);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.ctl[CTL_BLOCKS], 1u) == gridDim.x - 1) {
+      __threadfence();
+      const float me = *reinterpret_cast<volatile float *>(a.max_err);
+      const bool refined = a.phase == nullptr || a.phase[3] != 0u;
+      a.ctl[CTL_STEPS] += 1u;
+      if (!refined) a.ctl[CTL_LOW_STEPS] += 1u;
+      a.ctl[CTL_MAX_ERR] = __float_as_uint(me);
+      if ((a.stop_check && a.it > 0 && refined && (double)me < a.tolerance) ||
+          *reinterpret_cast<const volatile int *>(a.status) != 0)
+        a.ctl[CTL_STOP] = 1u;
+      a.ctl[CTL_BLOCKS] = 0u;
+    }
+  }
+}
+
+// One start's objective, change and logs (one warp; lane 0 writes).
+__device__ void finalize_start(const FinalizeArgs &a, int j, int lane) {
   const bool cons = a.formulation <= 3;
   const bool l1pen = a.formulation >= 6;
   float f;
@@ -1898,6 +1940,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g1.num_units = g1.splits * g1.m_tiles * g1.n_tiles;
   g1.timeout_ns = p.timeout_ns;
   g1.status = b.status;
+  g1.stop = b.ctl;
   g1.gate = b.max_nnz;  // dense steps only
   g1.gate_min = b.sparse_cap + 1;
   g1.gate_max = 0xFFFFFFFFu;
@@ -1908,15 +1951,18 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (mode == 0)
     gather_bv_kernel<0><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale,
+                                                        b.ctl);
   else if (mode == 1)
     gather_bv_kernel<1><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale,
+                                                        b.ctl);
   else
     gather_bv_kernel<2><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,
                                                         b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz,
-                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale);
+                                                        b.max_nnz, b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale,
+                                                        b.ctl);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   // 1b. dense V: TF32 hi/lo planes, tensor-core Z = B V (split-K partials) ...
@@ -1924,10 +1970,10 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (b.fp16_1)
     densify_fp16_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_h,
                                              (size_t)b.k * M.ldn, b.v_scale, b.max_nnz,
-                                             b.sparse_cap);
+                                             b.sparse_cap, b.ctl);
   else
     densify_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_hi, b.V_lo, b.max_nnz,
-                                        b.planes_nnz, b.sparse_cap);
+                                        b.planes_nnz, b.sparse_cap, b.ctl);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   EpiPartial ep{b.ws, b.bn1, b.m_tiles1, b.n_tiles1};
@@ -1949,15 +1995,15 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (mode == 0)
     z_reduce_kernel<0><<<b.k, 256, 0, st>>>(b.ws, splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
-                                             b.Z_b, b.Z_h, zplane, b.z_scale);
+                                             b.Z_b, b.Z_h, zplane, b.z_scale, b.ctl);
   else if (mode == 1)
     z_reduce_kernel<1><<<b.k, 256, 0, st>>>(b.ws, splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
-                                             b.Z_b, b.Z_h, zplane, b.z_scale);
+                                             b.Z_b, b.Z_h, zplane, b.z_scale, b.ctl);
   else
     z_reduce_kernel<2><<<b.k, 256, 0, st>>>(b.ws, splits1, b.m_tiles1, b.n_tiles1, b.bn1, M.m,
                                              b.Z_hi, b.Z_lo, M.ldm, b.fz, b.max_nnz, b.sparse_cap,
-                                             b.Z_b, b.Z_h, zplane, b.z_scale);
+                                             b.Z_b, b.Z_h, zplane, b.z_scale, b.ctl);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   nl++;
   // 3. V = B^T Z
@@ -1973,6 +2019,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   g2.num_units = g2.m_tiles * g2.n_tiles;
   g2.timeout_ns = p.timeout_ns;
   g2.status = b.status;
+  g2.stop = b.ctl;
   g2.gate = nullptr;
   g2.gate_min = 0;
   g2.gate_max = 0;
@@ -2023,17 +2070,18 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     if ((e = mark(3)) != cudaSuccess) return e;
     if (!is_l1_constrained(f)) {
       hard_select_kernel<<<b.k, HARD_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint, b.Vx,
-                                                        b.nnz, b.status, b.vmask, b.sel_hint);
+                                                        b.nnz, b.status, b.vmask, b.sel_hint,
+                                                        b.ctl);
       e = cudaGetLastError();
     } else {
       if (p.l1_mode == 0)
         soft_select_kernel<false><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
                                                                 b.Vx, b.nnz, b.status, b.vmask,
-                                                                b.sel_hint);
+                                                                b.sel_hint, b.ctl);
       else
         soft_select_kernel<true><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
                                                                b.Vx, b.nnz, b.status, b.vmask,
-                                                               b.sel_hint);
+                                                               b.sel_hint, b.ctl);
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
@@ -2043,7 +2091,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (b.mixed) {
     if ((e = mark(8)) != cudaSuccess) return e;
     support_kernel<<<b.k, 256, 0, st>>>(b.vmask, b.vmask_prev, M.ldn / 32, b.stable, b.phase,
-                                        b.k_stable, b.need_stable);
+                                        b.k_stable, b.need_stable, b.ctl);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     nl++;
   }
@@ -2067,6 +2115,10 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   fa.iters = b.iters;
   fa.cards = b.cards;
   fa.max_nnz = b.max_nnz;
+  fa.ctl = b.ctl;
+  fa.phase = b.mixed ? b.phase : nullptr;
+  fa.status = b.status;
+  fa.stop_check = p.stop_check;
   // Z = B V of this step has read max_nnz; finalize sets it for the next step
   // penalized forms: the count this step's epilogue saw (whether it wrote the
   // dense planes), for the next step's densify gate

@@ -214,7 +214,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  if (shape.gate && (*shape.gate < shape.gate_min || *shape.gate > shape.gate_max))
+  if ((shape.stop && *shape.stop) ||
+      (shape.gate && (*shape.gate < shape.gate_min || *shape.gate > shape.gate_max)))
     return;  // uniform over the grid
   const int rank = static_cast<int>(cluster_ctarank());
   const int pair = blockIdx.x >> 1;

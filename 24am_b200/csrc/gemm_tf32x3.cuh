@@ -65,6 +65,7 @@ struct GemmShape {
   // the operands' range scaling exactly.
   const float *row_scale = nullptr;
   const float *col_scale = nullptr;
+  const uint32_t *stop = nullptr;  // the launch returns at once while *stop is set
 };
 
 // One work unit as an epilogue sees it: rows [m0, m0 + 128) of C (this CTA's
@@ -135,7 +136,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  if (shape.gate && (*shape.gate < shape.gate_min || *shape.gate > shape.gate_max))
+  if ((shape.stop && *shape.stop) ||
+      (shape.gate && (*shape.gate < shape.gate_min || *shape.gate > shape.gate_max)))
     return;  // uniform over the grid
 
   if (threadIdx.x == 0) {
