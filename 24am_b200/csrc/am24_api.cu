@@ -731,6 +731,10 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   // TF32 planes: Z = B V off the FP16 pairs; V = B^T Z with neither FP16 nor BF16 operands
   const bool tf32_1 = !d.fp16_1, tf32_2 = !d.fp16_2 && !d.bf16_2;
   const size_t zh_planes = is_l1_variance(settings->formulation) ? 1 : 2;
+  // constrained forms: V = B^T Z's epilogue lists the selects' hinted
+  // candidates (AM24_SELECT_LIST=0 leaves the gather to the select kernels)
+  bool lists = is_constrained(settings->formulation);
+  if (const char *e = getenv("AM24_SELECT_LIST")) lists = lists && atoi(e) != 0;
   const int bk2 = d.pair2 ? PAIR_BK_TF32 : d.bk;  // K box of the TF32 maps of V = B^T Z
   const int kb_total1 = (M.n + d.bk - 1) / d.bk;
   choose_splits(d.m_tiles1 * d.n_tiles1, kb_total1, num_sms(), &d.splits1, &d.kbps1);
@@ -759,6 +763,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||
       (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.planes_nnz, 1)) ||
       (st = A.get(&d.sel_hint, k)) || (st = A.get(&d.ctl, (size_t)CTL_WORDS)) ||
+      (lists && (st = A.get(&d.cmask, (size_t)k * (M.ldn / 32)))) ||
       (need_bf16 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat)))) ||
       (d.fp16_2 && ((st = A.get(&d.Z_h, zh_planes * kz)) || (st = A.get(&d.z_scale, k)) ||
                     (st = ensure_fp16_planes(h, mat)))) ||
@@ -785,6 +790,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (!e) e = cudaMemsetAsync(d.planes_nnz, 0, sizeof(uint32_t), h->stream);
   if (!e) e = cudaMemsetAsync(d.sel_hint, 0, sizeof(float) * k, h->stream);
   if (!e) e = cudaMemsetAsync(d.ctl, 0, sizeof(uint32_t) * CTL_WORDS, h->stream);
+  if (!e && d.cmask)
+    e = cudaMemsetAsync(d.cmask, 0, sizeof(uint32_t) * k * (M.ldn / 32), h->stream);
   if (!e && d.Z_b) e = cudaMemsetAsync(d.Z_b, 0, sizeof(uint16_t) * kz, h->stream);
   if (!e && d.Z_h) e = cudaMemsetAsync(d.Z_h, 0, sizeof(uint16_t) * zh_planes * kz, h->stream);
   if (!e && d.z_scale) e = cudaMemsetAsync(d.z_scale, 0, sizeof(float) * k, h->stream);
@@ -1425,6 +1432,7 @@ uint64_t batch_bytes(uint32_t m, uint32_t n, uint32_t k) {
   const uint64_t kv = (uint64_t)k * ldn, kz = (uint64_t)k * ldm;
   const uint64_t ws = 2ull * ((m + 127) / 128) * ((k + 63) / 64 + 3) * 256 * 128 * 4 * 8;
   return 4 * kv * 4 + 2 * kv * 2 + 2 * kz * 4 + kz * 2 + 2 * kz * 2 + 2 * (kv / 32) * 4 + ws +
+         kv / 8 +
          (uint64_t)k * 256 + (4ull << 20);
 }
 

@@ -66,6 +66,10 @@ struct BatchDev {
   const float *bt_row_scale;  // the matrix's FP16 row scales of B^T
   size_t ws_len;  // floats in ws (the larger split-K layout)
   uint32_t *ctl;  // CTL_WORDS run-ahead control words
+  // constrained forms: k x (ldn/32) words, the candidates of the hinted select
+  // that V = B^T Z's epilogue marks (|v| at or above the bound of the column's
+  // previous level)
+  uint32_t *cmask;
   uint16_t *Z_h;  // FP16 Z for fp16_2: sgn(B V) exactly (one k x ldm plane, L1-variance
                   // forms), or two planes (second at Z_h + k * ldm) of z * 2^s_j
   float *z_scale;    // per start 2^-s_j (L2-variance forms with fp16_2)

@@ -137,12 +137,20 @@ __device__ __forceinline__ float transpose_reduce32(float (&v)[32], int lane) {
   return v[0];
 }
 
+// fraction of the previous level used as the gather bound of the hinted searches
+constexpr float HINT_FRACTION = 0.9f;
+// The hinted bound on |v| keys of a column whose previous level was `hint` (> 0).
+__device__ __forceinline__ uint32_t hinted_bound(float hint) {
+  return max(1u, abs_key(HINT_FRACTION * hint));
+}
+
 // ------------------------------------------------------------ GEMM epilogues
 // Z = B V split-K partial tile: ws[unit][col][row], whole 128 x bn tile.
 struct EpiPartial {
   float *ws;
   int bn, m_tiles, n_tiles;  // m_tiles: 128-row blocks of C
   __device__ void setup() {}
+  __device__ void unit_begin(const Unit &, int, int) {}
   __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
     if (t.m0 >= m_tiles * BM) return;  // a 2-CTA tile's second half can lie past the last block
     const size_t slot = ((size_t)t.split * m_tiles + t.m0 / BM) * n_tiles + t.nt;
@@ -152,18 +160,57 @@ struct EpiPartial {
   }
 };
 
-// V = B^T Z raw output (constrained forms): out[col * ld + row].
+// V = B^T Z raw output (constrained forms): out[col * ld + row].  With a
+// candidate mask (cmask != null) it also does the selects' hinted gather: bit
+// r of column col's mask (ld / 32 words per column, like vmask) is set when
+// the column has a previous level hint[col] > 0 and |V[r, col]|'s key is at
+// least hinted_bound(hint).  Every launch rewrites every word of rows < ld, so
+// nothing needs clearing; the select kernels list the set bits instead of
+// streaming the column.
 struct EpiRaw {
   float *out;
   int ld, M, N, bn;
+  const float *hint = nullptr;
+  uint32_t *cmask = nullptr;
+  // per unit: lane L holds the bound of column col_base + 32 c + L in bl[c]
+  // (0xFFFFFFFF: the column has no level and lists nothing)
+  int col_base = 0;
+  uint32_t bl[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
   __device__ void setup() {}
-  __device__ void chunk(const Unit &t, int, int, int row, int col0, float (&r)[32]) {
-    const int gi = t.m0 + row;
-    if (gi >= M) return;
-    const int c0 = t.nt * bn + col0;
+  __device__ void unit_begin(const Unit &t, int lane, int cb) {
+    if (!cmask) return;
+    col_base = cb;
 #pragma unroll
-    for (int j = 0; j < 32; j++)
-      if (c0 + j < N) out[(size_t)(c0 + j) * ld + gi] = r[j];
+    for (int c = 0; c < 4; c++) {
+      const int col = t.nt * bn + cb + c * 32 + lane;
+      const float h = col < N ? __ldg(hint + col) : 0.f;
+      bl[c] = h > 0.f ? hinted_bound(h) : 0xFFFFFFFFu;
+    }
+  }
+  __device__ void chunk(const Unit &t, int q, int lane, int row, int col0, float (&r)[32]) {
+    if (t.m0 >= M) return;  // uniform: a 2-CTA tile's second half past the last row
+    const int gi = t.m0 + row;
+    const bool rv = gi < M;
+    const int c0 = t.nt * bn + col0;
+    if (rv) {
+#pragma unroll
+      for (int j = 0; j < 32; j++)
+        if (c0 + j < N) out[(size_t)(c0 + j) * ld + gi] = r[j];
+    }
+    if (!cmask) return;
+    // lane L: the rows of column c0 + L at or above its bound, as one mask word
+    const int cl = c0 + lane;
+    const int ci = ((col0 - col_base) >> 5) & 3;  // selects, not a local-memory index
+    const uint32_t bound = ci == 0 ? bl[0] : ci == 1 ? bl[1] : ci == 2 ? bl[2] : bl[3];
+    uint32_t mine = 0u;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const uint32_t bj = __shfl_sync(FULL, bound, j);
+      const uint32_t bal = __ballot_sync(FULL, rv && bj != 0xFFFFFFFFu && abs_key(r[j]) >= bj);
+      if (lane == j) mine = bal;
+    }
+    const int w = (t.m0 >> 5) + q;
+    if (cl < N && w < (ld >> 5)) cmask[(size_t)cl * (ld >> 5) + w] = mine;
   }
 };
 
@@ -192,6 +239,7 @@ struct EpiPenalty {
   uint32_t cap;             // ... above which Z = B V runs dense
   bool planes = false;      // this launch writes V_hi / V_lo (set by setup)
   __device__ void setup() { planes = V_hi != nullptr && *max_nnz > cap; }
+  __device__ void unit_begin(const Unit &, int, int) {}
   // r holds this thread's 32 values (row `row`, columns col0..col0+31) and is
   // overwritten with the objective terms.
   __device__ void chunk(const Unit &t, int q, int lane, int row, int col0, float (&r)[32]) {
@@ -892,11 +940,50 @@ __device__ void bitonic_desc(T *a, int len) {
   }
 }
 
+// The (|v| key << 32 | ~index) pairs of the entries whose bit is set in a
+// column's mask (words 32-bit words), the first `cap` of them in index order,
+// into out; returns how many bits are set.  Each thread owns a contiguous run
+// of words, so an exclusive scan of their counts places the entries in order.
+// scratch: one word of shared memory per warp of the block.
+__device__ uint32_t pairs_from_mask(const uint32_t *__restrict__ mk, int words,
+                                    const float *__restrict__ colg, uint64_t *out, uint32_t cap,
+                                    uint32_t *scratch) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int per = (words + blockDim.x - 1) / blockDim.x;
+  const int w0 = min(words, (int)threadIdx.x * per), w1 = min(words, w0 + per);
+  uint32_t cnt = 0;
+  for (int q = w0; q < w1; q++) cnt += __popc(mk[q]);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += t;
+  }
+  __syncthreads();  // scratch may still be read by the caller's previous use
+  if (lane == 31) scratch[w] = incl;
+  __syncthreads();
+  uint32_t off = incl - cnt, total = 0;
+  for (int i = 0; i < nw; i++) {
+    if (i < w) off += scratch[i];
+    total += scratch[i];
+  }
+  for (int q = w0; q < w1; q++) {
+    uint32_t bits = mk[q];
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const uint32_t i = (uint32_t)(q * 32 + b);
+      if (off < cap) out[off] = ((uint64_t)abs_key(__ldg(colg + i)) << 32) | (uint32_t)~i;
+      off++;
+    }
+  }
+  __syncthreads();
+  return total;
+}
+
 // ------------------------------------------------------------ L0 constraint
 constexpr int HARD_THREADS = 256;
 constexpr int HARD_CAND = 2048;  // hinted (key, index) candidates resolved in shared memory
-// fraction of the previous level used as the gather bound of the hinted searches
-constexpr float HINT_FRACTION = 0.9f;
 
 // One streaming pass over a column in global memory (16-byte loads, four in
 // flight per thread): the entries with |v| key >= bound go to cand as
@@ -980,7 +1067,7 @@ __device__ uint32_t gather_pairs_above(const float *__restrict__ colg, int n, ui
 __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
-    float *__restrict__ hints, const uint32_t *stop) {
+    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask) {
   if (*stop) return;
   __shared__ uint64_t cand[HARD_CAND];  // also 2 * HARD_CAND keys for (b)
   __shared__ uint32_t hist[2048];
@@ -995,10 +1082,22 @@ __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
   double ss = 0.0, cnt = 0.0;
   bool done = false;
   const float hint = hints[j];
-  uint32_t bound = max(1u, abs_key(HINT_FRACTION * hint));
+  uint32_t bound = hinted_bound(hint);
   for (int attempt = 0; attempt < 2 && hint > 0.f && !done; attempt++) {
-    const uint32_t c = gather_pairs_above(colg, n, bound, cand, HARD_CAND, &res[0]);
-    const uint32_t below = res[1];
+    uint32_t c = 0, below = 0;
+    bool listed = false;
+    if (attempt == 0 && cmask) {
+      // V = B^T Z's epilogue marked the entries at or above the same bound
+      // (it keeps no largest key below the bound: with fewer than s entries the
+      // column is gathered here as before)
+      c = pairs_from_mask(cmask + (size_t)j * (ldv >> 5), ldv >> 5, colg, cand, HARD_CAND,
+                          &res[0]);
+      listed = c >= s;
+    }
+    if (!listed) {
+      c = gather_pairs_above(colg, n, bound, cand, HARD_CAND, &res[0]);
+      below = res[1];
+    }
     if (c > (uint32_t)HARD_CAND) break;  // too many: the histogram path
     if (c < s) {
       // short by one: the s-th largest is the largest key below the bound, so
@@ -1293,7 +1392,7 @@ template <bool EXACT>
 __global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
-    float *__restrict__ hints, const uint32_t *stop) {
+    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask) {
   if (*stop) return;
   __shared__ uint64_t pairs[SOFT_C];  // hinted (key, index) candidates
   __shared__ float cand[SOFT_C];
@@ -1322,9 +1421,14 @@ __global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
   // ---- hinted path: gather (key, index) with |v| >= HINT_FRACTION * (previous level)
   const float hint = hints[j];
   if (hint > 0.f) {
-    const uint32_t c =
-        gather_pairs_above(colg, n, max(1u, abs_key(HINT_FRACTION * hint)), pairs, SOFT_C, res);
-    const uint32_t below_key = res[1];
+    uint32_t c, below_key = 0;
+    const bool listed = cmask != nullptr;
+    if (listed) {  // marked by V = B^T Z's epilogue, with the same bound
+      c = pairs_from_mask(cmask + (size_t)j * (ldv >> 5), ldv >> 5, colg, pairs, SOFT_C, res);
+    } else {
+      c = gather_pairs_above(colg, n, hinted_bound(hint), pairs, SOFT_C, res);
+      below_key = res[1];
+    }
     __syncthreads();
     if (c > 0 && c <= (uint32_t)SOFT_C) {
       int len = 1;
@@ -1335,12 +1439,16 @@ __global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
       for (uint32_t q = threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x)
         cand[q] = (q < c) ? __uint_as_float((uint32_t)(pairs[q] >> 32)) : -1.f;
       __syncthreads();
+      // A listed set comes without the largest value below it, so its last
+      // position (whose test needs that value) is left to the paths below;
+      // the others see their next value in the set.
+      const uint32_t E = (listed && c < (uint32_t)n) ? c - 1 : c;
       const double lo_after = (c == (uint32_t)n) ? 0.0 : (double)__uint_as_float(below_key);
       block_scan2(cand, (int)c, 0.0, 0.0, p1, p2, red);
       const double lim = __dsub_rn((double)cand[0], 0.000001);  // ||v||_inf - 1e-6
       uint32_t best = NONE;
       double bw = 0.0, w_last = 0.0;
-      eval_chunk<EXACT>(cand, p1, p2, c, c, 0, (uint32_t)n, 0.0, 0.0, lo_after, sq, sq2, lim,
+      eval_chunk<EXACT>(cand, p1, p2, c, E, 0, (uint32_t)n, 0.0, 0.0, lo_after, sq, sq2, lim,
                         best, bw, w_last);
       brk = resolve_stop(best, bw, res, misc, w_sh, &w);
       if (brk == NONE && c == (uint32_t)n) {
@@ -1526,7 +1634,9 @@ __global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
   } else {
     write_column_global(colg, n, vx, mk, soft);
   }
-  if (threadIdx.x == 0) nnz_out[j] = (uint32_t)cnt;
+  if (threadIdx.x == 0) {
+    nnz_out[j] = (uint32_t)cnt;
+  }
 }
 
 // ------------------------------------------------------------ finalize
@@ -2052,6 +2162,10 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   float *vhi = b.fp16_1 ? nullptr : b.V_hi;
   if (is_constrained(f)) {
     EpiRaw er{b.Vraw, M.ldn, M.n, b.k, b.bn2};
+    if (b.cmask) {  // the selects' hinted gather, done while V is in registers
+      er.hint = b.sel_hint;
+      er.cmask = b.cmask;
+    }
     e = gemm2(er);
   } else if (is_l1_penalized(f)) {
     EpiPenalty<true> pe{b.Vx,       b.obj_part, b.nnz_part, M.ldn,    M.n,
@@ -2071,17 +2185,17 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     if (!is_l1_constrained(f)) {
       hard_select_kernel<<<b.k, HARD_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint, b.Vx,
                                                         b.nnz, b.status, b.vmask, b.sel_hint,
-                                                        b.ctl);
+                                                        b.ctl, b.cmask);
       e = cudaGetLastError();
     } else {
       if (p.l1_mode == 0)
         soft_select_kernel<false><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
                                                                 b.Vx, b.nnz, b.status, b.vmask,
-                                                                b.sel_hint, b.ctl);
+                                                                b.sel_hint, b.ctl, b.cmask);
       else
         soft_select_kernel<true><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
                                                                b.Vx, b.nnz, b.status, b.vmask,
-                                                               b.sel_hint, b.ctl);
+                                                               b.sel_hint, b.ctl, b.cmask);
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;

@@ -364,6 +364,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
     bool ok = true;
     for (int u = pair; ok && u < shape.num_units; u += pairs) {
       const Unit t = decode_pair_unit(shape, u, rank);
+      // per-column data of this unit, one value per lane and 32 columns,
+      // loaded before the drain so that their latency hides behind it
+      ep.unit_begin(t, lane, half * HALF);
+      float cs[HALF / 32];
+#pragma unroll
+      for (int c = 0; c < HALF / 32; c++)
+        cs[c] = shape.col_scale ? __ldg(shape.col_scale +
+                                        min(t.nt * BN + half * HALF + c * 32 + lane, shape.N - 1))
+                                : 1.f;
+      const float rs =
+          shape.row_scale ? __ldg(shape.row_scale + min(t.m0 + row, shape.M - 1)) : 1.f;
       float sum[HALF];
 #pragma unroll
       for (int i = 0; i < HALF; i++) sum[i] = 0.f;
@@ -395,14 +406,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
       }
       if (!ok) break;
       if (shape.row_scale) {  // exact: powers of two
-        const float rs = __ldg(shape.row_scale + min(t.m0 + row, shape.M - 1));
 #pragma unroll
         for (int i = 0; i < HALF; i++) sum[i] *= rs;
       }
       if (shape.col_scale) {
 #pragma unroll
-        for (int i = 0; i < HALF; i++)
-          sum[i] *= __ldg(shape.col_scale + min(t.nt * BN + half * HALF + i, shape.N - 1));
+        for (int i = 0; i < HALF; i++) sum[i] *= __shfl_sync(0xffffffffu, cs[i >> 5], i & 31);
       }
 #pragma unroll
       for (int c = 0; c < HALF / 32; c++)

@@ -283,6 +283,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     bool ok = true;
     for (int u = blockIdx.x; ok && u < shape.num_units; u += gridDim.x) {
       const Unit t = decode_unit(shape, u);
+      ep.unit_begin(t, lane, half * HALF);
       float sum[HALF];
 #pragma unroll
       for (int i = 0; i < HALF; i++) sum[i] = 0.f;

@@ -390,9 +390,10 @@ def run_serving(args):
     return 0
 
 
-PRECISION_NOTE = ("FP32-accurate products, FP32 accumulate: V = B^T Z on split FP16 operands "
-                  "with power-of-two scales (h0 + h1 per operand, 22 significant bits; Z of the "
-                  "L1-variance forms an exact sign), Z = B V on 3xTF32 or an FP32 gather")
+PRECISION_NOTE = ("FP32-accurate products, FP32 accumulate: both products on split FP16 "
+                  "operands with power-of-two scales (h0 + h1 per operand, 22 significant "
+                  "bits; Z of the L1-variance forms an exact sign), Z = B V of sparse V as an "
+                  "FP32 gather")
 
 
 def gemm_scheme(f):
@@ -498,7 +499,8 @@ def run_ours(args):
                 pf[key] = pf.get(key, 0.0) + kms
     n_timed = max(1, min(args.steps, 5))
     formulation_ms = {str(f): {"step_ms": sum(d.values()) / n_timed,
-                               "kernels": sorted(k for k in d if "skipped" not in k)}
+                               "kernels": {k: v / n_timed for k, v in sorted(d.items())
+                                           if "skipped" not in k}}
                       for f, d in per_form.items()}
     totals = {k: sum(v) for k, v in per_kind.items()}
     roof_kinds = {k: t for k, t in totals.items() if k.startswith(("gemm", "select"))

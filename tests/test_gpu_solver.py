@@ -113,3 +113,37 @@ def test_device_wait_gives_up_and_handle_stays_usable(solver, po):
                                  maximumIterations=30, totalStartingPoints=32, batchSize=32)
     x, f, stats = solver.solve(B, st)
     assert np.isfinite(f) and stats.it > 0
+
+
+@pytest.mark.parametrize("formulation", [0, 3, 4, 7])
+@pytest.mark.parametrize("k", [64, 256])
+def test_run_ahead_loop_stops_where_a_host_loop_stops(solver, po, formulation, k):
+    """The solve's batch loop queues steps ahead of its convergence check (the
+    check runs on the device and gates the steps queued past it); it must stop
+    at the same step as a loop that checks the largest change after every step
+    on the host, with the same best objective."""
+    am = _am()
+    m, n = 300, 2500
+    B = po.low_rank_data(m, n, 8, 30, seed=21 + formulation, dtype=np.float32)
+    V = po.uniform_starts(n, k, seed=22, dtype=np.float32)
+    g = {4: 0.05, 5: 4.0, 6: 0.02, 7: 1.0}.get(formulation, 0.0)
+    tol = 1e-5
+    st = am.OptimizationSettings(formulation=formulation, constraintParameter=10,
+                                 penaltyParameter=g, tolerance=tol, maximumIterations=80,
+                                 totalStartingPoints=k, batchSize=k, startMode=am.START_INJECTED)
+    M = solver.matrix(B)
+    b = M.batch(st, k)
+    b.load(V)
+    steps = 0
+    for it in range(80):
+        me = b.iterate(it, 1)
+        steps += 1
+        if it > 0 and me < tol:
+            break
+    _, val, _, _ = b.read()
+    b.close()
+    x, f, stats = M.solve(st, start_points=V)
+    M.close()
+    assert int(stats.it) == steps
+    assert int(stats.start_iterations) == steps * k
+    assert f == np.nanmax(val)
