@@ -41,17 +41,24 @@ def test_step_with_feature_scales_far_apart(solver, po, formulation, spread):
     check_step(solver, po, B.astype(np.float32), k, formulation)
 
 
-@pytest.mark.parametrize("scheme", ["tf32_bf16", "tf32"])
+@pytest.mark.parametrize("scheme", ["tf32_bf16", "tf32", "one_cta", "select_gather"])
 @pytest.mark.parametrize("shape", [(1000, 5000, 256), (129, 4097, 257)],
                          ids=lambda s: "x".join(map(str, s)))
 @pytest.mark.parametrize("formulation", range(8))
 def test_step_matches_oracle_other_pair_schemes(solver, po, shape, formulation, scheme,
                                                 monkeypatch):
-    """The CTA-pair V = B^T Z without the FP16 operands: 3xTF32 for every
-    formulation, or with exact BF16 operands for the L1-variance forms."""
-    monkeypatch.setenv("AM24_GEMM_FP16", "0")
+    """The switches of a wide batch: the CTA-pair products without the FP16
+    operands (3xTF32 for every formulation, or with exact BF16 operands for the
+    L1-variance forms), every product on one-CTA tiles, and the selects doing
+    their own hinted gather instead of reading V = B^T Z's candidate marks."""
+    if scheme in ("tf32_bf16", "tf32"):
+        monkeypatch.setenv("AM24_GEMM_FP16", "0")
     if scheme == "tf32":
         monkeypatch.setenv("AM24_GEMM_BF16", "0")
+    if scheme == "one_cta":
+        monkeypatch.setenv("AM24_GEMM_PAIR", "0")
+    if scheme == "select_gather":
+        monkeypatch.setenv("AM24_SELECT_LIST", "0")
     m, n, k = shape
     check_step(solver, po, po.low_rank_data(m, n, 8, 30, seed=m + n, dtype=np.float32), k,
                formulation)
@@ -140,14 +147,21 @@ def test_step_is_deterministic(solver, po):
             assert np.array_equal(x, y, equal_nan=True)
 
 
+@pytest.mark.parametrize("k,marks", [(96, True), (256, True), (256, False)],
+                         ids=["k96", "k256", "k256-select-gather"])
 @pytest.mark.parametrize("formulation", range(8))
-def test_steps_through_sparse_gather_match_oracle(solver, po, formulation):
+def test_steps_through_sparse_gather_match_oracle(solver, po, formulation, k, marks,
+                                                  monkeypatch):
     """Three steps: after the first, V is sparse and Z = B V runs as the gather
-    kernel (every column at most min(4096, n/32) non-zeros); the loadings stay
-    with the oracle's."""
+    kernel (every column at most min(4096, n/32) non-zeros); from the second the
+    selects start from the previous level, reading the candidates V = B^T Z's
+    epilogue marked (or, with marks off, gathering them themselves).  The
+    loadings stay with the oracle's."""
     import importlib
     am = importlib.import_module("24am_b200")
-    m, n, k = 300, 4096, 96
+    if not marks:
+        monkeypatch.setenv("AM24_SELECT_LIST", "0")
+    m, n = 300, 4096
     B = po.low_rank_data(m, n, 8, 30, seed=77, dtype=np.float32)
     B64 = B.astype(np.float64)
     V0 = po.uniform_starts(n, k, seed=78, dtype=np.float32)
