@@ -98,6 +98,8 @@ _SIGS = {
     "am24_matrix_create_f32": (C.c_int, [_VP, _VP, C.c_int32, C.c_uint32, C.c_uint32, C.c_int32,
                                          C.POINTER(_VP)]),
     "am24_matrix_destroy": (C.c_int, [_VP, _VP]),
+    "am24_matrix_deflate": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
+    "am24_matrix_read_f32": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
     "am24_solve_resident_f32": (C.c_int, [_VP, _VP, _VP, C.POINTER(am24_settings),
                                           C.POINTER(am24_statistics), _VP, C.POINTER(C.c_float)]),
     "am24_batch_create": (C.c_int, [_VP, _VP, C.POINTER(am24_settings), C.c_uint32,
@@ -397,6 +399,34 @@ class Matrix:
 
     def batch(self, settings, batch_size):
         return Batch(self, settings, batch_size)
+
+    def deflate(self, x):
+        """B <- B (I - x x^T) on the device (am24_matrix_deflate): the update the
+        reference's multi-component driver applies between solves."""
+        x = np.ascontiguousarray(x, np.float32)
+        assert x.shape == (self.n,)
+        check(lib().am24_matrix_deflate(self.solver.h, self.mh, _ptr(x), 0))
+
+    def read(self):
+        """The current B (m x n, column-major float32)."""
+        B = np.zeros((self.m, self.n), np.float32, order="F")
+        check(lib().am24_matrix_read_f32(self.solver.h, self.mh, _ptr(B), self.m))
+        return B
+
+    def components(self, settings, count, start_points=None):
+        """`count` sparse components one after another, deflating B by each
+        (c++/matlab/run_example.m:29-34).  Returns X (n x count), the objectives
+        and the statistics of each solve.  B is left deflated by all of them."""
+        X = np.zeros((self.n, count), np.float32, order="F")
+        fvals, stats = [], []
+        for i in range(count):
+            x, f, st = self.solve(settings, start_points=start_points)
+            X[:, i] = x
+            fvals.append(f)
+            stats.append(st)
+            if i + 1 < count:
+                self.deflate(x)
+        return X, fvals, stats
 
 
 class Batch:

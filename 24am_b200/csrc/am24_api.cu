@@ -672,6 +672,45 @@ am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, u
   return create_matrix(h, B, ldB, m, n, on_device, false, out);
 }
 
+am24_status am24_matrix_deflate(am24_handle h, am24_matrix mat, const float *x,
+                                int32_t on_device) {
+  if (!h || !mat || !x) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  AM24_CUDA(cudaSetDevice(h->device));
+  MatrixDev &M = mat->d;
+  Allocs local(h->stream);
+  float *xd = nullptr;
+  double *partial = nullptr, *y = nullptr;
+  AM24_TRY(local.get(&xd, (size_t)M.n));
+  AM24_TRY(local.get(&partial, ev_partial_len(M)));
+  AM24_TRY(local.get(&y, (size_t)M.m));
+  AM24_CUDA(cudaMemcpyAsync(xd, x, sizeof(float) * M.n,
+                            on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            h->stream));
+  AM24_CUDA(launch_deflate(M, xd, partial, y, h->stream));
+  // every layout made so far is rebuilt from the new B, in place
+  if (M.Bc_h2) AM24_CUDA(launch_prep_fp16x2(M, h->stream));
+  if (M.Bt_h2) {
+    uint32_t *key = nullptr;
+    AM24_TRY(local.get(&key, (size_t)M.m));
+    AM24_CUDA(launch_prep_bt_fp16x2(M, key, h->stream));
+  }
+  if (M.Bc_hi) AM24_CUDA(launch_prep_tf32_planes(M, h->stream));
+  if (M.Bc_b3) AM24_CUDA(launch_prep_bf16x3(M, h->stream));
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  return AM24_OK;
+}
+
+am24_status am24_matrix_read_f32(am24_handle h, am24_matrix mat, float *B, int32_t ldB) {
+  if (!h || !mat || !B) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  const MatrixDev &M = mat->d;
+  if (ldB < M.m) return fail(AM24_ERR_INVALID_ARG, "ldB must be >= m");
+  AM24_CUDA(cudaSetDevice(h->device));
+  AM24_CUDA(cudaMemcpy2DAsync(B, sizeof(float) * (size_t)ldB, M.Bc, sizeof(float) * M.ldm,
+                              sizeof(float) * M.m, M.n, cudaMemcpyDeviceToHost, h->stream));
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  return AM24_OK;
+}
+
 am24_status am24_matrix_destroy(am24_handle h, am24_matrix mat) {
   if (!mat) return AM24_OK;
   if (h) {

@@ -173,6 +173,10 @@ cudaError_t launch_finalize_x(const float *v, int n, float *x, cudaStream_t st);
 // timeout code in *status.
 cudaError_t launch_bounded_wait_probe(unsigned long long timeout_ns, int *status,
                                       cudaStream_t st);
+// B <- B (I - x x^T) on M.Bc (device x; partial: ev_partial_len(M) doubles of
+// scratch, y: m doubles).  The other layouts are not touched.
+cudaError_t launch_deflate(MatrixDev &M, const float *x, double *partial, double *y,
+                           cudaStream_t st);
 // ||B x||^2 in FP64 into *out; partial: ev_partial_len(M) doubles of scratch.
 cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double *partial,
                                       double *out, cudaStream_t st);

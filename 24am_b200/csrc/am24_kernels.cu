@@ -1779,6 +1779,28 @@ __global__ void ev_sum_kernel(const double *__restrict__ partial, int chunks, in
   if (threadIdx.x == 0) *out = acc;
 }
 
+// y_i = the sum of its chunks' partials (in chunk order), FP64.
+__global__ void rowsum_kernel(const double *__restrict__ partial, int chunks, int m,
+                              double *__restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double acc = 0.0;
+  for (int c = 0; c < chunks; c++) acc += partial[(size_t)c * m + i];
+  y[i] = acc;
+}
+
+// Deflation B <- B (I - x x^T) = B - y x^T with y = B x: every entry in FP64,
+// rounded to FP32 once.  One block per feature, threads over samples.
+__global__ void deflate_kernel(float *__restrict__ Bc, int ldm, int m,
+                               const double *__restrict__ y, const float *__restrict__ x) {
+  const size_t c = blockIdx.x;
+  const double xc = (double)x[c];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const size_t o = c * ldm + i;
+    Bc[o] = (float)((double)Bc[o] - y[i] * xc);
+  }
+}
+
 // ------------------------------------------------------------ GEMM launch
 struct GemmCfg {
   int bn, stages;
@@ -2019,6 +2041,19 @@ cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   ev_sum_kernel<<<1, 1024, 0, st>>>(partial, chunks, M.m, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_deflate(MatrixDev &M, const float *x, double *partial, double *y,
+                           cudaStream_t st) {
+  const int chunks = (M.n + EV_CHUNK - 1) / EV_CHUNK;
+  ev_partial_kernel<<<dim3((M.m + 255) / 256, chunks), 256, 0, st>>>(M.Bc, M.ldm, M.m, M.n, x,
+                                                                     partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  rowsum_kernel<<<(M.m + 255) / 256, 256, 0, st>>>(partial, chunks, M.m, y);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  deflate_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, y, x);
   return cudaGetLastError();
 }
 

@@ -185,6 +185,20 @@ am24_status am24_matrix_destroy(am24_handle h, am24_matrix mat);
 am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
                                     am24_settings *settings, am24_statistics *stats,
                                     const float *start_points, float *fval_out);
+/* Deflation for the next component: B <- B (I - x x^T) on the device, the
+ * update the reference's multi-component driver applies between solves
+ * (c++/matlab/run_example.m:33-34, in double).  Here y = B x is summed in
+ * FP64 and each entry becomes (float)(b - y_i x_c) in FP64.  x (n floats, host
+ * or device when on_device != 0) is normally the last solve's unit loading.
+ * Every layout the matrix holds is rebuilt in place, so batches created on it
+ * stay valid; work already queued on the handle's stream sees the old B, work
+ * queued after it the new one, and work on other handles must not use the
+ * matrix meanwhile. */
+am24_status am24_matrix_deflate(am24_handle h, am24_matrix mat, const float *x,
+                                int32_t on_device);
+/* Copies the matrix's current B (m x n, column-major, leading dimension ldB >=
+ * m) to host memory: the data as uploaded, or as deflated. */
+am24_status am24_matrix_read_f32(am24_handle h, am24_matrix mat, float *B, int32_t ldB);
 
 /* ---- batch stepping (one AM iteration at a time) -------------------------- */
 /* A batch of batch_size starting points on a resident matrix.  `settings` must
