@@ -99,6 +99,8 @@ _SIGS = {
                                          C.POINTER(_VP)]),
     "am24_matrix_destroy": (C.c_int, [_VP, _VP]),
     "am24_matrix_deflate": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
+    "am24_matrix_create_csc_f32": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.c_uint32, _VP,
+                                             _VP, _VP]),
     "am24_matrix_read_f32": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
     "am24_solve_resident_f32": (C.c_int, [_VP, _VP, _VP, C.POINTER(am24_settings),
                                           C.POINTER(am24_statistics), _VP, C.POINTER(C.c_float)]),
@@ -371,6 +373,34 @@ class Matrix:
         self.mh = mh
         self._batches = weakref.WeakSet()
         solver._matrices.add(self)
+
+    @classmethod
+    def from_csc(cls, solver, vals, row_ind, col_ptr, m, n, means=None, row_means=None):
+        """A resident matrix from compressed sparse columns
+        (am24_matrix_create_csc_f32), with the sparse solver's optional implicit
+        centring: the matrix solved is B - 1 means^T - row_means 1^T.  Also takes
+        a scipy.sparse matrix as `vals` (then row_ind / col_ptr / m / n may be None)."""
+        if hasattr(vals, "tocsc"):
+            S = vals.tocsc(copy=True)
+            S.sum_duplicates()  # canonical: one entry per (row, column), rows sorted
+            m, n = S.shape
+            vals, row_ind, col_ptr = S.data, S.indices, S.indptr
+        vals = np.ascontiguousarray(vals, np.float32)
+        row_ind = np.ascontiguousarray(row_ind, np.int32)
+        col_ptr = np.ascontiguousarray(col_ptr, np.int32)
+        mu = None if means is None else np.ascontiguousarray(means, np.float32)
+        rmu = None if row_means is None else np.ascontiguousarray(row_means, np.float32)
+        self = cls.__new__(cls)
+        self.solver = solver
+        mh = C.c_void_p()
+        check(lib().am24_matrix_create_csc_f32(solver.h, _ptr(vals), _ptr(row_ind),
+                                                _ptr(col_ptr), int(m), int(n), _ptr(mu),
+                                                _ptr(rmu), C.byref(mh)))
+        self.m, self.n = int(m), int(n)
+        self.mh = mh
+        self._batches = weakref.WeakSet()
+        solver._matrices.add(self)
+        return self
 
     def close(self):
         """Destroys the matrix, after any batch still open on it."""

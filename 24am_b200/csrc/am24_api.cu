@@ -672,6 +672,68 @@ am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, u
   return create_matrix(h, B, ldB, m, n, on_device, false, out);
 }
 
+am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const int32_t *row_ind,
+                                       const int32_t *col_ptr, uint32_t m, uint32_t n,
+                                       const float *means, const float *row_means,
+                                       am24_matrix *out) {
+  if (!h || !col_ptr || !out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  if (m == 0 || n == 0) return fail(AM24_ERR_INVALID_ARG, "m and n must be positive");
+  if (m > (1u << 30) || n > (1u << 30)) return fail(AM24_ERR_INVALID_ARG, "matrix too large");
+  // the arrays are checked here, before any device write can use an index
+  if (col_ptr[0] != 0) return fail(AM24_ERR_INVALID_ARG, "col_ptr[0] must be 0");
+  for (uint32_t c = 0; c < n; c++)
+    if (col_ptr[c + 1] < col_ptr[c])
+      return fail(AM24_ERR_INVALID_ARG, "col_ptr must be non-decreasing");
+  const size_t nnz = (size_t)col_ptr[n];
+  if (nnz > 0 && (!vals || !row_ind)) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  for (size_t q = 0; q < nnz; q++)
+    if (row_ind[q] < 0 || (uint32_t)row_ind[q] >= m)
+      return fail(AM24_ERR_INVALID_ARG, "row index out of range at entry " + std::to_string(q));
+  AM24_CUDA(cudaSetDevice(h->device));
+  auto *mat = new am24_matrix_s();
+  MatrixDev &M = mat->d;
+  M.m = (int)m;
+  M.n = (int)n;
+  M.ldm = round_up((int)m, 32);
+  M.ldn = round_up((int)n, 32);
+  am24_status st = mat->mem.get(&M.Bc, (size_t)n * M.ldm);
+  if (st != AM24_OK) {
+    delete mat;
+    return st;
+  }
+  Allocs local(h->stream);
+  float *dv = nullptr, *dmean = nullptr, *drmean = nullptr;
+  int32_t *dri = nullptr, *dcp = nullptr;
+  cudaError_t e = cudaSuccess;
+  if ((st = local.get(&dcp, (size_t)n + 1)) || (nnz && (st = local.get(&dv, nnz))) ||
+      (nnz && (st = local.get(&dri, nnz))) || (means && (st = local.get(&dmean, (size_t)n))) ||
+      (row_means && (st = local.get(&drmean, (size_t)m)))) {
+    delete mat;
+    return st;
+  }
+  e = cudaMemsetAsync(M.Bc, 0, sizeof(float) * (size_t)n * M.ldm, h->stream);
+  if (!e) e = cudaMemcpyAsync(dcp, col_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice,
+                              h->stream);
+  if (!e && nnz)
+    e = cudaMemcpyAsync(dv, vals, sizeof(float) * nnz, cudaMemcpyHostToDevice, h->stream);
+  if (!e && nnz)
+    e = cudaMemcpyAsync(dri, row_ind, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, h->stream);
+  if (!e && means)
+    e = cudaMemcpyAsync(dmean, means, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream);
+  if (!e && row_means)
+    e = cudaMemcpyAsync(drmean, row_means, sizeof(float) * m, cudaMemcpyHostToDevice, h->stream);
+  if (!e) e = launch_csc_to_dense(M, dv, dri, dcp, dmean, drmean, h->stream);
+  if (!e) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    delete mat;
+    return fail(e == cudaErrorMemoryAllocation ? AM24_ERR_OOM : AM24_ERR_CUDA,
+                std::string("sparse matrix upload: ") + cudaGetErrorString(e));
+  }
+  *out = mat;
+  return AM24_OK;
+}
+
 am24_status am24_matrix_deflate(am24_handle h, am24_matrix mat, const float *x,
                                 int32_t on_device) {
   if (!h || !mat || !x) return fail(AM24_ERR_INVALID_ARG, "NULL argument");

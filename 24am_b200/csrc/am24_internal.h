@@ -173,6 +173,11 @@ cudaError_t launch_finalize_x(const float *v, int n, float *x, cudaStream_t st);
 // timeout code in *status.
 cudaError_t launch_bounded_wait_probe(unsigned long long timeout_ns, int *status,
                                       cudaStream_t st);
+// M.Bc (zeroed) from device CSC arrays, then the optional centring
+// (means: n floats, row_means: m floats, either may be null).
+cudaError_t launch_csc_to_dense(MatrixDev &M, const float *vals, const int32_t *row_ind,
+                               const int32_t *col_ptr, const float *means,
+                               const float *row_means, cudaStream_t st);
 // B <- B (I - x x^T) on M.Bc (device x; partial: ev_partial_len(M) doubles of
 // scratch, y: m doubles).  The other layouts are not touched.
 cudaError_t launch_deflate(MatrixDev &M, const float *x, double *partial, double *y,

@@ -1779,6 +1779,32 @@ __global__ void ev_sum_kernel(const double *__restrict__ partial, int chunks, in
   if (threadIdx.x == 0) *out = acc;
 }
 
+// Compressed sparse columns into B's dense layout (zeroed before): one block
+// per column.
+__global__ void csc_scatter_kernel(const float *__restrict__ vals,
+                                   const int32_t *__restrict__ row_ind,
+                                   const int32_t *__restrict__ col_ptr, float *__restrict__ Bc,
+                                   int ldm) {
+  const size_t c = blockIdx.x;
+  for (int q = col_ptr[c] + threadIdx.x; q < col_ptr[c + 1]; q += blockDim.x)
+    Bc[c * ldm + row_ind[q]] = vals[q];
+}
+
+// The sparse solver's implicit centring made explicit:
+// b <- (b - means[c]) - row_means[i] in FP32, either correction optional.
+__global__ void center_kernel(float *__restrict__ Bc, int ldm, int m,
+                              const float *__restrict__ means,
+                              const float *__restrict__ row_means) {
+  const size_t c = blockIdx.x;
+  const float mc = means ? means[c] : 0.f;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    float b = Bc[c * ldm + i];
+    if (means) b = b - mc;
+    if (row_means) b = b - row_means[i];
+    Bc[c * ldm + i] = b;
+  }
+}
+
 // y_i = the sum of its chunks' partials (in chunk order), FP64.
 __global__ void rowsum_kernel(const double *__restrict__ partial, int chunks, int m,
                               double *__restrict__ y) {
@@ -2041,6 +2067,16 @@ cudaError_t launch_explained_variance(const MatrixDev &M, const float *x, double
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   ev_sum_kernel<<<1, 1024, 0, st>>>(partial, chunks, M.m, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_csc_to_dense(MatrixDev &M, const float *vals, const int32_t *row_ind,
+                               const int32_t *col_ptr, const float *means,
+                               const float *row_means, cudaStream_t st) {
+  csc_scatter_kernel<<<M.n, 256, 0, st>>>(vals, row_ind, col_ptr, M.Bc, M.ldm);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || (!means && !row_means)) return e;
+  center_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, means, row_means);
   return cudaGetLastError();
 }
 

@@ -57,8 +57,10 @@ typedef enum {
 } am24_formulation;
 
 /* Arithmetic of the two products (an extension: the reference computes in F).
- * FP32: FP32-accurate products every iteration (3xTF32, or an exact BF16 split
- * where the operand allows).  MIXED: single-pass BF16 operands with FP32
+ * FP32: FP32-accurate products every iteration (split FP16 operands with
+ * power-of-two scales on batches of more than 128 starts, 3xTF32 on narrower
+ * ones; the residual of each split is below 2^-22 of the value, or 2^-39 of its
+ * row's largest).  MIXED: single-pass BF16 operands with FP32
  * accumulation while the supports settle, then the FP32-accurate products from
  * the first iteration after which a share stable_share of the batch's starts
  * has kept the same support for stable_iterations iterations; the tolerance
@@ -181,6 +183,21 @@ am24_status am24_solve_dense_f64(am24_handle h, const double *B, int32_t ldB, do
  * keeps it until am24_matrix_destroy. */
 am24_status am24_matrix_create_f32(am24_handle h, const float *B, int32_t ldB, uint32_t m,
                                    uint32_t n, int32_t on_device, am24_matrix *out);
+/* A resident matrix from compressed sparse columns, the input of the
+ * reference's sparse solver (sparse_PCA_solver_CSC, c++/src/gpower/
+ * sparse_PCA_solver_for_CSC.h:111-117): vals and row_ind (col_ptr[n] entries,
+ * 0-based rows, at most one entry per row within a column) and col_ptr (n + 1,
+ * col_ptr[0] = 0), host arrays.  means (n floats) and row_means (m floats) are
+ * optional (NULL: no correction) and stand for its doMean / doRowMean: the
+ * matrix solved is B - 1 means^T - row_means 1^T.  Here it is densified on the
+ * device with the corrections applied to every entry ((b - means_c) -
+ * row_means_i in FP32), after which every solve runs on the dense tensor-core
+ * path.  Malformed CSC arrays are rejected on the host before anything is
+ * copied.  The dense matrix must fit in device memory (AM24_ERR_OOM). */
+am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const int32_t *row_ind,
+                                       const int32_t *col_ptr, uint32_t m, uint32_t n,
+                                       const float *means, const float *row_means,
+                                       am24_matrix *out);
 am24_status am24_matrix_destroy(am24_handle h, am24_matrix mat);
 am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
                                     am24_settings *settings, am24_statistics *stats,
