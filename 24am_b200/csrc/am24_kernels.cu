@@ -1389,7 +1389,7 @@ __device__ uint32_t resolve_stop(uint32_t best, double bw, uint32_t *res,
 // ||.||_1/||.||_2 >= sqrt(s) and take the root inside it -- the exact
 // L1-ball / unit-sphere projection.
 template <bool EXACT>
-__global__ void __launch_bounds__(SOFT_THREADS, 2) soft_select_kernel(
+__global__ void __launch_bounds__(SOFT_THREADS, 4) soft_select_kernel(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
     float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask) {
