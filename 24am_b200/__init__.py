@@ -134,7 +134,7 @@ _SIGS = {
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
 }
 KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV", "densify",
-                "gemm_BtZ_bf16", "support"]
+                "gemm_BtZ_bf16", "support", "gather_BV_group"]
 
 _lib = None
 

@@ -957,7 +957,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   }
   // a gather over V's non-zeros beats the dense product while they are few
   d.sparse_cap = (uint32_t)std::min(4096, M.n / 32);
-  b->launches = (is_constrained(settings->formulation) ? 7 : 6) + (d.mixed ? 2 : 0);
+  b->launches = (is_constrained(settings->formulation) ? 8 : 7) + (d.mixed ? 2 : 0);
   *out = b;
   return AM24_OK;
 }
@@ -1072,10 +1072,13 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
   // mark the kernels that a gate turned into no-ops: the Z = B V path the
   // step does not take, and (MIXED) the V = B^T Z of the other phase
   const bool sparse = gate <= b->d.sparse_cap;
+  const bool grouped = sparse && gate <= std::min(b->d.sparse_cap, GATHER_GROUP_MAX_NNZ);
   for (int i = 0; i < nl; i++) {
     bool skipped = sparse ? (kk[i] == AM24_KERNEL_GEMM_BV || kk[i] == AM24_KERNEL_Z_REDUCE ||
-                             kk[i] == AM24_KERNEL_DENSIFY)
-                          : (kk[i] == AM24_KERNEL_GATHER_BV ||
+                             kk[i] == AM24_KERNEL_DENSIFY ||
+                             kk[i] == (grouped ? AM24_KERNEL_GATHER_BV
+                                               : AM24_KERNEL_GATHER_BV_GROUP))
+                          : (kk[i] == AM24_KERNEL_GATHER_BV || kk[i] == AM24_KERNEL_GATHER_BV_GROUP ||
                              (kk[i] == AM24_KERNEL_DENSIFY && planes > b->d.sparse_cap));
     if (b->d.mixed)
       skipped = skipped || (phase == 0 ? kk[i] == AM24_KERNEL_GEMM_BTZ

@@ -122,6 +122,10 @@ struct StepParams {
   int stop_check = 0;  // the step sets the stop word when the batch loop would end
 };
 
+// The sparse Z = B V runs four starts per block while no column has more
+// than this many non-zeros (and the sparse bound allows the gather at all).
+constexpr uint32_t GATHER_GROUP_MAX_NNZ = 1024;
+
 // Run-ahead control words of a batch (BatchDev::ctl).  Every step kernel
 // returns at once while ctl[CTL_STOP] is set, so a driver can queue steps
 // ahead of the convergence test; a load clears the words.

@@ -623,7 +623,8 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
   __shared__ float val[GATHER_CAP];
   __shared__ uint32_t wsum[GATHER_THREADS / 32];
   __shared__ double red[32];
-  if (*stop || *gate > gate_max) return;  // dense V: gemm1 + z_reduce handle this step
+  // dense V (gemm1 + z_reduce), or few enough non-zeros for gather_bv_group_kernel
+  if (*stop || *gate > gate_max || *gate <= min(gate_max, GATHER_GROUP_MAX_NNZ)) return;
   const int j = blockIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int words = ldn >> 5;
@@ -767,6 +768,222 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
     if (zh0 && threadIdx.x == 0) zscale[j] = pow2f(-s);
   }
   if (MODE != 2 && threadIdx.x == 0) fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
+}
+
+// The sparse Z = B V for GATHER_GROUP starts per block, while every column
+// has at most GATHER_CAP / GATHER_GROUP non-zeros (*gate): the block lists the
+// union of the group's non-zero rows in index order, loads each row once, and
+// adds it to the sums of the starts it belongs to.  Every start's FMAs still
+// run over its own non-zeros in index order, so the result is bit for bit that
+// of gather_bv_kernel, with a quarter of the row loads where supports overlap.
+// Above the group bound this kernel returns at once and gather_bv_kernel runs.
+constexpr int GATHER_GROUP = 4;
+static_assert(GATHER_GROUP_MAX_NNZ == GATHER_CAP / GATHER_GROUP, "group bound");
+constexpr size_t GATHER_GROUP_SMEM =
+    (size_t)GATHER_CAP * (sizeof(int) + GATHER_GROUP * sizeof(float) + 1);
+
+template <int MODE>
+__global__ void __launch_bounds__(GATHER_THREADS) gather_bv_group_kernel(
+    const float *__restrict__ Bc, int ldm, int m, int ldn, int k,
+    const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
+    float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
+    uint16_t *__restrict__ Zb, uint16_t *__restrict__ Zh, size_t zplane,
+    float *__restrict__ zscale, const uint32_t *stop) {
+  constexpr int G = GATHER_GROUP;
+  extern __shared__ __align__(16) uint8_t gsm[];
+  int *idx = reinterpret_cast<int *>(gsm);                                  // GATHER_CAP
+  float *val = reinterpret_cast<float *>(gsm + sizeof(int) * GATHER_CAP);   // G x GATHER_CAP
+  uint8_t *memb = gsm + (sizeof(int) + G * sizeof(float)) * GATHER_CAP;     // GATHER_CAP
+  __shared__ uint32_t wsum[GATHER_THREADS / 32];
+  __shared__ double red[32];
+  // dense V (gemm1 + z_reduce), or gather_bv_kernel's case
+  if (*stop || *gate > min(gate_max, GATHER_GROUP_MAX_NNZ)) return;
+  const int j0 = blockIdx.x * G;
+  const int ng = min(G, k - j0);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int words = ldn >> 5;
+  const uint32_t *mk[G];
+  const float *vx[G];
+#pragma unroll
+  for (int g = 0; g < G; g++) {
+    const int j = j0 + min(g, ng - 1);  // past the last start: a repeat, never a member
+    mk[g] = vmask + (size_t)j * words;
+    vx[g] = Vx + (size_t)j * ldn;
+  }
+  auto word = [&](int g, int q) { return g < ng ? mk[g][q] : 0u; };
+  // the union's rows in index order: an exclusive scan over threads' word runs
+  const int per = (words + GATHER_THREADS - 1) / GATHER_THREADS;
+  const int w0 = min(words, threadIdx.x * per), w1 = min(words, w0 + per);
+  uint32_t cnt = 0;
+  for (int q = w0; q < w1; q++) {
+    uint32_t u = 0;
+#pragma unroll
+    for (int g = 0; g < G; g++) u |= word(g, q);
+    cnt += __popc(u);
+  }
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  uint32_t off = incl - cnt;
+  for (int i = 0; i < w; i++) off += wsum[i];
+  uint32_t total = 0;
+  for (int i = 0; i < GATHER_THREADS / 32; i++) total += wsum[i];
+  if (total > (uint32_t)GATHER_CAP) total = GATHER_CAP;  // cannot happen below the gate
+  for (int q = w0; q < w1; q++) {
+    uint32_t wg[G], u = 0;
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      wg[g] = word(g, q);
+      u |= wg[g];
+    }
+    while (u) {
+      const int b = __ffs(u) - 1;
+      u &= u - 1;
+      const int r = q * 32 + b;
+      if (off < (uint32_t)GATHER_CAP) {
+        idx[off] = r;
+        uint32_t mb = 0;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          const bool in = (wg[g] >> b) & 1u;
+          mb |= (uint32_t)in << g;
+          val[g * GATHER_CAP + off] = in ? vx[g][r] : 0.f;
+        }
+        memb[off] = (uint8_t)mb;
+      }
+      off++;
+    }
+  }
+  __syncthreads();
+  constexpr int G4 = GATHER_ROWS / 4;
+  double acc[G];
+  float4 y[G][G4];
+  const int chunk = GATHER_THREADS * GATHER_ROWS;
+  const int ld4 = ldm >> 2;
+  const bool one_pass = m <= chunk;
+  auto sample = [&](int base, int r) { return base + 4 * (r * GATHER_THREADS + (int)threadIdx.x); };
+  auto fma4 = [](float v, const float4 &b, float4 &acc4) {
+    acc4.x = fmaf(v, b.x, acc4.x);
+    acc4.y = fmaf(v, b.y, acc4.y);
+    acc4.z = fmaf(v, b.z, acc4.z);
+    acc4.w = fmaf(v, b.w, acc4.w);
+  };
+#pragma unroll
+  for (int g = 0; g < G; g++) acc[g] = 0.0;
+  // sample i of start g, as gather_bv_kernel's emit stores it
+  auto emit = [&](int g, int i, float yv) {
+    const size_t o = (size_t)(j0 + g) * ldm + i;
+    if (MODE == 1) {
+      acc[g] += (double)fabsf(yv);
+      Z_hi[o] = sgnf(yv);
+      Z_lo[o] = 0.f;
+      if (Zb) Zb[o] = bf16_sign(yv);
+      if (Zh) Zh[o] = f16_sign(yv);
+    } else {
+      acc[g] += (double)yv * (double)yv;
+      if (!(MODE == 2 && one_pass)) split_store(yv, Z_hi + o, Z_lo + o);
+      if (MODE == 0 && Zb) Zb[o] = bf16_bits(yv);
+    }
+  };
+  for (int base = 0; base < m; base += chunk) {
+    int i4[G4];
+    bool ok[G4];
+#pragma unroll
+    for (int r = 0; r < G4; r++) {
+      i4[r] = sample(base, r) >> 2;
+      ok[r] = i4[r] < ld4;
+#pragma unroll
+      for (int g = 0; g < G; g++) y[g][r] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    uint32_t q = 0;
+    for (; q + 4 <= total; q += 4) {
+      float4 bq[4][G4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const float4 *row4 = reinterpret_cast<const float4 *>(Bc + (size_t)idx[q + u] * ldm);
+#pragma unroll
+        for (int r = 0; r < G4; r++)
+          bq[u][r] = ok[r] ? __ldg(row4 + i4[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t mb = memb[q + u];
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          if (!((mb >> g) & 1u)) continue;
+          const float v = val[g * GATHER_CAP + q + u];
+#pragma unroll
+          for (int r = 0; r < G4; r++) fma4(v, bq[u][r], y[g][r]);
+        }
+      }
+    }
+    for (; q < total; q++) {
+      const float4 *row4 = reinterpret_cast<const float4 *>(Bc + (size_t)idx[q] * ldm);
+      const uint32_t mb = memb[q];
+      float4 b[G4];
+#pragma unroll
+      for (int r = 0; r < G4; r++) b[r] = ok[r] ? __ldg(row4 + i4[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int g = 0; g < G; g++) {
+        if (!((mb >> g) & 1u)) continue;
+        const float v = val[g * GATHER_CAP + q];
+#pragma unroll
+        for (int r = 0; r < G4; r++)
+          if (ok[r]) fma4(v, b[r], y[g][r]);
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      if (g >= ng) continue;
+#pragma unroll
+      for (int r = 0; r < G4; r++) {
+        const int i = sample(base, r);
+        const float e[4] = {y[g][r].x, y[g][r].y, y[g][r].z, y[g][r].w};
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+          if (i + c < m) emit(g, i + c, e[c]);
+      }
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < G; g++) {
+    if (g >= ng) continue;  // uniform over the block
+    const int j = j0 + g;
+    const double tot = block_sum(acc[g], red);
+    float *zh = Z_hi + (size_t)j * ldm, *zl = Z_lo + (size_t)j * ldm;
+    uint16_t *zb = Zb ? Zb + (size_t)j * ldm : nullptr;
+    uint16_t *zh0 = Zh ? Zh + (size_t)j * ldm : nullptr;
+    if (MODE == 2 || (MODE == 0 && zh0)) {
+      const float inv = MODE == 2 ? 1.0f / (float)sqrt(tot) : 1.0f;
+      const int s = fp16_shift(MODE == 2 ? 1.0f : (float)sqrt(tot));
+      const float sc = pow2f(s);
+      for (int base = 0; base < m; base += chunk) {
+#pragma unroll
+        for (int r = 0; r < G4; r++) {
+          const int i = sample(base, r);
+          const float e[4] = {y[g][r].x, y[g][r].y, y[g][r].z, y[g][r].w};
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            if (i + c >= m) continue;
+            const float v = one_pass ? e[c] : zh[i + c] + zl[i + c];
+            const float z = MODE == 2 ? v * inv : v;
+            if (MODE == 2) {
+              split_store(z, zh + i + c, zl + i + c);
+              if (zb) zb[i + c] = bf16_bits(z);
+            }
+            if (zh0) fp16_split(z * sc, zh0 + i + c, zh0 + zplane + i + c);
+          }
+        }
+      }
+      if (zh0 && threadIdx.x == 0) zscale[j] = pow2f(-s);
+    }
+    if (MODE != 2 && threadIdx.x == 0) fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
+  }
 }
 
 // ------------------------------------------------------------ radix select
@@ -2093,6 +2310,31 @@ cudaError_t launch_deflate(MatrixDev &M, const float *x, double *partial, double
   return cudaGetLastError();
 }
 
+template <int MODE>
+cudaError_t launch_gather_group_mode(const MatrixDev &M, const BatchDev &b, size_t zplane,
+                                     cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(gather_bv_group_kernel<MODE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)GATHER_GROUP_SMEM);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  gather_bv_group_kernel<MODE><<<(b.k + GATHER_GROUP - 1) / GATHER_GROUP, GATHER_THREADS,
+                                 GATHER_GROUP_SMEM, st>>>(
+      M.Bc, M.ldm, M.m, M.ldn, b.k, b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz, b.max_nnz,
+      b.sparse_cap, b.Z_b, b.Z_h, zplane, b.z_scale, b.ctl);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_group(const MatrixDev &M, const BatchDev &b, int mode, size_t zplane,
+                                cudaStream_t st) {
+  if (mode == 0) return launch_gather_group_mode<0>(M, b, zplane, st);
+  if (mode == 1) return launch_gather_group_mode<1>(M, b, zplane, st);
+  return launch_gather_group_mode<2>(M, b, zplane, st);
+}
+
 cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm,
                            const StepParams &p, cudaStream_t st, int *launches, cudaEvent_t *ev,
                            int *kinds) {
@@ -2128,6 +2370,9 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   const int mode = is_l1_variance(f) ? 1 : (is_constrained(f) ? 0 : 2);
   const size_t zplane = (size_t)b.k * M.ldm;  // second FP16 plane of Z
   // 1a. sparse V (every column <= sparse_cap non-zeros last step): gather
+  if ((e = mark(9)) != cudaSuccess) return e;
+  if ((e = launch_gather_group(M, b, mode, zplane, st)) != cudaSuccess) return e;
+  nl++;
   if ((e = mark(5)) != cudaSuccess) return e;
   if (mode == 0)
     gather_bv_kernel<0><<<b.k, GATHER_THREADS, 0, st>>>(M.Bc, M.ldm, M.m, M.ldn,

@@ -312,9 +312,10 @@ typedef enum {
   AM24_KERNEL_SELECT = 3,    /* top-s select or L1-ball level, normalise (constrained) */
   AM24_KERNEL_FINALIZE = 4,  /* per-start objective, change, logs, batch maximum */
   AM24_KERNEL_GATHER_BV = 5, /* Z = B V as a gather over V's non-zeros (sparse steps) */
-  AM24_KERNEL_DENSIFY = 6,   /* dense TF32 hi/lo planes of V for the tensor-core Z = B V */
+  AM24_KERNEL_DENSIFY = 6,   /* dense planes of V (FP16 or TF32) for the tensor-core Z = B V */
   AM24_KERNEL_GEMM_BTZ_BF16 = 7, /* V = B^T Z with single-pass BF16 operands (MIXED) */
   AM24_KERNEL_SUPPORT = 8,   /* support-stability count and phase switch (MIXED) */
+  AM24_KERNEL_GATHER_BV_GROUP = 9, /* the gather for four starts per block (few non-zeros) */
   AM24_KERNEL_SKIPPED = 0x100 /* or-ed into a kind: the launch returned at once */
 } am24_kernel_kind;
 /* One AM step like am24_batch_iterate(h, b, it, 1, NULL), with a CUDA event

@@ -182,8 +182,10 @@ def test_steps_through_sparse_gather_match_oracle(solver, po, formulation, k, ma
         Vo, _, val_o, _, _ = po.oracle_iteration(B64, Vo, os_, val_o, it=it)
     V, val, err, nnz = b.read()
     assert "gemm_BV" in kinds[0] and "gather_BV(skipped)" in kinds[0]
+    assert "gather_BV_group(skipped)" in kinds[0]
     if formulation <= 3 or np.count_nonzero(Vo, axis=0).max() <= n // 32:
-        assert "gather_BV" in kinds[2], kinds[2]
+        # four starts per block while no column has more than 1024 non-zeros
+        assert ("gather_BV" in kinds[2]) != ("gather_BV_group" in kinds[2]), kinds[2]
     ok = 0
     for j in range(k):
         same = np.array_equal(V[:, j] != 0, Vo[:, j] != 0)
