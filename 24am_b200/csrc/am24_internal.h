@@ -21,8 +21,9 @@ inline bool is_l1_constrained(int f) { return f == 2 || f == 3; }
 inline bool is_l1_variance(int f) { return f == 1 || f == 3 || f == 5 || f == 7; }
 inline bool is_l1_penalized(int f) { return f == 6 || f == 7; }
 
-// Layout of one resident data matrix.  B (m x n) is kept in two K-major
-// orientations, each as a TF32 hi plane and an exact FP32 remainder plane:
+// Layout of one resident data matrix.  B (m x n) is kept as FP32 in Bc, and
+// the products' operand planes are made from it in two K-major orientations
+// when a batch first needs them:
 //   Bc: n rows (features) of m samples, leading dimension ldm  -> A of V = B^T Z
 //   Bt: m rows (samples) of n features, leading dimension ldn  -> A of Z = B V
 struct MatrixDev {
@@ -86,8 +87,10 @@ struct BatchDev {
   float *Vx;            // k x ldn loadings; entry i of a column is defined only
                         // where its vmask bit is set (zero elsewhere)
   float *V_hi, *V_lo;   // k x ldn dense TF32 hi/lo planes of V: the B operand of the
-                        // tensor-core Z = B V, filled by densify on dense steps only
-  float *Z_hi, *Z_lo;   // k x ldm sample-space vectors (GEMM-2 B operand)
+                        // one-CTA tensor-core Z = B V, filled on dense steps only
+                        // (null when Z = B V runs on the FP16 pairs)
+  float *Z_hi, *Z_lo;   // k x ldm sample-space vectors z = hi + lo (the TF32 B
+                        // operand of V = B^T Z, and the store the reductions re-read)
   float *Vraw;          // k x ldn raw B^T Z (constrained forms)
   float *ws;            // split-K partial tiles of Z = B V
   float *fz;            // per start: ||y||_2 or ||y||_1 from the Z reduction
