@@ -65,12 +65,14 @@ inline void from_c(const am24_settings &s, SolverStructures::OptimizationSetting
   o->storeIterationsForAllPoints = s.store_all != 0;
 }
 
-// One solve in FP32 through am24_solve_dense_f32 (host B) or
-// am24_solve_device_f32 (device B); fills the reference's statistics.
+// One solve in FP32 through am24_solve_dense_f32 (host B), am24_solve_device_f32
+// (device B) or, given a resident matrix, am24_solve_resident_f32 (B unused);
+// fills the reference's statistics.
 inline float solve_f32(const float *B, int ldB, float *x, unsigned m, unsigned n, bool on_device,
                        SolverStructures::OptimizationSettings *o,
                        SolverStructures::OptimizationStatistics *st,
-                       am24_status *status = nullptr, const float *start_points = nullptr) {
+                       am24_status *status = nullptr, const float *start_points = nullptr,
+                       am24_matrix resident = nullptr) {
   const float nan = std::numeric_limits<float>::quiet_NaN();
   if (status) *status = AM24_ERR_CUDA;
   am24_handle h = default_handle(o->device);
@@ -94,8 +96,9 @@ inline float solve_f32(const float *B, int ldB, float *x, unsigned m, unsigned n
   }
   float f = nan;
   const am24_status rc =
-      on_device ? am24_solve_device_f32(h, B, ldB, x, m, n, &s, &cs, start_points, &f)
-                : am24_solve_dense_f32(h, B, ldB, x, m, n, &s, &cs, start_points, &f);
+      resident    ? am24_solve_resident_f32(h, resident, x, &s, &cs, start_points, &f)
+      : on_device ? am24_solve_device_f32(h, B, ldB, x, m, n, &s, &cs, start_points, &f)
+                  : am24_solve_dense_f32(h, B, ldB, x, m, n, &s, &cs, start_points, &f);
   from_c(s, o);
   if (status) *status = rc;
   if (rc != AM24_OK) return nan;

@@ -40,6 +40,41 @@ int call(cublasHandle_t& h, thrust::device_vector<float>& d_B, thrust::host_vect
 '''
 
 
+CSC_CALLER = r'''
+#include <am24/sparse_PCA_solver_for_CSC.h>
+#include <vector>
+using namespace SolverStructures;
+// the shape of the reference's sparse solver call, with its deflation collection
+// (c++/src/gpower/sparse_PCA_solver_for_CSC.h:111-117)
+template <typename F> F run(std::vector<F>& v, std::vector<int>& r, std::vector<int>& c, int m,
+                            int n, OptimizationSettings* s) {
+  OptimizationStatistics* st = new OptimizationStatistics();
+  SPCASolver::SparseDeflationCollection<F> defl;
+  std::vector<F> x(n, 0), means(n, 0), rowMeans(m, 0);
+  F f = SPCASolver::sparse_PCA_solver_CSC(&v[0], &r[0], &c[0], &x[0], m, n, s, st, true,
+                                          &means[0], false, &rowMeans[0], defl);
+  defl.addNewSparsePV(x);
+  std::vector<F> V(n * 2, 1);
+  defl.deflateV(&V[0], n, 2);
+  delete st;
+  return f;
+}
+int main() {
+  OptimizationSettings s;
+  std::vector<float> vf(2, 1.f); std::vector<double> vd(2, 1.0);
+  std::vector<int> r = {0, 1}, c = {0, 1, 2};
+  return (run(vf, r, c, 2, 2, &s) == run(vd, r, c, 2, 2, &s)) ? 0 : 0;
+}
+'''
+
+
+def test_csc_adapter_compiles_for_reference_callers(tmp_path):
+    src = tmp_path / "csc_caller.cpp"
+    src.write_text(CSC_CALLER)
+    subprocess.run(["g++", "-std=c++14", "-Wall", "-Werror", f"-I{ROOT}/include", "-c", str(src),
+                    "-o", str(tmp_path / "csc_caller.o")], check=True)
+
+
 def test_adapter_compiles_for_reference_callers(tmp_path):
     src = tmp_path / "caller.cpp"
     src.write_text(CALLER)

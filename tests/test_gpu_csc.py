@@ -83,3 +83,101 @@ def test_csc_rejects_malformed_arrays(solver):
         with pytest.raises(am.Am24Error) as e:
             am.Matrix.from_csc(solver, vals, rows, ptr, 3, 2)
         assert e.value.status == 1  # AM24_ERR_INVALID_ARG
+
+
+CSC_PROGRAM = r'''
+#include <am24/sparse_PCA_solver_for_CSC.h>
+#include <cstdio>
+#include <vector>
+// input: m n nnz, col_ptr, row_ind, vals, means (n), one component pv (n);
+// output: the objective and x of a solve, then of a solve after adding pv to
+// the deflation collection
+static SolverStructures::OptimizationSettings settings() {
+  SolverStructures::OptimizationSettings s;
+  s.formulation = SolverStructures::L0_constrained_L2_PCA;
+  s.constraintParameter = 10;
+  s.tolerance = 1e-6;
+  s.maximumIterations = 60;
+  s.totalStartingPoints = 32;
+  s.batchSize = 32;
+  return s;
+}
+int main(int argc, char **argv) {
+  FILE *f = fopen(argv[1], "rb");
+  int m = 0, n = 0, nnz = 0;
+  size_t got = fread(&m, 4, 1, f) + fread(&n, 4, 1, f) + fread(&nnz, 4, 1, f);
+  std::vector<int> cp(n + 1), ri(nnz);
+  std::vector<float> v(nnz), mu(n), pv(n), rmu(m, 0.f);
+  got += fread(cp.data(), 4, n + 1, f) + fread(ri.data(), 4, nnz, f) + fread(v.data(), 4, nnz, f);
+  got += fread(mu.data(), 4, n, f) + fread(pv.data(), 4, n, f);
+  fclose(f);
+  if (got != (size_t)(3 + n + 1 + 2 * nnz + 2 * n)) return 2;
+  SPCASolver::SparseDeflationCollection<float> defl;
+  std::vector<float> x0(n, 0.f), x1(n, 0.f);
+  SolverStructures::OptimizationSettings s0 = settings(), s1 = settings();
+  SolverStructures::OptimizationStatistics st0, st1;
+  float f0 = SPCASolver::sparse_PCA_solver_CSC(v.data(), ri.data(), cp.data(), x0.data(), m, n,
+                                               &s0, &st0, true, mu.data(), false, rmu.data(),
+                                               defl);
+  defl.addNewSparsePV(pv);
+  float f1 = SPCASolver::sparse_PCA_solver_CSC(v.data(), ri.data(), cp.data(), x1.data(), m, n,
+                                               &s1, &st1, true, mu.data(), false, rmu.data(),
+                                               defl);
+  FILE *o = fopen(argv[2], "wb");
+  fwrite(&f0, 4, 1, o);
+  fwrite(&f1, 4, 1, o);
+  fwrite(x0.data(), 4, n, o);
+  fwrite(x1.data(), 4, n, o);
+  fclose(o);
+  return (f0 == f0 && f1 == f1) ? 0 : 1;
+}
+'''
+
+
+def test_csc_adapter_runs_like_the_python_mirror(solver, tmp_path):
+    """A C++ caller of the reference's sparse_PCA_solver_CSC signature, linked to
+    the library: a solve, then one with a component in the deflation
+    collection, equal to the same two solves through the ABI (the mirror's
+    Matrix.from_csc, deflate and solve)."""
+    import os
+    import subprocess
+    am = _am()
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    m, n = 150, 1200
+    S = _sparse(m, n, 21, density=0.08)
+    S.sum_duplicates()
+    A = S.toarray().astype(np.float32)
+    mu = A.mean(axis=0).astype(np.float32)
+    rng = np.random.default_rng(22)
+    pv = np.zeros(n, np.float32)
+    pick = rng.permutation(n)[:15]
+    pv[pick] = rng.standard_normal(15).astype(np.float32)
+    pv /= np.linalg.norm(pv)
+    pv = pv.astype(np.float32)
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as fh:
+        np.array([m, n, S.nnz], np.int32).tofile(fh)
+        S.indptr.astype(np.int32).tofile(fh)
+        S.indices.astype(np.int32).tofile(fh)
+        S.data.astype(np.float32).tofile(fh)
+        mu.tofile(fh)
+        pv.tofile(fh)
+    src = tmp_path / "csc_run.cpp"
+    src.write_text(CSC_PROGRAM)
+    exe = tmp_path / "csc_run"
+    lib = os.path.join(root, "24am_b200")
+    subprocess.run(["g++", "-std=c++14", "-O1", f"-I{root}/include", str(src), f"-L{lib}",
+                    "-lam24", f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    out = tmp_path / "out.bin"
+    subprocess.run([str(exe), str(inp), str(out)], check=True)
+    r = np.fromfile(out, np.float32)
+    f0, f1, x0, x1 = r[0], r[1], r[2:2 + n], r[2 + n:]
+    kw = dict(formulation=0, constraintParameter=10, tolerance=1e-6, maximumIterations=60,
+              totalStartingPoints=32, batchSize=32)
+    M = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu)
+    y0, g0, _ = M.solve(am.OptimizationSettings(**kw))
+    M.deflate(pv)
+    y1, g1, _ = M.solve(am.OptimizationSettings(**kw))
+    M.close()
+    assert f0 == np.float32(g0) and np.array_equal(x0, y0)
+    assert f1 == np.float32(g1) and np.array_equal(x1, y1)
