@@ -676,11 +676,12 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
                                        const int32_t *col_ptr, uint32_t m, uint32_t n,
                                        const float *means, const float *row_means,
                                        am24_matrix *out) {
-  if (!h || !col_ptr || !out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  if (!col_ptr || !out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
   *out = nullptr;
   if (m == 0 || n == 0) return fail(AM24_ERR_INVALID_ARG, "m and n must be positive");
   if (m > (1u << 30) || n > (1u << 30)) return fail(AM24_ERR_INVALID_ARG, "matrix too large");
-  // the arrays are checked here, before any device write can use an index
+  // the arrays are checked on the host first (no handle or device needed),
+  // before any device write can use an index
   if (col_ptr[0] != 0) return fail(AM24_ERR_INVALID_ARG, "col_ptr[0] must be 0");
   for (uint32_t c = 0; c < n; c++)
     if (col_ptr[c + 1] < col_ptr[c])
@@ -690,6 +691,7 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
   for (size_t q = 0; q < nnz; q++)
     if (row_ind[q] < 0 || (uint32_t)row_ind[q] >= m)
       return fail(AM24_ERR_INVALID_ARG, "row index out of range at entry " + std::to_string(q));
+  if (!h) return fail(AM24_ERR_INVALID_ARG, "NULL handle");
   AM24_CUDA(cudaSetDevice(h->device));
   auto *mat = new am24_matrix_s();
   MatrixDev &M = mat->d;
