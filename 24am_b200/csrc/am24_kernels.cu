@@ -21,6 +21,9 @@
 #include <cuda_fp16.h>
 #include <climits>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "am24_internal.h"
 #include "gemm_tf32x3.cuh"
@@ -2049,25 +2052,7 @@ struct GemmCfg {
   int bn, stages;
 };
 
-template <int BN, int BKT, int ST, class Epi>
-cudaError_t run_gemm(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
-                     const CUtensorMap &b_lo, const GemmShape &sh, const Epi &epi,
-                     cudaStream_t st) {
-  using L = GemmSmem<BN, BKT, ST>;
-  auto kern = gemm_tf32x3_kernel<BN, BKT, ST, GEMM_PROMO_K / BKT, Epi>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  const int grid = sh.num_units < num_sms() ? sh.num_units : num_sms();
-  kern<<<grid, GEMM_THREADS, L::TOTAL, st>>>(a_hi, a_lo, b_hi, b_lo, sh, epi);
-  return cudaGetLastError();
-}
-
-// Stages per (N tile, K slab) fill ~192 KB of shared memory.
-// Co-resident clusters of two CTAs for a pair kernel (queried once per kernel).
+// Co-resident clusters of two CTAs for a pair kernel.
 template <class K>
 cudaError_t pair_clusters(K kern, int smem, int *out) {
   cudaLaunchConfig_t cfg = {};
@@ -2082,18 +2067,58 @@ cudaError_t pair_clusters(K kern, int smem, int *out) {
   return cudaSuccess;
 }
 
+// Launch set-up of a kernel on the current device, done once per (kernel,
+// device) under a lock (serving runs several host threads, and a process may
+// drive several devices): the dynamic shared-memory limit raised to smem and,
+// for pair kernels, the number of co-resident clusters of two.
+struct LaunchSetup {
+  cudaError_t err;
+  int clusters;
+};
+std::mutex g_setup_mu;
+std::map<std::pair<const void *, int>, LaunchSetup> g_setup;
+
+template <class K>
+cudaError_t kernel_setup(K kern, int smem, bool pair, int *clusters = nullptr) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_setup_mu);
+  const auto key = std::make_pair(reinterpret_cast<const void *>(kern), dev);
+  auto it = g_setup.find(key);
+  if (it == g_setup.end()) {
+    LaunchSetup c{cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                  0};
+    if (c.err == cudaSuccess && pair) c.err = pair_clusters(kern, smem, &c.clusters);
+    it = g_setup.emplace(key, c).first;
+  }
+  if (clusters) *clusters = it->second.clusters;
+  return it->second.err;
+}
+
+template <int BN, int BKT, int ST, class Epi>
+cudaError_t run_gemm(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
+                     const CUtensorMap &b_lo, const GemmShape &sh, const Epi &epi,
+                     cudaStream_t st) {
+  using L = GemmSmem<BN, BKT, ST>;
+  auto kern = gemm_tf32x3_kernel<BN, BKT, ST, GEMM_PROMO_K / BKT, Epi>;
+  const cudaError_t e = kernel_setup(kern, L::TOTAL, false);
+  if (e != cudaSuccess) return e;
+  const int grid = sh.num_units < num_sms() ? sh.num_units : num_sms();
+  kern<<<grid, GEMM_THREADS, L::TOTAL, st>>>(a_hi, a_lo, b_hi, b_lo, sh, epi);
+  return cudaGetLastError();
+}
+
+// Stages per (N tile, K slab) fill ~192 KB of shared memory.
 template <class S, int BN, int ST, class Epi>
 cudaError_t run_gemm_pair(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &m2,
                           const CUtensorMap &m3, const GemmShape &sh, const Epi &epi,
                           cudaStream_t st, int splits = 1) {
   using L = PairSmem<S, BN, ST>;
   auto kern = gemm_pair_kernel<S, BN, ST, S::PROMO_K / S::BK, Epi>;
-  static int clusters = 0;
-  if (clusters == 0) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
-    if (e != cudaSuccess) return e;
-    if ((e = pair_clusters(kern, L::TOTAL, &clusters)) != cudaSuccess) return e;
-  }
+  int clusters = 0;
+  const cudaError_t e = kernel_setup(kern, L::TOTAL, true, &clusters);
+  if (e != cudaSuccess) return e;
   GemmShape s2 = sh;  // K blocks of this scheme's BK; units are pair tiles x splits
   s2.kb_total = (sh.K + S::BK - 1) / S::BK;
   s2.kb_per_split = (s2.kb_total + splits - 1) / splits;
@@ -2152,13 +2177,14 @@ cudaError_t dispatch_gemm2(const BatchDev &b, const TensorMaps &tm, const GemmSh
 }  // namespace
 
 int num_sms() {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
+  // SMs of the first device that asks (every device of a B200 node has 148);
+  // a function-local static, initialised once however many threads ask
+  static const int sms = [] {
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 1;
-  }
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+  }();
   return sms;
 }
 
@@ -2313,14 +2339,8 @@ cudaError_t launch_deflate(MatrixDev &M, const float *x, double *partial, double
 template <int MODE>
 cudaError_t launch_gather_group_mode(const MatrixDev &M, const BatchDev &b, size_t zplane,
                                      cudaStream_t st) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(gather_bv_group_kernel<MODE>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)GATHER_GROUP_SMEM);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  const cudaError_t e = kernel_setup(gather_bv_group_kernel<MODE>, (int)GATHER_GROUP_SMEM, false);
+  if (e != cudaSuccess) return e;
   gather_bv_group_kernel<MODE><<<(b.k + GATHER_GROUP - 1) / GATHER_GROUP, GATHER_THREADS,
                                  GATHER_GROUP_SMEM, st>>>(
       M.Bc, M.ldm, M.m, M.ldn, b.k, b.Vx, b.vmask, b.Z_hi, b.Z_lo, b.fz, b.max_nnz,
