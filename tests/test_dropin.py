@@ -136,3 +136,40 @@ def test_console_matches_reference_console_runs(name, flags):
         f = _read_fval(out + "_optimizationStatistics")
     assert abs(f - float(z[f"{name}.fval"])) <= 1e-5 * abs(float(z[f"{name}.fval"]))
     assert np.allclose(x, z[f"{name}.x"], atol=1e-5)
+
+
+COLLECTION_PROGRAM = r'''
+#include <am24/sparse_PCA_solver_for_CSC.h>
+#include <cstdio>
+#include <vector>
+// V (n x 2) <- the collection's projections, then printed: the host-side part
+// of the sparse solver's deflation collection, which needs no device
+int main() {
+  const int n = 5;
+  SPCASolver::SparseDeflationCollection<double> defl;
+  std::vector<double> x1 = {0.6, 0.0, 0.8, 0.0, 0.0}, x2 = {0.0, 1.0, 0.0, 0.0, 0.0};
+  defl.addNewSparsePV(x1);
+  defl.addNewSparsePV(x2);
+  std::vector<double> V = {1, 2, 3, 4, 5, -1, 0.5, 2, 0, 1};
+  defl.deflateV(&V[0], n, 2);
+  for (double v : V) printf("%.17g\n", v);
+  return (defl.list.size() == 2 && defl.list[0].idx.size() == 2) ? 0 : 1;
+}
+'''
+
+
+def test_deflation_collection_projects_like_the_reference(tmp_path):
+    """SparseDeflationCollection keeps each component's non-zeros and projects a
+    block of vectors by each component in turn, V <- (I - x x^T) V."""
+    src = tmp_path / "coll.cpp"
+    src.write_text(COLLECTION_PROGRAM)
+    exe = tmp_path / "coll"
+    subprocess.run(["g++", "-std=c++14", "-Wall", "-Werror", f"-I{ROOT}/include", str(src),
+                    "-o", str(exe), f"-L{ROOT}/24am_b200", "-lam24",
+                    f"-Wl,-rpath,{ROOT}/24am_b200"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    got = np.array([float(t) for t in out.split()]).reshape(2, 5).T
+    V = np.array([[1, 2, 3, 4, 5], [-1, 0.5, 2, 0, 1]], float).T
+    for x in (np.array([0.6, 0, 0.8, 0, 0]), np.array([0, 1.0, 0, 0, 0])):
+        V = V - np.outer(x, x @ V)
+    assert np.allclose(got, V, rtol=0, atol=1e-15)
