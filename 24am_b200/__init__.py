@@ -75,7 +75,7 @@ class am24_statistics(C.Structure):
         ("cardinalities", C.POINTER(C.c_int32)), ("per_start_capacity", C.c_uint32),
         ("explained_variance", C.c_double), ("start_iterations", C.c_uint64),
         ("degenerate_starts", C.c_int32), ("low_precision_iterations", C.c_uint32),
-        ("reserved", C.c_uint32 * 6),
+        ("input_rounded_to_f32", C.c_int32), ("reserved", C.c_uint32 * 5),
     ]
 
 
@@ -262,6 +262,7 @@ class OptimizationStatistics:
         self.startIterations = 0
         self.degenerateStarts = 0
         self.lowPrecisionIterations = 0
+        self.inputRoundedToF32 = False
 
 
 class Solver:
@@ -335,6 +336,7 @@ class Solver:
         stats.startIterations = st.start_iterations
         stats.degenerateStarts = st.degenerate_starts
         stats.lowPrecisionIterations = st.low_precision_iterations
+        stats.inputRoundedToF32 = bool(st.input_rounded_to_f32)
         if settings.storeIterationsForAllPoints:
             k = settings.totalStartingPoints
             stats.values = values[:k].tolist()

@@ -1490,6 +1490,7 @@ am24_status am24_solve_dense_f64(am24_handle h, const double *B, int32_t ldB, do
   float f = 0.f;
   AM24_TRY(am24_solve_dense_f32(h, Bf.data(), (int32_t)m, xf.data(), m, n, settings, stats,
                                 sp.empty() ? nullptr : sp.data(), &f));
+  if (stats) stats->input_rounded_to_f32 = 1;
   for (uint32_t i = 0; i < n; i++) x[i] = xf[i];
   if (fval_out) *fval_out = f;
   return AM24_OK;

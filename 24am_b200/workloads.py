@@ -23,7 +23,9 @@ def low_rank_data(n, p, r, nnz_v, seed, noise=0.1, dtype=np.float64):
         idx = rng.choice(p, size=min(nnz_v, p), replace=False)
         v[idx] = rng.standard_normal(idx.size)
         v /= np.linalg.norm(v)
-        D += 10.0 * 0.8 ** k * np.outer(u, v)
+        # the rank-one term touches only the loading's non-zero columns (adding
+        # its zero columns would leave D unchanged)
+        D[:, idx] += 10.0 * 0.8 ** k * np.outer(u, v[idx])
     D -= D.mean(axis=0, keepdims=True)
     return np.asfortranarray(D.astype(dtype))
 

@@ -135,7 +135,10 @@ typedef struct {
   uint64_t start_iterations;  /* AM steps summed over starting points */
   int32_t degenerate_starts;  /* starts whose final objective was NaN */
   uint32_t low_precision_iterations; /* batch iterations run with BF16 operands */
-  uint32_t reserved[6];
+  int32_t input_rounded_to_f32;       /* 1 when FP64 input was rounded to FP32 before
+                                         the solve (am24_solve_dense_f64): the result is
+                                         the FP32 solve of the rounded data */
+  uint32_t reserved[5];
 } am24_statistics;
 
 typedef struct am24_handle_s *am24_handle;
@@ -170,9 +173,14 @@ am24_status am24_solve_device_f32(am24_handle h, const float *d_B, int32_t ldB, 
                                   am24_statistics *stats, const float *start_points,
                                   float *fval_out);
 
-/* FP64 host data (the reference's denseDataSolver<double> call): B and the
- * injected starts are rounded to FP32 and solved as am24_solve_dense_f32 does;
- * x and *fval_out are returned in double. */
+/* FP64 host data (the reference's denseDataSolver<double> call).  There is no
+ * FP64 arithmetic on this path: B, x and the injected starts are rounded to
+ * FP32 (relative error up to 2^-24 per entry) and solved as
+ * am24_solve_dense_f32 does; x and *fval_out are returned in double and
+ * stats->input_rounded_to_f32 is set to 1, so a caller that asked for double
+ * can tell.  The objective and explained variance then differ from an FP64
+ * solve of the unrounded data by the rounding's effect (about 1e-7 relative on
+ * well-conditioned data). */
 am24_status am24_solve_dense_f64(am24_handle h, const double *B, int32_t ldB, double *x,
                                  uint32_t m, uint32_t n, am24_settings *settings,
                                  am24_statistics *stats, const double *start_points,

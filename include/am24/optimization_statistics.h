@@ -25,10 +25,11 @@ class OptimizationStatistics {
   unsigned long long startIterations;
   int degenerateStarts;
   unsigned lowPrecisionIterations;  // batch iterations with BF16 operands (precision 1)
+  int inputRoundedToFloat;  // 1: the double data were rounded to float and solved in FP32
   OptimizationStatistics()
       : it(0), fval(0), error(0), totalTrueComputationTime(0), totalElapsedTime(0), n(0),
         totalThreadsUsed(1), explainedVariance(0), startIterations(0), degenerateStarts(0),
-        lowPrecisionIterations(0) {}
+        lowPrecisionIterations(0), inputRoundedToFloat(0) {}
 };
 }  // namespace SolverStructures
 #endif

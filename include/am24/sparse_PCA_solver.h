@@ -8,8 +8,9 @@
  * (chceckInputAndModifyIt and OTF's storeIterationsForAllPoints = false), same
  * statistics fields.  The solve runs on the GPU of settings->device; a
  * process-wide handle per device is created on first use.  The double
- * instantiation converts B to FP32 and computes in FP32 (the library's
- * arithmetic), returning x in double.
+ * instantiation has no FP64 arithmetic: it rounds B and x to FP32 (2^-24
+ * relative per entry), solves in FP32 (the library's arithmetic), returns x in
+ * double and sets statistics->inputRoundedToFloat = 1.
  * On failure the return value is NaN and am24_last_error() says why.
  */
 #ifndef AM24_SPARSE_PCA_SOLVER_H
@@ -112,6 +113,7 @@ inline float solve_f32(const float *B, int ldB, float *x, unsigned m, unsigned n
   st->startIterations = cs.start_iterations;
   st->degenerateStarts = cs.degenerate_starts;
   st->lowPrecisionIterations = cs.low_precision_iterations;
+  st->inputRoundedToFloat = cs.input_rounded_to_f32;
   return f;
 }
 
@@ -142,6 +144,7 @@ inline double denseDataSolver<double>(const double *B, const int ldB, double *x,
     for (unsigned r = 0; r < m; r++) Bf[(size_t)c * m + r] = (float)B[(size_t)c * ldB + r];
   for (unsigned i = 0; i < n; i++) xf[i] = (float)x[i];
   const float f = am24_detail::solve_f32(Bf.data(), (int)m, xf.data(), m, n, false, o, st);
+  st->inputRoundedToFloat = 1;  // no FP64 arithmetic on this path
   for (unsigned i = 0; i < n; i++) x[i] = xf[i];
   return f;
 }

@@ -49,11 +49,19 @@ def make_settings(formulation, constraint=10, penalty=0.0, tolerance=0.01, max_i
                     int(bool(use_sort_hard)), int(bool(store_all)), 0)
 
 
-def build():
-    """Compile liboracle.so (always) and the reference build (when its sources exist)."""
+def build(reference=None):
+    """Compile liboracle.so (always) and, given the reference's source tree
+    (`reference`, else the AM24_REFERENCE environment variable), the reference
+    build in _ref/ against naive loops and against the OpenBLAS found beside
+    the Python packages."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if os.path.isdir(os.environ.get("AM24_REFERENCE", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    reference = reference or os.environ.get("AM24_REFERENCE")
+    if reference and os.path.isdir(reference):
+        lib = _openblas_lib()
+        if lib is None:
+            raise FileNotFoundError("no libopenblas*.so found for the reference build")
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={reference}",
+                        f"OPENBLAS_LIB={lib}"], check=True)
 
 
 _LIBS = {}
@@ -77,6 +85,16 @@ def _openblas_dir():
         cand = os.path.join(d, "opencv_python_headless.libs")
         if os.path.isdir(cand):
             return cand
+    return None
+
+
+def _openblas_lib():
+    d = _openblas_dir()
+    if not d:
+        return None
+    for f in sorted(os.listdir(d)):
+        if f.startswith("libopenblas") and f.endswith(".so"):
+            return os.path.join(d, f)
     return None
 
 

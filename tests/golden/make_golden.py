@@ -9,7 +9,7 @@ inputs and outputs; tests/test_golden.py replays the inputs through the oracle
 and requires bit-identical outputs.  Needs the reference sources, so it runs
 only where they are mounted:
 
-    OMP_NUM_THREADS=1 python tests/golden/make_golden.py [/path/to/reference]
+    OMP_NUM_THREADS=1 python tests/golden/make_golden.py <reference source tree>
 """
 import os
 import sys
@@ -52,8 +52,7 @@ def solver_cases():
 
 def main(reference):
     os.environ.setdefault("OMP_NUM_THREADS", "1")
-    os.environ["AM24_REFERENCE"] = reference
-    po.build()
+    po.build(reference)
     po.ref_set_threads(1)
     out = {}
     for name, B, s, V in solver_cases():
@@ -116,4 +115,6 @@ def main(reference):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference source tree>")
+    main(sys.argv[1])

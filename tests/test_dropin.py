@@ -173,3 +173,79 @@ def test_deflation_collection_projects_like_the_reference(tmp_path):
     for x in (np.array([0.6, 0, 0.8, 0, 0]), np.array([0, 1.0, 0, 0, 0])):
         V = V - np.outer(x, x @ V)
     assert np.allclose(got, V, rtol=0, atol=1e-15)
+
+
+GPU_PROGRAM = r'''
+#include <am24/gpu_sparse_PCA_solver.h>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+// the reference GPU console's call (c++/src/frontends/gpu_console.cu:76): B copied
+// into a thrust::device_vector with its leading dimension padded to 128 bytes,
+// then SPCASolver::GPUSolver::denseDataSolver
+int main(int argc, char** argv) {
+  FILE* f = fopen(argv[1], "rb");
+  unsigned m = 0, n = 0;
+  if (fread(&m, 4, 1, f) != 1 || fread(&n, 4, 1, f) != 1) return 2;
+  std::vector<float> B((size_t)m * n);
+  if (fread(B.data(), 4, B.size(), f) != B.size()) return 2;
+  fclose(f);
+  const unsigned LD_M = (m + 31) / 32 * 32, LD_N = (n + 31) / 32 * 32;
+  thrust::host_vector<float> hB((size_t)LD_M * n, 0.f);
+  for (unsigned c = 0; c < n; c++)
+    for (unsigned r = 0; r < m; r++) hB[(size_t)c * LD_M + r] = B[(size_t)c * m + r];
+  thrust::device_vector<float> dB = hB;
+  thrust::host_vector<float> x(LD_N, 0.f);
+  SolverStructures::OptimizationSettings s;
+  s.formulation = (SolverStructures::SPCA_Formulation)atoi(argv[2]);
+  s.constraintParameter = atoi(argv[3]);
+  s.penaltyParameter = atof(argv[4]);
+  s.tolerance = 1e-6;
+  s.maximumIterations = 60;
+  s.totalStartingPoints = 40;
+  s.batchSize = 16;
+  SolverStructures::OptimizationStatistics st;
+  cublasHandle_t handle = nullptr;  // the adapter does not use cuBLAS
+  const int rc = SPCASolver::GPUSolver::denseDataSolver(handle, m, n, dB, x, &s, &st, LD_M, LD_N);
+  printf("%d %.9g %u %u\n", rc, st.fval, s.totalStartingPoints, s.totalBatches);
+  for (unsigned i = 0; i < n; i++) printf("%.9g\n", x[i]);
+  return rc;
+}
+'''
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("formulation,s,gamma", [(0, 12, 0.0), (3, 12, 0.0), (6, 0, 0.15),
+                                                 (5, 0, 60.0)])
+def test_gpu_adapter_solves_like_the_oracle(tmp_path, po, formulation, s, gamma):
+    """A program written against the reference's GPU entry point, linked to
+    libam24.so, solves a device-resident B (the reference's own starting
+    points, batch mode) to the oracle's best objective and loading."""
+    src = tmp_path / "gprog.cu"
+    src.write_text(GPU_PROGRAM)
+    exe = tmp_path / "gprog"
+    subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                    f"-I{ROOT}/include", str(src), "-o", str(exe), f"-L{ROOT}/24am_b200",
+                    "-lam24", f"-Xlinker=-rpath,{ROOT}/24am_b200"], check=True)
+    m, n = 120, 700
+    B = po.low_rank_data(m, n, 6, 20, seed=formulation, dtype=np.float32)
+    data = tmp_path / "B.bin"
+    with open(data, "wb") as f:
+        np.array([m, n], np.uint32).tofile(f)
+        np.asfortranarray(B).T.astype(np.float32).tofile(f)
+    out = subprocess.run([str(exe), str(data), str(formulation), str(max(s, 1)), repr(gamma)],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    lines = out.stdout.split("\n")
+    rc, fval, total, batches = lines[0].split()
+    x = np.array([float(t) for t in lines[1:1 + n]])
+    assert int(rc) == 0 and int(total) == 48 and int(batches) == 3
+    B64 = B.astype(np.float64)
+    st = po.make_settings(formulation, constraint=max(s, 1), penalty=gamma, tolerance=1e-6,
+                          max_iter=60, total_starts=40, batch_size=16)
+    r = po.oracle_solve(B64, st, po.reference_starts(n, 48, formulation <= 3, max(s, 1),
+                                                     dtype=np.float32).astype(np.float64))
+    assert abs(float(fval) - r["fval"]) <= 1e-5 * abs(r["fval"])
+    ev = np.linalg.norm(B64 @ x) ** 2
+    ev_o = np.linalg.norm(B64 @ r["x"]) ** 2
+    assert abs(ev - ev_o) <= 1e-5 * ev_o

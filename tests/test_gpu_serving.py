@@ -113,6 +113,43 @@ def test_f64_entry_matches_f32_on_float_data(solver, po):
                                            C.byref(stc), None, C.byref(f)))
     assert np.array_equal(x64.astype(np.float32), x32)
     assert f.value == pytest.approx(f32, rel=0, abs=0)
+    assert stc.input_rounded_to_f32 == 1
+
+
+@pytest.mark.parametrize("formulation", [0, 6])
+def test_f64_entry_on_double_data_reports_the_rounding(solver, po, formulation):
+    """Genuine FP64 data (not FP32 values): the entry point says it rounded
+    the input (input_rounded_to_f32 = 1), and its best objective and explained
+    variance differ from the FP64 oracle's solve of the unrounded data by the
+    rounding's effect, printed here and held to 1e-5 relative."""
+    am = _am()
+    m, n, k = 200, 1500, 64
+    B64 = po.low_rank_data(m, n, 6, 20, seed=46, dtype=np.float64)
+    assert not np.array_equal(B64.astype(np.float32).astype(np.float64), B64)
+    V = po.uniform_starts(n, k, seed=47, dtype=np.float64)
+    g = 0.15 if formulation == 6 else 0.0
+    s = am.OptimizationSettings(formulation=formulation, constraintParameter=12,
+                                penaltyParameter=g, tolerance=1e-6, maximumIterations=80,
+                                totalStartingPoints=k, batchSize=k,
+                                startMode=am.START_INJECTED).to_c()
+    x64 = np.zeros(n, np.float64)
+    stc = am.am24_statistics()
+    f = C.c_double()
+    Vf = np.asfortranarray(V)
+    am.check(am.lib().am24_solve_dense_f64(solver.h, B64.ctypes.data_as(C.c_void_p), m,
+                                           x64.ctypes.data_as(C.c_void_p), m, n, C.byref(s),
+                                           C.byref(stc), Vf.ctypes.data_as(C.c_void_p),
+                                           C.byref(f)))
+    assert stc.input_rounded_to_f32 == 1
+    r = po.oracle_solve(B64, po.make_settings(formulation, constraint=12, penalty=g,
+                                              tolerance=1e-6, max_iter=80, total_starts=k,
+                                              batch_size=k), V)
+    ev = float(np.linalg.norm(B64 @ x64) ** 2)
+    ev_o = float(np.linalg.norm(B64 @ r["x"]) ** 2)
+    e_f, e_ev = abs(f.value - r["fval"]) / abs(r["fval"]), abs(ev - ev_o) / ev_o
+    print(f"FP64 data through the FP32 path, formulation {formulation}: objective rel err "
+          f"{e_f:.2e}, explained variance rel err {e_ev:.2e} against the FP64 oracle")
+    assert e_f <= 1e-5 and e_ev <= 1e-5
 
 
 def splitmix64(x):
