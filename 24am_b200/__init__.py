@@ -132,6 +132,16 @@ _SIGS = {
     "am24_stream": (C.c_void_p, [_VP]),
     "am24_batch_step_timed": (C.c_int, [_VP, _VP, C.c_int32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "am24_group_create": (C.c_int, [_VP, C.c_uint32, C.POINTER(_VP)]),
+    "am24_group_destroy": (C.c_int, [_VP]),
+    "am24_group_add": (C.c_int, [_VP, _VP, C.POINTER(am24_settings), _VP,
+                                 C.POINTER(C.c_uint32)]),
+    "am24_group_run": (C.c_int, [_VP, C.c_uint32, C.POINTER(C.c_float)]),
+    "am24_group_state": (C.c_int, [_VP, C.c_uint32, C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_uint32)]),
+    "am24_group_result": (C.c_int, [_VP, C.c_uint32, _VP, C.POINTER(am24_statistics)]),
+    "am24_group_read": (C.c_int, [_VP, C.c_uint32, _VP, _VP, _VP, _VP]),
+    "am24_group_remove": (C.c_int, [_VP, C.c_uint32]),
 }
 KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV", "densify",
                 "gemm_BtZ_bf16", "support", "gather_BV_group"]
@@ -544,6 +554,79 @@ class Batch:
         v = C.c_int32()
         check(lib().am24_batch_launches_per_step(self.matrix.solver.h, self.bh, C.byref(v)))
         return v.value
+
+
+class Group:
+    """Many independent problems solved together (am24_group_*): every step of
+    every problem runs in one set of grouped launches inside one captured CUDA
+    graph that loops on the device until all have stopped."""
+
+    def __init__(self, solver, capacity=256):
+        self.solver = solver
+        gh = C.c_void_p()
+        check(lib().am24_group_create(solver.h, int(capacity), C.byref(gh)))
+        self.gh = gh
+        self.problems = {}  # id -> (matrix, k)
+
+    def close(self):
+        if self.gh:
+            lib().am24_group_destroy(self.gh)
+            self.gh = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, matrix, settings, start_points=None):
+        """One problem: all of settings.totalStartingPoints starts as one batch."""
+        s = settings.to_c()
+        sp = None if start_points is None else np.asfortranarray(start_points, np.float32)
+        pid = C.c_uint32()
+        check(lib().am24_group_add(self.gh, matrix.mh, C.byref(s), _ptr(sp), C.byref(pid)))
+        chk = settings.to_c()
+        check(lib().am24_check_input(C.byref(chk), matrix.n))
+        self.problems[pid.value] = (matrix, int(chk.total_starts))
+        return pid.value
+
+    def run(self, max_steps=0):
+        """Runs until every problem has stopped (or max_steps steps); returns the
+        launch's device time in ms."""
+        ms = C.c_float()
+        check(lib().am24_group_run(self.gh, int(max_steps), C.byref(ms)))
+        return ms.value
+
+    def state(self, pid):
+        stopped, steps = C.c_int32(), C.c_uint32()
+        check(lib().am24_group_state(self.gh, int(pid), C.byref(stopped), C.byref(steps)))
+        return bool(stopped.value), steps.value
+
+    def result(self, pid):
+        matrix, _ = self.problems[pid]
+        x = np.zeros(matrix.n, np.float32)
+        st = am24_statistics()
+        check(lib().am24_group_result(self.gh, int(pid), _ptr(x), C.byref(st)))
+        return x, st
+
+    def read(self, pid):
+        matrix, k = self.problems[pid]
+        V = np.zeros((matrix.n, k), np.float32, order="F")
+        val = np.zeros(k, np.float32)
+        err = np.zeros(k, np.float32)
+        nnz = np.zeros(k, np.uint32)
+        check(lib().am24_group_read(self.gh, int(pid), _ptr(V), _ptr(val), _ptr(err), _ptr(nnz)))
+        return V, val, err, nnz
+
+    def remove(self, pid):
+        check(lib().am24_group_remove(self.gh, int(pid)))
+        self.problems.pop(pid, None)
 
 
 class Server:

@@ -26,103 +26,16 @@
 
 #include "am24.h"
 #include "am24_internal.h"
+#include "am24_host.h"
 
 using namespace am24;
+using namespace am24host;
 
-namespace {
-
+namespace am24host {
 thread_local std::string g_last_error;
+}  // namespace am24host
 
-am24_status fail(am24_status s, const std::string &msg) {
-  g_last_error = msg;
-  return s;
-}
-
-#define AM24_CUDA(expr)                                                                  \
-  do {                                                                                   \
-    cudaError_t e_ = (expr);                                                             \
-    if (e_ != cudaSuccess) {                                                             \
-      if (e_ == cudaErrorMemoryAllocation) {                                             \
-        cudaGetLastError();                                                              \
-        return fail(AM24_ERR_OOM, std::string(#expr) + ": " + cudaGetErrorString(e_));  \
-      }                                                                                  \
-      return fail(AM24_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));   \
-    }                                                                                    \
-  } while (0)
-
-#define AM24_TRY(expr)                   \
-  do {                                   \
-    am24_status s_ = (expr);             \
-    if (s_ != AM24_OK) return s_;        \
-  } while (0)
-
-int round_up(int v, int a) { return (v + a - 1) / a * a; }
-
-// Scoped device allocations of one object.  With a stream, stream-ordered
-// (cudaMallocAsync / cudaFreeAsync on it, for memory only that stream uses):
-// freeing then waits for no other stream, which matters when several handles
-// work on one device at once.
-struct Allocs {
-  std::vector<void *> ptrs;
-  cudaStream_t stream = nullptr;
-  bool ordered = false;
-  Allocs() = default;
-  explicit Allocs(cudaStream_t st) : stream(st), ordered(true) {}
-  ~Allocs() {
-    for (void *p : ptrs) {
-      if (ordered)
-        cudaFreeAsync(p, stream);
-      else
-        cudaFree(p);
-    }
-  }
-  template <typename T>
-  am24_status get(T **out, size_t count) {
-    void *p = nullptr;
-    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    cudaError_t e = ordered ? cudaMallocAsync(&p, bytes, stream) : cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return fail(e == cudaErrorMemoryAllocation ? AM24_ERR_OOM : AM24_ERR_CUDA,
-                  std::string("device allocation: ") + cudaGetErrorString(e));
-    }
-    ptrs.push_back(p);
-    *out = static_cast<T *>(p);
-    return AM24_OK;
-  }
-};
-
-}  // namespace
-
-struct am24_handle_s {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaStream_t copy = nullptr;  // host-to-device copies that overlap work on `stream`
-  // run-ahead batch loops: the stop word of each queued step lands in pinned
-  // host memory, an event per slot
-  static constexpr int AHEAD = 4;
-  uint32_t *flags = nullptr;
-  cudaEvent_t run_ev[AHEAD] = {};
-  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  Allocs scratch;  // small per-handle buffers
-  double *ev_out = nullptr;
-};
-
-struct am24_matrix_s {
-  MatrixDev d{};
-  Allocs mem;
-};
-
-struct am24_batch_s {
-  BatchDev d{};
-  TensorMaps tm{};
-  am24_matrix mat = nullptr;
-  am24_settings s{};
-  int launches = 0;
-  Allocs mem;
-};
-
-namespace {
+namespace am24host {
 
 // K-major FP32 operand [rows][ld], loaded as bk x box_rows tiles; the swizzle
 // matches the row length (bk * 4 bytes) and the GEMM's smem descriptors.
@@ -145,7 +58,7 @@ am24_status make_map(am24_handle h, CUtensorMap *map, const float *base, int K, 
 // fp16), loaded as 32 x box_rows tiles (64-byte rows, 64-byte swizzle), as the
 // 16-bit pair GEMMs read them.
 am24_status make_map_bf16(am24_handle h, CUtensorMap *map, const uint16_t *base, int K, int rows,
-                          int ld, int box_rows, bool fp16 = false) {
+                          int ld, int box_rows, bool fp16) {
   cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(uint16_t)};
   cuuint32_t box[2] = {(cuuint32_t)PAIR_BK_BF16, (cuuint32_t)box_rows};
@@ -263,7 +176,7 @@ cudaError_t reset_mixed(const BatchDev &d, cudaStream_t st) {
   return e;
 }
 
-}  // namespace
+}  // namespace am24host
 
 // The starting points staged in b's Vraw (all batch_size columns) become the
 // batch's loadings: values and masks, dense-step gate, no select hints, and
@@ -282,7 +195,7 @@ static am24_status load_from_vraw(am24_handle h, am24_batch b) {
   return AM24_OK;
 }
 
-namespace {
+namespace am24host {
 
 // Split-K factor for Z = B V: minimise rounds * (K blocks per unit + fixed
 // per-unit cost) over the persistent grid.
@@ -456,7 +369,7 @@ am24_status upload_columns(am24_handle h, am24_batch b, const float *host, int c
   return AM24_OK;
 }
 
-}  // namespace
+}  // namespace am24host
 
 // ============================================================== library
 extern "C" {

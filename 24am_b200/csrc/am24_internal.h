@@ -149,6 +149,129 @@ struct TensorMaps {
   CUtensorMap a1_h0, a1_h1, b1_h0, b1_h1;  // Z = B V, FP16: A = Bt_h2, B = V_h
 };
 
+// ---- grouped steps: many independent problems, one set of launches per step
+//
+// A problem is one batch of starting points on one resident matrix (its own
+// formulation, s or gamma, tolerance, max_iter and precision).  Its device
+// state is a GProblem; every kernel of a grouped step reads the list of the
+// problems it serves from a GPlan that the step's first kernel writes, and
+// loops over their work items (columns, groups of columns or GEMM tiles) with
+// a grid sized to the GPU, not to the problems.  Every problem's arithmetic is
+// a function of that problem alone (its own tiles, split-K and reduction
+// order), so its result is the same bit for bit whatever else runs beside it.
+enum GList : int {
+  GL_GG0 = 0,  // sparse V with at most 1024 non-zeros: ceil(k / 4) items, by mode 0..2
+  GL_GG1,
+  GL_GG2,
+  GL_GA0,      // sparse V with more non-zeros: k items, by mode
+  GL_GA1,
+  GL_GA2,
+  GL_DN0,      // dense V (densify, then the split-K reduction): k items, by mode
+  GL_DN1,
+  GL_DN2,
+  GL_SEL_HARD,   // k (top-s)
+  GL_SEL_SCAN,   // k (L1 ball, the reference's scan)
+  GL_SEL_EXACT,  // k (L1 ball, exact)
+  GL_SUPPORT,    // k (MIXED support stability)
+  GL_FIN,        // ceil(k / 8)
+  GL_GEMM1_64,   // units of Z = B V on dense steps, by N tile (64, 128, 256)
+  GL_GEMM1_128,
+  GL_GEMM1_256,
+  GL_RAW_64,     // units of V = B^T Z, by epilogue (raw: the constraints; L1 / L0
+  GL_RAW_128,    // penalty) and N tile
+  GL_RAW_256,
+  GL_PL1_64,
+  GL_PL1_128,
+  GL_PL1_256,
+  GL_PL0_64,
+  GL_PL0_128,
+  GL_PL0_256,
+  GL_COUNT
+};
+// Epilogue of a grouped product's launch.
+enum GEpi : int { GE_PARTIAL = 0, GE_RAW = 1, GE_PL1 = 2, GE_PL0 = 3 };
+constexpr int FIN_STARTS = 8;  // starts per finalize item (a warp each)
+
+// Operand schemes of the grouped V = B^T Z, chosen per problem and step.
+enum GScheme : int { GS_FP16X3 = 0, GS_FP16X2A = 1, GS_BF16X1 = 2 };
+
+// The tensor maps of one problem (a separate, 64-byte aligned table).
+struct alignas(64) GMaps {
+  CUtensorMap a1_h0, a1_h1, b1_h0, b1_h1;  // Z = B V: Bt FP16 planes, V FP16 planes
+  CUtensorMap a2_h0, a2_h1, b2_h0, b2_h1;  // V = B^T Z: Bc FP16 planes, Z FP16 planes
+  CUtensorMap a2_b0, b2_b;                 // V = B^T Z, BF16 (MIXED): Bc b0 plane, Z BF16
+};
+
+struct GProblem {
+  int live;  // 0: a free slot
+  // matrix
+  int m, n, ldm, ldn;
+  const float *Bc;
+  const float *row_scale, *bt_row_scale;  // FP16 plane scales of Bc (features), Bt (samples)
+  // settings
+  int k, formulation, mode;  // mode: 0 L2-variance constrained, 1 L1 variance, 2 L2 penalized
+  int l1_exact, mixed, max_iter;
+  unsigned constraint;
+  float gamma;
+  double tolerance;
+  uint32_t sparse_cap, k_stable, need_stable;
+  // tiles
+  int bn;                          // N tile of both products (64, 128 or 256)
+  int m_tiles1, n_tiles1, splits1, kb_per_split1;  // Z = B V (pair tiles, K blocks of 32)
+  int m_tiles2, n_tiles2;          // V = B^T Z
+  int parts;                       // m_tiles2 * 4 penalty partials per start
+  // state
+  float *Vx, *Vraw, *sel_hint, *Z_hi, *Z_lo, *fz, *obj_part, *nnz_part, *val, *err, *max_err;
+  float *z_scale, *v_scale, *ws;
+  uint32_t *vmask, *cmask, *nnz, *ctl, *stable, *phase;
+  uint64_t *mask_hash;  // MIXED: per start, a hash of the last step's support
+  uint16_t *Z_h, *Z_b, *V_h;
+  size_t zplane;  // k * ldm: the second FP16 plane of Z
+  int *status;
+};
+
+// Per-problem control words (GProblem::ctl), beyond the run-ahead words.
+enum : int {
+  GCTL_GATE = 8,     // the largest non-zero count of the previous step (this step's gate)
+  GCTL_NEXT = 9,     // ... of this step, formed by finalize
+  GCTL_SCHEME = 10,  // this step's GScheme for V = B^T Z
+  GCTL_SUPPORT = 11, // MIXED: this step's stable starts (scratch)
+  GCTL_SBLOCKS = 12, // MIXED: support items done (scratch)
+  GCTL_WORDS = 16
+};
+
+struct GPlan {
+  int n[GL_COUNT];      // problems in each list
+  int total[GL_COUNT];  // work items in each list
+  int active;           // problems that ran this step
+  int loops;            // steps run since the last launch began
+  int loop_cap;         // the launch stops after this many steps
+  int status;           // a device-side wait of a grouped kernel gave up
+};
+
+// Device arrays of a group, sized for `cap` problems.
+struct GroupDev {
+  int cap;
+  GProblem *probs;
+  const GMaps *maps;
+  GPlan *plan;
+  int *prob;  // [GL_COUNT][cap]: the problems of each list
+  int *pref;  // [GL_COUNT][cap + 1]: exclusive prefix of their items
+  unsigned long long timeout_ns;
+};
+
+// One grouped AM step of every live, unstopped problem; the plan kernel first.
+// grids: per-kernel persistent grid sizes (from grouped_grids()).
+struct GroupGrids {
+  int plan_threads, col, select_hard, select_soft, gather, gather_group, fin, pairs;
+};
+cudaError_t grouped_grids(GroupGrids *g);
+cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &grids, cudaStream_t st);
+// Sets the WHILE condition of a captured loop: 1 while some problem is live and
+// unstopped, the plan's loop count is below its cap and no wait gave up.
+cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handle,
+                                     cudaStream_t st);
+
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
 int num_sms();
 // Fills M's TF32 planes (Bc_hi/lo, Bt_hi/lo) from M.Bc.

@@ -457,16 +457,16 @@ __global__ void densify_kernel(const float *__restrict__ Vx, const uint32_t *__r
 // Dense FP16 planes of V for the CTA-pair Z = B V (split FP16 operands): on
 // dense steps only (*gate > gate_max), one block per start, v * 2^s = h0 + h1
 // with s from the column's largest |v|, v_scale[c] = 2^-s.
-__global__ void __launch_bounds__(256) densify_fp16_kernel(const float *__restrict__ Vx,
-                                                           const uint32_t *__restrict__ mask,
-                                                           int ld, int rows,
-                                                           uint16_t *__restrict__ Vh, size_t plane,
-                                                           float *__restrict__ v_scale,
-                                                           const uint32_t *gate, uint32_t gate_max,
-                                                           const uint32_t *stop) {
+// The body for start c (one 256-thread block); densify_fp16_kernel runs it for
+// blockIdx.x, the grouped steps for every start of their dense problems.
+__device__ __forceinline__ void densify_fp16_body(const float *__restrict__ Vx,
+                                                  const uint32_t *__restrict__ mask, int ld,
+                                                  int rows, uint16_t *__restrict__ Vh,
+                                                  size_t plane, float *__restrict__ v_scale,
+                                                  const uint32_t *gate, uint32_t gate_max,
+                                                  const uint32_t *stop, size_t c) {
   __shared__ uint32_t red[8];
   if (*stop || *gate <= gate_max) return;
-  const size_t c = blockIdx.x;
   const uint32_t *mk = mask + c * (ld >> 5);
   const float4 *vx4 = reinterpret_cast<const float4 *>(Vx + c * ld);
   // four consecutive rows per thread and pass (ld is a multiple of 32)
@@ -508,25 +508,32 @@ __global__ void __launch_bounds__(256) densify_fp16_kernel(const float *__restri
     h1[q] = make_uint2(b[0] | ((uint32_t)b[1] << 16), b[2] | ((uint32_t)b[3] << 16));
   }
 }
+__global__ void __launch_bounds__(256) densify_fp16_kernel(const float *__restrict__ Vx,
+                                                           const uint32_t *__restrict__ mask,
+                                                           int ld, int rows,
+                                                           uint16_t *__restrict__ Vh, size_t plane,
+                                                           float *__restrict__ v_scale,
+                                                           const uint32_t *gate, uint32_t gate_max,
+                                                           const uint32_t *stop) {
+  densify_fp16_body(Vx, mask, ld, rows, Vh, plane, v_scale, gate, gate_max, stop, blockIdx.x);
+}
 
 // ------------------------------------------------------------ Z reduction
 // MODE 0: L2 variance, constrained  -> z = y, fz = ||y||_2  (gpower_commons.h:100)
 // MODE 1: L1 variance               -> z = sgn(y), fz = ||y||_1 (:85-86, :156)
 // MODE 2: L2 variance, penalized    -> z = y * (1/||y||_2)     (:163-164)
 template <int MODE>
-__global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__ ws, int splits,
-                                                       int m_tiles, int n_tiles, int bn, int m,
-                                                       float *__restrict__ Z_hi,
-                                                       float *__restrict__ Z_lo, int ldm,
-                                                       float *__restrict__ fz,
-                                                       const uint32_t *gate, uint32_t gate_max,
-                                                       uint16_t *__restrict__ Zb,
-                                                       uint16_t *__restrict__ Zh, size_t zplane,
-                                                       float *__restrict__ zscale,
-                                                       const uint32_t *stop) {
+__device__ __forceinline__ void z_reduce_body(const float *__restrict__ ws, int splits,
+                                              int m_tiles, int n_tiles, int bn, int m,
+                                              float *__restrict__ Z_hi, float *__restrict__ Z_lo,
+                                              int ldm, float *__restrict__ fz,
+                                              const uint32_t *gate, uint32_t gate_max,
+                                              uint16_t *__restrict__ Zb,
+                                              uint16_t *__restrict__ Zh, size_t zplane,
+                                              float *__restrict__ zscale, const uint32_t *stop,
+                                              int j) {
   __shared__ double red[32];
   if (*stop || *gate <= gate_max) return;  // the gather kernel produced Z this step
-  const int j = blockIdx.x;
   const int nt = j / bn, c = j - nt * bn;
   const size_t unit_stride = (size_t)bn * BM;
   float *zh = Z_hi + (size_t)j * ldm;
@@ -570,6 +577,20 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
     if (Zh && threadIdx.x == 0) zscale[j] = pow2f(-s);
   }
   if (MODE != 2 && threadIdx.x == 0) fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
+}
+template <int MODE>
+__global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__ ws, int splits,
+                                                       int m_tiles, int n_tiles, int bn, int m,
+                                                       float *__restrict__ Z_hi,
+                                                       float *__restrict__ Z_lo, int ldm,
+                                                       float *__restrict__ fz,
+                                                       const uint32_t *gate, uint32_t gate_max,
+                                                       uint16_t *__restrict__ Zb,
+                                                       uint16_t *__restrict__ Zh, size_t zplane,
+                                                       float *__restrict__ zscale,
+                                                       const uint32_t *stop) {
+  z_reduce_body<MODE>(ws, splits, m_tiles, n_tiles, bn, m, Z_hi, Z_lo, ldm, fz, gate, gate_max,
+                      Zb, Zh, zplane, zscale, stop, blockIdx.x);
 }
 
 // ------------------------------------------------------------ sparse Z = B V
@@ -616,19 +637,18 @@ __global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict
 // that fixed order (deterministic), and the same sign / norm / normalise
 // step as z_reduce_kernel<MODE> finishes the column.
 template <int MODE>
-__global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
+__device__ __forceinline__ void gather_bv_body(
     const float *__restrict__ Bc, int ldm, int m, int ldn,
     const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
     float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
     uint16_t *__restrict__ Zb, uint16_t *__restrict__ Zh, size_t zplane,
-    float *__restrict__ zscale, const uint32_t *stop) {
+    float *__restrict__ zscale, const uint32_t *stop, int j) {
   __shared__ int idx[GATHER_CAP];
   __shared__ float val[GATHER_CAP];
   __shared__ uint32_t wsum[GATHER_THREADS / 32];
   __shared__ double red[32];
   // dense V (gemm1 + z_reduce), or few enough non-zeros for gather_bv_group_kernel
   if (*stop || *gate > gate_max || *gate <= min(gate_max, GATHER_GROUP_MAX_NNZ)) return;
-  const int j = blockIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int words = ldn >> 5;
   const uint32_t *mk = vmask + (size_t)j * words;
@@ -772,6 +792,16 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
   }
   if (MODE != 2 && threadIdx.x == 0) fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
 }
+template <int MODE>
+__global__ void __launch_bounds__(GATHER_THREADS) gather_bv_kernel(
+    const float *__restrict__ Bc, int ldm, int m, int ldn,
+    const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
+    float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
+    uint16_t *__restrict__ Zb, uint16_t *__restrict__ Zh, size_t zplane,
+    float *__restrict__ zscale, const uint32_t *stop) {
+  gather_bv_body<MODE>(Bc, ldm, m, ldn, Vx, vmask, Z_hi, Z_lo, fz, gate, gate_max, Zb, Zh, zplane,
+                       zscale, stop, blockIdx.x);
+}
 
 // The sparse Z = B V for GATHER_GROUP starts per block, while every column
 // has at most GATHER_CAP / GATHER_GROUP non-zeros (*gate): the block lists the
@@ -786,12 +816,12 @@ constexpr size_t GATHER_GROUP_SMEM =
     (size_t)GATHER_CAP * (sizeof(int) + GATHER_GROUP * sizeof(float) + 1);
 
 template <int MODE>
-__global__ void __launch_bounds__(GATHER_THREADS) gather_bv_group_kernel(
+__device__ __forceinline__ void gather_bv_group_body(
     const float *__restrict__ Bc, int ldm, int m, int ldn, int k,
     const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
     float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
     uint16_t *__restrict__ Zb, uint16_t *__restrict__ Zh, size_t zplane,
-    float *__restrict__ zscale, const uint32_t *stop) {
+    float *__restrict__ zscale, const uint32_t *stop, int group) {
   constexpr int G = GATHER_GROUP;
   extern __shared__ __align__(16) uint8_t gsm[];
   int *idx = reinterpret_cast<int *>(gsm);                                  // GATHER_CAP
@@ -801,7 +831,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_group_kernel(
   __shared__ double red[32];
   // dense V (gemm1 + z_reduce), or gather_bv_kernel's case
   if (*stop || *gate > min(gate_max, GATHER_GROUP_MAX_NNZ)) return;
-  const int j0 = blockIdx.x * G;
+  const int j0 = group * G;
   const int ng = min(G, k - j0);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int words = ldn >> 5;
@@ -987,6 +1017,16 @@ __global__ void __launch_bounds__(GATHER_THREADS) gather_bv_group_kernel(
     }
     if (MODE != 2 && threadIdx.x == 0) fz[j] = (MODE == 1) ? (float)tot : (float)sqrt(tot);
   }
+}
+template <int MODE>
+__global__ void __launch_bounds__(GATHER_THREADS) gather_bv_group_kernel(
+    const float *__restrict__ Bc, int ldm, int m, int ldn, int k,
+    const float *__restrict__ Vx, const uint32_t *__restrict__ vmask, float *__restrict__ Z_hi,
+    float *__restrict__ Z_lo, float *__restrict__ fz, const uint32_t *gate, uint32_t gate_max,
+    uint16_t *__restrict__ Zb, uint16_t *__restrict__ Zh, size_t zplane,
+    float *__restrict__ zscale, const uint32_t *stop) {
+  gather_bv_group_body<MODE>(Bc, ldm, m, ldn, k, Vx, vmask, Z_hi, Z_lo, fz, gate, gate_max, Zb,
+                             Zh, zplane, zscale, stop, blockIdx.x);
 }
 
 // ------------------------------------------------------------ radix select
@@ -1284,17 +1324,16 @@ __device__ uint32_t gather_pairs_above(const float *__restrict__ colg, int n, ui
 // in it are gathered and sorted; a bin too full for shared memory falls back
 // to (c) the exact three-level radix select; the column is then written by a
 // full pass.
-__global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
+__device__ __forceinline__ void hard_select_body(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
-    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask) {
+    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask, int j) {
   if (*stop) return;
   __shared__ uint64_t cand[HARD_CAND];  // also 2 * HARD_CAND keys for (b)
   __shared__ uint32_t hist[2048];
   __shared__ uint32_t res[8];
   __shared__ double red[32];
   uint32_t *cand32 = reinterpret_cast<uint32_t *>(cand);
-  const int j = blockIdx.x;
   const float *colg = Vraw + (size_t)j * ldv;
   float *vx = Vx + (size_t)j * ldv;
   uint32_t *mk = vmask + (size_t)j * (ldv >> 5);
@@ -1414,6 +1453,12 @@ __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
     hints[j] = __uint_as_float(thr);
     nnz_out[j] = (uint32_t)cnt;
   }
+}
+__global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
+    const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
+    uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
+    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask) {
+  hard_select_body(Vraw, ldv, n, s, Vx, nnz_out, status, vmask, hints, stop, cmask, blockIdx.x);
 }
 
 // ------------------------------------------------------------ L1 constraint
@@ -1609,10 +1654,10 @@ __device__ uint32_t resolve_stop(uint32_t best, double bw, uint32_t *res,
 // ||.||_1/||.||_2 >= sqrt(s) and take the root inside it -- the exact
 // L1-ball / unit-sphere projection.
 template <bool EXACT>
-__global__ void __launch_bounds__(SOFT_THREADS, 4) soft_select_kernel(
+__device__ __forceinline__ void soft_select_body(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
-    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask) {
+    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask, int j) {
   if (*stop) return;
   __shared__ uint64_t pairs[SOFT_C];  // hinted (key, index) candidates
   __shared__ float cand[SOFT_C];
@@ -1625,7 +1670,6 @@ __global__ void __launch_bounds__(SOFT_THREADS, 4) soft_select_kernel(
   volatile uint32_t *misc = misc_raw;
   double *w_sh = &w_shared;
 
-  const int j = blockIdx.x;
   const float *colg = Vraw + (size_t)j * ldv;
   // sqrt(s), sqrt(s)^2 as the double-precision reference forms them
   const double sq = __dsqrt_rn((double)s);
@@ -1857,6 +1901,14 @@ __global__ void __launch_bounds__(SOFT_THREADS, 4) soft_select_kernel(
   if (threadIdx.x == 0) {
     nnz_out[j] = (uint32_t)cnt;
   }
+}
+template <bool EXACT>
+__global__ void __launch_bounds__(SOFT_THREADS, 4) soft_select_kernel(
+    const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
+    uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
+    float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask) {
+  soft_select_body<EXACT>(Vraw, ldv, n, s, Vx, nnz_out, status, vmask, hints, stop, cmask,
+                          blockIdx.x);
 }
 
 // ------------------------------------------------------------ finalize
@@ -2584,6 +2636,118 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (ev && (e = cudaEventRecord(ev[nl], st)) != cudaSuccess) return e;
   if (launches) *launches = nl;
   return cudaSuccess;
+}
+
+// ------------------------------------------------------------ grouped steps
+#include "gemm_pair_grouped.cuh"
+#include "am24_group_kernels.cuh"
+
+namespace {
+
+template <class K>
+cudaError_t persistent_grid(K kern, int threads, int smem, int *grid) {
+  int per = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (void *)kern, threads, smem);
+  if (e != cudaSuccess) return e;
+  *grid = num_sms() * (per > 0 ? per : 1);
+  return cudaSuccess;
+}
+
+template <int BN, int EPI>
+cudaError_t grouped_gemm_setup(int *clusters) {
+  return kernel_setup(gemm_pair_grouped_kernel<BN, EPI>, GPairSmem<BN>::TOTAL, true, clusters);
+}
+
+template <int BN, int EPI>
+cudaError_t launch_grouped_gemm(const GroupDev &g, int list, cudaStream_t st) {
+  int clusters = 0;
+  const cudaError_t e = grouped_gemm_setup<BN, EPI>(&clusters);
+  if (e != cudaSuccess) return e;
+  gemm_pair_grouped_kernel<BN, EPI>
+      <<<2 * clusters, GEMM_THREADS, GPairSmem<BN>::TOTAL, st>>>(g, list);
+  return cudaGetLastError();
+}
+
+// The three N tiles of one epilogue, lists l64, l64 + 1, l64 + 2.
+template <int EPI>
+cudaError_t launch_grouped_gemms(const GroupDev &g, int l64, cudaStream_t st) {
+  cudaError_t e;
+  if ((e = launch_grouped_gemm<64, EPI>(g, l64, st)) ||
+      (e = launch_grouped_gemm<128, EPI>(g, l64 + 1, st)) ||
+      (e = launch_grouped_gemm<256, EPI>(g, l64 + 2, st)))
+    return e;
+  return cudaSuccess;
+}
+
+template <int EPI>
+cudaError_t grouped_gemms_setup(int *c) {
+  cudaError_t e;
+  if ((e = grouped_gemm_setup<64, EPI>(c)) || (e = grouped_gemm_setup<128, EPI>(c)) ||
+      (e = grouped_gemm_setup<256, EPI>(c)))
+    return e;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t grouped_grids(GroupGrids *gr) {
+  cudaError_t e;
+  if ((e = kernel_setup(g_gather_group_kernel<0>, (int)GATHER_GROUP_SMEM, false)) ||
+      (e = kernel_setup(g_gather_group_kernel<1>, (int)GATHER_GROUP_SMEM, false)) ||
+      (e = kernel_setup(g_gather_group_kernel<2>, (int)GATHER_GROUP_SMEM, false)))
+    return e;
+  int c = 0;
+  if ((e = grouped_gemms_setup<GE_PARTIAL>(&c)) || (e = grouped_gemms_setup<GE_RAW>(&c)) ||
+      (e = grouped_gemms_setup<GE_PL1>(&c)) || (e = grouped_gemms_setup<GE_PL0>(&c)))
+    return e;
+  gr->plan_threads = PLAN_THREADS;
+  gr->pairs = c;
+  if ((e = persistent_grid(g_densify_kernel, 256, 0, &gr->col)) ||
+      (e = persistent_grid(g_hard_select_kernel, HARD_THREADS, 0, &gr->select_hard)) ||
+      (e = persistent_grid(g_soft_select_kernel<false>, SOFT_THREADS, 0, &gr->select_soft)) ||
+      (e = persistent_grid(g_gather_kernel<0>, GATHER_THREADS, 0, &gr->gather)) ||
+      (e = persistent_grid(g_gather_group_kernel<0>, GATHER_THREADS, (int)GATHER_GROUP_SMEM,
+                           &gr->gather_group)) ||
+      (e = persistent_grid(g_finalize_kernel, 256, 0, &gr->fin)))
+    return e;
+  return cudaSuccess;
+}
+
+cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &gr, cudaStream_t st) {
+  cudaError_t e;
+  group_plan_kernel<<<1, PLAN_THREADS, 0, st>>>(g);
+  if ((e = cudaGetLastError())) return e;
+  // Z = B V: the sparse gathers (by mode), or the dense path
+  g_gather_group_kernel<0><<<gr.gather_group, GATHER_THREADS, GATHER_GROUP_SMEM, st>>>(g);
+  g_gather_group_kernel<1><<<gr.gather_group, GATHER_THREADS, GATHER_GROUP_SMEM, st>>>(g);
+  g_gather_group_kernel<2><<<gr.gather_group, GATHER_THREADS, GATHER_GROUP_SMEM, st>>>(g);
+  g_gather_kernel<0><<<gr.gather, GATHER_THREADS, 0, st>>>(g);
+  g_gather_kernel<1><<<gr.gather, GATHER_THREADS, 0, st>>>(g);
+  g_gather_kernel<2><<<gr.gather, GATHER_THREADS, 0, st>>>(g);
+  for (int mode = 0; mode < 3; mode++) g_densify_kernel<<<gr.col, 256, 0, st>>>(g, mode);
+  if ((e = cudaGetLastError())) return e;
+  if ((e = launch_grouped_gemms<GE_PARTIAL>(g, GL_GEMM1_64, st))) return e;
+  g_z_reduce_kernel<0><<<gr.col, 256, 0, st>>>(g);
+  g_z_reduce_kernel<1><<<gr.col, 256, 0, st>>>(g);
+  g_z_reduce_kernel<2><<<gr.col, 256, 0, st>>>(g);
+  if ((e = cudaGetLastError())) return e;
+  // V = B^T Z with the penalty fused or the raw output marked for the selects
+  if ((e = launch_grouped_gemms<GE_RAW>(g, GL_RAW_64, st)) ||
+      (e = launch_grouped_gemms<GE_PL1>(g, GL_PL1_64, st)) ||
+      (e = launch_grouped_gemms<GE_PL0>(g, GL_PL0_64, st)))
+    return e;
+  g_hard_select_kernel<<<gr.select_hard, HARD_THREADS, 0, st>>>(g);
+  g_soft_select_kernel<false><<<gr.select_soft, SOFT_THREADS, 0, st>>>(g);
+  g_soft_select_kernel<true><<<gr.select_soft, SOFT_THREADS, 0, st>>>(g);
+  g_support_kernel<<<gr.col, 256, 0, st>>>(g);
+  g_finalize_kernel<<<gr.fin, 256, 0, st>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handle,
+                                     cudaStream_t st) {
+  g_condition_kernel<<<1, 256, 0, st>>>(g, (cudaGraphConditionalHandle)handle);
+  return cudaGetLastError();
 }
 
 }  // namespace am24

@@ -312,6 +312,54 @@ am24_status am24_poll(am24_server s, uint64_t ticket, float *x, am24_statistics 
 /* Blocking form of am24_poll. */
 am24_status am24_wait(am24_server s, uint64_t ticket, float *x, am24_statistics *stats);
 
+/* ---- groups: many independent problems in one set of launches per step --- */
+/* No counterpart in the reference, which solves one problem per call; its
+ * batch loop (c++/src/gpower/sparse_PCA_solver.h:171-232) is what each
+ * problem of a group runs.  A group holds up to `capacity` problems of uneven
+ * shape: each is one batch of starting points on a resident matrix with its
+ * own settings (formulation, s or gamma, tolerance, max_iter, precision).  A
+ * run repeats one grouped AM step for every problem that still iterates --
+ * one plan kernel, then each product of all problems' tiles as one persistent
+ * grouped tensor-core kernel (CTA pairs, split FP16 operands, or single-pass
+ * BF16 in a MIXED problem's first phase) and every per-start pass as one
+ * kernel over all problems' starts -- inside one captured CUDA graph whose
+ * WHILE node loops on the device until every problem has stopped, with no
+ * host round trip per step.  Each problem stops as a reference batch does
+ * (it > 0, largest change below the tolerance, in the refinement phase; or
+ * max_iter steps).  Its tiles, split-K and reduction order depend on it
+ * alone, so its result is the same bit for bit alone and among others.
+ * A group belongs to one handle and runs on its stream. */
+typedef struct am24_group_s *am24_group;
+am24_status am24_group_create(am24_handle h, uint32_t capacity, am24_group *out);
+/* Waits for the handle's stream, then frees every problem and the group. */
+am24_status am24_group_destroy(am24_group g);
+/* Adds one problem on resident matrix `mat` (which must outlive it): all of
+ * settings->total_starts starting points (after am24_check_input) form one
+ * batch.  start_mode REFERENCE, INJECTED (start_points: n x total_starts host
+ * floats, copied) or DEVICE_UNIFORM; use_otf and store_all are not supported.
+ * The problem's device memory comes from the handle's stream-ordered pool.
+ * *problem receives its id (a slot index below capacity). */
+am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *settings,
+                           const float *start_points, uint32_t *problem);
+/* Runs grouped steps of every added problem that has not stopped, until all
+ * have stopped, or for at most max_steps steps when max_steps > 0.  One graph
+ * launch; synchronizes the stream.  *device_ms (may be NULL) receives the
+ * launch's device time (CUDA events on the handle's stream). */
+am24_status am24_group_run(am24_group g, uint32_t max_steps, float *device_ms);
+/* *stopped = 1 once the problem has stopped iterating, *steps its steps. */
+am24_status am24_group_state(am24_group g, uint32_t problem, int32_t *stopped, uint32_t *steps);
+/* The problem's best start (the largest objective, the first on ties),
+ * normalised, into x (n floats), and its statistics (it = steps, fval, error,
+ * explained_variance in FP64 on the device, start_iterations,
+ * low_precision_iterations, degenerate_starts; times are the last run's). */
+am24_status am24_group_result(am24_group g, uint32_t problem, float *x, am24_statistics *stats);
+/* As am24_batch_read: the problem's loadings (n x k), objectives, changes and
+ * non-zero counts (any pointer may be NULL). */
+am24_status am24_group_read(am24_group g, uint32_t problem, float *V, float *val, float *err,
+                            uint32_t *nnz);
+/* Frees the problem's slot and device memory. */
+am24_status am24_group_remove(am24_group g, uint32_t problem);
+
 /* Kernel kinds reported by am24_batch_step_timed. */
 typedef enum {
   AM24_KERNEL_GEMM_BV = 0,   /* Z = B V, tensor cores, split-K partial tiles */
