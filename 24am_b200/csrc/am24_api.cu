@@ -74,19 +74,25 @@ am24_status make_map_bf16(am24_handle h, CUtensorMap *map, const uint16_t *base,
   return AM24_OK;
 }
 
-// The matrix's three BF16 planes of B (made once, on first use).
-am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat) {
+// The matrix's BF16 planes of B (made on first use): `planes` = 1 for b0
+// alone (the single-pass BF16 product of MIXED), 3 for the exact split.  A
+// matrix holding one plane that is asked for three gets a new buffer of three.
+am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat, int planes) {
   MatrixDev &M = mat->d;
-  if (M.Bc_b3) return AM24_OK;
+  if (M.Bc_b3 && M.bf16_planes >= planes) return AM24_OK;
   const size_t plane = (size_t)M.n * M.ldm;
   uint16_t *p = nullptr;
-  AM24_TRY(mat->mem.get(&p, 3 * plane));
-  AM24_CUDA(cudaMemsetAsync(p, 0, sizeof(uint16_t) * 3 * plane, h->stream));
+  AM24_TRY(mat->mem.get(&p, (size_t)planes * plane));
+  AM24_CUDA(cudaMemsetAsync(p, 0, sizeof(uint16_t) * planes * plane, h->stream));
+  uint16_t *old = M.Bc_b3;
+  const int old_planes = M.bf16_planes;
   M.Bc_b3 = p;
+  M.bf16_planes = planes;
   cudaError_t e = launch_prep_bf16x3(M, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
-    M.Bc_b3 = nullptr;
+    M.Bc_b3 = old;
+    M.bf16_planes = old_planes;
     return fail(AM24_ERR_CUDA, std::string("BF16 planes: ") + cudaGetErrorString(e));
   }
   return AM24_OK;
@@ -780,7 +786,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.max_nnz, 1)) || (st = A.get(&d.planes_nnz, 1)) ||
       (st = A.get(&d.sel_hint, k)) || (st = A.get(&d.ctl, (size_t)CTL_WORDS)) ||
       (lists && (st = A.get(&d.cmask, (size_t)k * (M.ldn / 32)))) ||
-      (need_bf16 && ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat)))) ||
+      (need_bf16 &&
+       ((st = A.get(&d.Z_b, kz)) || (st = ensure_bf16_planes(h, mat, d.bf16_2 ? 3 : 1)))) ||
       (d.fp16_2 && ((st = A.get(&d.Z_h, zh_planes * kz)) || (st = A.get(&d.z_scale, k)) ||
                     (st = ensure_fp16_planes(h, mat)))) ||
       (d.fp16_1 && ((st = A.get(&d.V_h, 2 * kv)) || (st = A.get(&d.v_scale, k)) ||
@@ -842,8 +849,9 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (need_bf16) {
     const size_t plane = (size_t)M.n * M.ldm;
     if ((st = make_map_bf16(h, &b->tm.a2_b0, M.Bc_b3, M.m, M.n, M.ldm, BM)) ||
-        (st = make_map_bf16(h, &b->tm.a2_b1, M.Bc_b3 + plane, M.m, M.n, M.ldm, BM)) ||
-        (st = make_map_bf16(h, &b->tm.a2_b2, M.Bc_b3 + 2 * plane, M.m, M.n, M.ldm, BM)) ||
+        (d.bf16_2 &&
+         ((st = make_map_bf16(h, &b->tm.a2_b1, M.Bc_b3 + plane, M.m, M.n, M.ldm, BM)) ||
+          (st = make_map_bf16(h, &b->tm.a2_b2, M.Bc_b3 + 2 * plane, M.m, M.n, M.ldm, BM)))) ||
         (st = make_map_bf16(h, &b->tm.b2_b, d.Z_b, M.m, k, M.ldm, d.bn2 / 2))) {
       delete b;
       return st;
@@ -1407,448 +1415,6 @@ am24_status am24_solve_dense_f64(am24_handle h, const double *B, int32_t ldB, do
   for (uint32_t i = 0; i < n; i++) x[i] = xf[i];
   if (fval_out) *fval_out = f;
   return AM24_OK;
-}
-
-}  // extern "C"
-
-// ---- serving ---------------------------------------------------------------
-namespace {
-
-struct ServeRequest {
-  uint64_t ticket = 0;
-  uint32_t matrix_id = 0;
-  am24_settings s{};          // after am24_check_input, one batch of all starts
-  std::vector<float> starts;  // n x total_starts (injected starts only)
-  std::chrono::steady_clock::time_point submitted;
-  bool done = false;
-  am24_status status = AM24_OK;
-  std::string error;
-  std::vector<float> x;
-  am24_statistics stats{};
-};
-using RequestPtr = std::shared_ptr<ServeRequest>;
-
-// Requests that may share one batch: same matrix, same step.
-bool same_step(const ServeRequest &a, const ServeRequest &b) {
-  return a.matrix_id == b.matrix_id && a.s.formulation == b.s.formulation &&
-         a.s.constraint == b.s.constraint && a.s.penalty == b.s.penalty &&
-         a.s.tolerance == b.s.tolerance && a.s.max_iter == b.s.max_iter &&
-         a.s.l1_mode == b.s.l1_mode && a.s.precision == b.s.precision &&
-         a.s.stable_iterations == b.s.stable_iterations &&
-         a.s.stable_share == b.s.stable_share && a.s.timeout_ms == b.s.timeout_ms;
-}
-
-// Device bytes of a matrix's layouts (the BF16 and FP16 planes included:
-// batches add them on first use).
-uint64_t matrix_bytes(uint32_t m, uint32_t n) {
-  const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
-  return 4ull * (2 * n * ldm + 2 * m * ldn + n * ldm) + 2ull * 3 * n * ldm +
-         2ull * 2 * n * ldm + 4ull * n + 2ull * 2 * m * ldn + 4ull * m;
-}
-
-// Device bytes of a batch of k starts on an m x n matrix (an upper estimate).
-uint64_t batch_bytes(uint32_t m, uint32_t n, uint32_t k) {
-  const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
-  const uint64_t kv = (uint64_t)k * ldn, kz = (uint64_t)k * ldm;
-  const uint64_t ws = 2ull * ((m + 127) / 128) * ((k + 63) / 64 + 3) * 256 * 128 * 4 * 8;
-  return 4 * kv * 4 + 2 * kv * 2 + 2 * kz * 4 + kz * 2 + 2 * kz * 2 + 2 * (kv / 32) * 4 + ws +
-         kv / 8 +
-         (uint64_t)k * 256 + (4ull << 20);
-}
-
-}  // namespace
-
-// One worker thread: its own handle (stream) and its last batch, reused while
-// the matrix, the batch size and the batch-shaping settings stay the same.
-struct ServeWorker {
-  am24_handle h = nullptr;
-  std::thread thread;
-  am24_batch cached = nullptr;
-  uint32_t cached_matrix = 0, cached_k = 0;
-  am24_settings cached_s{};
-};
-
-struct am24_server_s {
-  std::vector<ServeWorker> workers;  // each used by its own thread only
-  am24_handle upload_h = nullptr;    // matrix uploads from callers' threads
-  std::mutex upload_mu;
-  std::mutex create_mu;  // batch creation (it may add BF16 planes to a shared matrix)
-  uint64_t budget = 0;
-  std::mutex mu;  // everything below
-  std::condition_variable cv_work, cv_done;
-  struct Resident {
-    am24_matrix mat;
-    uint64_t bytes;
-    uint32_t m, n;
-    int pending;
-  };
-  std::map<uint32_t, Resident> matrices;
-  uint64_t resident = 0;
-  uint32_t next_matrix = 1;
-  uint64_t next_ticket = 1;
-  std::deque<RequestPtr> queue;
-  std::map<uint64_t, RequestPtr> tickets;
-  uint64_t inflight = 0;  // device bytes of the batches the workers are running
-  bool stop = false;
-  uint32_t max_batch = 8192;
-};
-
-namespace {
-
-// Runs one batch made of the requests' starts (worker thread).
-am24_status run_group(am24_server s, ServeWorker &w, am24_matrix mat, uint32_t matrix_id,
-                      std::vector<RequestPtr> &group) {
-  am24_handle h = w.h;
-  const MatrixDev &M = mat->d;
-  const unsigned n = (unsigned)M.n;
-  uint32_t K = 0;
-  for (auto &r : group) K += (uint32_t)r->s.total_starts;
-  am24_settings bs = group[0]->s;
-  bs.total_starts = (int32_t)K;
-  bs.batch_size = (int32_t)K;
-  bs.total_batches = 1;
-  bs.use_otf = 0;
-  bs.store_all = 0;
-  if (!(w.cached && w.cached_matrix == matrix_id && w.cached_k == K &&
-        w.cached_s.formulation == bs.formulation && w.cached_s.precision == bs.precision &&
-        w.cached_s.stable_iterations == bs.stable_iterations &&
-        w.cached_s.stable_share == bs.stable_share)) {
-    if (w.cached) am24_batch_destroy(h, w.cached);
-    w.cached = nullptr;
-    std::lock_guard<std::mutex> lk(s->create_mu);
-    AM24_TRY(am24_batch_create(h, mat, &bs, K, &w.cached));
-    w.cached_matrix = matrix_id;
-    w.cached_k = K;
-    w.cached_s = bs;
-  }
-  am24_batch b = w.cached;
-  b->s = bs;  // the step parameters of this group (penalty, tolerance, ...)
-  const BatchDev &d = b->d;
-  // starts: each request's own (injected, the reference generator or the
-  // device generator, by the request's own start indices), one segment after
-  // the other in the batch's staging plane
-  std::vector<float> seg;
-  uint32_t off = 0;
-  for (auto &r : group) {
-    const uint32_t k = (uint32_t)r->s.total_starts;
-    float *dst = d.Vraw + (size_t)off * M.ldn;
-    if (r->s.start_mode == AM24_START_DEVICE_UNIFORM) {
-      AM24_CUDA(launch_uniform_starts(dst, M.ldn, (int)n, (int)k, 0, h->stream));
-    } else {
-      std::vector<unsigned> gidx(k);
-      for (uint32_t i = 0; i < k; i++) gidx[i] = i;
-      host_starts(r->s, n, r->starts.empty() ? nullptr : r->starts.data(), gidx.data(), (int)k,
-                  seg);
-      AM24_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * M.ldn, seg.data(), sizeof(float) * n,
-                                  sizeof(float) * n, k, cudaMemcpyHostToDevice, h->stream));
-      AM24_CUDA(cudaStreamSynchronize(h->stream));  // `seg` is reused
-    }
-    off += k;
-  }
-  AM24_TRY(load_from_vraw(h, b));
-  cudaEvent_t e0, e1;
-  AM24_CUDA(cudaEventCreate(&e0));
-  AM24_CUDA(cudaEventCreate(&e1));
-  struct EvGuard {
-    cudaEvent_t a, c;
-    ~EvGuard() {
-      cudaEventDestroy(a);
-      cudaEventDestroy(c);
-    }
-  } evg{e0, e1};
-  AM24_CUDA(cudaEventRecord(e0, h->stream));
-  BatchRun run;
-  AM24_TRY(run_batch_steps(h, b, bs, 0, &run));
-  AM24_CUDA(cudaEventRecord(e1, h->stream));
-  const int it = run.steps;
-  const uint32_t low_its = run.low_steps;
-  const float max_err = run.max_err;
-  std::vector<float> val(K);
-  AM24_CUDA(cudaMemcpyAsync(val.data(), d.val, sizeof(float) * K, cudaMemcpyDeviceToHost,
-                            h->stream));
-  AM24_CUDA(cudaStreamSynchronize(h->stream));
-  float ms = 0.f;
-  AM24_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  // per request: the best of its own starts, normalised, and its ||B x||^2
-  Allocs local(h->stream);
-  float *xb = nullptr, *x_dev = nullptr;
-  double *ev_rows = nullptr;
-  AM24_TRY(local.get(&xb, n));
-  AM24_TRY(local.get(&x_dev, n));
-  AM24_TRY(local.get(&ev_rows, ev_partial_len(M)));
-  off = 0;
-  for (auto &r : group) {
-    const uint32_t k = (uint32_t)r->s.total_starts;
-    uint32_t sel = 0;
-    float bv = val[off];
-    int degenerate = std::isnan(val[off]) ? 1 : 0;
-    for (uint32_t i = 1; i < k; i++) {
-      degenerate += std::isnan(val[off + i]) ? 1 : 0;
-      if (val[off + i] > bv) {
-        bv = val[off + i];
-        sel = i;
-      }
-    }
-    const uint32_t j = off + sel;
-    AM24_CUDA(launch_masked_copy(d.Vx + (size_t)j * M.ldn, d.vmask + (size_t)j * (M.ldn / 32),
-                                 M.ldn, (int)n, 1, xb, (int)n, h->stream));
-    AM24_CUDA(launch_finalize_x(xb, (int)n, x_dev, h->stream));
-    AM24_CUDA(launch_explained_variance(M, x_dev, ev_rows, h->ev_out, h->stream));
-    r->x.resize(n);
-    double ev = 0.0;
-    AM24_CUDA(cudaMemcpyAsync(r->x.data(), x_dev, sizeof(float) * n, cudaMemcpyDeviceToHost,
-                              h->stream));
-    AM24_CUDA(cudaMemcpyAsync(&ev, h->ev_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    AM24_CUDA(cudaStreamSynchronize(h->stream));
-    am24_statistics &st = r->stats;
-    st = am24_statistics{};
-    st.it = (uint32_t)it;
-    st.fval = bv;
-    st.error = max_err;
-    st.total_true_computation_time = ms * 1e-3;
-    st.n = n;
-    st.total_threads_used = 1;
-    st.explained_variance = ev;
-    st.start_iterations = (uint64_t)k * (uint64_t)it;
-    st.degenerate_starts = degenerate;
-    st.low_precision_iterations = low_its;
-    off += k;
-  }
-  return AM24_OK;
-}
-
-void worker_loop(am24_server s, size_t wi) {
-  ServeWorker &w = s->workers[wi];
-  cudaSetDevice(w.h->device);
-  for (;;) {
-    // the oldest queued request and every later one that shares its step, while
-    // the batch fits the largest batch size and the budget left beside the
-    // resident matrices and the other workers' batches
-    std::vector<RequestPtr> group;
-    am24_matrix mat = nullptr;
-    uint64_t bytes = 0;
-    {
-      std::unique_lock<std::mutex> lk(s->mu);
-      for (;;) {
-        s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-        if (s->queue.empty()) return;  // stopping, nothing left
-        const RequestPtr head = s->queue.front();
-        const auto &res = s->matrices.at(head->matrix_id);
-        const uint64_t used = s->resident + s->inflight;
-        const uint64_t room = s->budget > used ? s->budget - used : 0;
-        uint32_t K = (uint32_t)head->s.total_starts;
-        if (batch_bytes(res.m, res.n, K) > room) {
-          if (s->inflight > 0) {  // wait for another worker's batch to finish
-            s->cv_work.wait(lk);
-            continue;
-          }
-          // the matrices admitted since this request was queued leave no room
-          s->queue.pop_front();
-          head->status = AM24_ERR_ADMISSION_REJECTED;
-          head->error = "the request's batch no longer fits the budget";
-          head->done = true;
-          s->matrices.at(head->matrix_id).pending--;
-          s->cv_done.notify_all();
-          continue;
-        }
-        group.push_back(head);
-        std::deque<RequestPtr> rest;
-        for (size_t i = 1; i < s->queue.size(); i++) {
-          const RequestPtr &r = s->queue[i];
-          const uint32_t k = (uint32_t)r->s.total_starts;
-          if (same_step(*head, *r) && K + k <= s->max_batch &&
-              batch_bytes(res.m, res.n, K + k) <= room) {
-            group.push_back(r);
-            K += k;
-          } else {
-            rest.push_back(r);
-          }
-        }
-        s->queue.swap(rest);
-        bytes = batch_bytes(res.m, res.n, K);
-        s->inflight += bytes;
-        mat = res.mat;
-        break;
-      }
-    }
-    const am24_status st = run_group(s, w, mat, group[0]->matrix_id, group);
-    const std::string err = st == AM24_OK ? std::string() : g_last_error;
-    if (st != AM24_OK && w.cached) {  // do not reuse a batch left in an unknown state
-      am24_batch_destroy(w.h, w.cached);
-      w.cached = nullptr;
-    }
-    const auto now = std::chrono::steady_clock::now();
-    {
-      std::lock_guard<std::mutex> lk(s->mu);
-      s->inflight -= bytes;
-      for (auto &r : group) {
-        r->status = st;
-        r->error = err;
-        r->stats.total_elapsed_time = std::chrono::duration<double>(now - r->submitted).count();
-        r->done = true;
-        s->matrices.at(r->matrix_id).pending--;
-      }
-    }
-    s->cv_done.notify_all();
-    s->cv_work.notify_all();  // budget freed
-  }
-}
-
-am24_status finish_ticket(am24_server s, const RequestPtr &r, float *x, am24_statistics *stats) {
-  // caller holds s->mu; the request is done
-  if (x && !r->x.empty()) std::memcpy(x, r->x.data(), sizeof(float) * r->x.size());
-  if (stats) *stats = r->stats;
-  s->tickets.erase(r->ticket);
-  if (r->status != AM24_OK) return fail(r->status, r->error);
-  return AM24_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-am24_status am24_server_create(int device, uint64_t hbm_budget_bytes, am24_server *out) {
-  if (!out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  *out = nullptr;
-  auto *s = new am24_server_s();
-  s->budget = hbm_budget_bytes;
-  s->workers.resize(AM24_SERVER_WORKERS);
-  am24_status st = am24_create(&s->upload_h, device);
-  for (size_t i = 0; st == AM24_OK && i < s->workers.size(); i++)
-    st = am24_create(&s->workers[i].h, device);
-  if (st != AM24_OK) {
-    for (auto &w : s->workers)
-      if (w.h) am24_destroy(w.h);
-    if (s->upload_h) am24_destroy(s->upload_h);
-    delete s;
-    return st;
-  }
-  for (size_t i = 0; i < s->workers.size(); i++)
-    s->workers[i].thread = std::thread(worker_loop, s, i);
-  *out = s;
-  return AM24_OK;
-}
-
-am24_status am24_server_destroy(am24_server s) {
-  if (!s) return AM24_OK;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->stop = true;
-  }
-  s->cv_work.notify_all();
-  for (auto &w : s->workers)
-    if (w.thread.joinable()) w.thread.join();
-  for (auto &w : s->workers) {
-    if (w.cached) am24_batch_destroy(w.h, w.cached);
-    am24_destroy(w.h);
-  }
-  for (auto &kv : s->matrices) am24_matrix_destroy(s->upload_h, kv.second.mat);
-  am24_destroy(s->upload_h);
-  delete s;
-  return AM24_OK;
-}
-
-am24_status am24_server_add_matrix_f32(am24_server s, const float *B, int32_t ldB, uint32_t m,
-                                       uint32_t n, int32_t on_device, uint32_t *matrix_id) {
-  if (!s || !B || !matrix_id) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  const uint64_t bytes = matrix_bytes(m, n);
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->resident + bytes > s->budget)
-      return fail(AM24_ERR_ADMISSION_REJECTED,
-                  "matrix needs " + std::to_string(bytes) + " bytes, " +
-                      std::to_string(s->budget - std::min(s->budget, s->resident)) +
-                      " left in the budget");
-    s->resident += bytes;  // reserved while uploading
-  }
-  am24_matrix mat = nullptr;
-  am24_status st;
-  {
-    std::lock_guard<std::mutex> lk(s->upload_mu);
-    st = am24_matrix_create_f32(s->upload_h, B, ldB, m, n, on_device, &mat);
-  }
-  std::lock_guard<std::mutex> lk(s->mu);
-  if (st != AM24_OK) {
-    s->resident -= bytes;
-    return st;
-  }
-  const uint32_t id = s->next_matrix++;
-  s->matrices[id] = am24_server_s::Resident{mat, bytes, m, n, 0};
-  *matrix_id = id;
-  return AM24_OK;
-}
-
-am24_status am24_server_remove_matrix(am24_server s, uint32_t matrix_id) {
-  if (!s) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  am24_matrix mat = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    auto it = s->matrices.find(matrix_id);
-    if (it == s->matrices.end()) return fail(AM24_ERR_INVALID_ARG, "unknown matrix id");
-    // (a worker's cached batch of this matrix is never reused: ids are not reused)
-    if (it->second.pending > 0)
-      return fail(AM24_ERR_INVALID_ARG, "requests for this matrix are pending");
-    mat = it->second.mat;
-    s->resident -= it->second.bytes;
-    s->matrices.erase(it);
-  }
-  std::lock_guard<std::mutex> lk(s->upload_mu);
-  return am24_matrix_destroy(s->upload_h, mat);
-}
-
-am24_status am24_submit(am24_server s, uint32_t matrix_id, const am24_settings *settings,
-                        const float *start_points, uint64_t *ticket) {
-  if (!s || !settings || !ticket) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  AM24_TRY(validate_settings(settings));
-  if (settings->use_otf || settings->store_all)
-    return fail(AM24_ERR_INVALID_ARG, "the server supports neither use_otf nor store_all");
-  if (settings->start_mode == AM24_START_INJECTED && !start_points)
-    return fail(AM24_ERR_INVALID_ARG, "start_mode INJECTED needs start_points");
-  auto r = std::make_shared<ServeRequest>();
-  r->s = *settings;
-  std::lock_guard<std::mutex> lk(s->mu);
-  auto it = s->matrices.find(matrix_id);
-  if (it == s->matrices.end()) return fail(AM24_ERR_INVALID_ARG, "unknown matrix id");
-  const uint32_t n = it->second.n, m = it->second.m;
-  AM24_TRY(am24_check_input(&r->s, n));
-  r->s.batch_size = r->s.total_starts;
-  r->s.total_batches = 1;
-  if ((uint32_t)r->s.total_starts > s->max_batch)
-    return fail(AM24_ERR_ADMISSION_REJECTED, "more starts than the server's largest batch");
-  if (s->resident + batch_bytes(m, n, (uint32_t)r->s.total_starts) > s->budget)
-    return fail(AM24_ERR_ADMISSION_REJECTED, "the request's batch does not fit the budget");
-  if (r->s.start_mode == AM24_START_INJECTED)
-    r->starts.assign(start_points, start_points + (size_t)n * r->s.total_starts);
-  r->matrix_id = matrix_id;
-  r->ticket = s->next_ticket++;
-  r->submitted = std::chrono::steady_clock::now();
-  it->second.pending++;
-  s->tickets[r->ticket] = r;
-  s->queue.push_back(r);
-  *ticket = r->ticket;
-  s->cv_work.notify_one();
-  return AM24_OK;
-}
-
-am24_status am24_poll(am24_server s, uint64_t ticket, float *x, am24_statistics *stats,
-                      int32_t *done) {
-  if (!s || !done) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lk(s->mu);
-  auto it = s->tickets.find(ticket);
-  if (it == s->tickets.end()) return fail(AM24_ERR_INVALID_ARG, "unknown ticket");
-  *done = it->second->done ? 1 : 0;
-  if (!*done) return AM24_OK;
-  return finish_ticket(s, it->second, x, stats);
-}
-
-am24_status am24_wait(am24_server s, uint64_t ticket, float *x, am24_statistics *stats) {
-  if (!s) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->tickets.find(ticket);
-  if (it == s->tickets.end()) return fail(AM24_ERR_INVALID_ARG, "unknown ticket");
-  RequestPtr r = it->second;
-  s->cv_done.wait(lk, [&] { return r->done; });
-  return finish_ticket(s, r, x, stats);
 }
 
 }  // extern "C"

@@ -107,6 +107,35 @@ am24_status read_ctl(am24_group g, const GroupSlot &sl, uint32_t *ctl) {
 
 }  // namespace
 
+namespace am24host {
+
+uint64_t group_problem_bytes(int m, int n, int k, int formulation, bool mixed) {
+  const uint64_t ldm = (uint64_t)(m + 31) / 32 * 32, ldn = (uint64_t)(n + 31) / 32 * 32;
+  const uint64_t kv = (uint64_t)k * ldn, kz = (uint64_t)k * ldm, words = kv / 32;
+  const int bn = pick_bn(k);
+  const uint64_t m_tiles1 = (m + BM - 1) / BM, n_tiles = (k + bn - 1) / bn;
+  int splits = 1, kbps = 1;
+  choose_splits((int)(((m_tiles1 + 1) / 2) * n_tiles), (n + PAIR_BK_BF16 - 1) / PAIR_BK_BF16,
+                std::max(1, num_sms() / 2), &splits, &kbps);
+  const uint64_t parts = (uint64_t)((n + BM - 1) / BM) * 4;
+  const uint64_t zh = is_l1_variance(formulation) ? 1 : 2;
+  uint64_t b = kv * 4 * 2 + kv * 2 * 2 + words * 4 * (is_constrained(formulation) ? 2 : 1) +
+               kz * (4 + 4 + 2 * zh + (mixed ? 2 : 0)) +
+               (uint64_t)ws_floats(splits, (int)m_tiles1, (int)n_tiles, bn) * 4 +
+               (uint64_t)k * (4 * 8 + parts * 8 + (mixed ? 16 : 0)) + 4096;
+  return b;
+}
+
+am24_status group_done_flags(am24_group g, std::vector<uint32_t> &out) {
+  out.resize(g->cap);
+  AM24_CUDA(cudaMemcpyAsync(out.data(), g->dev.done, sizeof(uint32_t) * g->cap,
+                            cudaMemcpyDeviceToHost, g->h->stream));
+  AM24_CUDA(cudaStreamSynchronize(g->h->stream));
+  return AM24_OK;
+}
+
+}  // namespace am24host
+
 extern "C" {
 
 am24_status am24_group_create(am24_handle h, uint32_t capacity, am24_group *out) {
@@ -128,7 +157,9 @@ am24_status am24_group_create(am24_handle h, uint32_t capacity, am24_group *out)
   AM24_TRY(g->mem.get(&d.plan, 1));
   AM24_TRY(g->mem.get(&d.prob, (size_t)GL_COUNT * capacity));
   AM24_TRY(g->mem.get(&d.pref, (size_t)GL_COUNT * (capacity + 1)));
+  AM24_TRY(g->mem.get(&d.done, capacity));
   d.maps = maps;
+  AM24_CUDA(cudaMemsetAsync(d.done, 0, sizeof(uint32_t) * capacity, h->stream));
   AM24_CUDA(cudaMemsetAsync(d.probs, 0, sizeof(GProblem) * capacity, h->stream));
   AM24_CUDA(cudaMemsetAsync(maps, 0, sizeof(GMaps) * capacity, h->stream));
   AM24_CUDA(cudaMemsetAsync(d.plan, 0, sizeof(GPlan), h->stream));
@@ -177,7 +208,7 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
   const int f = s.formulation;
   AM24_TRY(ensure_fp16_planes(h, mat));
   AM24_TRY(ensure_bt_fp16_planes(h, mat));
-  if (mixed) AM24_TRY(ensure_bf16_planes(h, mat));
+  if (mixed) AM24_TRY(ensure_bf16_planes(h, mat, 1));  // b0 only
 
   GroupSlot &sl = g->slots[slot];
   GProblem P{};

@@ -297,7 +297,8 @@ __global__ void __launch_bounds__(256) g_finalize_kernel(GroupDev g) {
 
 // The WHILE condition of a captured step loop: another step while some live
 // problem has not stopped, the launch's step cap is not reached and no wait
-// of a grouped product gave up.
+// of a grouped product gave up.  Also writes every slot's state to g.done,
+// which a host polls with one copy.
 __global__ void __launch_bounds__(256) g_condition_kernel(GroupDev g,
                                                           cudaGraphConditionalHandle handle) {
   __shared__ int any;
@@ -305,7 +306,12 @@ __global__ void __launch_bounds__(256) g_condition_kernel(GroupDev g,
   __syncthreads();
   for (int p = threadIdx.x; p < g.cap; p += blockDim.x) {
     const GProblem &P = g.probs[p];
-    if (P.live && *reinterpret_cast<volatile const uint32_t *>(P.ctl + CTL_STOP) == 0u) any = 1;
+    uint32_t d = 0u;
+    if (P.live) {
+      d = *reinterpret_cast<volatile const uint32_t *>(P.ctl + CTL_STOP) == 0u ? 1u : 2u;
+      if (d == 1u) any = 1;
+    }
+    g.done[p] = d;
   }
   __syncthreads();
   if (threadIdx.x == 0) {

@@ -115,7 +115,7 @@ am24_status make_map(am24_handle h, CUtensorMap *map, const float *base, int K, 
                      int box_rows, int bk);
 am24_status make_map_bf16(am24_handle h, CUtensorMap *map, const uint16_t *base, int K, int rows,
                           int ld, int box_rows, bool fp16 = false);
-am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat);
+am24_status ensure_bf16_planes(am24_handle h, am24_matrix mat, int planes);
 am24_status ensure_tf32_planes(am24_handle h, am24_matrix mat);
 am24_status ensure_fp16_planes(am24_handle h, am24_matrix mat);
 am24_status ensure_bt_fp16_planes(am24_handle h, am24_matrix mat);
@@ -124,5 +124,11 @@ am24_status validate_settings(const am24_settings *s);
 void reference_start(float *x, unsigned n, bool constrained, unsigned s, unsigned g);
 void host_starts(const am24_settings &s, unsigned n, const float *start_points,
                  const unsigned *global_idx, int cols, std::vector<float> &out);
+
+// Device bytes one problem of a group allocates (am24_group_add).
+uint64_t group_problem_bytes(int m, int n, int k, int formulation, bool mixed);
+// Every slot's state after the last step (0 free, 1 iterating, 2 stopped);
+// synchronizes the group's stream.
+am24_status group_done_flags(am24_group g, std::vector<uint32_t> &out);
 
 }  // namespace am24host

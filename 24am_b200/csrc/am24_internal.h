@@ -37,6 +37,7 @@ struct MatrixDev {
   // x = b0 + b1 + b2 exactly; made when a batch of an L1-variance form first
   // needs them (null before).
   uint16_t *Bc_b3;
+  int bf16_planes;  // planes Bc_b3 holds: 1 (b0 alone) or 3
   // Two FP16 planes of Bc scaled per feature (plane p at Bc_h2 + p * n * ldm):
   // x * 2^s_c = h0 + h1 (+ under 2^-22 |x|), row_scale[c] = 2^-s_c; made when a
   // batch first runs V = B^T Z on FP16 operands (null before).
@@ -257,6 +258,7 @@ struct GroupDev {
   GPlan *plan;
   int *prob;  // [GL_COUNT][cap]: the problems of each list
   int *pref;  // [GL_COUNT][cap + 1]: exclusive prefix of their items
+  uint32_t *done;  // per slot after each step: 0 free, 1 iterating, 2 stopped
   unsigned long long timeout_ns;
 };
 
@@ -276,7 +278,7 @@ cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handl
 int num_sms();
 // Fills M's TF32 planes (Bc_hi/lo, Bt_hi/lo) from M.Bc.
 cudaError_t launch_prep_tf32_planes(MatrixDev &M, cudaStream_t st);
-// Fills M.Bc_b3 from M.Bc.
+// Fills M.Bc_b3 from M.Bc (its M.bf16_planes planes).
 cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st);
 // Fills M.Bc_h2 and M.row_scale from M.Bc.
 cudaError_t launch_prep_fp16x2(const MatrixDev &M, cudaStream_t st);

@@ -313,7 +313,7 @@ __global__ void prep_copy_kernel(const float *__restrict__ B, int ldB, int m, fl
 // 16 significant bits and the second at most 8, so b2 is a BF16 value.  (FP32
 // subnormals below 2^-126 aside, where a tensor core may flush b2.)
 __global__ void prep_bf16x3_kernel(const float *__restrict__ Bc, int ldm, int m, size_t plane,
-                                   uint16_t *__restrict__ out) {
+                                   int planes, uint16_t *__restrict__ out) {
   const size_t c = blockIdx.x;
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
     const size_t o = c * ldm + r;
@@ -323,8 +323,10 @@ __global__ void prep_bf16x3_kernel(const float *__restrict__ Bc, int ldm, int m,
     const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
     const __nv_bfloat16 b2 = __float2bfloat16_rn(r1 - __bfloat162float(b1));
     out[o] = __bfloat16_as_ushort(b0);
-    out[plane + o] = __bfloat16_as_ushort(b1);
-    out[2 * plane + o] = __bfloat16_as_ushort(b2);
+    if (planes == 3) {
+      out[plane + o] = __bfloat16_as_ushort(b1);
+      out[2 * plane + o] = __bfloat16_as_ushort(b2);
+    }
   }
 }
 
@@ -2247,7 +2249,8 @@ size_t ws_floats(int splits, int m_tiles, int n_tiles, int bn) {
 }
 
 cudaError_t launch_prep_bf16x3(const MatrixDev &M, cudaStream_t st) {
-  prep_bf16x3_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, (size_t)M.n * M.ldm, M.Bc_b3);
+  prep_bf16x3_kernel<<<M.n, 256, 0, st>>>(M.Bc, M.ldm, M.m, (size_t)M.n * M.ldm, M.bf16_planes,
+                                          M.Bc_b3);
   return cudaGetLastError();
 }
 

@@ -300,6 +300,131 @@ def config3_problems(am, count, matrices, seed):
     return out
 
 
+def uneven_problems(am, wl, count, seed):
+    """The uneven-problem workload: `count` independent problems, each on its
+    own matrix from the low-rank-plus-noise generator (n log-uniform in
+    [100, 5000] samples, p log-uniform in [1e3, 1e5] features,
+    r = min(n, p) / 20, 64 non-zeros per loading), its own formulation
+    (uniform over the 8), s uniform in [8, 256], starts uniform in [32, 1024]
+    (U[-1, 1] normalised, generated on the device), gamma 0.1 x the matrix's
+    largest column 2-norm (L2-variance penalties) or 0.025 x its largest column
+    1-norm (L1-variance penalties), maxIter 200, tol 1e-6.  Yields
+    (m, n, seed, settings kwargs) per problem; matrices are generated on demand."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(100), np.log(5000))))
+        p = int(np.exp(rng.uniform(np.log(1000), np.log(100000))))
+        f = int(rng.integers(8))
+        s = int(rng.integers(8, 257))
+        k = int(rng.integers(32, 1025))
+        out.append((n, p, seed + 100 + i, dict(formulation=f, constraintParameter=s,
+                                                tolerance=1e-6, maximumIterations=200,
+                                                totalStartingPoints=k, batchSize=k,
+                                                startMode=am.START_DEVICE_UNIFORM)))
+    return out
+
+
+def run_uneven(args):
+    """Config 3 on one GPU: 256 independent problems of uneven shape.
+    Three arms over the same matrices, settings and device-generated starts:
+      plain   -- the plain FP32 path, one am24_solve_resident_f32 call per problem
+                 (the drop-in solve a caller makes), wall clock around all calls;
+      grouped -- every problem in one group (am24_group_run: one captured graph,
+                 grouped launches per step, device loop), FP32, device-timed;
+      mixed   -- the same group with MIXED precision (single-pass BF16 V = B^T Z
+                 until the supports settle, then FP32-accurate), device-timed.
+    start-iterations are counted per start to its problem's own stop.  Accuracy:
+    per problem, the best explained variance ||B x||^2 (FP64 on the device) of
+    grouped and mixed against the plain path's."""
+    import numpy as np
+    import torch
+    am = importlib.import_module("24am_b200")
+    wl = am.workloads
+    solver = am.Solver(0)
+    probs = uneven_problems(am, wl, args.problems, SEED + 7)
+    mats, sets = [], []
+    t_gen = time.perf_counter()
+    for (n, p, seed, kw) in probs:
+        Dt = wl.low_rank_data_torch(n, p, max(1, min(n, p) // 20), min(64, p), seed)
+        c2 = float(Dt.double().norm(dim=1).max())
+        c1 = float(Dt.double().abs().sum(dim=1).max())
+        torch.cuda.synchronize()
+        M = am.Matrix(solver, None, on_device_ptr=Dt.data_ptr(), m=n, n=p, ldB=n)
+        del Dt
+        f = kw["formulation"]
+        g = 0.1 * c2 if f in (4, 6) else (0.025 * c1 if f in (5, 7) else 0.0)
+        mats.append(M)
+        sets.append(dict(kw, penaltyParameter=g))
+    torch.cuda.empty_cache()
+    t_gen = time.perf_counter() - t_gen
+
+    # plain FP32 path: one solve per problem
+    plain_ev, plain_its, plain_steps = [], 0, []
+    solver.sync()
+    t0 = time.perf_counter()
+    for M, kw in zip(mats, sets):
+        x, f, st = M.solve(am.OptimizationSettings(**kw))
+        plain_ev.append(st.explained_variance)
+        plain_its += int(st.start_iterations)
+        plain_steps.append(int(st.it))
+    plain_s = time.perf_counter() - t0
+
+    def grouped(precision):
+        grp = am.Group(solver, capacity=len(mats))
+        ids = [grp.add(M, am.OptimizationSettings(precision=precision, **kw))
+               for M, kw in zip(mats, sets)]
+        ms = grp.run()
+        evs, its, low = [], 0, 0
+        for pid in ids:
+            _, st = grp.result(pid)
+            evs.append(st.explained_variance)
+            its += int(st.start_iterations)
+            low += int(st.low_precision_iterations)
+        grp.close()
+        return ms, evs, its, low
+
+    ms32, ev32, its32, _ = grouped(am.PRECISION_FP32)
+    msmx, evmx, itsmx, lowmx = grouped(am.PRECISION_MIXED)
+    pe = np.array(plain_ev)
+    rel32 = np.abs(np.array(ev32) - pe) / pe
+    relmx = np.abs(np.array(evmx) - pe) / pe
+    v_plain = plain_its / plain_s
+    v32 = its32 / (ms32 * 1e-3)
+    vmx = itsmx / (msmx * 1e-3)
+    ks = [kw["totalStartingPoints"] for kw in sets]
+    line = {"metric": "start-iterations/s (uneven problems, mixed precision, grouped)",
+            "value": vmx, "unit": "start-it/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "bf16+f32", "data": "synthetic",
+            "config": {"workload": f"{len(mats)} independent problems, each its own matrix: "
+                                   "n log-uniform 100..5000 x p log-uniform 1e3..1e5, "
+                                   "r = min(n,p)/20, 64 nnz/loading; formulation uniform, "
+                                   "s 8..256, starts 32..1024 (device U[-1,1]), maxIter 200, "
+                                   "tol 1e-6",
+                       "total_starts": int(sum(ks)),
+                       "matrix_elements": int(sum(n * p for n, p, _, _ in probs))},
+            "plain_fp32": {"value": v_plain, "seconds": plain_s, "start_iterations": plain_its,
+                           "timing": "wall clock around one am24_solve_resident_f32 per problem"},
+            "grouped_fp32": {"value": v32, "device_ms": ms32, "start_iterations": its32,
+                             "max_ev_rel_diff_vs_plain": float(rel32.max()),
+                             "median_ev_rel_diff_vs_plain": float(np.median(rel32))},
+            "grouped_mixed": {"value": vmx, "device_ms": msmx, "start_iterations": itsmx,
+                              "bf16_step_share": lowmx / max(1, sum(plain_steps)),
+                              "max_ev_rel_diff_vs_plain": float(relmx.max()),
+                              "median_ev_rel_diff_vs_plain": float(np.median(relmx)),
+                              "problems_within_1e-4": int((relmx <= 1e-4).sum())},
+            "speedup_mixed_vs_plain": vmx / v_plain,
+            "speedup_grouped_fp32_vs_plain": v32 / v_plain,
+            "speedup_mixed_vs_grouped_fp32": vmx / v32,
+            "setup_seconds": t_gen}
+    print(json.dumps(line), flush=True)
+    for M in mats:
+        M.close()
+    solver.close()
+    return 0
+
+
 def run_serving(args):
     """The serving layer on one GPU.  Resident matrices from the uneven-problem
     distribution (p log-uniform in [1e3, 1e5], n log-uniform in [100, 5000],
@@ -673,7 +798,8 @@ def main():
                          "problems of uneven shapes submitted at once")
     ap.add_argument("--rates", default="5,20,80", help="serve: request rates (req/s)")
     ap.add_argument("--seconds", type=float, default=5.0, help="serve: arrivals per rate")
-    ap.add_argument("--matrices", type=int, default=16, help="serve/uneven: resident matrices")
+    ap.add_argument("--matrices", type=int, default=16, help="serve: resident matrices")
+    ap.add_argument("--problems", type=int, default=256, help="uneven: problems")
     args = ap.parse_args()
     global N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS, S_CONS, GAMMA_C
     N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = SIZES[args.size]
@@ -687,7 +813,9 @@ def main():
         return run_reference_arm(args)
     if args.mode == "solve":
         return run_solves(args)
-    if args.mode in ("serve", "uneven"):
+    if args.mode == "uneven":
+        return run_uneven(args)
+    if args.mode == "serve":
         return run_serving(args)
     return run_ours(args)
 

@@ -274,19 +274,22 @@ am24_status am24_sync(am24_handle h);
  * events around library work. */
 void *am24_stream(am24_handle h);
 
-/* ---- serving: resident matrices, queued solves, batching on arrival ------- */
-/* A server owns its own handles on `device` and AM24_SERVER_WORKERS worker
- * threads, each with its own stream, which run different batches at once.  Matrices
- * are admitted while their device layouts fit hbm_budget_bytes (the budget
- * also bounds the largest request batch).  Queued requests that share a
- * matrix and the settings that shape the AM step (formulation, constraint,
- * penalty, tolerance, max_iter, l1_mode, precision and its stability rule) run
- * together as one batch of starting points; each request still gets the best
- * of its own starts, its own x and its own statistics.  Each request's starts
- * form one segment of that batch (batchSize = totalStartingPoints), and the
- * batch stops on its batch-wide maximum change as a reference batch does.
+/* ---- serving: resident matrices, continuous batching of solve requests ---- */
+/* No counterpart in the reference.  A server owns a handle on `device` and one
+ * engine thread that serves requests with a group (am24_group_*): requests
+ * are admitted, oldest first, into the running group at step boundaries
+ * (every AM24_SERVER_CHUNK grouped steps) while their device memory fits the
+ * budget left beside the resident matrices and the requests already on the
+ * device; every admitted request steps together with the others, and leaves
+ * as soon as its own batch loop ends (its x, statistics and memory are then
+ * released).  Each request is one batch of all its starting points
+ * (batchSize = totalStartingPoints) that stops on its own largest change, as a
+ * reference batch does, with tiles and reduction order of its own: its result
+ * is the same bit for bit whatever else is served beside it.  Matrices are
+ * admitted while their device layouts fit hbm_budget_bytes.
  * settings->use_otf and store_all are not supported by the server. */
-#define AM24_SERVER_WORKERS 4 /* worker threads (streams) per server */
+#define AM24_SERVER_WORKERS 1 /* engine threads per server */
+#define AM24_SERVER_CHUNK 4   /* grouped steps between admissions */
 typedef struct am24_server_s *am24_server;
 am24_status am24_server_create(int device, uint64_t hbm_budget_bytes, am24_server *out);
 /* Finishes queued requests, then frees everything the server holds. */

@@ -13,59 +13,86 @@ def _am():
     return importlib.import_module("24am_b200")
 
 
-def test_merged_requests_match_solo_solves(solver, po):
-    """Requests that share a matrix and a step run as one batch; each gets the
-    best of its own starts.  The batch stops when every start of every request
-    has converged, so each result is compared with a solo solve of the same
-    starts within the solver tolerance of the tests."""
+def _req(am, f, k, s=16, g=0.0, max_iter=100, tol=1e-6, injected=True, precision=0):
+    return am.OptimizationSettings(formulation=f, constraintParameter=s, penaltyParameter=g,
+                                   tolerance=tol, maximumIterations=max_iter,
+                                   totalStartingPoints=k, batchSize=k, precision=precision,
+                                   startMode=am.START_INJECTED if injected
+                                   else am.START_DEVICE_UNIFORM)
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp32", "mixed"])
+def test_request_is_the_same_alone_and_in_the_mix(solver, po, precision):
+    """Continuous batching: a request served alone and the same request served
+    while seven others of other matrices, formulations and start counts run,
+    arrive and leave, give the same x, objective, explained variance and
+    iteration count, bit for bit."""
     am = _am()
-    m, n, k = 300, 2000, 64
+    m, n, k = 300, 2000, 256
     B = po.low_rank_data(m, n, 8, 30, seed=41, dtype=np.float32)
-    B64 = B.astype(np.float64)
-    big = po.low_rank_data(1500, 40000, 8, 30, seed=42, dtype=np.float32)
+    big = po.low_rank_data(1500, 20000, 8, 30, seed=42, dtype=np.float32)
+    V = po.uniform_starts(n, k, seed=50, dtype=np.float32)
+    st = _req(am, 0, k, precision=precision)
     srv = am.Server(0, 40 << 30)
     mid = srv.add_matrix(B)
     mbig = srv.add_matrix(big)
-    starts = [po.uniform_starts(n, k, seed=50 + i, dtype=np.float32) for i in range(3)]
-    # long requests on the other matrix (tolerance 0: all 300 iterations, some
-    # 0.3 s each; different s, so they do not merge) keep every worker busy
-    # while the others queue
-    holds = [srv.submit(mbig, am.OptimizationSettings(
-        formulation=0, constraintParameter=16 + i, tolerance=0.0, maximumIterations=300,
-        totalStartingPoints=1024, batchSize=1024)) for i in range(4)]
-    st = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=1e-6,
-                                 maximumIterations=100, totalStartingPoints=k, batchSize=k,
-                                 startMode=am.START_INJECTED)
-    tickets = [srv.submit(mid, st, start_points=V) for V in starts]
-    st4 = am.OptimizationSettings(formulation=4, penaltyParameter=0.3, tolerance=1e-6,
-                                  maximumIterations=100, totalStartingPoints=k, batchSize=k,
-                                  startMode=am.START_INJECTED)
-    t4 = srv.submit(mid, st4, start_points=starts[0])
-    done, _, _ = srv.poll(tickets[0])
-    assert not done  # still queued behind the long request
-    results = [srv.wait(t) for t in tickets]
-    x4, s4 = srv.wait(t4)
-    for t in holds:
-        srv.wait(t)
-    # the three merged requests ran as one batch: same iteration count
-    its = {r[1].it for r in results}
-    assert len(its) == 1, its
-    for (x, s), V in zip(results, starts):
-        assert s.start_iterations == k * s.it
-        assert s.total_elapsed_time >= s.total_true_computation_time
-        M = solver.matrix(B)
-        xs, fs, ss = M.solve(am.OptimizationSettings(
-            formulation=0, constraintParameter=16, tolerance=1e-6, maximumIterations=100,
-            totalStartingPoints=k, batchSize=k, startMode=am.START_INJECTED), start_points=V)
-        M.close()
-        ev = float(np.linalg.norm(B64 @ x.astype(np.float64)) ** 2)
-        ev_solo = float(np.linalg.norm(B64 @ xs.astype(np.float64)) ** 2)
-        assert abs(ev - ev_solo) <= 1e-4 * ev_solo
-        assert abs(s.fval - fs) <= 1e-4 * abs(fs)
-        assert abs(s.explained_variance - ev) <= 1e-6 * ev
-    ev4 = float(np.linalg.norm(B64 @ x4.astype(np.float64)) ** 2)
-    assert np.isfinite(ev4) and ev4 > 0
+    xa, sa = srv.wait(srv.submit(mid, st, start_points=V))
+    # long requests first, then the request, then more while it runs
+    holds = [srv.submit(mbig, _req(am, f, 300 + 37 * f, s=16 + f, g=0.2, tol=0.0,
+                                   max_iter=120, injected=False, precision=precision))
+             for f in (0, 3, 4, 7)]
+    t = srv.submit(mid, st, start_points=V)
+    more = [srv.submit(mid, _req(am, f, 64 + 100 * f, g=0.3, injected=False))
+            for f in (1, 2, 6)]
+    xb, sb = srv.wait(t)
+    for h in holds + more:
+        srv.wait(h)
+    assert np.array_equal(xa, xb)
+    assert sa.fval == sb.fval and sa.it == sb.it
+    assert sa.explained_variance == sb.explained_variance
+    assert sa.start_iterations == sb.start_iterations == k * sa.it
+    assert sb.total_elapsed_time >= sb.total_true_computation_time > 0
     srv.remove_matrix(mbig)
+    srv.close()
+
+
+def test_request_matches_a_one_call_solve(solver, po):
+    """A served request of more than 128 starts runs the one-call solve's
+    kernels: the same x, objective and iteration count bit for bit."""
+    am = _am()
+    m, n, k = 300, 2000, 300
+    B = po.low_rank_data(m, n, 8, 30, seed=43, dtype=np.float32)
+    V = po.uniform_starts(n, k, seed=51, dtype=np.float32)
+    srv = am.Server(0, 40 << 30)
+    mid = srv.add_matrix(B)
+    for f, g in ((0, 0.0), (3, 0.0), (5, 240.0), (6, 0.15)):
+        st = _req(am, f, k, s=12, g=g)
+        x, s = srv.wait(srv.submit(mid, st, start_points=V))
+        M = solver.matrix(B)
+        xs, fs, ss = M.solve(_req(am, f, k, s=12, g=g), start_points=V)
+        M.close()
+        assert np.array_equal(x, xs), f
+        assert s.fval == fs and s.it == ss.it and s.explained_variance == ss.explained_variance
+    srv.close()
+
+
+def test_requests_join_while_others_run(solver, po):
+    """A short request submitted while a long one is on the device is admitted
+    at the next step boundary and finishes first."""
+    am = _am()
+    B = po.low_rank_data(300, 2000, 8, 30, seed=44, dtype=np.float32)
+    big = po.low_rank_data(2000, 40000, 8, 30, seed=45, dtype=np.float32)
+    srv = am.Server(0, 40 << 30)
+    mid, mbig = srv.add_matrix(B), srv.add_matrix(big)
+    long_t = srv.submit(mbig, _req(am, 0, 1024, tol=0.0, max_iter=200, injected=False))
+    import time
+    time.sleep(0.05)
+    short_t = srv.submit(mid, _req(am, 0, 64, injected=False))
+    xs, ss = srv.wait(short_t)
+    done, _, _ = srv.poll(long_t)
+    assert not done  # the short request did not wait for the long one
+    xl, sl = srv.wait(long_t)
+    assert sl.it == 200 and ss.total_elapsed_time < sl.total_elapsed_time
     srv.close()
 
 
