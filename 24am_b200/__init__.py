@@ -144,7 +144,7 @@ _SIGS = {
     "am24_group_remove": (C.c_int, [_VP, C.c_uint32]),
 }
 KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV", "densify",
-                "gemm_BtZ_bf16", "support", "gather_BV_group"]
+                "gemm_BtZ_low", "support", "gather_BV_group"]
 
 _lib = None
 

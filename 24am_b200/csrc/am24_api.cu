@@ -746,10 +746,14 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   if (const char *e = getenv("AM24_GEMM_BF16")) d.bf16_2 = d.bf16_2 && atoi(e) != 0;
   // MIXED runs its BF16 phase on CTA-pair tiles; narrower batches stay FP32
   d.mixed = settings->precision == AM24_PRECISION_MIXED && d.pair2;
+  // the low-precision phase on single-pass FP16 operands (AM24_MIXED_BF16=1:
+  // single-pass BF16, the FP16 planes off or not)
+  d.mixed_fp16 = d.mixed && d.fp16_2;
+  if (const char *e = getenv("AM24_MIXED_BF16")) d.mixed_fp16 = d.mixed_fp16 && atoi(e) == 0;
   d.k_stable = settings->stable_iterations;
   d.need_stable = (uint32_t)std::max(1.0, std::ceil((double)settings->stable_share * k - 1e-9));
   d.need_stable = std::min(d.need_stable, (uint32_t)k);
-  const bool need_bf16 = d.bf16_2 || d.mixed;
+  const bool need_bf16 = d.bf16_2 || (d.mixed && !d.mixed_fp16);
   // TF32 planes: Z = B V off the FP16 pairs; V = B^T Z with neither FP16 nor BF16 operands
   const bool tf32_1 = !d.fp16_1, tf32_2 = !d.fp16_2 && !d.bf16_2;
   const size_t zh_planes = is_l1_variance(settings->formulation) ? 1 : 2;
@@ -1005,7 +1009,7 @@ am24_status am24_batch_step_timed(am24_handle h, am24_batch b, int32_t it, float
                              (kk[i] == AM24_KERNEL_DENSIFY && planes > b->d.sparse_cap));
     if (b->d.mixed)
       skipped = skipped || (phase == 0 ? kk[i] == AM24_KERNEL_GEMM_BTZ
-                                       : kk[i] == AM24_KERNEL_GEMM_BTZ_BF16);
+                                       : kk[i] == AM24_KERNEL_GEMM_BTZ_LOW);
     kinds[i] = kk[i] | (skipped ? AM24_KERNEL_SKIPPED : 0);
   }
   *count = nl;

@@ -120,7 +120,7 @@ uint64_t group_problem_bytes(int m, int n, int k, int formulation, bool mixed) {
   const uint64_t parts = (uint64_t)((n + BM - 1) / BM) * 4;
   const uint64_t zh = is_l1_variance(formulation) ? 1 : 2;
   uint64_t b = kv * 4 * 2 + kv * 2 * 2 + words * 4 * (is_constrained(formulation) ? 2 : 1) +
-               kz * (4 + 4 + 2 * zh + (mixed ? 2 : 0)) +
+               kz * (4 + 4 + 2 * zh) +
                (uint64_t)ws_floats(splits, (int)m_tiles1, (int)n_tiles, bn) * 4 +
                (uint64_t)k * (4 * 8 + parts * 8 + (mixed ? 16 : 0)) + 4096;
   return b;
@@ -208,7 +208,6 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
   const int f = s.formulation;
   AM24_TRY(ensure_fp16_planes(h, mat));
   AM24_TRY(ensure_bt_fp16_planes(h, mat));
-  if (mixed) AM24_TRY(ensure_bf16_planes(h, mat, 1));  // b0 only
 
   GroupSlot &sl = g->slots[slot];
   GProblem P{};
@@ -252,7 +251,7 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
       (is_constrained(f) && (st = A->get(&P.cmask, words))) ||
       (st = A->get(&P.Z_hi, kz)) || (st = A->get(&P.Z_lo, kz)) ||
       (st = A->get(&P.Z_h, zh_planes * kz)) || (st = A->get(&P.z_scale, k)) ||
-      (mixed && (st = A->get(&P.Z_b, kz))) || (st = A->get(&P.V_h, 2 * kv)) ||
+      (st = A->get(&P.V_h, 2 * kv)) ||
       (st = A->get(&P.v_scale, k)) ||
       (st = A->get(&P.ws, ws_floats(P.splits1, P.m_tiles1, P.n_tiles1, P.bn))) ||
       (st = A->get(&P.fz, k)) || (st = A->get(&P.val, k)) || (st = A->get(&P.err, k)) ||
@@ -265,7 +264,6 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
   const cudaStream_t hs = h->stream;
   AM24_CUDA(cudaMemsetAsync(P.Z_h, 0, sizeof(uint16_t) * zh_planes * kz, hs));
   AM24_CUDA(cudaMemsetAsync(P.V_h, 0, sizeof(uint16_t) * 2 * kv, hs));
-  if (P.Z_b) AM24_CUDA(cudaMemsetAsync(P.Z_b, 0, sizeof(uint16_t) * kz, hs));
   if (P.cmask) AM24_CUDA(cudaMemsetAsync(P.cmask, 0, sizeof(uint32_t) * words, hs));
   AM24_CUDA(cudaMemsetAsync(P.sel_hint, 0, sizeof(float) * k, hs));
   AM24_CUDA(cudaMemsetAsync(P.val, 0, sizeof(float) * k, hs));
@@ -312,9 +310,7 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
       (st = make_map_bf16(h, &maps.a2_h1, M.Bc_h2 + pc, M.m, M.n, M.ldm, BM, true)) ||
       (st = make_map_bf16(h, &maps.b2_h0, P.Z_h, M.m, k, M.ldm, P.bn / 2, true)) ||
       (zh_planes == 2 &&
-       (st = make_map_bf16(h, &maps.b2_h1, P.Z_h + kz, M.m, k, M.ldm, P.bn / 2, true))) ||
-      (mixed && ((st = make_map_bf16(h, &maps.a2_b0, M.Bc_b3, M.m, M.n, M.ldm, BM)) ||
-                 (st = make_map_bf16(h, &maps.b2_b, P.Z_b, M.m, k, M.ldm, P.bn / 2)))))
+       (st = make_map_bf16(h, &maps.b2_h1, P.Z_h + kz, M.m, k, M.ldm, P.bn / 2, true))))
     return st;
   AM24_CUDA(cudaMemcpyAsync(const_cast<GMaps *>(g->dev.maps) + slot, &maps, sizeof maps,
                             cudaMemcpyHostToDevice, hs));

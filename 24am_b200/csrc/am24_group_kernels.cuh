@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) group_plan_kernel(GroupDev g) {
         P.ctl[GCTL_NEXT] = 0u;
         *P.max_err = 0.f;
         const bool low = P.mixed && P.phase[0] == 0u;
-        const uint32_t sc = low ? GS_BF16X1 : (P.mode == 1 ? GS_FP16X2A : GS_FP16X3);
+        const uint32_t sc = low ? GS_FP16X1 : (P.mode == 1 ? GS_FP16X2A : GS_FP16X3);
         P.ctl[GCTL_SCHEME] = sc;
 #pragma unroll
         for (int l = 0; l < GL_COUNT; l++) items[l] = plan_items(P, l, gate, sc);

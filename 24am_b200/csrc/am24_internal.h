@@ -78,7 +78,8 @@ struct BatchDev {
   const float *row_scale;  // the matrix's FP16 row scales (fp16_2)
   uint16_t *Z_b;  // k x ldm BF16 Z: sgn(B V) exactly (L1-variance forms with bf16_2),
                   // or Z rounded to BF16 (MIXED); else null
-  int mixed;             // MIXED precision: single-pass BF16 V = B^T Z until supports settle
+  int mixed;             // MIXED precision: single-pass V = B^T Z until supports settle ...
+  int mixed_fp16;        // ... on FP16 operands (the scaled h0 / g0 planes); else BF16
   uint32_t k_stable;     // steps of unchanged support a start needs ...
   uint32_t need_stable;  // ... in this many starts before the batch refines
   uint32_t *vmask_prev;  // k x (ldn/32): the previous step's non-zero masks (MIXED)
@@ -194,13 +195,12 @@ enum GEpi : int { GE_PARTIAL = 0, GE_RAW = 1, GE_PL1 = 2, GE_PL0 = 3 };
 constexpr int FIN_STARTS = 8;  // starts per finalize item (a warp each)
 
 // Operand schemes of the grouped V = B^T Z, chosen per problem and step.
-enum GScheme : int { GS_FP16X3 = 0, GS_FP16X2A = 1, GS_BF16X1 = 2 };
+enum GScheme : int { GS_FP16X3 = 0, GS_FP16X2A = 1, GS_FP16X1 = 2 };
 
 // The tensor maps of one problem (a separate, 64-byte aligned table).
 struct alignas(64) GMaps {
   CUtensorMap a1_h0, a1_h1, b1_h0, b1_h1;  // Z = B V: Bt FP16 planes, V FP16 planes
   CUtensorMap a2_h0, a2_h1, b2_h0, b2_h1;  // V = B^T Z: Bc FP16 planes, Z FP16 planes
-  CUtensorMap a2_b0, b2_b;                 // V = B^T Z, BF16 (MIXED): Bc b0 plane, Z BF16
 };
 
 struct GProblem {

@@ -2535,9 +2535,16 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
       gl.gate_min = 0;
       gl.gate_max = 0;
       if ((e2 = mark(7)) != cudaSuccess) return e2;
-      if ((e2 = run_gemm_pair<PairBF16x1, 256, 12>(tm.a2_b0, tm.b2_b, tm.a2_b0, tm.b2_b, gl, epi,
-                                                   st)) != cudaSuccess)
-        return e2;
+      if (b.mixed_fp16) {
+        gl.row_scale = b.row_scale;
+        gl.col_scale = is_l1_variance(f) ? nullptr : b.z_scale;  // sgn(z) is exact
+        e2 = run_gemm_pair<PairFP16x1, 256, 12>(tm.a2_h0, tm.b2_h0, tm.a2_h0, tm.b2_h0, gl, epi,
+                                                st);
+      } else {
+        e2 = run_gemm_pair<PairBF16x1, 256, 12>(tm.a2_b0, tm.b2_b, tm.a2_b0, tm.b2_b, gl, epi,
+                                                st);
+      }
+      if (e2 != cudaSuccess) return e2;
       nl++;
       g2.gate = b.phase;
       g2.gate_min = 1;

@@ -58,13 +58,12 @@ struct ServeRequest {
 };
 using RequestPtr = std::shared_ptr<ServeRequest>;
 
-// Device bytes of a matrix's layouts: FP32 B, the two FP16 planes of B and of
-// B^T with their scales, and the BF16 plane of MIXED requests, all made when
-// the matrix is added.
+// Device bytes of a matrix's layouts: FP32 B and the two FP16 planes of B and
+// of B^T with their scales, all made when the matrix is added.
 uint64_t matrix_bytes(uint32_t m, uint32_t n) {
   const uint64_t ldm = (m + 31) / 32 * 32, ldn = (n + 31) / 32 * 32;
   return 4ull * n * ldm + 2ull * 2 * n * ldm + 4ull * n + 2ull * 2 * m * ldn + 4ull * m +
-         4ull * m + 2ull * n * ldm;
+         4ull * m;
 }
 
 }  // namespace
@@ -274,7 +273,6 @@ am24_status am24_server_add_matrix_f32(am24_server s, const float *B, int32_t ld
     st = am24_matrix_create_f32(s->upload_h, B, ldB, m, n, on_device, &mat);
     if (st == AM24_OK) st = ensure_fp16_planes(s->upload_h, mat);
     if (st == AM24_OK) st = ensure_bt_fp16_planes(s->upload_h, mat);
-    if (st == AM24_OK) st = ensure_bf16_planes(s->upload_h, mat, 1);
     if (st != AM24_OK && mat) {
       const std::string err = g_last_error;
       am24_matrix_destroy(s->upload_h, mat);

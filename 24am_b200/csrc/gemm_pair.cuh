@@ -173,6 +173,29 @@ struct PairBF16x1 {
   static constexpr uint32_t FMT = 1u;
 };
 
+// Single-pass FP16 operands (A = h0 of B's scaled split, B = g0 of Z's, or
+// the exact sign of the L1-variance forms) for the low-precision phase of the
+// mixed mode: one MMA per 16 K elements, as PairBF16x1, with FP16's 11-bit
+// significands where BF16 keeps 8 (the power-of-two scales of the FP16 planes
+// keep every row and column in range), so each product carries about 2^-12
+// relative error instead of 2^-9.  A work unit is accumulated whole in tensor
+// memory.
+struct PairFP16x1 {
+  static constexpr int NA = 1, NB = 1, BK = PAIR_BK_BF16;
+  static constexpr int PROMO_K = 1 << 20;
+  template <uint32_t ID>
+  __device__ static void k_block(uint32_t d, const uint32_t (&a)[1], const uint32_t (&b)[1],
+                                 uint32_t sbo, bool first) {
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+      const uint32_t off = kk * 32;
+      mma_f16_pair(d, sdesc_kmajor(a[0] + off, sbo, 4u), sdesc_kmajor(b[0] + off, sbo, 4u), ID,
+                   (first && kk == 0) ? 0u : 1u);
+    }
+  }
+  static constexpr uint32_t FMT = 0u;
+};
+
 template <class S, int BN, int STAGES>
 struct PairSmem {
   static constexpr int ROW = 64;  // bytes of K per shared-memory row

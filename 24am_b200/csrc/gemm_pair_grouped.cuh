@@ -14,9 +14,9 @@
 //     preceded by a tensormap acquire fence, as tables are rewritten between
 //     launches when a serving loop admits new problems),
 //   * its operand scheme (Z = B V: split FP16, three MMAs per 16 K; V = B^T Z:
-//     that, or two MMAs for the L1-variance forms' exact sgn(z), or one BF16
-//     MMA in a MIXED problem's low-precision phase), the scheme's promotion
-//     chunk and its output scales,
+//     that, or two MMAs for the L1-variance forms' exact sgn(z), or one FP16
+//     MMA on the h0 / g0 planes in a MIXED problem's low-precision phase), the
+//     scheme's promotion chunk and its output scales,
 //   * its epilogue: split-K partial tiles (Z = B V), raw V with the selects'
 //     candidate marks (constraints) or the fused L1 / L0 penalty.
 // A stage holds the largest scheme's planes (two A, two B); smaller schemes
@@ -90,7 +90,7 @@ __device__ __forceinline__ GUnit grouped_unit(const GroupDev &g, int list, int n
   return r;
 }
 
-__device__ __forceinline__ int scheme_na(int sc) { return sc == GS_BF16X1 ? 1 : 2; }
+__device__ __forceinline__ int scheme_na(int sc) { return sc == GS_FP16X1 ? 1 : 2; }
 __device__ __forceinline__ int scheme_nb(int sc) { return sc == GS_FP16X3 ? 2 : 1; }
 // K blocks (of 32) per TMEM chunk before the FP32 promotion: 48 MMA
 // accumulations for the split schemes, the whole unit for single-pass BF16
@@ -174,7 +174,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
   constexpr uint32_t SBO = L::ROW * 8;
   constexpr uint32_t TMEM_COLS = (2 * BN <= 128) ? 128 : (2 * BN <= 256) ? 256 : 512;
   constexpr uint32_t ID_F16 = make_idesc(2 * GEMM_BM, BN, 0u, 0u);
-  constexpr uint32_t ID_BF16 = make_idesc(2 * GEMM_BM, BN, 1u, 1u);
   constexpr uint16_t BOTH = 0x3;
 
   extern __shared__ uint8_t smem_raw[];
@@ -234,8 +233,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
         const CUtensorMap *ma[2], *mb[2];
         if (Z1) {
           ma[0] = &mp.a1_h0; ma[1] = &mp.a1_h1; mb[0] = &mp.b1_h0; mb[1] = &mp.b1_h1;
-        } else if (gu.scheme == GS_BF16X1) {
-          ma[0] = &mp.a2_b0; ma[1] = &mp.a2_b0; mb[0] = &mp.b2_b; mb[1] = &mp.b2_b;
         } else {
           ma[0] = &mp.a2_h0; ma[1] = &mp.a2_h1; mb[0] = &mp.b2_h0; mb[1] = &mp.b2_h1;
         }
@@ -319,7 +316,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
               PairFP16x2A::k_block<ID_F16>(d_tmem, a, b, SBO, first);
             } else {
               const uint32_t a1[1] = {base}, b[1] = {bq};
-              PairBF16x1::k_block<ID_BF16>(d_tmem, a1, b, SBO, first);
+              PairFP16x1::k_block<ID_F16>(d_tmem, a1, b, SBO, first);
             }
             mma_commit_pair(&empty[stage], BOTH);
             if (++stage == STAGES) {
@@ -356,9 +353,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
         ok = grouped_drain<BN>(ep, gu.t, promo, P.k, P.m, P.bt_row_scale, P.v_scale, tmem_base,
                                tfull, tempty, abort, status, tmo, acc, acc_phase, warp, lane);
       } else {
-        const bool fp16 = gu.scheme != GS_BF16X1;
-        const float *rsc = fp16 ? P.row_scale : nullptr;
-        const float *csc = gu.scheme == GS_FP16X3 ? P.z_scale : nullptr;
+        // every scheme reads the scaled FP16 planes; Z's scale only where Z is
+        // not an exact sign (the L1-variance forms)
+        const float *rsc = P.row_scale;
+        const float *csc = P.mode != 1 ? P.z_scale : nullptr;
         if (EPI == GE_RAW) {
           EpiRaw ep{P.Vraw, P.ldn, P.n, P.k, BN};
           ep.hint = P.sel_hint;

@@ -60,8 +60,10 @@ typedef enum {
  * FP32: FP32-accurate products every iteration (split FP16 operands with
  * power-of-two scales on batches of more than 128 starts, 3xTF32 on narrower
  * ones; the residual of each split is below 2^-22 of the value, or 2^-39 of its
- * row's largest).  MIXED: single-pass BF16 operands with FP32
- * accumulation while the supports settle, then the FP32-accurate products from
+ * row's largest).  MIXED: single-pass V = B^T Z (one FP16 MMA per product on
+ * the scaled h0 / g0 planes, 11 significant bits per operand; single-pass BF16
+ * with the environment switch AM24_MIXED_BF16=1) with FP32 accumulation while
+ * the supports settle, then the FP32-accurate products from
  * the first iteration after which a share stable_share of the batch's starts
  * has kept the same support for stable_iterations iterations; the tolerance
  * test applies only from then on.  MIXED needs batches of more than 128 starts
@@ -134,7 +136,7 @@ typedef struct {
   double explained_variance;  /* ||B x||_2^2 of the returned x, FP64 on the device */
   uint64_t start_iterations;  /* AM steps summed over starting points */
   int32_t degenerate_starts;  /* starts whose final objective was NaN */
-  uint32_t low_precision_iterations; /* batch iterations run with BF16 operands */
+  uint32_t low_precision_iterations; /* batch iterations run with single-pass operands */
   int32_t input_rounded_to_f32;       /* 1 when FP64 input was rounded to FP32 before
                                          the solve (am24_solve_dense_f64): the result is
                                          the FP32 solve of the rounded data */
@@ -372,7 +374,9 @@ typedef enum {
   AM24_KERNEL_FINALIZE = 4,  /* per-start objective, change, logs, batch maximum */
   AM24_KERNEL_GATHER_BV = 5, /* Z = B V as a gather over V's non-zeros (sparse steps) */
   AM24_KERNEL_DENSIFY = 6,   /* dense planes of V (FP16 or TF32) for the tensor-core Z = B V */
-  AM24_KERNEL_GEMM_BTZ_BF16 = 7, /* V = B^T Z with single-pass BF16 operands (MIXED) */
+  AM24_KERNEL_GEMM_BTZ_LOW = 7, /* V = B^T Z with single-pass operands (MIXED's first
+                                   phase: FP16, or BF16 with AM24_MIXED_BF16=1) */
+  AM24_KERNEL_GEMM_BTZ_BF16 = 7, /* the same kind under its earlier name */
   AM24_KERNEL_SUPPORT = 8,   /* support-stability count and phase switch (MIXED) */
   AM24_KERNEL_GATHER_BV_GROUP = 9, /* the gather for four starts per block (few non-zeros) */
   AM24_KERNEL_SKIPPED = 0x100 /* or-ed into a kind: the launch returned at once */

@@ -1,7 +1,9 @@
-"""The MIXED precision mode: single-pass BF16 V = B^T Z while the supports
-settle, then the FP32-accurate products.  One BF16 step against an FP64
-product of the BF16-rounded operands, the phase switch, and whole solves that
-reach the FP32 path's explained variance within 1e-4."""
+"""The MIXED precision mode: single-pass V = B^T Z (FP16 operands on the
+scaled h0 / g0 planes, or BF16 with AM24_MIXED_BF16=1) while the supports
+settle, then the FP32-accurate products.  One low-precision step against the
+FP64 product within the single pass's rounding (and, for BF16, against the
+product of the BF16-rounded operands), the phase switch, and whole solves
+that reach the FP32 path's explained variance within 1e-4."""
 import importlib
 
 import numpy as np
@@ -22,10 +24,12 @@ def bf16_round(x):
 
 
 @pytest.mark.parametrize("formulation", [5, 4])
-def test_bf16_step_matches_rounded_product(solver, po, formulation):
-    """With gamma = 0 the L0 penalty keeps every non-zero v, so one BF16-phase
-    step returns V = b0(B)^T Z_b, b0 the BF16 rounding of B and Z_b that of Z
-    (exact for the L1-variance sgn)."""
+def test_bf16_step_matches_rounded_product(solver, po, formulation, monkeypatch):
+    """With AM24_MIXED_BF16=1 the first phase runs single-pass BF16.  With
+    gamma = 0 the L0 penalty keeps every non-zero v, so one such step returns
+    V = b0(B)^T Z_b, b0 the BF16 rounding of B and Z_b that of Z (exact for the
+    L1-variance sgn)."""
+    monkeypatch.setenv("AM24_MIXED_BF16", "1")
     am = _am()
     m, n, k = 300, 2000, 256  # k > 128: CTA-pair tiles, where MIXED applies
     B = po.low_rank_data(m, n, 8, 30, seed=3, dtype=np.float32)
@@ -69,6 +73,47 @@ def test_bf16_step_matches_rounded_product(solver, po, formulation):
     M.close()
 
 
+@pytest.mark.parametrize("formulation", [5, 4])
+def test_fp16_step_is_within_the_single_pass_bound(solver, po, formulation):
+    """The default first phase: one FP16 MMA per product on the scaled h0 / g0
+    planes (each operand rounded to 11 significant bits after a power-of-two
+    scale per feature and per start).  With gamma = 0 one step returns V = B^T Z
+    up to that rounding: each term within 2^-11 (the L1-variance forms, whose
+    sgn(z) is exact) or 2 x 2^-11 of |b| |z|, plus FP32 accumulation; and the
+    error is that of a single pass, far above the FP32-accurate products'."""
+    am = _am()
+    m, n, k = 300, 2000, 256
+    B = po.low_rank_data(m, n, 8, 30, seed=3, dtype=np.float32)
+    V0 = po.uniform_starts(n, k, seed=4, dtype=np.float32)
+    st = am.OptimizationSettings(formulation=formulation, penaltyParameter=0.0, tolerance=1e-6,
+                                 maximumIterations=10, totalStartingPoints=k, batchSize=k,
+                                 precision=am.PRECISION_MIXED)
+    M = solver.matrix(B)
+    b = M.batch(st, k)
+    b.load(V0)
+    kinds = dict(b.step_timed(0))
+    assert "gemm_BtZ_low" in kinds and "gemm_BtZ(skipped)" in kinds
+    assert not b.refining()
+    V1 = b.read()[0].astype(np.float64)
+    B64 = B.astype(np.float64)
+    Y = B64 @ V0.astype(np.float64)
+    if formulation == 5:
+        Z = np.sign(Y)
+        ok = np.abs(Y).min(0) > 1e-4 * np.abs(Y).max(0)
+        unit = 2.0 ** -11
+    else:
+        Z = Y / np.linalg.norm(Y, axis=0)
+        ok = np.ones(k, bool)
+        unit = 2.0 * 2.0 ** -11
+    Vref = B64.T @ Z
+    scale = np.abs(B64).T @ np.abs(Z)
+    rel = np.abs(V1 - Vref)[:, ok] / scale[:, ok]
+    assert rel.max() <= unit + 5e-5, rel.max()
+    assert rel.max() > 1e-5  # a single pass, not the FP32-accurate split
+    b.close()
+    M.close()
+
+
 def test_phase_switches_to_fp32_products(solver, po):
     """Step kernels before and after the switch: the BF16 V = B^T Z runs while
     the supports move, the FP32-accurate one after every start has kept its
@@ -84,7 +129,7 @@ def test_phase_switches_to_fp32_products(solver, po):
     b = M.batch(st, k)
     b.load(V0)
     first = dict(b.step_timed(0))
-    assert "gemm_BtZ_bf16" in first and "gemm_BtZ(skipped)" in first and "support" in first
+    assert "gemm_BtZ_low" in first and "gemm_BtZ(skipped)" in first and "support" in first
     switched_at = None
     for it in range(1, 60):
         b.iterate(it, 1)
@@ -93,7 +138,7 @@ def test_phase_switches_to_fp32_products(solver, po):
             break
     assert switched_at is not None and switched_at >= 3
     after = dict(b.step_timed(switched_at + 1))
-    assert "gemm_BtZ" in after and "gemm_BtZ_bf16(skipped)" in after
+    assert "gemm_BtZ" in after and "gemm_BtZ_low(skipped)" in after
     b.close()
     M.close()
 
