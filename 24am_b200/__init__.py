@@ -142,6 +142,10 @@ _SIGS = {
     "am24_group_result": (C.c_int, [_VP, C.c_uint32, _VP, C.POINTER(am24_statistics)]),
     "am24_group_read": (C.c_int, [_VP, C.c_uint32, _VP, _VP, _VP, _VP]),
     "am24_group_remove": (C.c_int, [_VP, C.c_uint32]),
+    "am24_group_set_autotune": (C.c_int, [_VP, C.c_int32]),
+    "am24_autotune_save": (C.c_int, [C.c_char_p]),
+    "am24_autotune_load": (C.c_int, [C.c_char_p]),
+    "am24_autotune_clear": (C.c_int, []),
 }
 KERNEL_KINDS = ["gemm_BV", "z_reduce", "gemm_BtZ", "select", "finalize", "gather_BV", "densify",
                 "gemm_BtZ_low", "support", "gather_BV_group"]
@@ -627,6 +631,22 @@ class Group:
     def remove(self, pid):
         check(lib().am24_group_remove(self.gh, int(pid)))
         self.problems.pop(pid, None)
+
+    def set_autotune(self, on=True):
+        """Tiles of problems added from now on chosen by timing (am24_group_set_autotune)."""
+        check(lib().am24_group_set_autotune(self.gh, 1 if on else 0))
+
+
+def autotune_save(path):
+    check(lib().am24_autotune_save(os.fsencode(path)))
+
+
+def autotune_load(path):
+    check(lib().am24_autotune_load(os.fsencode(path)))
+
+
+def autotune_clear():
+    check(lib().am24_autotune_clear())
 
 
 class Server:

@@ -11,8 +11,12 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "am24.h"
@@ -45,6 +49,8 @@ struct am24_group_s {
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   float last_ms = 0.f;
+  int autotune = 0;             // am24_group_set_autotune
+  am24_group tuner = nullptr;   // the scratch group the tuner times candidates in
   ~am24_group_s() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -172,6 +178,7 @@ am24_status am24_group_create(am24_handle h, uint32_t capacity, am24_group *out)
 
 am24_status am24_group_destroy(am24_group g) {
   if (!g) return AM24_OK;
+  if (g->tuner) am24_group_destroy(g->tuner);
   cudaSetDevice(g->h->device);
   cudaStreamSynchronize(g->h->stream);
   for (auto &sl : g->slots) sl.mem.reset();  // stream-ordered frees
@@ -180,9 +187,39 @@ am24_status am24_group_destroy(am24_group g) {
   return AM24_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Tile choices of one problem: the N tile of both products and the split-K
+// factor of Z = B V (0: the cost model's).
+struct TileCfg {
+  int bn = 0, splits = 0;
+};
+
+am24_status group_add_impl(am24_group g, am24_matrix mat, const am24_settings *settings,
+                           const float *start_points, const TileCfg &cfg, uint32_t *problem);
+am24_status autotune(am24_group g, am24_matrix mat, const am24_settings &s, TileCfg *out);
+
+}  // namespace
+
+extern "C" {
+
 am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *settings,
                            const float *start_points, uint32_t *problem) {
   if (!g || !mat || !settings || !problem) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  AM24_TRY(validate_settings(settings));
+  TileCfg cfg;
+  if (g->autotune) AM24_TRY(autotune(g, mat, *settings, &cfg));
+  return group_add_impl(g, mat, settings, start_points, cfg, problem);
+}
+
+}  // extern "C"
+
+namespace {
+
+am24_status group_add_impl(am24_group g, am24_matrix mat, const am24_settings *settings,
+                           const float *start_points, const TileCfg &cfg, uint32_t *problem) {
   AM24_TRY(validate_settings(settings));
   if (settings->use_otf || settings->store_all)
     return fail(AM24_ERR_INVALID_ARG, "a group supports neither use_otf nor store_all");
@@ -232,11 +269,17 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
   P.k_stable = s.stable_iterations;
   P.need_stable =
       std::min((uint32_t)k, (uint32_t)std::max(1.0, std::ceil((double)s.stable_share * k - 1e-9)));
-  P.bn = pick_bn(k);
+  P.bn = cfg.bn ? cfg.bn : pick_bn(k);
   P.m_tiles1 = (M.m + BM - 1) / BM;
   P.n_tiles1 = (k + P.bn - 1) / P.bn;
-  choose_splits(((P.m_tiles1 + 1) / 2) * P.n_tiles1, (M.n + PAIR_BK_BF16 - 1) / PAIR_BK_BF16,
-                std::max(1, num_sms() / 2), &P.splits1, &P.kb_per_split1);
+  const int kb1 = (M.n + PAIR_BK_BF16 - 1) / PAIR_BK_BF16;
+  if (cfg.splits > 0) {
+    P.kb_per_split1 = (kb1 + std::min(cfg.splits, kb1) - 1) / std::min(cfg.splits, kb1);
+    P.splits1 = (kb1 + P.kb_per_split1 - 1) / P.kb_per_split1;  // every split non-empty
+  } else {
+    choose_splits(((P.m_tiles1 + 1) / 2) * P.n_tiles1, kb1, std::max(1, num_sms() / 2),
+                  &P.splits1, &P.kb_per_split1);
+  }
   P.m_tiles2 = (M.n + BM - 1) / BM;
   P.n_tiles2 = (k + P.bn - 1) / P.bn;
   P.parts = P.m_tiles2 * 4;
@@ -324,6 +367,10 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
   *problem = (uint32_t)slot;
   return AM24_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 am24_status am24_group_run(am24_group g, uint32_t max_steps, float *device_ms) {
   if (!g) return fail(AM24_ERR_INVALID_ARG, "NULL group");
@@ -475,6 +522,155 @@ am24_status am24_group_remove(am24_group g, uint32_t problem) {
   AM24_CUDA(cudaStreamSynchronize(g->h->stream));
   sl.mem.reset();
   sl = GroupSlot{};
+  return AM24_OK;
+}
+
+}  // extern "C"
+
+// ---- autotuner ------------------------------------------------------------
+// The N tile of a problem's products and the split-K factor of its dense
+// Z = B V are chosen by timing.  Problems fall into buckets of half an octave
+// in each of m, n and k, per formulation mode (L2-variance constrained, L1
+// variance, L2-variance penalized: their operand schemes and selects differ);
+// the first problem of a bucket is timed in a scratch group of its own under
+// each candidate (N tile 64, 128 or 256 where it covers the starts in at most
+// eight tiles; the cost model's split-K, half of it and twice it), three steps
+// from device-generated starts with the tolerance test off, and the fastest
+// (the cost model's choice unless another is more than 2% faster) is kept in a
+// process-wide table for every later problem of the bucket.  A problem's tiles
+// are then a function of its bucket and the table alone, so problems stay the
+// same bit for bit alone and among others for as long as the table holds.
+namespace {
+
+struct TuneKey {
+  int mode, bm, bn, bk;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(mode, bm, bn, bk) < std::tie(o.mode, o.bm, o.bn, o.bk);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TileCfg> g_tune;
+
+int half_octave(int v) { return (int)std::lround(2.0 * std::log2((double)std::max(v, 1))); }
+
+TuneKey tune_key(const MatrixDev &M, const am24_settings &s) {
+  const int f = s.formulation;
+  return TuneKey{is_l1_variance(f) ? 1 : (is_constrained(f) ? 0 : 2), half_octave(M.m),
+                 half_octave(M.n), half_octave(std::max(s.total_starts, 1))};
+}
+
+am24_status autotune(am24_group g, am24_matrix mat, const am24_settings &s0, TileCfg *out) {
+  const MatrixDev &M = mat->d;
+  am24_settings s = s0;
+  AM24_TRY(am24_check_input(&s, (uint32_t)M.n));
+  const TuneKey key = tune_key(M, s);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      *out = it->second;
+      return AM24_OK;
+    }
+  }
+  const int k = s.total_starts;
+  const int kb1 = (M.n + PAIR_BK_BF16 - 1) / PAIR_BK_BF16;
+  const int m_tiles1 = (M.m + BM - 1) / BM;
+  std::vector<TileCfg> cands;
+  for (int bn : {64, 128, 256}) {
+    if (bn != pick_bn(k) && ((k + bn - 1) / bn > 8 || bn >= 2 * k)) continue;
+    int s_model = 1, kbps = 1;
+    choose_splits(((m_tiles1 + 1) / 2) * ((k + bn - 1) / bn), kb1, std::max(1, num_sms() / 2),
+                  &s_model, &kbps);
+    for (int sp : {s_model, std::max(1, s_model / 2), std::min(kb1, 2 * s_model)}) {
+      bool dup = false;
+      for (const auto &c : cands) dup = dup || (c.bn == bn && c.splits == sp);
+      if (!dup) cands.push_back(TileCfg{bn, sp});
+    }
+  }
+  TileCfg best{pick_bn(k), 0};
+  if (cands.size() > 1) {
+    if (!g->tuner) AM24_TRY(am24_group_create(g->h, 1, &g->tuner));
+    am24_settings t = s;
+    t.start_mode = AM24_START_DEVICE_UNIFORM;
+    t.tolerance = 0.0;
+    t.max_iter = 3;
+    t.precision = AM24_PRECISION_FP32;
+    double best_ms = 1e300, model_ms = 1e300;
+    for (size_t i = 0; i <= cands.size(); i++) {
+      const TileCfg &c = cands[i == 0 ? 0 : i - 1];  // the first one twice: warm-up
+      uint32_t slot = 0;
+      AM24_TRY(group_add_impl(g->tuner, mat, &t, nullptr, c, &slot));
+      float ms = 0.f;
+      const am24_status st = am24_group_run(g->tuner, 0, &ms);
+      am24_group_remove(g->tuner, slot);
+      AM24_TRY(st);
+      if (i == 0) continue;
+      if (c.bn == pick_bn(k) && c.splits == cands[0].splits) model_ms = ms;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+    if (model_ms <= 1.02 * best_ms) best = cands[0];
+  } else if (!cands.empty()) {
+    best = cands[0];
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  *out = best;
+  return AM24_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+am24_status am24_group_set_autotune(am24_group g, int32_t on) {
+  if (!g) return fail(AM24_ERR_INVALID_ARG, "NULL group");
+  g->autotune = on ? 1 : 0;
+  return AM24_OK;
+}
+
+am24_status am24_autotune_save(const char *path) {
+  if (!path) return fail(AM24_ERR_INVALID_ARG, "NULL path");
+  FILE *f = fopen(path, "w");
+  if (!f) return fail(AM24_ERR_INVALID_ARG, std::string("cannot write ") + path);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  fprintf(f, "# am24 autotune: mode m n k (half-octave buckets) -> n_tile splitk\n");
+  for (const auto &kv : g_tune)
+    fprintf(f, "%d %d %d %d %d %d\n", kv.first.mode, kv.first.bm, kv.first.bn, kv.first.bk,
+            kv.second.bn, kv.second.splits);
+  fclose(f);
+  return AM24_OK;
+}
+
+am24_status am24_autotune_load(const char *path) {
+  if (!path) return fail(AM24_ERR_INVALID_ARG, "NULL path");
+  FILE *f = fopen(path, "r");
+  if (!f) return fail(AM24_ERR_INVALID_ARG, std::string("cannot read ") + path);
+  char line[256];
+  std::map<TuneKey, TileCfg> add;
+  while (fgets(line, sizeof line, f)) {
+    if (line[0] == '#') continue;
+    TuneKey k{};
+    TileCfg c{};
+    if (sscanf(line, "%d %d %d %d %d %d", &k.mode, &k.bm, &k.bn, &k.bk, &c.bn, &c.splits) != 6)
+      continue;
+    if ((c.bn != 64 && c.bn != 128 && c.bn != 256) || c.splits < 0) {
+      fclose(f);
+      return fail(AM24_ERR_INVALID_ARG, std::string("bad autotune entry in ") + path);
+    }
+    add[k] = c;
+  }
+  fclose(f);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (const auto &kv : add) g_tune[kv.first] = kv.second;
+  return AM24_OK;
+}
+
+am24_status am24_autotune_clear(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
   return AM24_OK;
 }
 

@@ -364,6 +364,20 @@ am24_status am24_group_read(am24_group g, uint32_t problem, float *V, float *val
                             uint32_t *nnz);
 /* Frees the problem's slot and device memory. */
 am24_status am24_group_remove(am24_group g, uint32_t problem);
+/* With on != 0, problems added from now on take tiles chosen by timing: the N
+ * tile of both products (64, 128 or 256) and the split-K factor of the dense
+ * Z = B V.  Problems fall into buckets of half an octave in m, n and k per
+ * formulation mode; the first problem of a bucket is timed in a scratch group
+ * under each candidate (three steps each, from device-generated starts) and
+ * the fastest is kept in a process-wide table that every later problem of the
+ * bucket uses.  Off (the default), the tiles come from a fixed cost model.
+ * A problem's result depends on its tiles only through FP32 summation order. */
+am24_status am24_group_set_autotune(am24_group g, int32_t on);
+/* The autotuner's table: written to / merged from a text file (one line per
+ * bucket), or emptied. */
+am24_status am24_autotune_save(const char *path);
+am24_status am24_autotune_load(const char *path);
+am24_status am24_autotune_clear(void);
 
 /* Kernel kinds reported by am24_batch_step_timed. */
 typedef enum {

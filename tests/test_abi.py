@@ -118,3 +118,21 @@ def test_csc_arrays_checked_on_the_host(am, rows, ptr, msg):
                                       r.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p),
                                       3, 2, None, None, C.byref(out))
     assert st == 1 and msg in am.last_error()
+
+
+def test_autotune_table_round_trip(am, tmp_path):
+    """The autotuner's table: a file loaded, saved back the same, a malformed
+    entry rejected (no device needed)."""
+    src = tmp_path / "t.txt"
+    src.write_text("# header\n0 16 26 18 256 6\n1 14 24 16 128 0\n")
+    am.autotune_clear()
+    am.autotune_load(str(src))
+    out = tmp_path / "o.txt"
+    am.autotune_save(str(out))
+    body = [l for l in out.read_text().splitlines() if not l.startswith("#")]
+    assert body == ["0 16 26 18 256 6", "1 14 24 16 128 0"]
+    bad = tmp_path / "bad.txt"
+    bad.write_text("0 16 26 18 96 1\n")
+    with pytest.raises(am.Am24Error):
+        am.autotune_load(str(bad))
+    am.autotune_clear()

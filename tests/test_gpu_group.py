@@ -168,3 +168,39 @@ def test_slots_are_reused_and_results_stay_put(solver, po):
         grp.add(M, st, start_points=V)  # full
     grp.close()
     M.close()
+
+
+def test_autotuned_tiles_solve_like_the_cost_model(solver, po, tmp_path):
+    """Problems added with autotuning on take the tiles the tuner timed (kept
+    per bucket: a second problem of the bucket reuses them); the solves reach
+    the same explained variance as with the cost model's tiles, and the table
+    saved and loaded back gives the same tiles without timing again."""
+    am = _am()
+    am.autotune_clear()
+    specs = [(300, 2048, 200, 0, 12), (300, 2048, 200, 0, 12), (129, 4097, 300, 5, 0)]
+    runs = []
+    for tuned in (False, True):
+        grp = am.Group(solver, capacity=8)
+        grp.set_autotune(tuned)
+        mats, ids = [], []
+        for i, spec in enumerate(specs):
+            B, V, st = _setup(am, po, spec, 400 + (i % 2 if i < 2 else i))
+            M = solver.matrix(B)
+            mats.append(M)
+            ids.append(grp.add(M, st, start_points=V))
+        grp.run()
+        runs.append([grp.result(p) for p in ids])
+        grp.close()
+        for M in mats:
+            M.close()
+    for (x0, s0), (x1, s1) in zip(*runs):
+        assert abs(s1.explained_variance - s0.explained_variance) <= 1e-5 * s0.explained_variance
+        assert abs(int(s1.it) - int(s0.it)) <= 2
+    path = str(tmp_path / "tune.txt")
+    am.autotune_save(path)
+    lines = [l for l in open(path) if not l.startswith("#")]
+    assert len(lines) == 2  # two buckets
+    am.autotune_clear()
+    am.autotune_load(path)
+    am.autotune_save(path + ".2")
+    assert open(path).read() == open(path + ".2").read()
