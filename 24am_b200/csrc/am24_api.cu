@@ -369,10 +369,8 @@ am24_status upload_columns(am24_handle h, am24_batch b, const float *host, int c
                                   b->d.vmask + (size_t)slots[c] * (M.ldn / 32), h->stream));
     AM24_CUDA(cudaMemsetAsync(b->d.sel_hint + slots[c], 0, sizeof(float), h->stream));
   }
-  // new starts are dense: the next Z = B V runs on the tensor cores, and
-  // densify takes their column scales from a pass over them
+  // new starts are dense: the next Z = B V runs on the tensor cores
   AM24_CUDA(cudaMemsetAsync(b->d.max_nnz, 0xFF, sizeof(uint32_t), h->stream));
-  AM24_CUDA(cudaMemsetAsync(b->d.ctl + CTL_PARTS_OK, 0, sizeof(uint32_t), h->stream));
   AM24_CUDA(cudaMemsetAsync(b->d.planes_nnz, 0, sizeof(uint32_t), h->stream));  // stale planes
   return AM24_OK;
 }
@@ -786,8 +784,6 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
       (st = A.get(&d.ws, d.ws_len)) ||
       (st = A.get(&d.fz, k)) || (st = A.get(&d.obj_part, (size_t)k * parts)) ||
       (st = A.get(&d.nnz_part, (size_t)k * parts)) || (st = A.get(&d.nnz, k)) ||
-      (d.fp16_1 && !is_constrained(settings->formulation) &&
-       (st = A.get(&d.max_part, (size_t)k * parts))) ||
       (st = A.get(&d.val, k)) || (st = A.get(&d.err, k)) || (st = A.get(&d.max_err, 1)) ||
       (st = A.get(&d.iters, d.log_capacity)) || (st = A.get(&d.cards, d.log_capacity)) ||
       (st = A.get(&d.status, 1)) || (st = A.get(&d.vmask, (size_t)k * (M.ldn / 32))) ||

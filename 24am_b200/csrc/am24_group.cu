@@ -128,7 +128,7 @@ uint64_t group_problem_bytes(int m, int n, int k, int formulation, bool mixed) {
   uint64_t b = kv * 4 * 2 + kv * 2 * 2 + words * 4 * (is_constrained(formulation) ? 2 : 1) +
                kz * (4 + 4 + 2 * zh) +
                (uint64_t)ws_floats(splits, (int)m_tiles1, (int)n_tiles, bn) * 4 +
-               (uint64_t)k * (4 * 8 + parts * 12 + (mixed ? 16 : 0)) + 4096;
+               (uint64_t)k * (4 * 8 + parts * 8 + (mixed ? 16 : 0)) + 4096;
   return b;
 }
 
@@ -299,7 +299,6 @@ am24_status group_add_impl(am24_group g, am24_matrix mat, const am24_settings *s
       (st = A->get(&P.ws, ws_floats(P.splits1, P.m_tiles1, P.n_tiles1, P.bn))) ||
       (st = A->get(&P.fz, k)) || (st = A->get(&P.val, k)) || (st = A->get(&P.err, k)) ||
       (st = A->get(&P.max_err, 1)) || (st = A->get(&P.obj_part, (size_t)k * P.parts)) ||
-      (!is_constrained(f) && (st = A->get(&P.max_part, (size_t)k * P.parts))) ||
       (st = A->get(&P.nnz_part, (size_t)k * P.parts)) || (st = A->get(&P.ctl, GCTL_WORDS)) ||
       (st = A->get(&P.status, 1)) ||
       (mixed && ((st = A->get(&P.stable, k)) || (st = A->get(&P.phase, 4)) ||

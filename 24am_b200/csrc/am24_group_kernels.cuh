@@ -174,8 +174,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) g_gather_kernel(GroupDev g) {
 __global__ void __launch_bounds__(256) g_densify_kernel(GroupDev g, int mode) {
   for_items(g, GL_DN0 + mode, [](const GProblem &P, int j) {
     densify_fp16_body(P.Vx, P.vmask, P.ldn, P.n, P.V_h, (size_t)P.k * P.ldn, P.v_scale,
-                      P.ctl + GCTL_GATE, P.sparse_cap, P.ctl + CTL_STOP, j, P.max_part, P.parts,
-                      P.ctl + CTL_PARTS_OK);
+                      P.ctl + GCTL_GATE, P.sparse_cap, P.ctl + CTL_STOP, j);
   });
 }
 
@@ -286,7 +285,6 @@ __global__ void __launch_bounds__(256) g_finalize_kernel(GroupDev g) {
         P.ctl[CTL_STEPS] = steps;
         if (!refined) P.ctl[CTL_LOW_STEPS] += 1u;
         P.ctl[CTL_MAX_ERR] = __float_as_uint(me);
-        P.ctl[CTL_PARTS_OK] = 1u;  // this step's V = B^T Z wrote every max part
         if ((a.it > 0 && refined && (double)me < P.tolerance) ||
             steps >= (uint32_t)P.max_iter ||
             *reinterpret_cast<const volatile int *>(P.status) != 0)

@@ -97,8 +97,6 @@ struct BatchDev {
   float *ws;            // split-K partial tiles of Z = B V
   float *fz;            // per start: ||y||_2 or ||y||_1 from the Z reduction
   float *obj_part;      // per start x (m_tiles2*4): penalized objective partials
-  uint32_t *max_part;   // ... and the kept entries' largest |x| key (penalized forms
-                        // on the FP16 pairs: densify's column scale), else null
   float *nnz_part;      // per start x (m_tiles2*4): penalized non-zero partials
   uint32_t *nnz;        // per start: non-zeros after thresholding
   float *sel_hint;      // per start: last threshold level (0 = none), a search hint
@@ -142,8 +140,6 @@ enum : int {
   CTL_LOW_STEPS = 2,  // ... of them in the BF16 phase (MIXED)
   CTL_MAX_ERR = 3,    // the last executed step's largest change (float bits)
   CTL_BLOCKS = 4,     // finalize's block counter (scratch)
-  CTL_PARTS_OK = 5,   // a step has run since the load: the penalty epilogue's
-                      // max parts cover every start's current loadings
   CTL_WORDS = 8
 };
 
@@ -227,7 +223,6 @@ struct GProblem {
   int parts;                       // m_tiles2 * 4 penalty partials per start
   // state
   float *Vx, *Vraw, *sel_hint, *Z_hi, *Z_lo, *fz, *obj_part, *nnz_part, *val, *err, *max_err;
-  uint32_t *max_part;  // penalized forms: the largest kept |x| key per start and part
   float *z_scale, *v_scale, *ws;
   uint32_t *vmask, *cmask, *nnz, *ctl, *stable, *phase;
   uint64_t *mask_hash;  // MIXED: per start, a hash of the last step's support

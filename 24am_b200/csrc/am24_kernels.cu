@@ -241,10 +241,6 @@ struct EpiPenalty {
   const uint32_t *max_nnz;  // the previous step's largest non-zero count
   uint32_t cap;             // ... above which Z = B V runs dense
   bool planes = false;      // this launch writes V_hi / V_lo (set by setup)
-  // optional, per start and (128-row block, warp): the largest |x| key of the
-  // kept entries, so that the next dense step's FP16 planes of V take their
-  // column scale from these parts instead of a pass over the column
-  uint32_t *max_part = nullptr;
   __device__ void setup() { planes = V_hi != nullptr && *max_nnz > cap; }
   __device__ void unit_begin(const Unit &, int, int) {}
   // r holds this thread's 32 values (row `row`, columns col0..col0+31) and is
@@ -264,7 +260,6 @@ struct EpiPenalty {
     const int c0 = t.nt * bn + col0;
     const int ncols = rv ? min(32, N - c0) : 0;  // valid columns of this row
     uint32_t bits = 0u;  // bit j: (row, column c0 + j) is a non-zero
-    uint32_t mine = 0u;  // lane j: the largest kept |x| key of column c0 + j
 #pragma unroll
     for (int j = 0; j < 32; j++) {
       const float v = r[j];
@@ -288,10 +283,6 @@ struct EpiPenalty {
         const size_t o = (size_t)(c0 + j) * ld + gi;
         split_store(nz ? x : 0.f, V_hi + o, V_lo + o);
       }
-      if (max_part) {  // uniform over the warp
-        const uint32_t mk = __reduce_max_sync(FULL, nz ? abs_key(x) : 0u);
-        if (lane == j) mine = mk;
-      }
     }
     const uint32_t word = bit_transpose32(bits, lane);  // lane j: column c0 + j, bit = row
     const float so = transpose_reduce32(r, lane);
@@ -299,7 +290,6 @@ struct EpiPenalty {
     if (col < N) {
       obj_part[(size_t)col * parts + mb * 4 + q] = so;
       nnz_part[(size_t)col * parts + mb * 4 + q] = (float)__popc(word);
-      if (max_part) max_part[(size_t)col * parts + mb * 4 + q] = mine;
       if (mb * 4 + q < (ld >> 5)) vmask[(size_t)col * (ld >> 5) + mb * 4 + q] = word;
     }
   }
@@ -471,20 +461,14 @@ __global__ void densify_kernel(const float *__restrict__ Vx, const uint32_t *__r
 // with s from the column's largest |v|, v_scale[c] = 2^-s.
 // The body for start c (one 256-thread block); densify_fp16_kernel runs it for
 // blockIdx.x, the grouped steps for every start of their dense problems.
-// With max_part (parts words per start) valid (*parts_ok), the column's
-// largest |v| comes from the penalty epilogue's parts and V is read once.
 __device__ __forceinline__ void densify_fp16_body(const float *__restrict__ Vx,
                                                   const uint32_t *__restrict__ mask, int ld,
                                                   int rows, uint16_t *__restrict__ Vh,
                                                   size_t plane, float *__restrict__ v_scale,
                                                   const uint32_t *gate, uint32_t gate_max,
-                                                  const uint32_t *stop, size_t c,
-                                                  const uint32_t *__restrict__ max_part = nullptr,
-                                                  int parts = 0,
-                                                  const uint32_t *parts_ok = nullptr) {
+                                                  const uint32_t *stop, size_t c) {
   __shared__ uint32_t red[8];
   if (*stop || *gate <= gate_max) return;
-  const bool from_parts = max_part && *parts_ok != 0u;
   const uint32_t *mk = mask + c * (ld >> 5);
   const float4 *vx4 = reinterpret_cast<const float4 *>(Vx + c * ld);
   // four consecutive rows per thread and pass (ld is a multiple of 32)
@@ -498,15 +482,11 @@ __device__ __forceinline__ void densify_fp16_body(const float *__restrict__ Vx,
   };
   const int quads = ld >> 2;
   uint32_t mx = 0;
-  if (from_parts) {
-    for (int i = threadIdx.x; i < parts; i += blockDim.x) mx = max(mx, max_part[c * parts + i]);
-  } else {
 #pragma unroll 4
-    for (int q = threadIdx.x; q < quads; q += blockDim.x) {
-      float v[4];
-      quad(q, v);
-      mx = max(mx, max(max(abs_key(v[0]), abs_key(v[1])), max(abs_key(v[2]), abs_key(v[3]))));
-    }
+  for (int q = threadIdx.x; q < quads; q += blockDim.x) {
+    float v[4];
+    quad(q, v);
+    mx = max(mx, max(max(abs_key(v[0]), abs_key(v[1])), max(abs_key(v[2]), abs_key(v[3]))));
   }
   mx = __reduce_max_sync(FULL, mx);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
@@ -536,11 +516,8 @@ __global__ void __launch_bounds__(256) densify_fp16_kernel(const float *__restri
                                                            uint16_t *__restrict__ Vh, size_t plane,
                                                            float *__restrict__ v_scale,
                                                            const uint32_t *gate, uint32_t gate_max,
-                                                           const uint32_t *stop,
-                                                           const uint32_t *max_part, int parts,
-                                                           const uint32_t *parts_ok) {
-  densify_fp16_body(Vx, mask, ld, rows, Vh, plane, v_scale, gate, gate_max, stop, blockIdx.x,
-                    max_part, parts, parts_ok);
+                                                           const uint32_t *stop) {
+  densify_fp16_body(Vx, mask, ld, rows, Vh, plane, v_scale, gate, gate_max, stop, blockIdx.x);
 }
 
 // ------------------------------------------------------------ Z reduction
@@ -1982,7 +1959,6 @@ __global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs a) {
       a.ctl[CTL_STEPS] += 1u;
       if (!refined) a.ctl[CTL_LOW_STEPS] += 1u;
       a.ctl[CTL_MAX_ERR] = __float_as_uint(me);
-      a.ctl[CTL_PARTS_OK] = 1u;  // this step's V = B^T Z wrote every max part
       if ((a.stop_check && a.it > 0 && refined && (double)me < a.tolerance) ||
           *reinterpret_cast<const volatile int *>(a.status) != 0)
         a.ctl[CTL_STOP] = 1u;
@@ -2495,8 +2471,7 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   if (b.fp16_1)
     densify_fp16_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_h,
                                              (size_t)b.k * M.ldn, b.v_scale, b.max_nnz,
-                                             b.sparse_cap, b.ctl, b.max_part, b.m_tiles2 * 4,
-                                             b.ctl + CTL_PARTS_OK);
+                                             b.sparse_cap, b.ctl);
   else
     densify_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_hi, b.V_lo, b.max_nnz,
                                         b.planes_nnz, b.sparse_cap, b.ctl);
@@ -2594,13 +2569,11 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
     EpiPenalty<true> pe{b.Vx,       b.obj_part, b.nnz_part, M.ldn,    M.n,
                         b.k,        b.bn2,      parts,      (float)p.penalty,
                         b.vmask,    vhi,        b.V_lo,     b.max_nnz, b.sparse_cap};
-    pe.max_part = b.max_part;
     e = gemm2(pe);
   } else {
     EpiPenalty<false> pe{b.Vx,       b.obj_part, b.nnz_part, M.ldn,    M.n,
                          b.k,        b.bn2,      parts,      (float)p.penalty,
                          b.vmask,    vhi,        b.V_lo,     b.max_nnz, b.sparse_cap};
-    pe.max_part = b.max_part;
     e = gemm2(pe);
   }
   if (e != cudaSuccess) return e;

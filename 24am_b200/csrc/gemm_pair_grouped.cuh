@@ -367,14 +367,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
           EpiPenalty<true> ep{P.Vx,  P.obj_part, P.nnz_part, P.ldn,   P.n,       P.k,
                               BN,    P.parts,    P.gamma,    P.vmask, nullptr,   nullptr,
                               P.ctl + GCTL_GATE, P.sparse_cap};
-          ep.max_part = P.max_part;
           ok = grouped_drain<BN>(ep, gu.t, promo, P.k, P.n, rsc, csc, tmem_base, tfull, tempty,
                                  abort, status, tmo, acc, acc_phase, warp, lane);
         } else {
           EpiPenalty<false> ep{P.Vx,  P.obj_part, P.nnz_part, P.ldn,   P.n,       P.k,
                                BN,    P.parts,    P.gamma,    P.vmask, nullptr,   nullptr,
                                P.ctl + GCTL_GATE, P.sparse_cap};
-          ep.max_part = P.max_part;
           ok = grouped_drain<BN>(ep, gu.t, promo, P.k, P.n, rsc, csc, tmem_base, tfull, tempty,
                                  abort, status, tmo, acc, acc_phase, warp, lane);
         }
