@@ -289,9 +289,12 @@ class Solver:
         check(lib().am24_create(C.byref(h), int(device)))
         self.h = h
         self._matrices = weakref.WeakSet()
+        self._groups = weakref.WeakSet()
 
     def close(self):
         if self.h:
+            for g in list(self._groups):  # their problems read the matrices
+                g.close()
             for m in list(self._matrices):
                 m.close()
             lib().am24_destroy(self.h)
@@ -419,10 +422,15 @@ class Matrix:
         return self
 
     def close(self):
-        """Destroys the matrix, after any batch still open on it."""
+        """Destroys the matrix, after any batch still open on it and any group
+        problem on it."""
         if self.mh:
             for b in list(self._batches):
                 b.close()
+            for g in list(getattr(self.solver, "_groups", ())):
+                for pid, (mat, _) in list(g.problems.items()):
+                    if mat is self:
+                        g.remove(pid)
             lib().am24_matrix_destroy(self.solver.h, self.mh)
             self.mh = None
 
@@ -571,6 +579,7 @@ class Group:
         check(lib().am24_group_create(solver.h, int(capacity), C.byref(gh)))
         self.gh = gh
         self.problems = {}  # id -> (matrix, k)
+        solver._groups.add(self)
 
     def close(self):
         if self.gh:

@@ -171,7 +171,8 @@ __global__ void __launch_bounds__(GATHER_THREADS) g_gather_kernel(GroupDev g) {
 }
 
 // dense steps before Z = B V: the FP16 planes of V (the problems of mode `mode`)
-__global__ void __launch_bounds__(256) g_densify_kernel(GroupDev g, int mode) {
+__global__ void __launch_bounds__(DENSIFY_THREADS, DENSIFY_BLOCKS_PER_SM)
+    g_densify_kernel(GroupDev g, int mode) {
   for_items(g, GL_DN0 + mode, [](const GProblem &P, int j) {
     densify_fp16_body(P.Vx, P.vmask, P.ldn, P.n, P.V_h, (size_t)P.k * P.ldn, P.v_scale,
                       P.ctl + GCTL_GATE, P.sparse_cap, P.ctl + CTL_STOP, j);

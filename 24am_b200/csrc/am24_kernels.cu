@@ -467,7 +467,7 @@ __device__ __forceinline__ void densify_fp16_body(const float *__restrict__ Vx,
                                                   size_t plane, float *__restrict__ v_scale,
                                                   const uint32_t *gate, uint32_t gate_max,
                                                   const uint32_t *stop, size_t c) {
-  __shared__ uint32_t red[8];
+  __shared__ uint32_t red[32];
   if (*stop || *gate <= gate_max) return;
   const uint32_t *mk = mask + c * (ld >> 5);
   const float4 *vx4 = reinterpret_cast<const float4 *>(Vx + c * ld);
@@ -482,7 +482,7 @@ __device__ __forceinline__ void densify_fp16_body(const float *__restrict__ Vx,
   };
   const int quads = ld >> 2;
   uint32_t mx = 0;
-#pragma unroll 4
+#pragma unroll 8
   for (int q = threadIdx.x; q < quads; q += blockDim.x) {
     float v[4];
     quad(q, v);
@@ -492,8 +492,7 @@ __device__ __forceinline__ void densify_fp16_body(const float *__restrict__ Vx,
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
   __syncthreads();
   mx = 0;
-#pragma unroll
-  for (int w = 0; w < 8; w++) mx = max(mx, red[w]);
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) mx = max(mx, red[w]);
   const int s = fp16_shift(__uint_as_float(mx));
   const float sc = pow2f(s);
   if (threadIdx.x == 0) v_scale[c] = pow2f(-s);
@@ -510,14 +509,19 @@ __device__ __forceinline__ void densify_fp16_body(const float *__restrict__ Vx,
     h1[q] = make_uint2(b[0] | ((uint32_t)b[1] << 16), b[2] | ((uint32_t)b[3] << 16));
   }
 }
-__global__ void __launch_bounds__(256) densify_fp16_kernel(const float *__restrict__ Vx,
-                                                           const uint32_t *__restrict__ mask,
-                                                           int ld, int rows,
-                                                           uint16_t *__restrict__ Vh, size_t plane,
-                                                           float *__restrict__ v_scale,
-                                                           const uint32_t *gate, uint32_t gate_max,
-                                                           const uint32_t *stop) {
-  densify_fp16_body(Vx, mask, ld, rows, Vh, plane, v_scale, gate, gate_max, stop, blockIdx.x);
+// Persistent over the k columns with DENSIFY_BLOCKS_PER_SM blocks of 512
+// threads per SM: a column's first pass (its largest |v|) streams it from HBM,
+// and with this few columns in flight (2 x 148 x 4 B x p, 59 MB at p = 50000)
+// the second pass finds it in L2, so V crosses HBM once.
+constexpr int DENSIFY_THREADS = 512, DENSIFY_BLOCKS_PER_SM = 2;
+__global__ void __launch_bounds__(DENSIFY_THREADS, DENSIFY_BLOCKS_PER_SM) densify_fp16_kernel(
+    const float *__restrict__ Vx, const uint32_t *__restrict__ mask, int ld, int rows,
+    uint16_t *__restrict__ Vh, size_t plane, float *__restrict__ v_scale, const uint32_t *gate,
+    uint32_t gate_max, const uint32_t *stop, int k) {
+  for (int c = blockIdx.x; c < k; c += gridDim.x) {
+    densify_fp16_body(Vx, mask, ld, rows, Vh, plane, v_scale, gate, gate_max, stop, c);
+    __syncthreads();  // red[] is reused by the next column
+  }
 }
 
 // ------------------------------------------------------------ Z reduction
@@ -2469,9 +2473,9 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
   // 1b. dense V: TF32 hi/lo planes, tensor-core Z = B V (split-K partials) ...
   if ((e = mark(6)) != cudaSuccess) return e;
   if (b.fp16_1)
-    densify_fp16_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_h,
-                                             (size_t)b.k * M.ldn, b.v_scale, b.max_nnz,
-                                             b.sparse_cap, b.ctl);
+    densify_fp16_kernel<<<std::min(b.k, DENSIFY_BLOCKS_PER_SM * num_sms()), DENSIFY_THREADS, 0,
+                          st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_h, (size_t)b.k * M.ldn, b.v_scale,
+                                b.max_nnz, b.sparse_cap, b.ctl, b.k);
   else
     densify_kernel<<<b.k, 256, 0, st>>>(b.Vx, b.vmask, M.ldn, M.n, b.V_hi, b.V_lo, b.max_nnz,
                                         b.planes_nnz, b.sparse_cap, b.ctl);
@@ -2712,7 +2716,7 @@ cudaError_t grouped_grids(GroupGrids *gr) {
     return e;
   gr->plan_threads = PLAN_THREADS;
   gr->pairs = c;
-  if ((e = persistent_grid(g_densify_kernel, 256, 0, &gr->col)) ||
+  if ((e = persistent_grid(g_z_reduce_kernel<0>, 256, 0, &gr->col)) ||
       (e = persistent_grid(g_hard_select_kernel, HARD_THREADS, 0, &gr->select_hard)) ||
       (e = persistent_grid(g_soft_select_kernel<false>, SOFT_THREADS, 0, &gr->select_soft)) ||
       (e = persistent_grid(g_gather_kernel<0>, GATHER_THREADS, 0, &gr->gather)) ||
@@ -2734,7 +2738,8 @@ cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &gr, cudaStr
   g_gather_kernel<0><<<gr.gather, GATHER_THREADS, 0, st>>>(g);
   g_gather_kernel<1><<<gr.gather, GATHER_THREADS, 0, st>>>(g);
   g_gather_kernel<2><<<gr.gather, GATHER_THREADS, 0, st>>>(g);
-  for (int mode = 0; mode < 3; mode++) g_densify_kernel<<<gr.col, 256, 0, st>>>(g, mode);
+  for (int mode = 0; mode < 3; mode++)
+    g_densify_kernel<<<DENSIFY_BLOCKS_PER_SM * num_sms(), DENSIFY_THREADS, 0, st>>>(g, mode);
   if ((e = cudaGetLastError())) return e;
   if ((e = launch_grouped_gemms<GE_PARTIAL>(g, GL_GEMM1_64, st))) return e;
   g_z_reduce_kernel<0><<<gr.col, 256, 0, st>>>(g);

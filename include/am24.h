@@ -333,7 +333,9 @@ am24_status am24_wait(am24_server s, uint64_t ticket, float *x, am24_statistics 
  * (it > 0, largest change below the tolerance, in the refinement phase; or
  * max_iter steps).  Its tiles, split-K and reduction order depend on it
  * alone, so its result is the same bit for bit alone and among others.
- * A group belongs to one handle and runs on its stream. */
+ * A group belongs to one handle and runs on its stream; destroy it before the
+ * handle, and remove a matrix's problems (or destroy the group) before the
+ * matrix. */
 typedef struct am24_group_s *am24_group;
 am24_status am24_group_create(am24_handle h, uint32_t capacity, am24_group *out);
 /* Waits for the handle's stream, then frees every problem and the group. */

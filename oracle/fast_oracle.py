@@ -98,16 +98,23 @@ def soft_levels(Vr, s, cols=None):
     return np.array([a for a, _ in r]), np.array([b for _, b in r], np.int64)
 
 
-def _soft_ill(Vr, s, w0, b0, trials=1, seed=0):
-    """L1 ball: the scan's rank or level moves under FP32-size noise, an entry
-    lies within rounding of the level, or the scan stops at its first rank."""
+# Per-entry size of the noise the L1-ball check perturbs v with, relative to
+# the column's largest |v|: a few times the error of an FP32-accurate product
+# entry (about 1e-7 of that scale), the same for every column length.
+SOFT_NOISE = 3e-7
+
+
+def _soft_ill(Vr, s, w0, b0, trials=3, seed=0):
+    """L1 ball: the scan's rank or level moves under noise of the size of the
+    products' FP32 error, an entry lies within rounding of the level, or the
+    scan stops at its first rank."""
     n, k = Vr.shape
     scale = np.abs(Vr).max(axis=0)
     ill = (b0 == 0)
     ill |= np.min(np.abs(np.abs(Vr) - w0[None, :]), axis=0) <= MARGIN * scale
     rng = np.random.default_rng(seed)
     for _ in range(trials):
-        P = Vr + (MARGIN * scale / np.sqrt(n))[None, :] * rng.standard_normal(Vr.shape)
+        P = Vr + (SOFT_NOISE * scale)[None, :] * rng.standard_normal(Vr.shape)
         w, b = soft_levels(P, s)
         ill |= (b != b0) | (np.abs(w - w0) > 1e-4 * np.maximum(np.abs(w0), 1e-300))
     return ill
