@@ -428,6 +428,8 @@ class Matrix:
             for b in list(self._batches):
                 b.close()
             for g in list(getattr(self.solver, "_groups", ())):
+                if not g.gh:
+                    continue
                 for pid, (mat, _) in list(g.problems.items()):
                     if mat is self:
                         g.remove(pid)
@@ -585,6 +587,8 @@ class Group:
         if self.gh:
             lib().am24_group_destroy(self.gh)
             self.gh = None
+            self.problems = {}
+            self.solver._groups.discard(self)
 
     def __enter__(self):
         return self

@@ -91,6 +91,7 @@ struct am24_server_s {
   std::deque<RequestPtr> queue;
   std::map<uint64_t, RequestPtr> tickets;
   bool stop = false;
+  std::string stop_reason;  // why the engine stopped before destroy, for callers
 };
 
 namespace {
@@ -169,11 +170,14 @@ void engine_loop(am24_server s) {
       am24_group_destroy(s->g);
       s->g = nullptr;
       if (am24_group_create(s->h, SERVE_SLOTS, &s->g) != AM24_OK) {
+        const std::string create_err = g_last_error;
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;  // cannot serve any more: drain the queue with errors
+        s->stop_reason = "a grouped run failed (" + err +
+                         ") and the engine could not be restarted (" + create_err + ")";
         for (auto &r : s->queue) {
           r->status = AM24_ERR_CUDA;
-          r->error = "the serving engine could not be restarted";
+          r->error = s->stop_reason;
           r->done = true;
           s->matrices.at(r->matrix_id).pending--;
         }
@@ -318,7 +322,10 @@ am24_status am24_submit(am24_server s, uint32_t matrix_id, const am24_settings *
   auto r = std::make_shared<ServeRequest>();
   r->s = *settings;
   std::lock_guard<std::mutex> lk(s->mu);
-  if (s->stop) return fail(AM24_ERR_CUDA, "the server has stopped");
+  if (s->stop)
+    return fail(AM24_ERR_CUDA, "the server has stopped" +
+                                   (s->stop_reason.empty() ? std::string()
+                                                           : ": " + s->stop_reason));
   auto it = s->matrices.find(matrix_id);
   if (it == s->matrices.end()) return fail(AM24_ERR_INVALID_ARG, "unknown matrix id");
   const uint32_t n = it->second.n, m = it->second.m;

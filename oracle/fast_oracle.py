@@ -188,8 +188,9 @@ def iteration(B, V, formulation, s=0, gamma=0.0, val=None, check=True, keep_vraw
     if check and l1var:
         # a sign within rounding of zero: |y_i| within MARGIN of the 2-norm of
         # the terms b_ij v_j it sums (the scale of a blocked FP32 sum's error)
+        # (a column of zeros gives y = 0 and sign 0 on both sides: not a tie)
         bound = np.sqrt((B * B) @ (V * V))
-        ill |= np.any(np.abs(Y) <= MARGIN * bound, axis=0)
+        ill |= np.any((np.abs(Y) <= MARGIN * bound) & (bound > 0), axis=0)
     with np.errstate(divide="ignore", invalid="ignore"):
         if form <= 3:
             if l1var:
