@@ -305,6 +305,18 @@ am24_status group_add_impl(am24_group g, am24_matrix mat, const am24_settings *s
                  (st = A->get(&P.mask_hash, k)))))
     return st;
   const cudaStream_t hs = h->stream;
+  // every buffer starts zeroed, as a batch's do: a slot's memory may come back
+  // from the pool holding an earlier problem's state
+  AM24_CUDA(cudaMemsetAsync(P.Vx, 0, sizeof(float) * kv, hs));
+  AM24_CUDA(cudaMemsetAsync(P.Vraw, 0, sizeof(float) * kv, hs));
+  AM24_CUDA(cudaMemsetAsync(P.vmask, 0, sizeof(uint32_t) * words, hs));
+  AM24_CUDA(cudaMemsetAsync(P.Z_hi, 0, sizeof(float) * kz, hs));
+  AM24_CUDA(cudaMemsetAsync(P.Z_lo, 0, sizeof(float) * kz, hs));
+  AM24_CUDA(cudaMemsetAsync(P.z_scale, 0, sizeof(float) * k, hs));
+  AM24_CUDA(cudaMemsetAsync(P.v_scale, 0, sizeof(float) * k, hs));
+  AM24_CUDA(cudaMemsetAsync(P.obj_part, 0, sizeof(float) * k * P.parts, hs));
+  AM24_CUDA(cudaMemsetAsync(P.nnz_part, 0, sizeof(float) * k * P.parts, hs));
+  AM24_CUDA(cudaMemsetAsync(P.max_err, 0, sizeof(float), hs));
   AM24_CUDA(cudaMemsetAsync(P.Z_h, 0, sizeof(uint16_t) * zh_planes * kz, hs));
   AM24_CUDA(cudaMemsetAsync(P.V_h, 0, sizeof(uint16_t) * 2 * kv, hs));
   if (P.cmask) AM24_CUDA(cudaMemsetAsync(P.cmask, 0, sizeof(uint32_t) * words, hs));
@@ -395,6 +407,9 @@ am24_status am24_group_run(am24_group g, uint32_t max_steps, float *device_ms) {
   AM24_CUDA(cudaStreamSynchronize(h->stream));
   AM24_CUDA(cudaEventElapsedTime(&g->last_ms, g->e0, g->e1));
   if (device_ms) *device_ms = g->last_ms;
+  if (plan.status == (int)DEV_ERR_GROUP_ITEM)
+    return fail(AM24_ERR_CUDA, "grouped step: a work list named a problem that is not live "
+                               "(the items were skipped)");
   if (plan.status != 0) {
     char buf[96];
     snprintf(buf, sizeof buf, "device-side wait timed out (code 0x%x)", plan.status);

@@ -147,7 +147,15 @@ __device__ __forceinline__ void for_items(const GroupDev &g, int l, Fn fn) {
   const int *prob = g.prob + (size_t)l * g.cap;
   for (int it = blockIdx.x; it < total; it += gridDim.x) {
     const int i = find_item(pref, np, it);
-    fn(g.probs[__ldg(prob + i)], it - __ldg(pref + i));
+    const int p = __ldg(prob + i);
+    const int local = it - __ldg(pref + i);
+    // self-check: the plan only lists live problems' items
+    if (np <= 0 || p < 0 || p >= g.cap || !g.probs[p].live || local < 0 ||
+        local >= __ldg(pref + i + 1) - __ldg(pref + i)) {
+      if (threadIdx.x == 0) atomicCAS(&g.plan->status, 0, (int)DEV_ERR_GROUP_ITEM);
+      continue;  // uniform over the block
+    }
+    fn(g.probs[p], local);
     __syncthreads();  // shared memory is reused by the next item
   }
 }

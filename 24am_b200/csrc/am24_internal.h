@@ -241,6 +241,10 @@ enum : int {
   GCTL_WORDS = 16
 };
 
+// GPlan::status when a grouped work item named a slot out of range, a problem
+// not live or an item past its problem's count (the item is skipped)
+constexpr int DEV_ERR_GROUP_ITEM = 0x201;
+
 struct GPlan {
   int n[GL_COUNT];      // problems in each list
   int total[GL_COUNT];  // work items in each list

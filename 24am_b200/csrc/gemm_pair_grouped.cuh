@@ -62,6 +62,7 @@ struct GUnit {
   int p;       // problem (slot)
   Unit t;
   int scheme;  // GScheme
+  bool ok;     // the self-check passed (every role skips a unit that failed it)
 };
 
 template <bool Z1>
@@ -71,6 +72,16 @@ __device__ __forceinline__ GUnit grouped_unit(const GroupDev &g, int list, int n
   const int i = find_item(pref, np, u);
   GUnit r;
   r.p = __ldg(g.prob + (size_t)list * g.cap + i);
+  const int local = u - __ldg(pref + i);
+  r.ok = np > 0 && r.p >= 0 && r.p < g.cap && g.probs[r.p].live && local >= 0 &&
+         local < __ldg(pref + i + 1) - __ldg(pref + i);
+  if (!r.ok) {
+    r.p = 0;
+    r.scheme = GS_FP16X3;
+    r.t = Unit{};
+    if (rank == 0) atomicCAS(&g.plan->status, 0, (int)DEV_ERR_GROUP_ITEM);
+    return r;
+  }
   const GProblem &P = g.probs[r.p];
   GemmShape s;
   if (Z1) {
@@ -86,7 +97,7 @@ __device__ __forceinline__ GUnit grouped_unit(const GroupDev &g, int list, int n
     s.kb_per_split = s.kb_total;
     r.scheme = (int)*reinterpret_cast<volatile const uint32_t *>(P.ctl + GCTL_SCHEME);
   }
-  r.t = decode_pair_unit(s, u - __ldg(pref + i), rank);
+  r.t = decode_pair_unit(s, local, rank);
   return r;
 }
 
@@ -229,6 +240,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
       uint32_t armed = 0, armed_parity = 0;
       for (int u = pair; u < num_units && !*abort; u += pairs) {
         const GUnit gu = grouped_unit<Z1>(g, list, np, u, rank);
+        if (!gu.ok) continue;
         const GMaps &mp = g.maps[gu.p];
         const CUtensorMap *ma[2], *mb[2];
         if (Z1) {
@@ -286,6 +298,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
       bool ok = true;
       for (int u = pair; ok && u < num_units && !*abort; u += pairs) {
         const GUnit gu = grouped_unit<Z1>(g, list, np, u, 0);
+        if (!gu.ok) continue;
         const Unit &t = gu.t;
         const int promo = scheme_promo(gu.scheme);
         for (int c0 = t.kb0; ok && c0 < t.kb1; c0 += promo) {
@@ -345,6 +358,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
     uint32_t acc_phase = 0;
     for (int u = pair; u < num_units; u += pairs) {
       const GUnit gu = grouped_unit<Z1>(g, list, np, u, rank);
+      if (!gu.ok) continue;
       const GProblem &P = g.probs[gu.p];
       const int promo = scheme_promo(gu.scheme);
       bool ok;

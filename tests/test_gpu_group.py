@@ -204,3 +204,52 @@ def test_autotuned_tiles_solve_like_the_cost_model(solver, po, tmp_path):
     am.autotune_load(path)
     am.autotune_save(path + ".2")
     assert open(path).read() == open(path + ".2").read()
+
+
+def test_admission_in_chunks_matches_solo_runs(solver, po):
+    """The serving pattern: problems join a group while others are mid-solve,
+    the group runs four steps at a time, stopped problems are read and removed
+    and their slots refilled.  Every problem ends bit for bit as it does
+    solved alone in a group of its own."""
+    am = _am()
+    specs = [(300, 2048, 256, 0, 12), (129, 4097, 257, 1, 16), (500, 1000, 384, 2, 9),
+             (257, 3000, 300, 3, 20), (200, 1500, 256, 4, 0), (400, 2500, 512, 5, 0),
+             (150, 900, 260, 6, 0), (333, 2222, 256, 7, 0), (300, 2048, 200, 0, 30),
+             (200, 1500, 300, 6, 0), (129, 4097, 256, 3, 8), (400, 2500, 256, 1, 40)]
+    probs = []
+    for i, spec in enumerate(specs):
+        B, V, st = _setup(am, po, spec, 500 + i, max_iter=40)
+        probs.append((solver.matrix(B), V, st))
+    solo = []
+    for M, V, st in probs:
+        g1 = am.Group(solver, capacity=1)
+        p = g1.add(M, st, start_points=V)
+        g1.run()
+        solo.append((g1.read(p), g1.result(p)[0], g1.state(p)))
+        g1.close()
+    grp = am.Group(solver, capacity=4)
+    queue = list(range(len(probs)))
+    running, done = {}, {}
+    chunks = 0
+    while queue or running:
+        while queue and len(running) < 4:
+            i = queue.pop(0)
+            M, V, st = probs[i]
+            running[grp.add(M, st, start_points=V)] = i
+        grp.run(max_steps=4)
+        chunks += 1
+        assert chunks < 200
+        for pid in list(running):
+            stopped, _ = grp.state(pid)
+            if stopped:
+                i = running.pop(pid)
+                done[i] = (grp.read(pid), grp.result(pid)[0], grp.state(pid))
+                grp.remove(pid)
+    grp.close()
+    for i, (ref, got) in enumerate(zip(solo, (done[i] for i in range(len(probs))))):
+        for a, c in zip(ref[0], got[0]):
+            assert np.array_equal(a, c, equal_nan=True), f"problem {i}"
+        assert np.array_equal(ref[1], got[1]), f"problem {i}: x"
+        assert ref[2] == got[2], (i, ref[2], got[2])
+    for M, _, _ in probs:
+        M.close()
