@@ -88,7 +88,7 @@ def peaks():
 def profiled_traffic(kernel):
     """DRAM bytes per launch of `kernel` on this workload from the committed ncu
     summary (profiles/), or None."""
-    path = os.path.join(ROOT, "profiles", "am_step_config1.md")
+    path = os.path.join(ROOT, "profiles", "am_step_2000x50000_k1024.md")
     try:
         txt = open(path).read()
     except OSError:
