@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -94,6 +95,16 @@ am24_status build_graph(am24_group g) {
   }
   AM24_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
   return AM24_OK;
+}
+
+// AM24_GROUP_EAGER=1: runs step by step from the host instead of one graph
+// launch (same kernels and results; for profilers).
+bool eager_steps() {
+  static const bool on = [] {
+    const char *e = std::getenv("AM24_GROUP_EAGER");
+    return e && e[0] == '1';
+  }();
+  return on;
 }
 
 am24_status check_slot(am24_group g, uint32_t problem) {
@@ -400,7 +411,22 @@ am24_status am24_group_run(am24_group g, uint32_t max_steps, float *device_ms) {
   AM24_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(g->dev.plan) + offsetof(GPlan, loops), &head,
                             sizeof head, cudaMemcpyHostToDevice, h->stream));
   AM24_CUDA(cudaEventRecord(g->e0, h->stream));
-  AM24_CUDA(cudaGraphLaunch(g->exec, h->stream));
+  if (eager_steps()) {
+    // profiling aid: the same step kernels launched from a host loop, so that
+    // a profiler sees each of them (kernel nodes of a graph with a conditional
+    // node are not profiled one by one); one host round trip per step
+    std::vector<uint32_t> flags;
+    for (int i = 0; i < head.loop_cap; i++) {
+      AM24_CUDA(launch_grouped_step(g->dev, g->grids, h->stream));
+      AM24_CUDA(launch_grouped_condition(g->dev, 0ull, h->stream, false));
+      GPlan pl;
+      AM24_CUDA(cudaMemcpyAsync(&pl, g->dev.plan, sizeof pl, cudaMemcpyDeviceToHost, h->stream));
+      AM24_TRY(group_done_flags(g, flags));
+      if (pl.status != 0 || std::find(flags.begin(), flags.end(), 1u) == flags.end()) break;
+    }
+  } else {
+    AM24_CUDA(cudaGraphLaunch(g->exec, h->stream));
+  }
   AM24_CUDA(cudaEventRecord(g->e1, h->stream));
   GPlan plan;
   AM24_CUDA(cudaMemcpyAsync(&plan, g->dev.plan, sizeof plan, cudaMemcpyDeviceToHost, h->stream));

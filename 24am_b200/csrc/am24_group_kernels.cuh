@@ -309,7 +309,8 @@ __global__ void __launch_bounds__(256) g_finalize_kernel(GroupDev g) {
 // of a grouped product gave up.  Also writes every slot's state to g.done,
 // which a host polls with one copy.
 __global__ void __launch_bounds__(256) g_condition_kernel(GroupDev g,
-                                                          cudaGraphConditionalHandle handle) {
+                                                          cudaGraphConditionalHandle handle,
+                                                          bool in_graph) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
@@ -326,6 +327,6 @@ __global__ void __launch_bounds__(256) g_condition_kernel(GroupDev g,
   if (threadIdx.x == 0) {
     const GPlan &pl = *g.plan;
     const bool more = any && pl.loops < pl.loop_cap && pl.status == 0;
-    cudaGraphSetConditional(handle, more ? 1u : 0u);
+    if (in_graph) cudaGraphSetConditional(handle, more ? 1u : 0u);
   }
 }

@@ -276,7 +276,7 @@ cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &grids, cuda
 // Sets the WHILE condition of a captured loop: 1 while some problem is live and
 // unstopped, the plan's loop count is below its cap and no wait gave up.
 cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handle,
-                                     cudaStream_t st);
+                                     cudaStream_t st, bool in_graph = true);
 
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
 int num_sms();

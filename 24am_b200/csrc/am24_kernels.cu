@@ -2760,8 +2760,8 @@ cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &gr, cudaStr
 }
 
 cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handle,
-                                     cudaStream_t st) {
-  g_condition_kernel<<<1, 256, 0, st>>>(g, (cudaGraphConditionalHandle)handle);
+                                     cudaStream_t st, bool in_graph) {
+  g_condition_kernel<<<1, 256, 0, st>>>(g, (cudaGraphConditionalHandle)handle, in_graph);
   return cudaGetLastError();
 }
 

@@ -5,7 +5,9 @@
     whole batch solves of all 8 formulations;
   * config 1's shape (2000 x 50000, r = 50, 256 non-zeros per loading; 1024
     starts), one step and three more of all 8 formulations with s in {16, 128}
-    (constraints) and gamma = {0.1, 0.5} x the largest column norm (penalties).
+    (constraints) and gamma = {0.1, 0.5} x the largest column norm and one that
+    keeps 0.6 % of the entries (penalties), each step against the oracle's step
+    from the same state.
 
 The checker is the FP64 iteration of oracle/fast_oracle.py (BLAS products, the
 C oracle's thresholds), on the same FP32 data and starting points.  Per start
@@ -201,15 +203,21 @@ def _quantile_gamma(B64, V, formulation, share=0.006):
 def test_config1_shape_steps_per_start(solver, config1, formulation, param):
     """One step from the dense starts (tensor-core Z = B V, split-FP16 pair
     GEMMs at K = 2000 and K = 50000), then three more (sparse gather, hinted
-    selects from the second on), all 1024 columns against the FP64 oracle.
+    selects from the second on), all 1024 columns.  Each GPU step is checked
+    against the FP64 oracle's step from the same state: the starting points for
+    step 1, the GPU's own loadings after step t for step t + 1.  (Along a whole
+    trajectory the thresholds amplify rounding: x = |v| - gamma or |v| - w has
+    few correct digits for |v| near the level, and the next step's signs or
+    supports can turn on them; stepping both sides from the same x checks every
+    step's kernels without that amplification.)
 
     Penalties: gamma = 0.1 and 0.5 x the largest column norm (the benchmark's
     choice) and "q", a gamma that keeps about 0.6% of the entries.  The L1-ball
-    forms step one at a time: the reference's scan at its first rank solves a
-    quadratic whose discriminant is exactly zero, so whether it stops there
-    (a support of one entry) is decided by the last bits of the largest |v|;
-    a start that stopped there on either side is set aside, as are the
-    oracle's ill-conditioned starts."""
+    forms: the reference's scan at its first rank solves a quadratic whose
+    discriminant is exactly zero, so whether it stops there (a support of one
+    entry) is decided by the last bits of the largest |v|; a start that stopped
+    there on the GPU's side is set aside with the oracle's ill-conditioned
+    starts (which include its own first-rank stops)."""
     am = _am()
     B, B64, V = config1
     k = V.shape[1]
@@ -226,36 +234,21 @@ def test_config1_shape_steps_per_start(solver, config1, formulation, param):
     M = solver.matrix(B)
     b = M.batch(st, k)
     b.load(V)
-    outs = {}
+    prev_V, prev_val = V.astype(np.float64), np.zeros(k)
+    counts = []
     for it in range(4):
-        if formulation in (2, 3) or it in (0, 3):
-            b.iterate(it, 1)
-        elif it == 1:
-            b.iterate(1, 2)  # steps 2 and 3 in one call (the hinted path)
-        if formulation in (2, 3) or it in (0, 3):
-            Vs, vals, _, _ = b.read()
-            outs[it] = (Vs, vals)
+        b.iterate(it, 1)
+        Vg, valg, _, nnz = b.read()
+        r = fo.iteration(B64, prev_V, formulation, s, g, prev_val, keep_vraw=True)
+        ill = r.ill.copy()
+        if formulation in (2, 3):
+            ill |= np.count_nonzero(Vg, axis=0) == 1  # the GPU's first-rank stops
+        scale = _objective_scales(formulation, r.vraw, g) if formulation >= 4 else None
+        counts.append(_compare(B64, Vg, valg.astype(np.float64), r.V, r.val, ill,
+                               f"config 1 shape, formulation {formulation} ({param}), "
+                               f"step {it + 1}", scale, r.vraw, g))
+        prev_V, prev_val = Vg.astype(np.float64), valg.astype(np.float64)
     b.close()
     M.close()
-    Vo, valo = V.astype(np.float64), np.zeros(k)
-    ill = np.zeros(k, bool)
-    counts = {}
-    for it in range(4):
-        r = fo.iteration(B64, Vo, formulation, s, g, valo, keep_vraw=True)
-        Vo, valo = r.V, r.val
-        ill |= r.ill
-        if formulation in (2, 3):
-            # a stop at the first rank on the GPU's side (the oracle's own is
-            # among its ill-conditioning flags)
-            ill |= np.count_nonzero(outs[it][0], axis=0) == 1
-        if it in (0, 3):
-            scale = _objective_scales(formulation, r.vraw, g) if formulation >= 4 else None
-            Vg, valg = outs[it]
-            counts[it] = _compare(B64, Vg, valg.astype(np.float64), Vo, valo, ill,
-                                  f"config 1 shape, formulation {formulation} ({param}), "
-                                  f"step {it + 1}", scale, r.vraw, g)
-    c1, c4 = counts[0], counts[3]
-    # the share set aside depends on the formulation: near-ties of the L1-ball
-    # scan and entries near gamma are common at p = 50000; every start that is
-    # compared must match, and enough must be comparable
-    assert c1 >= k // 2 and c4 >= (k // 50 if formulation in (2, 3) else k // 10), (c1, c4)
+    # every start that is compared must match, and most must be comparable
+    assert min(counts) >= k // 2, counts
