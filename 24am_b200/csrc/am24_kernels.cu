@@ -1046,8 +1046,28 @@ struct SelResult {
 // Key of descending rank `rank` (1 = largest) among |col[0..n)|, by three
 // histogram passes over 11, 11 and 9 key bits.  All threads of the block
 // call it; hist has 2048 entries, res 4.
-__device__ SelResult block_select(const float *__restrict__ colg, int n, uint32_t rank,
-                                  uint32_t *hist, uint32_t *res) {
+// Readers of the values a selection walks: a column of V (read-only in the
+// kernel) or a list of keys the kernel wrote itself (read through L2, never the
+// non-coherent path).
+struct ColumnSrc {
+  const float *__restrict__ p;
+  __device__ __forceinline__ float operator()(int i) const { return p[i]; }
+};
+struct ListSrc {
+  const float *p;
+  __device__ __forceinline__ float operator()(int i) const { return __ldcg(p + i); }
+};
+
+template <class Src>
+__device__ SelResult block_select_src(Src colg, int n, uint32_t rank, uint32_t *hist,
+                                      uint32_t *res);
+__device__ __forceinline__ SelResult block_select(const float *__restrict__ colg, int n,
+                                                  uint32_t rank, uint32_t *hist, uint32_t *res) {
+  return block_select_src(ColumnSrc{colg}, n, rank, hist, res);
+}
+template <class Src>
+__device__ SelResult block_select_src(Src colg, int n, uint32_t rank, uint32_t *hist,
+                                      uint32_t *res) {
   uint32_t prefix = 0, pmask = 0, gt = 0, need = rank, eq = 0;
 #pragma unroll 1
   for (int lvl = 0; lvl < 3; lvl++) {
@@ -1057,7 +1077,7 @@ __device__ SelResult block_select(const float *__restrict__ colg, int n, uint32_
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t key = abs_key(colg[i]);
+      const uint32_t key = abs_key(colg(i));
       if ((key & pmask) == prefix) {
         const uint32_t bin = (key >> sh) & bmask;
         const unsigned peers = __match_any_sync(__activemask(), bin);
@@ -1307,6 +1327,36 @@ __device__ uint32_t gather_pairs_above(const float *__restrict__ colg, int n, ui
           pos++;
         }
     }
+  }
+  below = __reduce_max_sync(FULL, below);
+  if (lane == 0) atomicMax(&counter[1], below);
+  __syncthreads();
+  return counter[0];
+}
+
+// One streaming pass over a column: every |v| with key >= bound goes to
+// list[] (global memory, room for n) as a float, in any order; returns how
+// many, and leaves in counter[1] the largest key below the bound (0 if none).
+__device__ uint32_t gather_keys_above(const float *__restrict__ colg, int n, uint32_t bound,
+                                      float *list, uint32_t *counter) {
+  if (threadIdx.x == 0) {
+    counter[0] = 0;
+    counter[1] = 0;
+  }
+  __syncthreads();
+  uint32_t below = 0;
+  const int lane = threadIdx.x & 31;
+  for (int base = (threadIdx.x & ~31); base < n; base += blockDim.x) {
+    const int i = base + lane;
+    const uint32_t key = i < n ? abs_key(colg[i]) : 0u;
+    const bool take = i < n && key >= bound;
+    if (i < n && !take) below = max(below, key);
+    const unsigned bal = __ballot_sync(FULL, take);
+    if (!bal) continue;
+    uint32_t wbase = 0;
+    if (lane == 0) wbase = atomicAdd(&counter[0], (uint32_t)__popc(bal));
+    wbase = __shfl_sync(FULL, wbase, 0);
+    if (take) list[wbase + __popc(bal & ((1u << lane) - 1u))] = __uint_as_float(key);
   }
   below = __reduce_max_sync(FULL, below);
   if (lane == 0) atomicMax(&counter[1], below);
@@ -1659,6 +1709,84 @@ __device__ uint32_t resolve_stop(uint32_t best, double bw, uint32_t *res,
 // EXACT: stop at the first segment whose lower knot already gives
 // ||.||_1/||.||_2 >= sqrt(s) and take the root inside it -- the exact
 // L1-ball / unit-sphere projection.
+// The reference scan's exact walk over the values src(0..len) (all of a
+// column's entries above some bound, or the whole column when len == n), a
+// chunk of SOFT_C ranks at a time: each chunk's keys are found by a radix
+// select of its lowest rank, gathered, sorted and scanned, and the stopping
+// predicates evaluated rank by rank.  lo_end is the largest value below the
+// set (0 for the whole column).  Returns the stopping rank and sets *w; NONE
+// when the set ran out first (len < n), and the caller walks the column.
+template <bool EXACT, class Src>
+__device__ __noinline__ uint32_t exact_walk(Src src, uint32_t len, uint32_t n, double lo_end, float *cand,
+                               double *p1, double *p2, uint32_t *hist, uint32_t *res,
+                               double *red, volatile uint32_t *misc, double *w_sh, double sq,
+                               double sq2, double *w) {
+  const uint32_t NONE = 0xFFFFFFFFu;
+  if (len == 0) return NONE;
+  uint32_t brk = NONE;
+  const SelResult top = block_select_src(src, (int)len, 1u, hist, res);
+  const double lim = __dsub_rn((double)__uint_as_float(top.key), 0.000001);
+  uint32_t consumed = 0, khi = NONE, ge_hi = 0;
+  double S1 = 0.0, S2 = 0.0;
+  while (true) {
+    const uint32_t R = min(consumed + (uint32_t)SOFT_C, len);
+    const uint32_t total = R - consumed;
+    const SelResult lo = block_select_src(src, (int)len, R, hist, res);
+    if (threadIdx.x == 0) misc[0] = 0;
+    __syncthreads();
+    if (lo.key == khi) {
+      const float v = __uint_as_float(khi);
+      for (uint32_t q = threadIdx.x; q < total; q += blockDim.x) cand[q] = v;
+    } else {
+      for (int i = threadIdx.x; i < (int)len; i += blockDim.x) {
+        const uint32_t key = abs_key(src(i));
+        if (key > lo.key && key < khi)
+          cand[atomicAdd((uint32_t *)&misc[0], 1u)] = __uint_as_float(key);
+      }
+      __syncthreads();
+      const uint32_t nb = misc[0];
+      const uint32_t c_hi = ge_hi - consumed;
+      const uint32_t c_lo = R - lo.gt;
+      const float vhi = __uint_as_float(khi), vlo = __uint_as_float(lo.key);
+      for (uint32_t q = threadIdx.x; q < c_hi + c_lo; q += blockDim.x)
+        cand[nb + q] = (q < c_hi) ? vhi : vlo;
+    }
+    for (uint32_t q = total + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
+    __syncthreads();
+    bitonic_sort_desc(cand);
+    block_scan2(cand, (int)total, S1, S2, p1, p2, red);
+    // the last position of a chunk waits for the next chunk's first value,
+    // except at the end of the set, where the value below it is lo_end
+    const uint32_t E = (R == len) ? total : total - 1;
+    uint32_t best = NONE;
+    double bw = 0.0, w_last = 0.0;
+    eval_chunk<EXACT>(cand, p1, p2, total, E, consumed, n, S1, S2, lo_end, sq, sq2, lim, best, bw,
+                      w_last);
+    brk = resolve_stop(best, bw, res, misc, w_sh, w);
+    if (brk != NONE) break;
+    if (R == len) {
+      if (len == n) {
+        // never stopped: the reference keeps the '+' root of its last step;
+        // the exact projection with ratio < sqrt(s) everywhere is lambda = 0
+        if (!EXACT && consumed + E - 1 == n - 1 && threadIdx.x == (E - 1) % blockDim.x)
+          *w_sh = w_last;
+        if (EXACT && threadIdx.x == 0) *w_sh = 0.0;
+        __syncthreads();
+        *w = *w_sh;
+        __syncthreads();
+      }
+      break;
+    }
+    consumed += E;
+    S1 = p1[E - 1];
+    S2 = p2[E - 1];
+    khi = lo.key;
+    ge_hi = lo.gt + lo.eq;
+    __syncthreads();
+  }
+  return brk;
+}
+
 template <bool EXACT>
 __device__ __forceinline__ void soft_select_body(
     const float *__restrict__ Vraw, int ldv, int n, unsigned s, float *__restrict__ Vx,
@@ -1690,6 +1818,7 @@ __device__ __forceinline__ void soft_select_body(
   double ss = 0.0, cnt = 0.0;
   // ---- hinted path: gather (key, index) with |v| >= HINT_FRACTION * (previous level)
   const float hint = hints[j];
+  uint32_t c_hint = 0;  // entries at or above the hinted bound
   if (hint > 0.f) {
     uint32_t c, below_key = 0;
     const bool listed = cmask != nullptr;
@@ -1699,6 +1828,7 @@ __device__ __forceinline__ void soft_select_body(
       c = gather_pairs_above(colg, n, hinted_bound(hint), pairs, SOFT_C, res);
       below_key = res[1];
     }
+    c_hint = c;
     __syncthreads();
     if (c > 0 && c <= (uint32_t)SOFT_C) {
       int len = 1;
@@ -1747,10 +1877,23 @@ __device__ __forceinline__ void soft_select_body(
     __syncthreads();
   }
 
+  // ---- more than SOFT_C entries above the hinted bound: the exact walk over
+  // them alone (a compact list in this column of Vx, which the writes below
+  // overwrite); it gives up if the stop lies below the bound
+  if (brk == NONE && c_hint > (uint32_t)SOFT_C && c_hint < (uint32_t)n) {
+    float *list = Vx + (size_t)j * ldv;
+    const uint32_t cl = gather_keys_above(colg, n, hinted_bound(hint), list, res);
+    const double lo_end = (double)__uint_as_float(res[1]);
+    brk = exact_walk<EXACT>(ListSrc{list}, cl, (uint32_t)n, lo_end, cand, p1, p2, hist, res, red,
+                            misc, w_sh, sq, sq2, &w);
+  }
+
   // ---- fast path: the highest bins holding at most SOFT_C values
   uint32_t c = 0, bstar = 0;
+  bool hist_ok = false;  // hist holds the column's top-bit histogram
   if (brk == NONE) {
     key_histogram(colg, n, hist);
+    hist_ok = true;
     find_rank_bin(hist, 2048, (uint32_t)SOFT_C + 1u, res);
     const bool whole = (uint32_t)n <= (uint32_t)SOFT_C;
     bstar = whole ? 0u : res[0] + 1u;  // gather bins >= bstar
@@ -1807,63 +1950,26 @@ __device__ __forceinline__ void soft_select_body(
     }
   }
 
-  // ---- exact walk, a chunk of SOFT_C ranks at a time
-  if (brk == NONE) {
-    const SelResult top = block_select(colg, n, 1u, hist, res);
-    const double lim = __dsub_rn((double)__uint_as_float(top.key), 0.000001);
-    uint32_t consumed = 0, khi = NONE, ge_hi = 0;
-    double S1 = 0.0, S2 = 0.0;
-    while (true) {
-      const uint32_t R = min(consumed + (uint32_t)SOFT_C, (uint32_t)n);
-      const uint32_t total = R - consumed;
-      const SelResult lo = block_select(colg, n, R, hist, res);
-      if (threadIdx.x == 0) misc[0] = 0;
-      __syncthreads();
-      if (lo.key == khi) {
-        const float v = __uint_as_float(khi);
-        for (uint32_t q = threadIdx.x; q < total; q += blockDim.x) cand[q] = v;
-      } else {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-          const uint32_t key = abs_key(colg[i]);
-          if (key > lo.key && key < khi)
-            cand[atomicAdd((uint32_t *)&misc[0], 1u)] = __uint_as_float(key);
-        }
-        __syncthreads();
-        const uint32_t nb = misc[0];
-        const uint32_t c_hi = ge_hi - consumed;
-        const uint32_t c_lo = R - lo.gt;
-        const float vhi = __uint_as_float(khi), vlo = __uint_as_float(lo.key);
-        for (uint32_t q = threadIdx.x; q < c_hi + c_lo; q += blockDim.x)
-          cand[nb + q] = (q < c_hi) ? vhi : vlo;
-      }
-      for (uint32_t q = total + threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x) cand[q] = -1.f;
-      __syncthreads();
-      bitonic_sort_desc(cand);
-      block_scan2(cand, (int)total, S1, S2, p1, p2, red);
-      const uint32_t E = (R == (uint32_t)n) ? total : total - 1;
-      uint32_t best = NONE;
-      double bw = 0.0, w_last = 0.0;
-      eval_chunk<EXACT>(cand, p1, p2, total, E, consumed, (uint32_t)n, S1, S2, 0.0, sq, sq2, lim,
-                        best, bw, w_last);
-      brk = resolve_stop(best, bw, res, misc, w_sh, &w);
-      if (brk != NONE) break;
-      if (R == (uint32_t)n) {
-        if (!EXACT && consumed + E - 1 == (uint32_t)n - 1 && threadIdx.x == (E - 1) % blockDim.x)
-          *w_sh = w_last;
-        if (EXACT && threadIdx.x == 0) *w_sh = 0.0;
-        __syncthreads();
-        w = *w_sh;
-        __syncthreads();
-        break;
-      }
-      consumed += E;
-      S1 = p1[E - 1];
-      S2 = p2[E - 1];
-      khi = lo.key;
-      ge_hi = lo.gt + lo.eq;
-      __syncthreads();
+  // ---- exact walk, a chunk of SOFT_C ranks at a time: over the entries in
+  // the histogram's bins holding the top 8 * SOFT_C ranks first (a compact
+  // list in this column of Vx), then, if the stop lies below them, over the
+  // column
+  if (brk == NONE && hist_ok && n > 8 * SOFT_C) {
+    // the fast path's histogram: the bins holding the top 8 * SOFT_C ranks
+    find_rank_bin(hist, 2048, 8u * (uint32_t)SOFT_C, res);
+    const uint32_t bound = res[0] << 20;
+    __syncthreads();
+    float *list = Vx + (size_t)j * ldv;
+    const uint32_t cl = gather_keys_above(colg, n, bound, list, res);
+    if (cl < (uint32_t)n) {
+      const double lo_end = (double)__uint_as_float(res[1]);
+      brk = exact_walk<EXACT>(ListSrc{list}, cl, (uint32_t)n, lo_end, cand, p1, p2, hist, res,
+                              red, misc, w_sh, sq, sq2, &w);
     }
   }
+  if (brk == NONE)
+    brk = exact_walk<EXACT>(ColumnSrc{colg}, (uint32_t)n, (uint32_t)n, 0.0, cand, p1, p2, hist,
+                            res, red, misc, w_sh, sq, sq2, &w);
 
   if (threadIdx.x == 0) hints[j] = (float)w;
   // x = sgn(v)(|v| - w)_+ with w kept in double: a level that lands within

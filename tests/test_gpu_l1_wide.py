@@ -1,0 +1,101 @@
+"""The L1-ball selects on wide supports: constraints whose level keeps
+thousands of entries, so the reference's scan stops beyond the first chunk of
+ranks the select sorts at once.  The first step (no hint) walks the entries
+of the histogram's top bins; later steps walk the entries above the previous
+level's bound; either falls back to the whole column.  Each GPU step is
+checked against the FP64 oracle's step from the GPU's own previous loadings
+(supports per start, loadings and objectives), for the reference's scan and
+the exact projection, in a one-problem batch and in a group of problems."""
+import importlib
+
+import numpy as np
+import pytest
+
+import fast_oracle as fo
+
+pytestmark = pytest.mark.gpu
+
+
+def _am():
+    return importlib.import_module("24am_b200")
+
+
+def _check_step(Vg, valg, r, what):
+    keep = np.flatnonzero(~r.ill & np.isfinite(r.val))
+    assert len(keep) >= Vg.shape[1] // 2, f"{what}: {Vg.shape[1] - len(keep)} ill-conditioned"
+    for j in keep:
+        assert np.array_equal(Vg[:, j] != 0, r.V[:, j] != 0), f"{what}: support of start {j}"
+        scale = np.abs(r.V[:, j]).max()
+        assert np.abs(Vg[:, j] - r.V[:, j]).max() <= 1e-4 * scale, f"{what}: loadings of {j}"
+    rel = np.abs(valg[keep] - r.val[keep]) / np.abs(r.val[keep])
+    assert rel.max(initial=0.0) <= 1e-5, f"{what}: objective rel err {rel.max():.3g}"
+    return keep
+
+
+@pytest.mark.parametrize("exact", [False, True], ids=["scan", "exact"])
+@pytest.mark.parametrize("s", [256, 2048])
+@pytest.mark.parametrize("formulation", [2, 3])
+def test_wide_l1_supports_step_like_the_oracle(solver, po, formulation, s, exact):
+    am = _am()
+    m, n, k = 200, 30000, 32
+    B = po.low_rank_data(m, n, 6, 400, seed=61 + s, dtype=np.float32)
+    B64 = B.astype(np.float64)
+    V0 = po.uniform_starts(n, k, seed=62, dtype=np.float32)
+    st = am.OptimizationSettings(formulation=formulation, constraintParameter=s, tolerance=1e-6,
+                                 maximumIterations=10, totalStartingPoints=k, batchSize=k,
+                                 l1Mode=am.L1_EXACT if exact else am.L1_REFERENCE_SCAN)
+    M = solver.matrix(B)
+    b = M.batch(st, k)
+    b.load(V0)
+    prev, prev_val = V0.astype(np.float64), np.zeros(k)
+    widest = 0
+    for it in range(4):
+        b.iterate(it, 1)
+        Vg, valg, _, nnz = b.read()
+        r = fo.iteration(B64, prev, formulation, s, 0.0, prev_val, l1_exact=exact)
+        if not exact:
+            r.ill |= np.count_nonzero(Vg, axis=0) == 1  # the GPU's first-rank stops
+        keep = _check_step(Vg, valg.astype(np.float64), r,
+                           f"formulation {formulation}, s = {s}, step {it + 1}")
+        widest = max(widest, int(np.count_nonzero(r.V[:, keep], axis=0).max(initial=0)))
+        print(f"formulation {formulation}, s = {s}, {'exact' if exact else 'scan'}, step "
+              f"{it + 1}: {len(keep)} of {k} compared, widest support {widest}")
+        prev, prev_val = Vg.astype(np.float64), valg.astype(np.float64)
+    b.close()
+    M.close()
+    if s == 2048:
+        assert widest > 1024  # supports of about 3700: the walks past the first chunk ran
+
+
+@pytest.mark.parametrize("formulation", [2, 3])
+def test_wide_l1_supports_in_a_group(solver, po, formulation):
+    """The same selects in the grouped step: problems whose supports hold about
+    3700, 500 and a few tens of entries in one group, one step at a time, each
+    against the oracle's step from the group's own loadings."""
+    am = _am()
+    specs = [(200, 30000, 64, 2048), (150, 20000, 48, 256), (300, 9000, 40, 16)]
+    grp = am.Group(solver, capacity=4)
+    probs = []
+    for i, (m, n, k, s) in enumerate(specs):
+        B = po.low_rank_data(m, n, 6, 300, seed=71 + i, dtype=np.float32)
+        V0 = po.uniform_starts(n, k, seed=72 + i, dtype=np.float32)
+        st = am.OptimizationSettings(formulation=formulation, constraintParameter=s,
+                                     tolerance=1e-6, maximumIterations=10,
+                                     totalStartingPoints=k, batchSize=k,
+                                     startMode=am.START_INJECTED)
+        M = solver.matrix(B)
+        pid = grp.add(M, st, start_points=V0)
+        probs.append([M, pid, B.astype(np.float64), s, V0.astype(np.float64), np.zeros(k)])
+    for it in range(3):
+        grp.run(max_steps=1)
+        for q in probs:
+            M, pid, B64, s, prev, prev_val = q
+            Vg, valg, _, _ = grp.read(pid)
+            r = fo.iteration(B64, prev, formulation, s, 0.0, prev_val)
+            r.ill |= np.count_nonzero(Vg, axis=0) == 1
+            _check_step(Vg, valg.astype(np.float64), r,
+                        f"group, formulation {formulation}, s = {s}, step {it + 1}")
+            q[4], q[5] = Vg.astype(np.float64), valg.astype(np.float64)
+    grp.close()
+    for q in probs:
+        q[0].close()
