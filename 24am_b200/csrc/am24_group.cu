@@ -122,6 +122,23 @@ am24_status read_ctl(am24_group g, const GroupSlot &sl, uint32_t *ctl) {
   return AM24_OK;
 }
 
+// The order in which the plan lists the slots: live problems by descending
+// feature count (their per-column passes are the longest, so their items go
+// first), then the rest.  Written after every add and remove.
+am24_status upload_order(am24_group g) {
+  std::vector<int> order(g->cap);
+  for (int i = 0; i < g->cap; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const int na = g->slots[a].used ? g->slots[a].P.n : -1;
+    const int nb = g->slots[b].used ? g->slots[b].P.n : -1;
+    return na > nb;
+  });
+  AM24_CUDA(cudaMemcpyAsync(const_cast<int *>(g->dev.order), order.data(), sizeof(int) * g->cap,
+                            cudaMemcpyHostToDevice, g->h->stream));
+  AM24_CUDA(cudaStreamSynchronize(g->h->stream));
+  return AM24_OK;
+}
+
 }  // namespace
 
 namespace am24host {
@@ -175,11 +192,15 @@ am24_status am24_group_create(am24_handle h, uint32_t capacity, am24_group *out)
   AM24_TRY(g->mem.get(&d.prob, (size_t)GL_COUNT * capacity));
   AM24_TRY(g->mem.get(&d.pref, (size_t)GL_COUNT * (capacity + 1)));
   AM24_TRY(g->mem.get(&d.done, capacity));
+  int *order = nullptr;
+  AM24_TRY(g->mem.get(&order, capacity));
+  d.order = order;
   d.maps = maps;
   AM24_CUDA(cudaMemsetAsync(d.done, 0, sizeof(uint32_t) * capacity, h->stream));
   AM24_CUDA(cudaMemsetAsync(d.probs, 0, sizeof(GProblem) * capacity, h->stream));
   AM24_CUDA(cudaMemsetAsync(maps, 0, sizeof(GMaps) * capacity, h->stream));
   AM24_CUDA(cudaMemsetAsync(d.plan, 0, sizeof(GPlan), h->stream));
+  AM24_TRY(upload_order(g.get()));
   AM24_CUDA(cudaEventCreate(&g->e0));
   AM24_CUDA(cudaEventCreate(&g->e1));
   AM24_CUDA(cudaStreamSynchronize(h->stream));
@@ -387,6 +408,7 @@ am24_status group_add_impl(am24_group g, am24_matrix mat, const am24_settings *s
   sl.s = s;
   sl.P = P;
   sl.mem = std::move(A);
+  AM24_TRY(upload_order(g));
   *problem = (uint32_t)slot;
   return AM24_OK;
 }
@@ -563,7 +585,7 @@ am24_status am24_group_remove(am24_group g, uint32_t problem) {
   AM24_CUDA(cudaStreamSynchronize(g->h->stream));
   sl.mem.reset();
   sl = GroupSlot{};
-  return AM24_OK;
+  return upload_order(g);
 }
 
 }  // extern "C"

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) group_plan_kernel(GroupDev g) {
   if (tid == 0) act_sum = 0;
   __syncthreads();
   for (int base = 0; base < g.cap; base += PLAN_THREADS) {
-    const int p = base + tid;
+    const int p = base + tid < g.cap ? g.order[base + tid] : g.cap;
     int items[GL_COUNT];
     bool act = false;
     if (p < g.cap) {
@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) group_plan_kernel(GroupDev g) {
       __syncthreads();
     }
   }
+  if (tid < GL_COUNT + 3) g.plan->next[tid] = 0;
   if (tid < GL_COUNT) {
     g.plan->n[tid] = carry_n[tid];
     g.plan->total[tid] = carry_t[tid];
@@ -139,13 +140,21 @@ __global__ void __launch_bounds__(PLAN_THREADS) group_plan_kernel(GroupDev g) {
 
 // ------------------------------------------------------------ per-column kernels
 // The item loop of one list: fn(problem, local item) for every item of list l.
+// Blocks take items from the list's counter, so the widest problems' items
+// (listed first) start first and no block idles while another holds a queue.
 template <class Fn>
-__device__ __forceinline__ void for_items(const GroupDev &g, int l, Fn fn) {
+__device__ __forceinline__ void for_items(const GroupDev &g, int l, Fn fn, int counter = -1) {
+  __shared__ int taken;
   const int total = g.plan->total[l];
   const int np = g.plan->n[l];
   const int *pref = g.pref + (size_t)l * (g.cap + 1);
   const int *prob = g.prob + (size_t)l * g.cap;
-  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+  for (;;) {
+    if (threadIdx.x == 0) taken = atomicAdd(&g.plan->next[counter < 0 ? l : counter], 1);
+    __syncthreads();
+    const int it = taken;
+    __syncthreads();
+    if (it >= total) break;
     const int i = find_item(pref, np, it);
     const int p = __ldg(prob + i);
     const int local = it - __ldg(pref + i);
@@ -194,7 +203,7 @@ __global__ void __launch_bounds__(256) g_z_reduce_kernel(GroupDev g) {
     z_reduce_body<MODE>(P.ws, P.splits1, P.m_tiles1, P.n_tiles1, P.bn, P.m, P.Z_hi, P.Z_lo,
                         P.ldm, P.fz, P.ctl + GCTL_GATE, P.sparse_cap, P.Z_b, P.Z_h, P.zplane,
                         P.z_scale, P.ctl + CTL_STOP, j);
-  });
+  }, GL_COUNT + MODE);
 }
 
 __global__ void __launch_bounds__(HARD_THREADS) g_hard_select_kernel(GroupDev g) {

@@ -252,6 +252,10 @@ struct GPlan {
   int loops;            // steps run since the last launch began
   int loop_cap;         // the launch stops after this many steps
   int status;           // a device-side wait of a grouped kernel gave up
+  // per list, the next item a per-column kernel's block takes; the dense lists
+  // are walked twice a step (densify, then the split-K reduction), which the
+  // last three counters serve
+  int next[GL_COUNT + 3];
 };
 
 // Device arrays of a group, sized for `cap` problems.
@@ -263,6 +267,7 @@ struct GroupDev {
   int *prob;  // [GL_COUNT][cap]: the problems of each list
   int *pref;  // [GL_COUNT][cap + 1]: exclusive prefix of their items
   uint32_t *done;  // per slot after each step: 0 free, 1 iterating, 2 stopped
+  const int *order;  // [cap]: the slots in the order the plan lists them (widest first)
   unsigned long long timeout_ns;
 };
 
