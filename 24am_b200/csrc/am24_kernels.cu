@@ -1520,6 +1520,9 @@ __global__ void __launch_bounds__(HARD_THREADS) hard_select_kernel(
 // ------------------------------------------------------------ L1 constraint
 constexpr int SOFT_C = 1024;  // sorted-candidate chunk (power of two for the bitonic sort)
 constexpr int SOFT_THREADS = 256;
+// hinted candidates sorted at once (then scanned a chunk at a time)
+constexpr int SOFT_HINT_CAP = 4096;
+constexpr int SOFT_SMEM = 8 * SOFT_HINT_CAP + 4 * SOFT_C + 2 * 8 * SOFT_C;
 
 // Unfused double arithmetic (no FMA contraction), as host C++ evaluates it.
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
@@ -1793,10 +1796,16 @@ __device__ __forceinline__ void soft_select_body(
     uint32_t *__restrict__ nnz_out, int *status, uint32_t *__restrict__ vmask,
     float *__restrict__ hints, const uint32_t *stop, const uint32_t *__restrict__ cmask, int j) {
   if (*stop) return;
-  __shared__ uint64_t pairs[SOFT_C];  // hinted (key, index) candidates
-  __shared__ float cand[SOFT_C];
-  __shared__ double p1[SOFT_C], p2[SOFT_C];
-  __shared__ uint32_t hist[2048];
+  // dynamic shared memory (SOFT_SMEM bytes): the hinted (key, index)
+  // candidates, a chunk of sorted values and its prefix sums; the histogram
+  // of the slower paths reuses the candidates' space (those paths run only
+  // when the hinted one found no stop, and then its pairs are not needed)
+  extern __shared__ __align__(16) uint8_t soft_smem[];
+  uint64_t *pairs = reinterpret_cast<uint64_t *>(soft_smem);        // SOFT_HINT_CAP
+  float *cand = reinterpret_cast<float *>(soft_smem + 8 * SOFT_HINT_CAP);  // SOFT_C
+  double *p1 = reinterpret_cast<double *>(soft_smem + 8 * SOFT_HINT_CAP + 4 * SOFT_C);
+  double *p2 = p1 + SOFT_C;
+  uint32_t *hist = reinterpret_cast<uint32_t *>(soft_smem);           // 2048, over pairs
   __shared__ uint32_t res[32];
   __shared__ double red[32];
   __shared__ uint32_t misc_raw[16];
@@ -1823,36 +1832,53 @@ __device__ __forceinline__ void soft_select_body(
     uint32_t c, below_key = 0;
     const bool listed = cmask != nullptr;
     if (listed) {  // marked by V = B^T Z's epilogue, with the same bound
-      c = pairs_from_mask(cmask + (size_t)j * (ldv >> 5), ldv >> 5, colg, pairs, SOFT_C, res);
+      c = pairs_from_mask(cmask + (size_t)j * (ldv >> 5), ldv >> 5, colg, pairs, SOFT_HINT_CAP,
+                          res);
     } else {
-      c = gather_pairs_above(colg, n, hinted_bound(hint), pairs, SOFT_C, res);
+      c = gather_pairs_above(colg, n, hinted_bound(hint), pairs, SOFT_HINT_CAP, res);
       below_key = res[1];
     }
     c_hint = c;
     __syncthreads();
-    if (c > 0 && c <= (uint32_t)SOFT_C) {
+    if (c > 0 && c <= (uint32_t)SOFT_HINT_CAP) {
       int len = 1;
       while (len < (int)c) len <<= 1;
       for (int q = c + threadIdx.x; q < len; q += blockDim.x) pairs[q] = 0ull;
       __syncthreads();
       bitonic_desc(pairs, len);
-      for (uint32_t q = threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x)
-        cand[q] = (q < c) ? __uint_as_float((uint32_t)(pairs[q] >> 32)) : -1.f;
-      __syncthreads();
-      // A listed set comes without the largest value below it, so its last
-      // position (whose test needs that value) is left to the paths below;
-      // the others see their next value in the set.
-      const uint32_t E = (listed && c < (uint32_t)n) ? c - 1 : c;
+      // the sorted set, a chunk of SOFT_C ranks at a time; every position sees
+      // its next value in the set, except the set's last: for a listed set
+      // (no largest value below it) that one is left to the paths below
+      const double lim =
+          __dsub_rn((double)__uint_as_float((uint32_t)(pairs[0] >> 32)), 0.000001);
       const double lo_after = (c == (uint32_t)n) ? 0.0 : (double)__uint_as_float(below_key);
-      block_scan2(cand, (int)c, 0.0, 0.0, p1, p2, red);
-      const double lim = __dsub_rn((double)cand[0], 0.000001);  // ||v||_inf - 1e-6
-      uint32_t best = NONE;
-      double bw = 0.0, w_last = 0.0;
-      eval_chunk<EXACT>(cand, p1, p2, c, E, 0, (uint32_t)n, 0.0, 0.0, lo_after, sq, sq2, lim,
-                        best, bw, w_last);
-      brk = resolve_stop(best, bw, res, misc, w_sh, &w);
+      double S1 = 0.0, S2 = 0.0, w_last = 0.0;
+      uint32_t q0 = 0;
+      for (;;) {
+        const uint32_t total = min((uint32_t)SOFT_C, c - q0);
+        const bool last = q0 + total == c;
+        for (uint32_t q = threadIdx.x; q < (uint32_t)SOFT_C; q += blockDim.x)
+          cand[q] = (q < total) ? __uint_as_float((uint32_t)(pairs[q0 + q] >> 32)) : -1.f;
+        __syncthreads();
+        const double next =
+            last ? lo_after : (double)__uint_as_float((uint32_t)(pairs[q0 + total] >> 32));
+        const uint32_t E = (last && listed && c < (uint32_t)n) ? total - 1 : total;
+        block_scan2(cand, (int)total, S1, S2, p1, p2, red);
+        uint32_t best = NONE;
+        double bw = 0.0;
+        eval_chunk<EXACT>(cand, p1, p2, total, E, q0, (uint32_t)n, S1, S2, next, sq, sq2, lim,
+                          best, bw, w_last);
+        brk = resolve_stop(best, bw, res, misc, w_sh, &w);
+        if (brk != NONE || last) break;
+        S1 = p1[total - 1];
+        S2 = p2[total - 1];
+        q0 += total;
+        __syncthreads();
+      }
       if (brk == NONE && c == (uint32_t)n) {
-        if (!EXACT && threadIdx.x == (c - 1) % blockDim.x) *w_sh = w_last;
+        // never stopped: the '+' root at the column's last rank (evaluated by
+        // the thread holding that position of the last chunk)
+        if (!EXACT && threadIdx.x == (c - 1 - q0) % blockDim.x) *w_sh = w_last;
         if (EXACT && threadIdx.x == 0) *w_sh = 0.0;
         __syncthreads();
         w = *w_sh;
@@ -1862,7 +1888,7 @@ __device__ __forceinline__ void soft_select_body(
       if (brk != NONE) {
         // the level lies at or above every value outside the gathered set
         for (uint32_t q = threadIdx.x; q < c; q += blockDim.x) {
-          const double d = (double)cand[q] - w;
+          const double d = (double)__uint_as_float((uint32_t)(pairs[q] >> 32)) - w;
           if (d > 0.0) {
             const double x = (double)(float)d;
             ss += x * x;
@@ -1877,10 +1903,10 @@ __device__ __forceinline__ void soft_select_body(
     __syncthreads();
   }
 
-  // ---- more than SOFT_C entries above the hinted bound: the exact walk over
-  // them alone (a compact list in this column of Vx, which the writes below
-  // overwrite); it gives up if the stop lies below the bound
-  if (brk == NONE && c_hint > (uint32_t)SOFT_C && c_hint < (uint32_t)n) {
+  // ---- more than SOFT_HINT_CAP entries above the hinted bound: the exact
+  // walk over them alone (a compact list in this column of Vx, which the
+  // writes below overwrite); it gives up if the stop lies below the bound
+  if (brk == NONE && c_hint > (uint32_t)SOFT_HINT_CAP && c_hint < (uint32_t)n) {
     float *list = Vx + (size_t)j * ldv;
     const uint32_t cl = gather_keys_above(colg, n, hinted_bound(hint), list, res);
     const double lo_end = (double)__uint_as_float(res[1]);
@@ -2696,14 +2722,19 @@ cudaError_t launch_am_step(const MatrixDev &M, BatchDev &b, const TensorMaps &tm
                                                         b.ctl, b.cmask);
       e = cudaGetLastError();
     } else {
-      if (p.l1_mode == 0)
-        soft_select_kernel<false><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
-                                                                b.Vx, b.nnz, b.status, b.vmask,
-                                                                b.sel_hint, b.ctl, b.cmask);
-      else
-        soft_select_kernel<true><<<b.k, SOFT_THREADS, 0, st>>>(b.Vraw, M.ldn, M.n, p.constraint,
-                                                               b.Vx, b.nnz, b.status, b.vmask,
-                                                               b.sel_hint, b.ctl, b.cmask);
+      if (p.l1_mode == 0) {
+        if ((e = kernel_setup(soft_select_kernel<false>, SOFT_SMEM, false)) != cudaSuccess)
+          return e;
+        soft_select_kernel<false><<<b.k, SOFT_THREADS, SOFT_SMEM, st>>>(
+            b.Vraw, M.ldn, M.n, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint, b.ctl,
+            b.cmask);
+      } else {
+        if ((e = kernel_setup(soft_select_kernel<true>, SOFT_SMEM, false)) != cudaSuccess)
+          return e;
+        soft_select_kernel<true><<<b.k, SOFT_THREADS, SOFT_SMEM, st>>>(
+            b.Vraw, M.ldn, M.n, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint, b.ctl,
+            b.cmask);
+      }
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
@@ -2824,7 +2855,10 @@ cudaError_t grouped_grids(GroupGrids *gr) {
   gr->pairs = c;
   if ((e = persistent_grid(g_z_reduce_kernel<0>, 256, 0, &gr->col)) ||
       (e = persistent_grid(g_hard_select_kernel, HARD_THREADS, 0, &gr->select_hard)) ||
-      (e = persistent_grid(g_soft_select_kernel<false>, SOFT_THREADS, 0, &gr->select_soft)) ||
+      (e = kernel_setup(g_soft_select_kernel<false>, SOFT_SMEM, false)) ||
+      (e = kernel_setup(g_soft_select_kernel<true>, SOFT_SMEM, false)) ||
+      (e = persistent_grid(g_soft_select_kernel<false>, SOFT_THREADS, SOFT_SMEM,
+                           &gr->select_soft)) ||
       (e = persistent_grid(g_gather_kernel<0>, GATHER_THREADS, 0, &gr->gather)) ||
       (e = persistent_grid(g_gather_group_kernel<0>, GATHER_THREADS, (int)GATHER_GROUP_SMEM,
                            &gr->gather_group)) ||
@@ -2858,8 +2892,8 @@ cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &gr, cudaStr
       (e = launch_grouped_gemms<GE_PL0>(g, GL_PL0_64, st)))
     return e;
   g_hard_select_kernel<<<gr.select_hard, HARD_THREADS, 0, st>>>(g);
-  g_soft_select_kernel<false><<<gr.select_soft, SOFT_THREADS, 0, st>>>(g);
-  g_soft_select_kernel<true><<<gr.select_soft, SOFT_THREADS, 0, st>>>(g);
+  g_soft_select_kernel<false><<<gr.select_soft, SOFT_THREADS, SOFT_SMEM, st>>>(g);
+  g_soft_select_kernel<true><<<gr.select_soft, SOFT_THREADS, SOFT_SMEM, st>>>(g);
   g_support_kernel<<<gr.col, 256, 0, st>>>(g);
   g_finalize_kernel<<<gr.fin, 256, 0, st>>>(g);
   return cudaGetLastError();
