@@ -62,7 +62,7 @@ class am24_settings(C.Structure):
         ("store_all", C.c_int32), ("total_batches", C.c_uint32), ("verbose", C.c_int32),
         ("start_mode", C.c_int32), ("l1_mode", C.c_int32), ("timeout_ms", C.c_uint32),
         ("precision", C.c_int32), ("stable_iterations", C.c_uint32), ("stable_share", C.c_float),
-        ("reserved", C.c_uint32 * 4),
+        ("lead_iterations", C.c_uint32), ("reserved", C.c_uint32 * 3),
     ]
 
 
@@ -101,6 +101,8 @@ _SIGS = {
     "am24_matrix_deflate": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
     "am24_matrix_create_csc_f32": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.c_uint32, _VP,
                                              _VP, _VP]),
+    "am24_matrix_create_csc_sparse_f32": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.c_uint32,
+                                                    _VP, _VP, _VP]),
     "am24_matrix_read_f32": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
     "am24_solve_resident_f32": (C.c_int, [_VP, _VP, _VP, C.POINTER(am24_settings),
                                           C.POINTER(am24_statistics), _VP, C.POINTER(C.c_float)]),
@@ -185,7 +187,7 @@ class OptimizationSettings:
     """Mirror of SolverStructures::OptimizationSettings (reference field names
     and defaults, c++/src/class/optimization_settings.h:71-123), plus the
     extensions startMode / l1Mode / timeoutMs / precision / stableIterations /
-    stableShare of this library."""
+    stableShare / leadIterations of this library."""
 
     def __init__(self, **kw):
         self.formulation = L0_constrained_L2_PCA
@@ -206,6 +208,7 @@ class OptimizationSettings:
         self.precision = PRECISION_FP32
         self.stableIterations = 5
         self.stableShare = 1.0
+        self.leadIterations = 0
         for k, v in kw.items():
             if not hasattr(self, k):
                 raise AttributeError(f"OptimizationSettings has no field {k}")
@@ -246,6 +249,7 @@ class OptimizationSettings:
         s.precision = int(self.precision)
         s.stable_iterations = int(self.stableIterations)
         s.stable_share = float(self.stableShare)
+        s.lead_iterations = int(self.leadIterations)
         return s
 
     def from_c(self, s):
@@ -394,11 +398,15 @@ class Matrix:
         solver._matrices.add(self)
 
     @classmethod
-    def from_csc(cls, solver, vals, row_ind, col_ptr, m, n, means=None, row_means=None):
-        """A resident matrix from compressed sparse columns
-        (am24_matrix_create_csc_f32), with the sparse solver's optional implicit
-        centring: the matrix solved is B - 1 means^T - row_means 1^T.  Also takes
-        a scipy.sparse matrix as `vals` (then row_ind / col_ptr / m / n may be None)."""
+    def from_csc(cls, solver, vals, row_ind, col_ptr, m, n, means=None, row_means=None,
+                 keep_sparse=False):
+        """A resident matrix from compressed sparse columns, with the sparse
+        solver's optional implicit centring: the matrix solved is
+        B - 1 means^T - row_means 1^T.  Densified on the device
+        (am24_matrix_create_csc_f32), or with keep_sparse=True kept compressed
+        (am24_matrix_create_csc_sparse_f32: O(nnz) memory, solves only).  Also
+        takes a scipy.sparse matrix as `vals` (then row_ind / col_ptr / m / n may
+        be None)."""
         if hasattr(vals, "tocsc"):
             S = vals.tocsc(copy=True)
             S.sum_duplicates()  # canonical: one entry per (row, column), rows sorted
@@ -412,9 +420,10 @@ class Matrix:
         self = cls.__new__(cls)
         self.solver = solver
         mh = C.c_void_p()
-        check(lib().am24_matrix_create_csc_f32(solver.h, _ptr(vals), _ptr(row_ind),
-                                                _ptr(col_ptr), int(m), int(n), _ptr(mu),
-                                                _ptr(rmu), C.byref(mh)))
+        create = (lib().am24_matrix_create_csc_sparse_f32 if keep_sparse
+                  else lib().am24_matrix_create_csc_f32)
+        check(create(solver.h, _ptr(vals), _ptr(row_ind), _ptr(col_ptr), int(m), int(n),
+                     _ptr(mu), _ptr(rmu), C.byref(mh)))
         self.m, self.n = int(m), int(n)
         self.mh = mh
         self._batches = weakref.WeakSet()

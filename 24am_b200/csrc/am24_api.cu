@@ -175,10 +175,17 @@ am24_status ensure_bt_fp16_planes(am24_handle h, am24_matrix mat) {
   return AM24_OK;
 }
 
-// MIXED: back to the BF16 phase with no start counted stable (a new batch).
+// The phase word a MIXED batch starts in: the FP32 lead-in when it has one
+// (lead + 1: that many accurate steps left, plus one), else the single-pass phase 0.
+uint32_t mixed_first_phase(uint32_t lead) { return lead > 0 ? lead + 1u : 0u; }
+
+// MIXED: back to the first phase with no start counted stable (a new batch).
 cudaError_t reset_mixed(const BatchDev &d, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(d.stable, 0, sizeof(uint32_t) * d.k, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d.phase, 0, sizeof(uint32_t) * 4, st);
+  const uint32_t words[4] = {mixed_first_phase(d.lead), 0u, 0u, 0u};
+  // pageable source: staged before the call returns
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d.phase, words, sizeof words, cudaMemcpyHostToDevice, st);
   return e;
 }
 
@@ -597,19 +604,10 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
                                        am24_matrix *out) {
   if (!col_ptr || !out) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
   *out = nullptr;
-  if (m == 0 || n == 0) return fail(AM24_ERR_INVALID_ARG, "m and n must be positive");
-  if (m > (1u << 30) || n > (1u << 30)) return fail(AM24_ERR_INVALID_ARG, "matrix too large");
   // the arrays are checked on the host first (no handle or device needed),
   // before any device write can use an index
-  if (col_ptr[0] != 0) return fail(AM24_ERR_INVALID_ARG, "col_ptr[0] must be 0");
-  for (uint32_t c = 0; c < n; c++)
-    if (col_ptr[c + 1] < col_ptr[c])
-      return fail(AM24_ERR_INVALID_ARG, "col_ptr must be non-decreasing");
+  AM24_TRY(validate_csc(vals, row_ind, col_ptr, m, n));
   const size_t nnz = (size_t)col_ptr[n];
-  if (nnz > 0 && (!vals || !row_ind)) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  for (size_t q = 0; q < nnz; q++)
-    if (row_ind[q] < 0 || (uint32_t)row_ind[q] >= m)
-      return fail(AM24_ERR_INVALID_ARG, "row index out of range at entry " + std::to_string(q));
   if (!h) return fail(AM24_ERR_INVALID_ARG, "NULL handle");
   AM24_CUDA(cudaSetDevice(h->device));
   auto *mat = new am24_matrix_s();
@@ -658,6 +656,7 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
 am24_status am24_matrix_deflate(am24_handle h, am24_matrix mat, const float *x,
                                 int32_t on_device) {
   if (!h || !mat || !x) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  if (mat->sparse) return fail(AM24_ERR_UNSUPPORTED, "sparse-resident matrices are not deflated");
   AM24_CUDA(cudaSetDevice(h->device));
   MatrixDev &M = mat->d;
   Allocs local(h->stream);
@@ -685,6 +684,7 @@ am24_status am24_matrix_deflate(am24_handle h, am24_matrix mat, const float *x,
 
 am24_status am24_matrix_read_f32(am24_handle h, am24_matrix mat, float *B, int32_t ldB) {
   if (!h || !mat || !B) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
+  if (mat->sparse) return fail(AM24_ERR_UNSUPPORTED, "a sparse-resident matrix has no dense copy");
   const MatrixDev &M = mat->d;
   if (ldB < M.m) return fail(AM24_ERR_INVALID_ARG, "ldB must be >= m");
   AM24_CUDA(cudaSetDevice(h->device));
@@ -714,6 +714,8 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
     return fail(AM24_ERR_INVALID_ARG, "batch_size must be in [1, 2^20]");
   if (is_constrained(settings->formulation) && settings->constraint > (uint32_t)mat->d.n)
     return fail(AM24_ERR_INVALID_ARG, "constraint exceeds n (run am24_check_input first)");
+  if (mat->sparse)
+    return fail(AM24_ERR_UNSUPPORTED, "sparse-resident matrices are solved by am24_solve_resident_f32 only");
   AM24_CUDA(cudaSetDevice(h->device));
   auto *b = new am24_batch_s();
   b->mem.stream = h->stream;  // used on this handle's stream only
@@ -751,6 +753,7 @@ am24_status am24_batch_create(am24_handle h, am24_matrix mat, const am24_setting
   d.mixed_fp16 = d.mixed && d.fp16_2;
   if (const char *e = getenv("AM24_MIXED_BF16")) d.mixed_fp16 = d.mixed_fp16 && atoi(e) == 0;
   d.k_stable = settings->stable_iterations;
+  d.lead = settings->lead_iterations;
   d.need_stable = (uint32_t)std::max(1.0, std::ceil((double)settings->stable_share * k - 1e-9));
   d.need_stable = std::min(d.need_stable, (uint32_t)k);
   const bool need_bf16 = d.bf16_2 || (d.mixed && !d.mixed_fp16);
@@ -1049,6 +1052,7 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
   const MatrixDev &M = mat->d;
   const unsigned n = (unsigned)M.n;
   AM24_TRY(am24_check_input(settings, n));
+  if (mat->sparse) return solve_sparse(h, mat, x, *settings, stats, start_points, fval_out);
   am24_settings &s = *settings;
   const int bs = s.batch_size;
   Allocs local(h->stream);
@@ -1204,7 +1208,7 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
     // MIXED: one BF16 phase for the whole run (starts refilled after the switch
     // run refinement steps only); the tolerance test applies to refinement steps
     if (d.mixed) AM24_CUDA(reset_mixed(d, h->stream));
-    uint32_t phase = d.mixed ? 0u : 1u;
+    uint32_t phase = d.mixed ? mixed_first_phase(d.lead) : 1u;
     AM24_CUDA(cudaEventRecord(e0, h->stream));
     while (go) {
       total_it++;

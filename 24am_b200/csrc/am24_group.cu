@@ -241,6 +241,8 @@ am24_status am24_group_add(am24_group g, am24_matrix mat, const am24_settings *s
                            const float *start_points, uint32_t *problem) {
   if (!g || !mat || !settings || !problem) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
   AM24_TRY(validate_settings(settings));
+  if (mat->sparse)
+    return fail(AM24_ERR_UNSUPPORTED, "sparse-resident matrices are not grouped");
   TileCfg cfg;
   if (g->autotune) AM24_TRY(autotune(g, mat, *settings, &cfg));
   return group_add_impl(g, mat, settings, start_points, cfg, problem);
@@ -360,7 +362,8 @@ am24_status group_add_impl(am24_group g, am24_matrix mat, const am24_settings *s
   AM24_CUDA(cudaMemsetAsync(P.status, 0, sizeof(int), hs));
   if (mixed) {
     AM24_CUDA(cudaMemsetAsync(P.stable, 0, sizeof(uint32_t) * k, hs));
-    AM24_CUDA(cudaMemsetAsync(P.phase, 0, sizeof(uint32_t) * 4, hs));
+    const uint32_t words[4] = {mixed_first_phase(s.lead_iterations), 0u, 0u, 0u};
+    AM24_CUDA(cudaMemcpyAsync(P.phase, words, sizeof words, cudaMemcpyHostToDevice, hs));
     AM24_CUDA(cudaMemsetAsync(P.mask_hash, 0, sizeof(uint64_t) * k, hs));
   }
   // control words: dense first step, and no step at all when max_iter is 0

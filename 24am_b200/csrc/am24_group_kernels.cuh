@@ -244,15 +244,18 @@ __global__ void __launch_bounds__(256) g_support_kernel(GroupDev g) {
       for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += red[i];
       const bool same = P.mask_hash[j] == t;
       P.mask_hash[j] = t;
-      const uint32_t st = same ? min(P.stable[j] + 1u, 0x7FFFFFFFu) : 0u;
+      // no start counts as stable during the FP32 lead-in (phase[0] >= 2)
+      const bool lead = *reinterpret_cast<volatile uint32_t *>(P.phase) >= 2u;
+      const uint32_t st = (same && !lead) ? min(P.stable[j] + 1u, 0x7FFFFFFFu) : 0u;
       P.stable[j] = st;
       if (st >= P.k_stable) atomicAdd(&P.ctl[GCTL_SUPPORT], 1u);
       __threadfence();
       if (atomicAdd(&P.ctl[GCTL_SBLOCKS], 1u) == (uint32_t)P.k - 1) {
         __threadfence();
         const uint32_t count = atomicExch(&P.ctl[GCTL_SUPPORT], 0u);
-        P.phase[3] = P.phase[0];
-        if (count >= P.need_stable) P.phase[0] = 1u;
+        const uint32_t ph = P.phase[0];
+        P.phase[3] = ph;
+        P.phase[0] = mixed_next_phase(ph, count >= P.need_stable);
         P.ctl[GCTL_SBLOCKS] = 0u;
       }
     }

@@ -95,8 +95,10 @@ struct am24_handle_s {
 };
 
 struct am24_matrix_s {
-  am24::MatrixDev d{};
+  am24::MatrixDev d{};  // sizes only (no layouts) when the matrix is sparse-resident
   am24host::Allocs mem;
+  bool sparse = false;  // am24_matrix_create_csc_sparse_f32: kept compressed
+  am24::SparseDev sp{};
 };
 
 struct am24_batch_s {
@@ -121,6 +123,17 @@ am24_status ensure_fp16_planes(am24_handle h, am24_matrix mat);
 am24_status ensure_bt_fp16_planes(am24_handle h, am24_matrix mat);
 void choose_splits(int tiles, int kb_total, int sms, int *splits, int *kbps);
 am24_status validate_settings(const am24_settings *s);
+// The phase word a MIXED batch or problem starts in (lead_iterations > 0: the FP32 lead-in).
+uint32_t mixed_first_phase(uint32_t lead);
+// The kernels' parameters of step `it` of a batch whose first global start is `shift`.
+StepParams step_params(const am24_settings &s, int it, int shift);
+// Host check of compressed sparse columns (col_ptr n + 1 entries from 0,
+// non-decreasing; row indices in [0, m)); the shared rule of both CSC entry points.
+am24_status validate_csc(const float *vals, const int32_t *row_ind, const int32_t *col_ptr,
+                         uint32_t m, uint32_t n);
+// am24_solve_resident_f32 on a sparse-resident matrix (settings already checked).
+am24_status solve_sparse(am24_handle h, am24_matrix mat, float *x, am24_settings &s,
+                         am24_statistics *stats, const float *start_points, float *fval_out);
 void reference_start(float *x, unsigned n, bool constrained, unsigned s, unsigned g);
 void host_starts(const am24_settings &s, unsigned n, const float *start_points,
                  const unsigned *global_idx, int cols, std::vector<float> &out);

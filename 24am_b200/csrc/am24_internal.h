@@ -82,10 +82,12 @@ struct BatchDev {
   int mixed_fp16;        // ... on FP16 operands (the scaled h0 / g0 planes); else BF16
   uint32_t k_stable;     // steps of unchanged support a start needs ...
   uint32_t need_stable;  // ... in this many starts before the batch refines
+  uint32_t lead;         // FP32-accurate steps before the single-pass phase
   uint32_t *vmask_prev;  // k x (ldn/32): the previous step's non-zero masks (MIXED)
   uint32_t *stable;      // per start: consecutive steps with an unchanged support (MIXED)
-  uint32_t *phase;       // [0] 0 = BF16 phase, 1 = refinement (sticky); [1] the step's
-                         // count of stable starts; [2] blocks done (MIXED)
+  uint32_t *phase;       // [0] 0 = BF16 phase, 1 = refinement (sticky), >= 2 the FP32
+                         // lead-in ([0] - 1 steps left); [1] the step's count of
+                         // stable starts; [2] blocks done (MIXED)
   float *Vx;            // k x ldn loadings; entry i of a column is defined only
                         // where its vmask bit is set (zero elsewhere)
   float *V_hi, *V_lo;   // k x ldn dense TF32 hi/lo planes of V: the B operand of the
@@ -283,7 +285,50 @@ cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &grids, cuda
 cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handle,
                                      cudaStream_t st, bool in_graph = true);
 
+// ---- sparse-resident matrices (am24_matrix_create_csc_sparse_f32)
+// The data matrix in compressed form: CSC for V = B^T Z, CSR for Z = B V,
+// and the optional implicit centring B - 1 means^T - row_means 1^T.
+struct SparseDev {
+  int m = 0, n = 0;
+  int64_t nnz = 0;
+  int32_t *col_ptr = nullptr, *row_ind = nullptr;  // CSC: n + 1, nnz (rows ascending)
+  float *cvals = nullptr;
+  int32_t *row_ptr = nullptr, *col_ind = nullptr;  // CSR: m + 1, nnz (columns ascending)
+  float *rvals = nullptr;
+  float *means = nullptr;      // n floats, or null
+  float *row_means = nullptr;  // m floats, or null
+};
+
+// A batch of k starts on a sparse matrix.  Start-major planes have columns of
+// ldn (features) or ldm (samples) floats; the row-major planes Vt (n rows) and
+// Zt (m rows) hold kp = round_up(k, 32) floats per row.
+struct SparseBatchDev {
+  int k = 0, kp = 0, ldn = 0, ldm = 0;
+  float *Vx = nullptr;       // k x ldn loadings, defined where vmask is set
+  uint32_t *vmask = nullptr; // k x ldn / 32
+  float *Vraw = nullptr;     // k x ldn raw V = B^T Z (and the staging of loads)
+  float *Vt = nullptr;       // n x kp
+  float *Zs = nullptr;       // k x ldm
+  float *Zt = nullptr;       // m x kp
+  float *fz = nullptr, *val = nullptr, *err = nullptr, *max_err = nullptr;
+  float *sel_hint = nullptr, *obj_part = nullptr, *nnz_part = nullptr;
+  uint32_t *nnz = nullptr, *max_nnz = nullptr;
+  uint32_t *ctl = nullptr;  // CTL_WORDS
+  double *sum_v = nullptr, *dot_mu = nullptr, *zsum = nullptr, *zdot = nullptr;  // per start
+  int *status = nullptr;
+  int *iters = nullptr, *cards = nullptr;
+  int log_capacity = 0;
+};
+
 // ---- launchers (am24_kernels.cu); all enqueue on `st` and return the CUDA error
+// One AM step of a sparse batch (the dense step's iteration, with both
+// products on the compressed matrix); sets the stop word as finalize does.
+cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, const StepParams &p,
+                               cudaStream_t st);
+// ||(B - centring) x||^2 in FP64 into *out; scratch: sparse_ev_scratch(S) doubles.
+cudaError_t launch_sparse_ev(const SparseDev &S, const float *x, double *scratch, double *out,
+                             cudaStream_t st);
+inline size_t sparse_ev_scratch(const SparseDev &S) { return (size_t)(S.m + 255) / 256 + 2; }
 int num_sms();
 // Fills M's TF32 planes (Bc_hi/lo, Bt_hi/lo) from M.Bc.
 cudaError_t launch_prep_tf32_planes(MatrixDev &M, cudaStream_t st);

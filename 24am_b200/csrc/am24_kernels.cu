@@ -601,6 +601,13 @@ __global__ void __launch_bounds__(256) z_reduce_kernel(const float *__restrict__
 
 // ------------------------------------------------------------ sparse Z = B V
 constexpr int GATHER_THREADS = 256;
+
+// MIXED phase word after a step: the lead-in counts down to the single-pass
+// phase 0, which switches to refinement (1, sticky) once enough starts are stable.
+__device__ __forceinline__ uint32_t mixed_next_phase(uint32_t ph, bool stable_enough) {
+  if (ph >= 2u) return ph == 2u ? 0u : ph - 1u;
+  return (ph == 0u && stable_enough) ? 1u : ph;
+}
 constexpr int GATHER_ROWS = 8;  // samples per thread per pass
 constexpr int GATHER_CAP = 4096;
 
@@ -609,7 +616,9 @@ constexpr int GATHER_CAP = 4096;
 // equals the previous step's.  When at least `need` starts of the batch have
 // kept their support for k_stable steps, phase[0] switches to refinement for
 // good; the last block to finish decides, keeps the phase the step ran in as
-// phase[3] and resets the step's scratch words.
+// phase[3] and resets the step's scratch words.  phase[0] >= 2 is the FP32
+// lead-in (phase[0] - 1 accurate steps left, no start counted stable); its
+// last step hands over to the single-pass phase 0.
 __global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict__ vmask,
                                                       const uint32_t *__restrict__ prev, int words,
                                                       uint32_t *stable, uint32_t *phase,
@@ -622,15 +631,19 @@ __global__ void __launch_bounds__(256) support_kernel(const uint32_t *__restrict
   for (int w = threadIdx.x; w < words; w += blockDim.x) diff |= (a[w] != b[w]);
   diff = __syncthreads_or(diff);
   if (threadIdx.x == 0) {
-    const uint32_t st = diff ? 0u : min(stable[j] + 1u, 0x7FFFFFFFu);
+    // read before this block's arrival: the last block rewrites phase[0] only
+    // after every block has arrived
+    const bool lead = *reinterpret_cast<volatile uint32_t *>(phase) >= 2u;
+    const uint32_t st = (diff || lead) ? 0u : min(stable[j] + 1u, 0x7FFFFFFFu);
     stable[j] = st;
     if (st >= k_stable) atomicAdd(&phase[1], 1u);
     __threadfence();
     if (atomicAdd(&phase[2], 1u) == gridDim.x - 1) {
       __threadfence();
       const uint32_t count = atomicExch(&phase[1], 0u);
-      phase[3] = phase[0];
-      if (count >= need) phase[0] = 1u;
+      const uint32_t ph = phase[0];
+      phase[3] = ph;
+      phase[0] = mixed_next_phase(ph, count >= need);
       phase[2] = 0u;
     }
   }
@@ -2902,6 +2915,101 @@ cudaError_t launch_grouped_step(const GroupDev &g, const GroupGrids &gr, cudaStr
 cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handle,
                                      cudaStream_t st, bool in_graph) {
   g_condition_kernel<<<1, 256, 0, st>>>(g, (cudaGraphConditionalHandle)handle, in_graph);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ sparse steps
+#include "am24_sparse_kernels.cuh"
+
+cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, const StepParams &p,
+                               cudaStream_t st) {
+  cudaError_t e;
+  const int f = p.formulation;
+  const bool centred = S.means || S.row_means;
+  if ((e = cudaMemsetAsync(b.max_err, 0, sizeof(float), st))) return e;
+  // 1. Z = (B - 1 mu^T - r 1^T) V: CSR rows against V transposed
+  if (centred)
+    sp_vstats_kernel<<<b.k, SP_THREADS, 0, st>>>(b.Vx, b.vmask, b.ldn, S.n, S.means, b.sum_v,
+                                                 b.dot_mu, b.ctl);
+  sp_transpose_v_kernel<<<dim3((S.n + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0,
+                          st>>>(b.Vx, b.vmask, b.ldn, S.n, b.k, b.Vt, b.kp, b.ctl);
+  sp_spmm_kernel<<<dim3((S.m + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
+      S.row_ptr, S.col_ind, S.rvals, S.m, b.Vt, b.kp, b.k, b.Zs, b.ldm, S.row_means,
+      S.row_means ? b.sum_v : nullptr, S.means ? b.dot_mu : nullptr, b.ctl);
+  // 2. the formulation's sign / norm of z, and the sums V's correction needs
+  sp_zreduce_kernel<<<b.k, SP_THREADS, 0, st>>>(b.Zs, b.ldm, S.m, f, b.fz, S.row_means,
+                                                centred ? b.zsum : nullptr, b.zdot, b.ctl);
+  sp_transpose_z_kernel<<<dim3((S.m + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0,
+                          st>>>(b.Zs, b.ldm, S.m, b.k, b.Zt, b.kp, b.ctl);
+  // 3. V = (B - 1 mu^T - r 1^T)^T Z: CSC columns against Z transposed
+  sp_spmm_kernel<<<dim3((S.n + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
+      S.col_ptr, S.row_ind, S.cvals, S.n, b.Zt, b.kp, b.k, b.Vraw, b.ldn, S.means,
+      S.means ? b.zsum : nullptr, S.row_means ? b.zdot : nullptr, b.ctl);
+  if ((e = cudaGetLastError())) return e;
+  // 4. thresholds: the dense path's selects (own candidate gather), or the penalties
+  if (is_constrained(f)) {
+    if (!is_l1_constrained(f)) {
+      hard_select_kernel<<<b.k, HARD_THREADS, 0, st>>>(b.Vraw, b.ldn, S.n, p.constraint, b.Vx,
+                                                        b.nnz, b.status, b.vmask, b.sel_hint,
+                                                        b.ctl, nullptr);
+    } else if (p.l1_mode == 0) {
+      if ((e = kernel_setup(soft_select_kernel<false>, SOFT_SMEM, false))) return e;
+      soft_select_kernel<false><<<b.k, SOFT_THREADS, SOFT_SMEM, st>>>(
+          b.Vraw, b.ldn, S.n, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint, b.ctl,
+          nullptr);
+    } else {
+      if ((e = kernel_setup(soft_select_kernel<true>, SOFT_SMEM, false))) return e;
+      soft_select_kernel<true><<<b.k, SOFT_THREADS, SOFT_SMEM, st>>>(
+          b.Vraw, b.ldn, S.n, p.constraint, b.Vx, b.nnz, b.status, b.vmask, b.sel_hint, b.ctl,
+          nullptr);
+    }
+  } else if (is_l1_penalized(f)) {
+    sp_penalty_kernel<true><<<b.k, SP_THREADS, 0, st>>>(b.Vraw, b.ldn, S.n, (float)p.penalty,
+                                                        b.Vx, b.vmask, b.obj_part, b.nnz_part,
+                                                        b.ctl);
+  } else {
+    sp_penalty_kernel<false><<<b.k, SP_THREADS, 0, st>>>(b.Vraw, b.ldn, S.n, (float)p.penalty,
+                                                         b.Vx, b.vmask, b.obj_part, b.nnz_part,
+                                                         b.ctl);
+  }
+  if ((e = cudaGetLastError())) return e;
+  // 5. objective, change, logs and the batch loop's termination test
+  FinalizeArgs fa;
+  fa.k = b.k;
+  fa.formulation = f;
+  fa.parts = 1;
+  fa.it = p.it;
+  fa.store_all = p.store_all;
+  fa.log_shift = p.log_shift;
+  fa.log_capacity = b.log_capacity;
+  fa.tolerance = p.tolerance;
+  fa.fz = b.fz;
+  fa.obj_part = b.obj_part;
+  fa.nnz_part = b.nnz_part;
+  fa.nnz_sel = b.nnz;
+  fa.val = b.val;
+  fa.err = b.err;
+  fa.max_err = b.max_err;
+  fa.iters = b.iters;
+  fa.cards = b.cards;
+  fa.max_nnz = b.max_nnz;
+  fa.ctl = b.ctl;
+  fa.phase = nullptr;
+  fa.status = b.status;
+  fa.stop_check = p.stop_check;
+  if ((e = cudaMemsetAsync(b.max_nnz, 0, sizeof(uint32_t), st))) return e;
+  finalize_kernel<<<(b.k + 7) / 8, 256, 0, st>>>(fa);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sparse_ev(const SparseDev &S, const float *x, double *scratch, double *out,
+                             cudaStream_t st) {
+  const int blocks = (S.m + SP_THREADS - 1) / SP_THREADS;
+  double *xs = scratch, *partial = scratch + 2;
+  sp_ev_xstats_kernel<<<1, SP_THREADS, 0, st>>>(x, S.n, S.means, xs);
+  sp_ev_rows_kernel<<<blocks, SP_THREADS, 0, st>>>(S.row_ptr, S.col_ind, S.rvals, S.m, x,
+                                                   S.row_means, xs, partial);
+  sp_ev_sum_kernel<<<1, SP_THREADS, 0, st>>>(partial, blocks, out);
   return cudaGetLastError();
 }
 

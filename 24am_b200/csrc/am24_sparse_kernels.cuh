@@ -1,0 +1,285 @@
+// Kernels of the sparse-resident AM step (included by am24_kernels.cu).
+//
+// The data matrix stays in compressed form on the device, as the reference's
+// sparse solver keeps it (sparse_PCA_solver_CSC,
+// c++/src/gpower/sparse_PCA_solver_for_CSC.h:111-508): CSC for V = B^T Z and
+// CSR for Z = B V, with its implicit centring (doMean / doRowMean, :223-248,
+// :277-309) folded into the products' epilogues as rank-one corrections:
+//   Z = (B - 1 mu^T - r 1^T) V = B V - 1 (mu^T V) - r (1^T V)
+//   V = (B - 1 mu^T - r 1^T)^T Z = B^T Z - mu (1^T Z) - 1 (r^T Z).
+// Both products are the same tile kernel: for a compressed structure with
+// `ncols` outer entries (CSR rows or CSC columns), out[j][c] = sum over the
+// entries e of outer entry c of val[e] * X[idx[e]][j], X row-major with one
+// row of kp floats per inner index (the starts side by side), out start-major.
+// The per-column passes around them (selects, finalize) are the dense path's.
+
+constexpr int SP_TILE = 32;        // outer entries x starts per tile
+constexpr int SP_THREADS = 256;    // 8 warps, 4 outer entries each
+
+// out[j][c] (j < k, c < ncols) = sum_e val[e] X[idx[e] * kp + j]
+//                                - (cvec ? cvec[c] * a[j] : 0) - (b ? b[j] : 0)
+// One warp per outer entry, a lane per start: every entry reads one 128-byte
+// row segment of X.  Each sum runs over the outer entry's entries in storage
+// order with FP32 FMAs (deterministic); the correction is applied in FP64.
+__global__ void __launch_bounds__(SP_THREADS) sp_spmm_kernel(
+    const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+    const float *__restrict__ val, int ncols, const float *__restrict__ X, int kp, int k,
+    float *__restrict__ out, int ld_out, const float *__restrict__ cvec,
+    const double *__restrict__ a, const double *__restrict__ b, const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ float tile[SP_TILE][SP_TILE + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c0 = blockIdx.x * SP_TILE, j0 = blockIdx.y * SP_TILE;
+  const int j = j0 + lane;  // < kp always (kp is a multiple of 32)
+  for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
+    const int c = c0 + r;
+    float acc = 0.f;
+    if (c < ncols) {
+      const int e1 = ptr[c + 1];
+      for (int e = ptr[c]; e < e1; e++) acc = fmaf(val[e], X[(size_t)idx[e] * kp + j], acc);
+      if (j < k && (cvec || b)) {
+        double corr = 0.0;
+        if (cvec) corr += (double)cvec[c] * a[j];
+        if (b) corr += b[j];
+        acc = (float)((double)acc - corr);
+      }
+    }
+    tile[lane][r] = acc;
+  }
+  __syncthreads();
+  for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
+    const int jj = j0 + r, c = c0 + lane;
+    if (jj < k && c < ncols) out[(size_t)jj * ld_out + c] = tile[r][lane];
+  }
+}
+
+// Vt[q][j] = V's column j at row q (zero where its mask bit is clear), for
+// q < n, j < kp (columns k..kp-1 zero): the row-major X of Z = B V.
+__global__ void __launch_bounds__(SP_THREADS) sp_transpose_v_kernel(
+    const float *__restrict__ Vx, const uint32_t *__restrict__ mask, int ldn, int n, int k,
+    float *__restrict__ Vt, int kp, const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ float tile[SP_TILE][SP_TILE + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int q0 = blockIdx.x * SP_TILE, j0 = blockIdx.y * SP_TILE;
+  const int words = ldn >> 5;
+  for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
+    const int j = j0 + r, q = q0 + lane;
+    float v = 0.f;
+    if (j < k && q < n) {
+      const uint32_t w = mask[(size_t)j * words + (q >> 5)];
+      if ((w >> (q & 31)) & 1u) v = Vx[(size_t)j * ldn + q];
+    }
+    tile[r][lane] = v;
+  }
+  __syncthreads();
+  for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
+    const int q = q0 + r;
+    if (q < n) Vt[(size_t)q * kp + j0 + lane] = tile[lane][r];
+  }
+}
+
+// Zt[i][j] = Zs[j][i] for i < m, j < kp (columns k..kp-1 zero): the row-major
+// X of V = B^T Z.
+__global__ void __launch_bounds__(SP_THREADS) sp_transpose_z_kernel(
+    const float *__restrict__ Zs, int ldm, int m, int k, float *__restrict__ Zt, int kp,
+    const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ float tile[SP_TILE][SP_TILE + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i0 = blockIdx.x * SP_TILE, j0 = blockIdx.y * SP_TILE;
+  for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
+    const int j = j0 + r, i = i0 + lane;
+    tile[r][lane] = (j < k && i < m) ? Zs[(size_t)j * ldm + i] : 0.f;
+  }
+  __syncthreads();
+  for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
+    const int i = i0 + r;
+    if (i < m) Zt[(size_t)i * kp + j0 + lane] = tile[lane][r];
+  }
+}
+
+// Fixed-order block sum of one double per thread (SP_THREADS threads).
+__device__ __forceinline__ double sp_block_sum(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int w = 0; w < SP_THREADS / 32; w++) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// Per start j (one block): sum_v[j] = sum_q v_q and dot_mu[j] = sum_q mu_q v_q
+// over V's defined entries, in FP64: the rank-one corrections of Z = B V.
+__global__ void __launch_bounds__(SP_THREADS) sp_vstats_kernel(
+    const float *__restrict__ Vx, const uint32_t *__restrict__ mask, int ldn, int n,
+    const float *__restrict__ means, double *__restrict__ sum_v, double *__restrict__ dot_mu,
+    const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ double red[SP_THREADS / 32];
+  const int j = blockIdx.x;
+  const int words = ldn >> 5;
+  double s = 0.0, d = 0.0;
+  for (int q = threadIdx.x; q < n; q += SP_THREADS) {
+    const uint32_t w = mask[(size_t)j * words + (q >> 5)];
+    if ((w >> (q & 31)) & 1u) {
+      const double v = (double)Vx[(size_t)j * ldn + q];
+      s += v;
+      if (means) d += (double)means[q] * v;
+    }
+  }
+  s = sp_block_sum(s, red);
+  d = sp_block_sum(d, red);
+  if (threadIdx.x == 0) {
+    sum_v[j] = s;
+    dot_mu[j] = d;
+  }
+}
+
+// Per start j (one block), on z = Zs[j] after the centred product:
+//   constrained L2 variance (forms 0, 2): fz = ||z||_2, z kept;
+//   constrained L1 variance (1, 3): fz = ||z||_1, z <- sgn z;
+//   penalized L2 variance (4, 6): z <- z / ||z||_2;
+//   penalized L1 variance (5, 7): z <- sgn z
+// (gpower_commons.h:68-177 as the dense path runs it), then, when the matrix
+// is centred, zsum[j] = sum_i z_i and zdot[j] = sum_i r_i z_i of the result
+// (the corrections of V = B^T Z).  Norms and sums in FP64, fixed order.
+__global__ void __launch_bounds__(SP_THREADS) sp_zreduce_kernel(
+    float *__restrict__ Zs, int ldm, int m, int formulation, float *__restrict__ fz,
+    const float *__restrict__ row_means, double *__restrict__ zsum, double *__restrict__ zdot,
+    const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ double red[SP_THREADS / 32];
+  const int j = blockIdx.x;
+  float *z = Zs + (size_t)j * ldm;
+  const bool l1var = formulation == 1 || formulation == 3 || formulation == 5 || formulation == 7;
+  const bool cons = formulation <= 3;
+  float inv = 1.f;
+  if (cons || !l1var) {
+    double t = 0.0;
+    for (int i = threadIdx.x; i < m; i += SP_THREADS) {
+      const double v = (double)z[i];
+      t += l1var ? fabs(v) : v * v;
+    }
+    t = sp_block_sum(t, red);
+    if (cons && threadIdx.x == 0) fz[j] = l1var ? (float)t : (float)sqrt(t);
+    if (!cons) inv = 1.0f / (float)sqrt(t);
+  }
+  double s = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < m; i += SP_THREADS) {
+    float v = z[i];
+    if (l1var)
+      v = (float)((v > 0.f) - (v < 0.f));
+    else if (!cons)
+      v *= inv;
+    if (l1var || !cons) z[i] = v;
+    if (zsum) {
+      s += (double)v;
+      if (row_means) d += (double)row_means[i] * (double)v;
+    }
+  }
+  if (zsum) {
+    s = sp_block_sum(s, red);
+    d = sp_block_sum(d, red);
+    if (threadIdx.x == 0) {
+      zsum[j] = s;
+      zdot[j] = d;
+    }
+  }
+}
+
+// Penalized thresholds on raw V (sparse_PCA_thresholding.h:26-102), per start
+// j (one block): L1 (forms 6, 7) x = sgn(v)(|v| - gamma)_+ with objective
+// sqrt(sum (|v| - gamma)_+^2); L0 (4, 5) x = v [v^2 > gamma] with objective
+// sum (v^2 - gamma)_+, gamma rounded to FP32 as the dense epilogue rounds it.
+// Writes x and its mask words, and the objective and non-zero count as the
+// start's single partial (obj_part[j], nnz_part[j]) for finalize.
+template <bool L1>
+__global__ void __launch_bounds__(SP_THREADS) sp_penalty_kernel(
+    const float *__restrict__ Vraw, int ldn, int n, float gamma, float *__restrict__ Vx,
+    uint32_t *__restrict__ mask, float *__restrict__ obj_part, float *__restrict__ nnz_part,
+    const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ double red[SP_THREADS / 32];
+  const int j = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int words = ldn >> 5;
+  const float *v = Vraw + (size_t)j * ldn;
+  float *x = Vx + (size_t)j * ldn;
+  double obj = 0.0, cnt = 0.0;
+  for (int w = warp; w < words; w += SP_THREADS / 32) {
+    const int q = (w << 5) + lane;
+    bool keep = false;
+    float xv = 0.f;
+    if (q < n) {
+      const float a = v[q];
+      const float d = L1 ? fabsf(a) - gamma : a * a - gamma;
+      keep = d > 0.f;
+      if (keep) {
+        xv = L1 ? copysignf(d, a) : a;
+        obj += L1 ? (double)d * (double)d : (double)d;
+        cnt += 1.0;
+      }
+    }
+    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, keep);
+    x[q] = xv;  // q < ldn: the plane's padding takes zeros
+    if (lane == 0) mask[(size_t)j * words + w] = bits;
+  }
+  obj = sp_block_sum(obj, red);
+  cnt = sp_block_sum(cnt, red);
+  if (threadIdx.x == 0) {
+    obj_part[j] = (float)obj;
+    nnz_part[j] = (float)cnt;
+  }
+}
+
+// Explained variance ||(B - 1 mu^T - r 1^T) x||^2 of a unit loading in FP64:
+// a thread per sample row, y_i = sum_e b_e x_col(e) - mu^T x - r_i 1^T x, each
+// block's sum of y_i^2 into partial[block]; xs = {1^T x, mu^T x} precomputed.
+__global__ void __launch_bounds__(SP_THREADS) sp_ev_rows_kernel(
+    const int32_t *__restrict__ row_ptr, const int32_t *__restrict__ col_ind,
+    const float *__restrict__ rvals, int m, const float *__restrict__ x,
+    const float *__restrict__ row_means, const double *__restrict__ xs,
+    double *__restrict__ partial) {
+  __shared__ double red[SP_THREADS / 32];
+  const int i = blockIdx.x * SP_THREADS + threadIdx.x;
+  double y2 = 0.0;
+  if (i < m) {
+    double y = 0.0;
+    for (int e = row_ptr[i]; e < row_ptr[i + 1]; e++) y += (double)rvals[e] * (double)x[col_ind[e]];
+    y -= xs[1];
+    if (row_means) y -= (double)row_means[i] * xs[0];
+    y2 = y * y;
+  }
+  y2 = sp_block_sum(y2, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = y2;
+}
+
+// xs = {sum_q x_q, sum_q mu_q x_q} (one block), then, after sp_ev_rows_kernel,
+// *out = the fixed-order sum of the partials (sp_ev_sum_kernel).
+__global__ void __launch_bounds__(SP_THREADS) sp_ev_xstats_kernel(
+    const float *__restrict__ x, int n, const float *__restrict__ means, double *__restrict__ xs) {
+  __shared__ double red[SP_THREADS / 32];
+  double s = 0.0, d = 0.0;
+  for (int q = threadIdx.x; q < n; q += SP_THREADS) {
+    s += (double)x[q];
+    if (means) d += (double)means[q] * (double)x[q];
+  }
+  s = sp_block_sum(s, red);
+  d = sp_block_sum(d, red);
+  if (threadIdx.x == 0) {
+    xs[0] = s;
+    xs[1] = d;
+  }
+}
+__global__ void __launch_bounds__(SP_THREADS) sp_ev_sum_kernel(const double *__restrict__ partial,
+                                                               int count, double *__restrict__ out) {
+  __shared__ double red[SP_THREADS / 32];
+  double t = 0.0;
+  for (int b = threadIdx.x; b < count; b += SP_THREADS) t += partial[b];
+  t = sp_block_sum(t, red);
+  if (threadIdx.x == 0) *out = t;
+}

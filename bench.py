@@ -262,7 +262,8 @@ def run_solves(args):
                                          penaltyParameter=gam.get(f, 0.0), tolerance=E2E_TOL,
                                          maximumIterations=E2E_MAX_IT, totalStartingPoints=STARTS,
                                          batchSize=STARTS, startMode=am.START_INJECTED,
-                                         precision=prec)
+                                         precision=prec,
+                                         leadIterations=args.mixed_lead if prec else 0)
             _, fval, s = M.solve(st, start_points=V)
             row[name] = {"start_it_per_s": s.start_iterations / s.total_true_computation_time,
                          "iterations": int(s.it), "bf16_iterations": int(s.low_precision_iterations),
@@ -282,8 +283,9 @@ def run_solves(args):
                                    f"(r={RANK}, {NNZ_V} nnz/loading), k={STARTS} starts, "
                                    f"s={S_CONS}, gamma {GAMMA_C} x max column norm, "
                                    f"formulations {forms}, maxIter {E2E_MAX_IT}, tol {E2E_TOL}",
-                       "precision": "MIXED: single-pass BF16 V = B^T Z until every start's "
-                                    "support is unchanged for 5 iterations, then FP32-accurate"},
+                       "precision": (f"MIXED: {args.mixed_lead} FP32-accurate iterations, then "
+                                     "single-pass FP16 V = B^T Z until every start's support is "
+                                     "unchanged for 5 iterations, then FP32-accurate")},
             "fp32_value": v32, "speedup_vs_fp32": vmx / v32,
             "max_ev_rel_diff": max(r["ev_rel_diff"] for r in res.values()),
             "formulations": res}
@@ -349,8 +351,9 @@ def run_uneven(args):
                  (the drop-in solve a caller makes), wall clock around all calls;
       grouped -- every problem in one group (am24_group_run: one captured graph,
                  grouped launches per step, device loop), FP32, device-timed;
-      mixed   -- the same group with MIXED precision (single-pass BF16 V = B^T Z
-                 until the supports settle, then FP32-accurate), device-timed.
+      mixed   -- the same group with MIXED precision (--mixed-lead FP32-accurate
+                 steps, then single-pass FP16 V = B^T Z until the supports
+                 settle, then FP32-accurate), device-timed.
     start-iterations are counted per start to its problem's own stop.  Accuracy:
     per problem, the best explained variance ||B x||^2 (FP64 on the device) of
     grouped and mixed against the plain path's."""
@@ -393,7 +396,8 @@ def run_uneven(args):
         grp = am.Group(solver, capacity=len(mats))
         grp.set_autotune(not args.no_autotune)
         t_add = time.perf_counter()
-        ids = [grp.add(M, am.OptimizationSettings(precision=precision, **kw))
+        lead = args.mixed_lead if precision == am.PRECISION_MIXED else 0
+        ids = [grp.add(M, am.OptimizationSettings(precision=precision, leadIterations=lead, **kw))
                for M, kw in zip(mats, sets)]
         tune["seconds"] += time.perf_counter() - t_add
         ms = grp.run()
@@ -437,6 +441,7 @@ def run_uneven(args):
                                    "s 8..256, starts 32..1024 (device U[-1,1]), maxIter 200, "
                                    "tol 1e-6",
                        "total_starts": int(sum(ks)),
+                       "mixed_lead_iterations": args.mixed_lead,
                        "matrix_elements": int(sum(n * p for n, p, _, _ in probs))},
             "plain_fp32": {"value": v_plain, "seconds": plain_s, "start_iterations": plain_its,
                            "timing": "wall clock around one am24_solve_resident_f32 per problem"},
@@ -841,6 +846,9 @@ def main():
     ap.add_argument("--matrices", type=int, default=32, help="serve: resident matrices")
     ap.add_argument("--problems", type=int, default=256, help="uneven: problems")
     ap.add_argument("--no-autotune", action="store_true", help="uneven: cost-model tiles")
+    ap.add_argument("--mixed-lead", type=int, default=20,
+                    help="solve / uneven: FP32-accurate iterations before MIXED's single-pass "
+                         "phase (0: single-pass from the first iteration)")
     args = ap.parse_args()
     global N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS, S_CONS, GAMMA_C
     N_SAMPLES, P_FEATURES, RANK, NNZ_V, STARTS = SIZES[args.size]

@@ -66,7 +66,9 @@ typedef enum {
  * the supports settle, then the FP32-accurate products from
  * the first iteration after which a share stable_share of the batch's starts
  * has kept the same support for stable_iterations iterations; the tolerance
- * test applies only from then on.  MIXED needs batches of more than 128 starts
+ * test applies only from then on.  With lead_iterations = L > 0 the first L
+ * iterations run the FP32-accurate products (their tolerance test applies)
+ * before the single-pass phase begins.  MIXED needs batches of more than 128 starts
  * (CTA-pair tiles); smaller batches run FP32 throughout. */
 typedef enum { AM24_PRECISION_FP32 = 0, AM24_PRECISION_MIXED = 1 } am24_precision;
 
@@ -113,7 +115,10 @@ typedef struct {
                                  support must stay unchanged (default 5) ... */
   float stable_share;         /* ... in this share of the batch's starts before the
                                  batch refines (default 1: every start) */
-  uint32_t reserved[4];
+  uint32_t lead_iterations;   /* AM24_PRECISION_MIXED: FP32-accurate iterations run
+                                 before the single-pass phase starts (default 0);
+                                 supports are counted stable only from then on */
+  uint32_t reserved[3];
 } am24_settings;
 
 /* Mirror of OptimizationStatistics (c++/src/class/optimization_statistics.h:27-46).
@@ -208,6 +213,23 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
                                        const int32_t *col_ptr, uint32_t m, uint32_t n,
                                        const float *means, const float *row_means,
                                        am24_matrix *out);
+/* The same input kept compressed on the device, for matrices whose dense form
+ * does not fit (or is mostly zeros): the reference's sparse_PCA_solver_CSC
+ * (c++/src/gpower/sparse_PCA_solver_for_CSC.h:111-117) holds B only as CSC
+ * too.  Device memory is 16 bytes per non-zero (CSC plus a CSR copy built on
+ * the host) and the centring vectors; a solve adds 4 (3 n + 2 m) bytes per
+ * start of its batch.  The centring is applied implicitly as rank-one
+ * corrections of both products (the reference's doMean / doRowMean arithmetic,
+ * :223-248, :277-309, here with the corrections' sums in FP64).  Duplicate
+ * (row, column) entries add up.  Such a matrix is solved by
+ * am24_solve_resident_f32 (batch mode: the dense path's iteration, both
+ * products as FP32 kernels on the compressed arrays, AM24_PRECISION_MIXED runs
+ * as FP32; use_otf returns AM24_ERR_UNSUPPORTED); the batch, group, deflation
+ * and read entry points return AM24_ERR_UNSUPPORTED for it. */
+am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const float *vals,
+                                              const int32_t *row_ind, const int32_t *col_ptr,
+                                              uint32_t m, uint32_t n, const float *means,
+                                              const float *row_means, am24_matrix *out);
 am24_status am24_matrix_destroy(am24_handle h, am24_matrix mat);
 am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
                                     am24_settings *settings, am24_statistics *stats,
@@ -259,9 +281,10 @@ am24_status am24_batch_read(am24_handle h, am24_batch b, float *V, float *val, f
 #define AM24_STATIC_WS_BYTES (16u << 20)
 am24_status am24_batch_iterate_static_ws(am24_handle h, am24_batch b, int32_t it0,
                                          int32_t iterations, float *max_error);
-/* AM24_PRECISION_MIXED batches: *refining = 1 once the batch has switched to
- * the FP32-accurate products (0 while its steps use BF16 operands); FP32
- * batches report 1.  Synchronizes the handle's stream. */
+/* AM24_PRECISION_MIXED batches: *refining = 0 while the batch's next step
+ * uses single-pass operands, 1 when it runs the FP32-accurate products (the
+ * lead-in steps, and every step after the switch); FP32 batches report 1.
+ * Synchronizes the handle's stream. */
 am24_status am24_batch_phase(am24_handle h, am24_batch b, int32_t *refining);
 /* Number of kernel launches one am24_batch_iterate step issues. */
 am24_status am24_batch_launches_per_step(am24_handle h, am24_batch b, int32_t *launches);

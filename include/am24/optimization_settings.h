@@ -3,7 +3,7 @@
  * reference's member names, types and defaults
  * (c++/src/class/optimization_settings.h:27-170), so code written against the
  * reference compiles unchanged.  Extra members (startMode, l1Mode, timeoutMs,
- * precision, stableIterations, stableShare, device) select this library's options and
+ * precision, stableIterations, stableShare, leadIterations, device) select this library's options and
  * default to reference behaviour.
  */
 #ifndef AM24_OPTIMIZATION_SETTINGS_H
@@ -66,6 +66,7 @@ class OptimizationSettings {
   int precision;       // 0: FP32-accurate products, 1: BF16 until supports settle, then FP32
   unsigned stableIterations;  // precision 1: iterations of unchanged supports before refining
   float stableShare;          // precision 1: share of the starts that must be that stable
+  unsigned leadIterations;    // precision 1: FP32-accurate iterations before the single-pass phase
   int device;          // CUDA device of the default handle
 
   OptimizationSettings()
@@ -77,7 +78,7 @@ class OptimizationSettings {
         storeIterationsForAllPoints(false), maximumIterations(20), totalStartingPoints(64),
         batchSize(64), totalBatches(0), useOTF(false), doColumnMean(true), doRowMean(false),
         L2RowNormalization(true), tfidf(true), startMode(0), l1Mode(0), timeoutMs(5000),
-        precision(0), stableIterations(5), stableShare(1.0f),
+        precision(0), stableIterations(5), stableShare(1.0f), leadIterations(0),
         device(0) {}
 
   bool isConstrainedProblem() const { return (int)formulation <= 3; }

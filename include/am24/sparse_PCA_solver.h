@@ -56,6 +56,7 @@ inline void to_c(const SolverStructures::OptimizationSettings &o, am24_settings 
   s->precision = o.precision;
   s->stable_iterations = o.stableIterations;
   s->stable_share = o.stableShare;
+  s->lead_iterations = o.leadIterations;
 }
 
 inline void from_c(const am24_settings &s, SolverStructures::OptimizationSettings *o) {

@@ -106,17 +106,20 @@ def test_struct_layouts_match_the_header(am, tmp_path):
     ([0, 2, 1], [1, 2, 3], "col_ptr[0]"),
     ([0, 2, 1], [0, 2, 3], "NULL handle"),  # well formed: only the handle is missing
 ])
-def test_csc_arrays_checked_on_the_host(am, rows, ptr, msg):
-    """am24_matrix_create_csc_f32 checks the CSC arrays on the host before it
-    needs a handle or a device: malformed arrays never reach a kernel."""
+@pytest.mark.parametrize("entry", ["am24_matrix_create_csc_f32",
+                                   "am24_matrix_create_csc_sparse_f32"])
+def test_csc_arrays_checked_on_the_host(am, rows, ptr, msg, entry):
+    """Both CSC entry points (densified and sparse-resident) check the CSC
+    arrays on the host before they need a handle or a device: malformed arrays
+    never reach a kernel."""
     L = am.lib()
     vals = np.ones(3, np.float32)
     r = np.array(rows, np.int32)
     p = np.array(ptr, np.int32)
     out = C.c_void_p()
-    st = L.am24_matrix_create_csc_f32(None, vals.ctypes.data_as(C.c_void_p),
-                                      r.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p),
-                                      3, 2, None, None, C.byref(out))
+    st = getattr(L, entry)(None, vals.ctypes.data_as(C.c_void_p),
+                           r.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p),
+                           3, 2, None, None, C.byref(out))
     assert st == 1 and msg in am.last_error()
 
 

@@ -168,3 +168,71 @@ def test_mixed_solve_reaches_fp32_variance(solver, po, formulation):
     assert s32.lowPrecisionIterations == 0
     assert 5 <= smx.lowPrecisionIterations < smx.it
     assert abs(evmx - ev32) <= 1e-4 * ev32
+
+
+def test_lead_in_runs_fp32_products_first(solver, po):
+    """leadIterations = 4: the first four steps run the FP32-accurate
+    V = B^T Z (the batch reports refining), then the single-pass phase, which
+    lasts at least stableIterations steps (no start counts as stable during the
+    lead-in) before the switch back to the accurate products."""
+    am = _am()
+    m, n, k = 300, 2000, 256
+    B = po.low_rank_data(m, n, 8, 30, seed=5, dtype=np.float32)
+    V0 = po.uniform_starts(n, k, seed=6, dtype=np.float32)
+    st = am.OptimizationSettings(formulation=0, constraintParameter=16, tolerance=1e-6,
+                                 maximumIterations=100, totalStartingPoints=k, batchSize=k,
+                                 precision=am.PRECISION_MIXED, stableIterations=3,
+                                 leadIterations=4)
+    M = solver.matrix(B)
+    b = M.batch(st, k)
+    b.load(V0)
+    for it in range(4):
+        kinds = dict(b.step_timed(it))
+        assert "gemm_BtZ" in kinds and "gemm_BtZ_low(skipped)" in kinds, (it, kinds)
+        # the last lead-in step hands over: the next step is single-pass
+        assert b.refining() == (it < 3), it
+    low = dict(b.step_timed(4))
+    assert "gemm_BtZ_low" in low and "gemm_BtZ(skipped)" in low
+    assert not b.refining()
+    switched_at = None
+    for it in range(5, 80):
+        b.iterate(it, 1)
+        if b.refining():
+            switched_at = it
+            break
+    assert switched_at is not None and switched_at >= 4 + 3
+    b.close()
+    M.close()
+
+
+@pytest.mark.parametrize("formulation", [0, 7])
+def test_lead_in_solve_counts_and_group(solver, po, formulation):
+    """Whole solves with a lead-in: the single-pass iterations exclude the
+    lead-in, the result reaches the FP32 run's explained variance within 1e-4,
+    and the same problem in a group gives the one-problem path's result bit for
+    bit (same kernels, same phase rule)."""
+    am = _am()
+    m, n, k = 400, 3000, 256
+    B = po.low_rank_data(m, n, 10, 40, seed=20 + formulation, dtype=np.float32)
+    B64 = B.astype(np.float64)
+    g = {7: 8.0}.get(formulation, 0.0)
+    kw = dict(formulation=formulation, constraintParameter=32, penaltyParameter=g,
+              tolerance=1e-6, maximumIterations=200, totalStartingPoints=k, batchSize=k,
+              startMode=am.START_DEVICE_UNIFORM)
+    M = solver.matrix(B)
+    x32, _, s32 = M.solve(am.OptimizationSettings(**kw))
+    mixed = am.OptimizationSettings(precision=am.PRECISION_MIXED, leadIterations=6, **kw)
+    xmx, fmx, smx = M.solve(mixed)
+    ev32 = float(np.linalg.norm(B64 @ np.asarray(x32, np.float64)) ** 2)
+    evmx = float(np.linalg.norm(B64 @ np.asarray(xmx, np.float64)) ** 2)
+    assert 1 <= smx.low_precision_iterations <= smx.it - 6
+    assert abs(evmx - ev32) <= 1e-4 * ev32
+    grp = am.Group(solver, capacity=2)
+    pid = grp.add(M, am.OptimizationSettings(precision=am.PRECISION_MIXED, leadIterations=6, **kw))
+    grp.run()
+    xg, sg = grp.result(pid)
+    assert sg.low_precision_iterations == smx.low_precision_iterations
+    assert sg.it == smx.it
+    assert np.array_equal(xg, xmx)
+    grp.close()
+    M.close()
