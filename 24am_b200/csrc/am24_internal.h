@@ -286,6 +286,21 @@ cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handl
                                      cudaStream_t st, bool in_graph = true);
 
 // ---- sparse-resident matrices (am24_matrix_create_csc_sparse_f32)
+// Outer entries (CSC columns, CSR rows) longer than SP_LONG entries are summed
+// in segments of SP_SEG entries, many warps per entry, then combined in
+// segment order: one very long column (a common term of a corpus) would
+// otherwise hold a single warp for the whole product.
+constexpr int SP_LONG = 1024;
+constexpr int SP_SEG = 1024;
+struct SparseLong {
+  int count = 0;                // outer entries longer than SP_LONG
+  int segs = 0;                 // their segments
+  int32_t *outer = nullptr;     // count: the outer entries
+  int32_t *seg_first = nullptr; // count + 1: each one's first segment
+  int32_t *seg_e0 = nullptr;    // segs: entry range [seg_e0, seg_e1) of each segment
+  int32_t *seg_e1 = nullptr;
+};
+
 // The data matrix in compressed form: CSC for V = B^T Z, CSR for Z = B V,
 // and the optional implicit centring B - 1 means^T - row_means 1^T.
 struct SparseDev {
@@ -297,6 +312,7 @@ struct SparseDev {
   float *rvals = nullptr;
   float *means = nullptr;      // n floats, or null
   float *row_means = nullptr;  // m floats, or null
+  SparseLong long_cols, long_rows;  // of the CSC and the CSR arrays
 };
 
 // A batch of k starts on a sparse matrix.  Start-major planes have columns of
@@ -315,6 +331,7 @@ struct SparseBatchDev {
   uint32_t *nnz = nullptr, *max_nnz = nullptr;
   uint32_t *ctl = nullptr;  // CTL_WORDS
   double *sum_v = nullptr, *dot_mu = nullptr, *zsum = nullptr, *zdot = nullptr;  // per start
+  float *part_cols = nullptr, *part_rows = nullptr;  // segments x kp partial sums
   int *status = nullptr;
   int *iters = nullptr, *cards = nullptr;
   int log_capacity = 0;

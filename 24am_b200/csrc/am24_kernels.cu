@@ -2921,6 +2921,24 @@ cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handl
 // ------------------------------------------------------------ sparse steps
 #include "am24_sparse_kernels.cuh"
 
+namespace {
+// One product on the compressed arrays: the tile kernel for the outer entries
+// of at most SP_LONG entries, the segment and combine kernels for the others.
+void sparse_product(const int32_t *ptr, const int32_t *idx, const float *val, int ncols,
+                    const SparseLong &L, const float *X, float *part, const SparseBatchDev &b,
+                    float *out, int ld_out, const float *cvec, const double *a, const double *bv,
+                    cudaStream_t st) {
+  sp_spmm_kernel<<<dim3((ncols + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
+      ptr, idx, val, ncols, X, b.kp, b.k, out, ld_out, cvec, a, bv, b.ctl);
+  if (L.count == 0) return;
+  constexpr int WARPS = SP_THREADS / 32;
+  sp_spmm_seg_kernel<<<dim3((L.segs + WARPS - 1) / WARPS, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
+      L.seg_e0, L.seg_e1, L.segs, idx, val, X, b.kp, part, b.ctl);
+  sp_spmm_long_kernel<<<dim3(L.count, b.kp / SP_TILE), SP_TILE, 0, st>>>(
+      L.outer, L.seg_first, part, b.kp, b.k, out, ld_out, cvec, a, bv, b.ctl);
+}
+}  // namespace
+
 cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, const StepParams &p,
                                cudaStream_t st) {
   cudaError_t e;
@@ -2933,18 +2951,17 @@ cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, cons
                                                  b.dot_mu, b.ctl);
   sp_transpose_v_kernel<<<dim3((S.n + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0,
                           st>>>(b.Vx, b.vmask, b.ldn, S.n, b.k, b.Vt, b.kp, b.ctl);
-  sp_spmm_kernel<<<dim3((S.m + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
-      S.row_ptr, S.col_ind, S.rvals, S.m, b.Vt, b.kp, b.k, b.Zs, b.ldm, S.row_means,
-      S.row_means ? b.sum_v : nullptr, S.means ? b.dot_mu : nullptr, b.ctl);
+  sparse_product(S.row_ptr, S.col_ind, S.rvals, S.m, S.long_rows, b.Vt, b.part_rows, b, b.Zs,
+                 b.ldm, S.row_means, S.row_means ? b.sum_v : nullptr,
+                 S.means ? b.dot_mu : nullptr, st);
   // 2. the formulation's sign / norm of z, and the sums V's correction needs
   sp_zreduce_kernel<<<b.k, SP_THREADS, 0, st>>>(b.Zs, b.ldm, S.m, f, b.fz, S.row_means,
                                                 centred ? b.zsum : nullptr, b.zdot, b.ctl);
   sp_transpose_z_kernel<<<dim3((S.m + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0,
                           st>>>(b.Zs, b.ldm, S.m, b.k, b.Zt, b.kp, b.ctl);
   // 3. V = (B - 1 mu^T - r 1^T)^T Z: CSC columns against Z transposed
-  sp_spmm_kernel<<<dim3((S.n + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
-      S.col_ptr, S.row_ind, S.cvals, S.n, b.Zt, b.kp, b.k, b.Vraw, b.ldn, S.means,
-      S.means ? b.zsum : nullptr, S.row_means ? b.zdot : nullptr, b.ctl);
+  sparse_product(S.col_ptr, S.row_ind, S.cvals, S.n, S.long_cols, b.Zt, b.part_cols, b, b.Vraw,
+                 b.ldn, S.means, S.means ? b.zsum : nullptr, S.row_means ? b.zdot : nullptr, st);
   if ((e = cudaGetLastError())) return e;
   // 4. thresholds: the dense path's selects (own candidate gather), or the penalties
   if (is_constrained(f)) {

@@ -2,9 +2,10 @@
 // (sparse_PCA_solver_CSC, c++/src/gpower/sparse_PCA_solver_for_CSC.h:111-117:
 // CSC arrays, optional doMean / doRowMean centring) kept compressed on the
 // device, and the batch driver that solves on it.  Device memory is O(nnz):
-// CSC plus a CSR copy (8 bytes per non-zero each), the centring vectors, and
-// per batch the start-major and row-major planes of V and Z
-// (4 (3 n + 2 m) bytes per start).  The iteration is the dense path's (the
+// CSC plus a CSR copy (8 bytes per non-zero each), the centring vectors, the
+// segment lists of columns and rows longer than SP_LONG entries, and per batch
+// the start-major and row-major planes of V and Z (4 (3 n + 2 m) bytes per
+// start) plus the long entries' segment sums (4 bytes per segment and start).  The iteration is the dense path's (the
 // reference's batch loop, c++/src/gpower/sparse_PCA_solver.h:171-232), so a
 // sparse-resident solve gives the dense solve of the centred matrix up to FP32
 // summation order; both products run as FP32 tile kernels on the compressed
@@ -42,6 +43,24 @@ am24_status validate_csc(const float *vals, const int32_t *row_ind, const int32_
   return AM24_OK;
 }
 
+// The segments of the outer entries longer than SP_LONG (host lists; see SparseLong).
+struct LongLists {
+  std::vector<int32_t> outer, first, e0, e1;
+  void build(const int32_t *ptr, int outer_n) {
+    for (int c = 0; c < outer_n; c++) {
+      const int32_t a = ptr[c], z = ptr[c + 1];
+      if (z - a <= SP_LONG) continue;
+      outer.push_back(c);
+      first.push_back((int32_t)e0.size());
+      for (int32_t e = a; e < z; e += SP_SEG) {
+        e0.push_back(e);
+        e1.push_back(std::min(z, e + SP_SEG));
+      }
+    }
+    first.push_back((int32_t)e0.size());
+  }
+};
+
 }  // namespace am24host
 
 extern "C" am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const float *vals,
@@ -71,6 +90,9 @@ extern "C" am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const fl
         rvals[at] = vals[e];
       }
   }
+  LongLists lc, lr;
+  lc.build(col_ptr, (int)n);
+  lr.build(row_ptr.data(), (int)m);
   AM24_CUDA(cudaSetDevice(h->device));
   auto *mat = new am24_matrix_s();
   mat->sparse = true;
@@ -92,6 +114,21 @@ extern "C" am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const fl
     delete mat;
     return st;
   }
+  auto alloc_long = [&](const LongLists &l, SparseLong &L) -> am24_status {
+    L.count = (int)l.outer.size();
+    L.segs = (int)l.e0.size();
+    if (L.count == 0) return AM24_OK;
+    am24_status s2;
+    if ((s2 = mat->mem.get(&L.outer, l.outer.size())) ||
+        (s2 = mat->mem.get(&L.seg_first, l.first.size())) ||
+        (s2 = mat->mem.get(&L.seg_e0, l.e0.size())) || (s2 = mat->mem.get(&L.seg_e1, l.e1.size())))
+      return s2;
+    return AM24_OK;
+  };
+  if ((st = alloc_long(lc, S.long_cols)) || (st = alloc_long(lr, S.long_rows))) {
+    delete mat;
+    return st;
+  }
   cudaError_t e = cudaSuccess;
   auto up = [&](void *dst, const void *src, size_t bytes) {
     if (e == cudaSuccess && bytes)
@@ -105,6 +142,13 @@ extern "C" am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const fl
   up(S.rvals, rvals.data(), sizeof(float) * nnz);
   if (means) up(S.means, means, sizeof(float) * n);
   if (row_means) up(S.row_means, row_means, sizeof(float) * m);
+  for (auto [l, L] : {std::make_pair(&lc, &S.long_cols), std::make_pair(&lr, &S.long_rows)}) {
+    if (L->count == 0) continue;
+    up(L->outer, l->outer.data(), sizeof(int32_t) * l->outer.size());
+    up(L->seg_first, l->first.data(), sizeof(int32_t) * l->first.size());
+    up(L->seg_e0, l->e0.data(), sizeof(int32_t) * l->e0.size());
+    up(L->seg_e1, l->e1.data(), sizeof(int32_t) * l->e1.size());
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);  // the host staging dies here
   if (e != cudaSuccess) {
     delete mat;
@@ -165,6 +209,8 @@ am24_status solve_sparse(am24_handle h, am24_matrix mat, float *x, am24_settings
   AM24_TRY(A.get(&xb, n));
   AM24_TRY(A.get(&x_dev, n));
   AM24_TRY(A.get(&ev_scratch, sparse_ev_scratch(S)));
+  if (S.long_cols.segs) AM24_TRY(A.get(&b.part_cols, (size_t)S.long_cols.segs * b.kp));
+  if (S.long_rows.segs) AM24_TRY(A.get(&b.part_rows, (size_t)S.long_rows.segs * b.kp));
   // every buffer starts defined: pool memory can hold an earlier call's state
   AM24_CUDA(cudaMemsetAsync(b.vmask, 0, sizeof(uint32_t) * (size_t)k * (b.ldn / 32), h->stream));
   AM24_CUDA(cudaMemsetAsync(b.Vx, 0, sizeof(float) * (size_t)k * b.ldn, h->stream));

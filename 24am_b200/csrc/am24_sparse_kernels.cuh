@@ -16,11 +16,52 @@
 constexpr int SP_TILE = 32;        // outer entries x starts per tile
 constexpr int SP_THREADS = 256;    // 8 warps, 4 outer entries each
 
+// sum over entries e in [e0, e1) of val[e] * X[idx[e] * kp + j], in entry
+// order with FP32 FMAs, for the lane's start j.  The warp loads 32 (index,
+// value) pairs at once, one per lane, and broadcasts them, so the X loads of
+// consecutive entries do not wait on one another.
+__device__ __forceinline__ float sp_dot(const int32_t *__restrict__ idx,
+                                        const float *__restrict__ val,
+                                        const float *__restrict__ X, int kp, int j, int e0,
+                                        int e1) {
+  const int lane = threadIdx.x & 31;
+  float acc = 0.f;
+  for (int base = e0; base < e1; base += 32) {
+    const int e = base + lane;
+    int ii = 0;
+    float vv = 0.f;
+    if (e < e1) {
+      ii = idx[e];
+      vv = val[e];
+    }
+    const int cnt = min(32, e1 - base);
+#pragma unroll 8
+    for (int t = 0; t < cnt; t++) {
+      const int i = __shfl_sync(0xFFFFFFFFu, ii, t);
+      const float v = __shfl_sync(0xFFFFFFFFu, vv, t);
+      acc = fmaf(v, X[(size_t)i * kp + j], acc);
+    }
+  }
+  return acc;
+}
+
+// The rank-one centring of one output: acc - (cvec ? cvec[c] a[j] : 0) - (b ? b[j] : 0) in FP64.
+__device__ __forceinline__ float sp_correct(float acc, int c, int j, const float *cvec,
+                                            const double *a, const double *b) {
+  if (!cvec && !b) return acc;
+  double corr = 0.0;
+  if (cvec) corr += (double)cvec[c] * a[j];
+  if (b) corr += b[j];
+  return (float)((double)acc - corr);
+}
+
 // out[j][c] (j < k, c < ncols) = sum_e val[e] X[idx[e] * kp + j]
 //                                - (cvec ? cvec[c] * a[j] : 0) - (b ? b[j] : 0)
 // One warp per outer entry, a lane per start: every entry reads one 128-byte
 // row segment of X.  Each sum runs over the outer entry's entries in storage
 // order with FP32 FMAs (deterministic); the correction is applied in FP64.
+// Outer entries longer than SP_LONG are left to sp_spmm_seg_kernel and
+// sp_spmm_long_kernel.
 __global__ void __launch_bounds__(SP_THREADS) sp_spmm_kernel(
     const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
     const float *__restrict__ val, int ncols, const float *__restrict__ X, int kp, int k,
@@ -28,29 +69,60 @@ __global__ void __launch_bounds__(SP_THREADS) sp_spmm_kernel(
     const double *__restrict__ a, const double *__restrict__ b, const uint32_t *stop) {
   if (*stop) return;
   __shared__ float tile[SP_TILE][SP_TILE + 1];
+  __shared__ int skip[SP_TILE];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int c0 = blockIdx.x * SP_TILE, j0 = blockIdx.y * SP_TILE;
   const int j = j0 + lane;  // < kp always (kp is a multiple of 32)
   for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
     const int c = c0 + r;
     float acc = 0.f;
+    bool own = false;
     if (c < ncols) {
-      const int e1 = ptr[c + 1];
-      for (int e = ptr[c]; e < e1; e++) acc = fmaf(val[e], X[(size_t)idx[e] * kp + j], acc);
-      if (j < k && (cvec || b)) {
-        double corr = 0.0;
-        if (cvec) corr += (double)cvec[c] * a[j];
-        if (b) corr += b[j];
-        acc = (float)((double)acc - corr);
+      const int e0 = ptr[c], e1 = ptr[c + 1];
+      own = e1 - e0 <= SP_LONG;
+      if (own) {
+        acc = sp_dot(idx, val, X, kp, j, e0, e1);
+        if (j < k) acc = sp_correct(acc, c, j, cvec, a, b);
       }
     }
     tile[lane][r] = acc;
+    if (lane == 0) skip[r] = !own;
   }
   __syncthreads();
   for (int r = warp; r < SP_TILE; r += SP_THREADS / 32) {
     const int jj = j0 + r, c = c0 + lane;
-    if (jj < k && c < ncols) out[(size_t)jj * ld_out + c] = tile[r][lane];
+    if (jj < k && c < ncols && !skip[lane]) out[(size_t)jj * ld_out + c] = tile[r][lane];
   }
+}
+
+// Long outer entries, step 1: one warp per (segment, 32 starts), the
+// segment's sum into part[s][j].
+__global__ void __launch_bounds__(SP_THREADS) sp_spmm_seg_kernel(
+    const int32_t *__restrict__ seg_e0, const int32_t *__restrict__ seg_e1, int segs,
+    const int32_t *__restrict__ idx, const float *__restrict__ val,
+    const float *__restrict__ X, int kp, float *__restrict__ part, const uint32_t *stop) {
+  if (*stop) return;
+  const int s = blockIdx.x * (SP_THREADS / 32) + (threadIdx.x >> 5);
+  const int j = blockIdx.y * SP_TILE + (threadIdx.x & 31);
+  if (s >= segs) return;  // whole warps leave together
+  part[(size_t)s * kp + j] = sp_dot(idx, val, X, kp, j, seg_e0[s], seg_e1[s]);
+}
+
+// Long outer entries, step 2: per (entry, start) the segments' sums in
+// segment order, then the centring, into out[j][c].
+__global__ void __launch_bounds__(SP_TILE) sp_spmm_long_kernel(
+    const int32_t *__restrict__ outer, const int32_t *__restrict__ seg_first,
+    const float *__restrict__ part, int kp, int k, float *__restrict__ out, int ld_out,
+    const float *__restrict__ cvec, const double *__restrict__ a, const double *__restrict__ b,
+    const uint32_t *stop) {
+  if (*stop) return;
+  const int x = blockIdx.x;
+  const int j = blockIdx.y * SP_TILE + threadIdx.x;
+  if (j >= k) return;
+  const int c = outer[x];
+  float acc = 0.f;
+  for (int s = seg_first[x]; s < seg_first[x + 1]; s++) acc += part[(size_t)s * kp + j];
+  out[(size_t)j * ld_out + c] = sp_correct(acc, c, j, cvec, a, b);
 }
 
 // Vt[q][j] = V's column j at row q (zero where its mask bit is clear), for

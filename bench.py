@@ -465,6 +465,75 @@ def run_uneven(args):
     return 0
 
 
+def corpus_csc(m, n, nnz, seed):
+    """A bag-of-words-like CSC matrix: m documents x n terms, about nnz entries,
+    term popularity Zipf-like (p_t ~ 1 / (t + 10)^1.1), documents uniform,
+    counts-like positive values; duplicates summed.  Returns (scipy CSC,
+    column means)."""
+    import numpy as np
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    p = 1.0 / (np.arange(n) + 10.0) ** 1.1
+    p /= p.sum()
+    cols = rng.choice(n, size=nnz, p=p).astype(np.int32)
+    rows = rng.integers(0, m, nnz, dtype=np.int32)
+    vals = (1.0 + rng.exponential(1.0, nnz)).astype(np.float32)
+    S = sp.csc_matrix((vals, (rows, cols)), shape=(m, n), dtype=np.float32)
+    S.sum_duplicates()
+    mu = np.asarray(S.mean(axis=0), np.float32).ravel()
+    return S, mu
+
+
+def run_sparse(args):
+    """Sparse (CSC) input, column-centred as the reference's text-corpus runs
+    are: whole solves of a fixed number of steps (tolerance 0) from device
+    starts, on the sparse-resident matrix and, where its dense form fits, on
+    the densified one.  start-iterations/s from the library's CUDA-event time
+    of the iterations."""
+    import numpy as np
+    am = importlib.import_module("24am_b200")
+    solver = am.Solver(0)
+    cases = [("corpus 200000 x 100000, 20M nnz", 200_000, 100_000, 20_000_000, False),
+             ("20000 x 50000 at 1 % density", 20_000, 50_000, 10_000_000, True)]
+    out = []
+    for name, m, n, nnz, dense_too in cases:
+        t0 = time.perf_counter()
+        S, mu = corpus_csc(m, n, nnz, SEED)
+        gen_s = time.perf_counter() - t0
+        row = {"case": name, "m": m, "n": n, "nnz": int(S.nnz), "generate_s": gen_s}
+        for keep in ([True, False] if dense_too else [True]):
+            t0 = time.perf_counter()
+            M = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu, keep_sparse=keep)
+            solver.sync()
+            up_s = time.perf_counter() - t0
+            res = {"upload_s": up_s}
+            for f, kw in ((0, dict(constraintParameter=32)), (3, dict(constraintParameter=32))):
+                st = am.OptimizationSettings(formulation=f, tolerance=0.0, maximumIterations=20,
+                                             totalStartingPoints=1024, batchSize=1024,
+                                             startMode=am.START_DEVICE_UNIFORM, **kw)
+                M.solve(st)  # warm-up: module loading, pool growth
+                _, fval, s = M.solve(st)
+                res[f"form{f}"] = {"start_it_per_s": s.start_iterations / s.total_true_computation_time,
+                                   "ms_per_step": 1e3 * s.total_true_computation_time / max(1, s.it),
+                                   "explained_variance": s.explained_variance}
+            M.close()
+            row["sparse_resident" if keep else "densified"] = res
+        out.append(row)
+    v = out[0]["sparse_resident"]
+    vals = [v[k]["start_it_per_s"] for k in v if k.startswith("form")]
+    line = {"metric": "start-iterations/s (sparse CSC input, column-centred)",
+            "value": float(np.mean(vals)), "unit": "start-it/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "bag-of-words-like CSC (Zipf term popularity), column means "
+                                   "subtracted implicitly; 1024 device starts; forms 0 and 3 "
+                                   "(s = 32); 20 steps per solve",
+                       "value_case": out[0]["case"]},
+            "cases": out}
+    print(json.dumps(line), flush=True)
+    solver.close()
+    return 0
+
+
 def run_serving(args):
     """The serving layer on one GPU.  Resident matrices from the uneven-problem
     distribution (p log-uniform in [1e3, 1e5], n log-uniform in [100, 5000],
@@ -833,11 +902,13 @@ def main():
     ap.add_argument("--formulations", default=None,
                     help="subset for profiling runs; the headline uses all 8 "
                          "(config2: 0 and 7, its two forms)")
-    ap.add_argument("--mode", default="step", choices=["step", "solve", "serve", "uneven"],
+    ap.add_argument("--mode", default="step",
+                    choices=["step", "solve", "serve", "uneven", "sparse"],
                     help="step: the AM-step throughput line; solve: whole solves to tol, "
                          "FP32 and MIXED precision from the same starts; serve: Poisson "
                          "requests to the serving layer (p50/p99 latency); uneven: 256 "
-                         "problems of uneven shapes submitted at once")
+                         "problems of uneven shapes submitted at once; sparse: CSC input kept "
+                         "compressed on the device against its densified form")
     ap.add_argument("--rates", default="10,30,100,300,1000,2000",
                     help="serve: request rates (req/s)")
     ap.add_argument("--max-requests", type=int, default=400,
@@ -866,6 +937,8 @@ def main():
         return run_uneven(args)
     if args.mode == "serve":
         return run_serving(args)
+    if args.mode == "sparse":
+        return run_sparse(args)
     return run_ours(args)
 
 

@@ -3,7 +3,7 @@
  * reference's member names, types and defaults
  * (c++/src/class/optimization_settings.h:27-170), so code written against the
  * reference compiles unchanged.  Extra members (startMode, l1Mode, timeoutMs,
- * precision, stableIterations, stableShare, leadIterations, device) select this library's options and
+ * precision, stableIterations, stableShare, leadIterations, device, sparseResident) select this library's options and
  * default to reference behaviour.
  */
 #ifndef AM24_OPTIMIZATION_SETTINGS_H
@@ -68,6 +68,9 @@ class OptimizationSettings {
   float stableShare;          // precision 1: share of the starts that must be that stable
   unsigned leadIterations;    // precision 1: FP32-accurate iterations before the single-pass phase
   int device;          // CUDA device of the default handle
+  int sparseResident;  // sparse_PCA_solver_CSC: 1 keeps B compressed on the device, 0
+                       // densifies it, -1 (default) keeps it compressed when its dense
+                       // FP32 form would exceed 8 GiB or its density is below 0.5 %
 
   OptimizationSettings()
       : proccessNode(0), distributedRowGridFile(0), tolerance(0.01), verbose(false),
@@ -79,7 +82,7 @@ class OptimizationSettings {
         batchSize(64), totalBatches(0), useOTF(false), doColumnMean(true), doRowMean(false),
         L2RowNormalization(true), tfidf(true), startMode(0), l1Mode(0), timeoutMs(5000),
         precision(0), stableIterations(5), stableShare(1.0f), leadIterations(0),
-        device(0) {}
+        device(0), sparseResident(-1) {}
 
   bool isConstrainedProblem() const { return (int)formulation <= 3; }
   bool isL1ConstrainedProblem() const {

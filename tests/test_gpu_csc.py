@@ -90,8 +90,8 @@ CSC_PROGRAM = r'''
 #include <cstdio>
 #include <vector>
 // input: m n nnz, col_ptr, row_ind, vals, means (n), one component pv (n);
-// output: the objective and x of a solve, then of a solve after adding pv to
-// the deflation collection
+// output: the objectives and x of a solve, of a solve after adding pv to the
+// deflation collection, and of a solve with B kept compressed on the device
 static SolverStructures::OptimizationSettings settings() {
   SolverStructures::OptimizationSettings s;
   s.formulation = SolverStructures::L0_constrained_L2_PCA;
@@ -123,22 +123,33 @@ int main(int argc, char **argv) {
   float f1 = SPCASolver::sparse_PCA_solver_CSC(v.data(), ri.data(), cp.data(), x1.data(), m, n,
                                                &s1, &st1, true, mu.data(), false, rmu.data(),
                                                defl);
+  SPCASolver::SparseDeflationCollection<float> none;
+  std::vector<float> x2(n, 0.f);
+  SolverStructures::OptimizationSettings s2 = settings();
+  s2.sparseResident = 1;
+  SolverStructures::OptimizationStatistics st2;
+  float f2 = SPCASolver::sparse_PCA_solver_CSC(v.data(), ri.data(), cp.data(), x2.data(), m, n,
+                                               &s2, &st2, true, mu.data(), false, rmu.data(),
+                                               none);
   FILE *o = fopen(argv[2], "wb");
   fwrite(&f0, 4, 1, o);
   fwrite(&f1, 4, 1, o);
+  fwrite(&f2, 4, 1, o);
   fwrite(x0.data(), 4, n, o);
   fwrite(x1.data(), 4, n, o);
+  fwrite(x2.data(), 4, n, o);
   fclose(o);
-  return (f0 == f0 && f1 == f1) ? 0 : 1;
+  return (f0 == f0 && f1 == f1 && f2 == f2) ? 0 : 1;
 }
 '''
 
 
 def test_csc_adapter_runs_like_the_python_mirror(solver, tmp_path):
     """A C++ caller of the reference's sparse_PCA_solver_CSC signature, linked to
-    the library: a solve, then one with a component in the deflation
-    collection, equal to the same two solves through the ABI (the mirror's
-    Matrix.from_csc, deflate and solve)."""
+    the library: a solve, one with a component in the deflation collection, and
+    one with the matrix kept compressed (settings.sparseResident = 1), equal to
+    the same three solves through the ABI (the mirror's Matrix.from_csc,
+    deflate and solve)."""
     import os
     import subprocess
     am = _am()
@@ -171,7 +182,8 @@ def test_csc_adapter_runs_like_the_python_mirror(solver, tmp_path):
     out = tmp_path / "out.bin"
     subprocess.run([str(exe), str(inp), str(out)], check=True)
     r = np.fromfile(out, np.float32)
-    f0, f1, x0, x1 = r[0], r[1], r[2:2 + n], r[2 + n:]
+    f0, f1, f2 = r[0], r[1], r[2]
+    x0, x1, x2 = r[3:3 + n], r[3 + n:3 + 2 * n], r[3 + 2 * n:]
     kw = dict(formulation=0, constraintParameter=10, tolerance=1e-6, maximumIterations=60,
               totalStartingPoints=32, batchSize=32)
     M = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu)
@@ -181,3 +193,8 @@ def test_csc_adapter_runs_like_the_python_mirror(solver, tmp_path):
     M.close()
     assert f0 == np.float32(g0) and np.array_equal(x0, y0)
     assert f1 == np.float32(g1) and np.array_equal(x1, y1)
+    # settings.sparseResident = 1: the sparse-resident path of the mirror
+    M = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu, keep_sparse=True)
+    y2, g2, _ = M.solve(am.OptimizationSettings(**kw))
+    M.close()
+    assert f2 == np.float32(g2) and np.array_equal(x2, y2)

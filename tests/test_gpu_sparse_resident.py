@@ -126,6 +126,62 @@ def test_sparse_resident_matches_densified_path(solver, formulation):
     assert abs(ss.it - sd.it) <= 3, (ss.it, sd.it)
 
 
+def _with_long_entries(m, n, seed):
+    """1 % noise plus four columns with 90 % of the rows filled and two rows
+    with 60 % of the columns filled: both products then have outer entries
+    longer than the 1024 entries one warp sums alone (SP_LONG)."""
+    rng = np.random.default_rng(seed)
+    A = _sparse(m, n, seed, density=0.01).toarray()
+    for c in rng.choice(n, 4, replace=False):
+        rows = rng.random(m) < 0.9
+        A[rows, c] = rng.standard_normal(int(rows.sum())).astype(np.float32) + 1.0
+    for r in rng.choice(m, 2, replace=False):
+        cols = rng.random(n) < 0.6
+        A[r, cols] = rng.standard_normal(int(cols.sum())).astype(np.float32)
+    return sp.csc_matrix(A)
+
+
+@pytest.mark.parametrize("formulation", [0, 1, 4, 6])
+def test_sparse_resident_long_columns_and_rows(solver, po, formulation):
+    """Columns and rows longer than SP_LONG entries (summed in segments, then
+    combined): whole solves against the densified path (device starts, 256
+    starts), and for the top-s form against the oracle (reference starts, 16
+    starts, 10 steps).  The L1-ball forms are left out here: their reference
+    scan cycles on such data, so two roundings of the same solve end on
+    different supports (the other tests hold them to the oracle)."""
+    am = _am()
+    m, n = 3000, 2000
+    S = _with_long_entries(m, n, 70 + formulation)
+    assert np.diff(S.indptr).max() > 1024 and np.diff(S.tocsr().indptr).max() > 1024
+    A = S.toarray()
+    mu, _, C = _centring(A, "columns")
+    g = _gamma(C, formulation, c=0.1)  # the long columns dominate the singular vector
+    kw = dict(formulation=formulation, constraintParameter=12, penaltyParameter=g,
+              tolerance=1e-6, maximumIterations=80, totalStartingPoints=256, batchSize=256,
+              startMode=am.START_DEVICE_UNIFORM)
+    out = {}
+    for keep in (False, True):
+        M = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu, keep_sparse=keep)
+        _, f, stats = M.solve(am.OptimizationSettings(**kw))
+        M.close()
+        out[keep] = (f, stats)
+    (fd, sd), (fs, ss) = out[False], out[True]
+    assert abs(ss.explained_variance - sd.explained_variance) <= 1e-4 * sd.explained_variance
+    assert abs(fs - fd) <= 1e-4 * abs(fd)
+    if formulation == 0:
+        k = 16
+        kw = dict(formulation=0, constraintParameter=12, tolerance=1e-6, maximumIterations=10,
+                  totalStartingPoints=k, batchSize=k)
+        M = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu, keep_sparse=True)
+        x, f, _ = M.solve(am.OptimizationSettings(**kw))
+        M.close()
+        s = po.make_settings(0, constraint=12, tolerance=1e-6, max_iter=10, total_starts=k,
+                             batch_size=k)
+        starts = po.reference_starts(n, k, True, 12, dtype=np.float32)
+        r = po.oracle_solve(C, s, starts.astype(np.float64))
+        assert abs(f - r["fval"]) <= 1e-5 * abs(r["fval"]), (f, r["fval"])
+
+
 def test_sparse_resident_beyond_dense_memory(solver):
     """400000 x 200000 at 2.5e-5 density (2 M non-zeros): its dense FP32 form
     alone (320 GB) would not fit in device memory.  A few iterations of the
