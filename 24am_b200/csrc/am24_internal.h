@@ -332,6 +332,8 @@ struct SparseBatchDev {
   uint32_t *ctl = nullptr;  // CTL_WORDS
   double *sum_v = nullptr, *dot_mu = nullptr, *zsum = nullptr, *zdot = nullptr;  // per start
   float *part_cols = nullptr, *part_rows = nullptr;  // segments x kp partial sums
+  unsigned long long *work = nullptr;  // matrix entries in the supports' columns (this step)
+  uint32_t *zgate = nullptr;           // this step's Z = B V path: 0 scatter, 1 CSR product
   int *status = nullptr;
   int *iters = nullptr, *cards = nullptr;
   int log_capacity = 0;

@@ -2924,18 +2924,19 @@ cudaError_t launch_grouped_condition(const GroupDev &g, unsigned long long handl
 namespace {
 // One product on the compressed arrays: the tile kernel for the outer entries
 // of at most SP_LONG entries, the segment and combine kernels for the others.
+// gate (may be null): the launches do their work only when *gate >= gate_min.
 void sparse_product(const int32_t *ptr, const int32_t *idx, const float *val, int ncols,
                     const SparseLong &L, const float *X, float *part, const SparseBatchDev &b,
                     float *out, int ld_out, const float *cvec, const double *a, const double *bv,
-                    cudaStream_t st) {
+                    const uint32_t *gate, uint32_t gate_min, cudaStream_t st) {
   sp_spmm_kernel<<<dim3((ncols + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
-      ptr, idx, val, ncols, X, b.kp, b.k, out, ld_out, cvec, a, bv, b.ctl);
+      ptr, idx, val, ncols, X, b.kp, b.k, out, ld_out, cvec, a, bv, b.ctl, gate, gate_min);
   if (L.count == 0) return;
   constexpr int WARPS = SP_THREADS / 32;
   sp_spmm_seg_kernel<<<dim3((L.segs + WARPS - 1) / WARPS, b.kp / SP_TILE), SP_THREADS, 0, st>>>(
-      L.seg_e0, L.seg_e1, L.segs, idx, val, X, b.kp, part, b.ctl);
+      L.seg_e0, L.seg_e1, L.segs, idx, val, X, b.kp, part, b.ctl, gate, gate_min);
   sp_spmm_long_kernel<<<dim3(L.count, b.kp / SP_TILE), SP_TILE, 0, st>>>(
-      L.outer, L.seg_first, part, b.kp, b.k, out, ld_out, cvec, a, bv, b.ctl);
+      L.outer, L.seg_first, part, b.kp, b.k, out, ld_out, cvec, a, bv, b.ctl, gate, gate_min);
 }
 }  // namespace
 
@@ -2946,14 +2947,25 @@ cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, cons
   const bool centred = S.means || S.row_means;
   if ((e = cudaMemsetAsync(b.max_err, 0, sizeof(float), st))) return e;
   // 1. Z = (B - 1 mu^T - r 1^T) V: CSR rows against V transposed
-  if (centred)
-    sp_vstats_kernel<<<b.k, SP_THREADS, 0, st>>>(b.Vx, b.vmask, b.ldn, S.n, S.means, b.sum_v,
-                                                 b.dot_mu, b.ctl);
+  // the centring's sums, and the entries a scatter of the supports would touch
+  if ((e = cudaMemsetAsync(b.work, 0, sizeof(unsigned long long), st))) return e;
+  sp_vstats_kernel<<<b.k, SP_THREADS, 0, st>>>(b.Vx, b.vmask, b.ldn, S.n, S.means,
+                                               centred ? b.sum_v : nullptr, b.dot_mu, S.col_ptr,
+                                               b.work, b.ctl);
+  // the scatter of each support when the previous step left at most
+  // SP_SCATTER_CAP loadings in every start and the scatter touches fewer
+  // entries than the CSR product steps through; else the CSR product
+  sp_zgate_kernel<<<1, 1, 0, st>>>(b.max_nnz, (uint32_t)SP_SCATTER_CAP, b.work,
+                                   SP_SCATTER_PER_STEP * (double)S.nnz * (double)(b.kp / 32),
+                                   b.zgate, b.ctl);
   sp_transpose_v_kernel<<<dim3((S.n + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0,
-                          st>>>(b.Vx, b.vmask, b.ldn, S.n, b.k, b.Vt, b.kp, b.ctl);
+                          st>>>(b.Vx, b.vmask, b.ldn, S.n, b.k, b.Vt, b.kp, b.ctl, b.zgate, 1u);
   sparse_product(S.row_ptr, S.col_ind, S.rvals, S.m, S.long_rows, b.Vt, b.part_rows, b, b.Zs,
                  b.ldm, S.row_means, S.row_means ? b.sum_v : nullptr,
-                 S.means ? b.dot_mu : nullptr, st);
+                 S.means ? b.dot_mu : nullptr, b.zgate, 1u, st);
+  sp_scatter_z_kernel<<<b.k, SP_THREADS, 0, st>>>(
+      S.col_ptr, S.row_ind, S.cvals, b.Vx, b.vmask, b.ldn, b.Zs, b.ldm, S.m, S.row_means,
+      S.row_means ? b.sum_v : nullptr, S.means ? b.dot_mu : nullptr, b.zgate, 0u, b.ctl);
   // 2. the formulation's sign / norm of z, and the sums V's correction needs
   sp_zreduce_kernel<<<b.k, SP_THREADS, 0, st>>>(b.Zs, b.ldm, S.m, f, b.fz, S.row_means,
                                                 centred ? b.zsum : nullptr, b.zdot, b.ctl);
@@ -2961,7 +2973,8 @@ cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, cons
                           st>>>(b.Zs, b.ldm, S.m, b.k, b.Zt, b.kp, b.ctl);
   // 3. V = (B - 1 mu^T - r 1^T)^T Z: CSC columns against Z transposed
   sparse_product(S.col_ptr, S.row_ind, S.cvals, S.n, S.long_cols, b.Zt, b.part_cols, b, b.Vraw,
-                 b.ldn, S.means, S.means ? b.zsum : nullptr, S.row_means ? b.zdot : nullptr, st);
+                 b.ldn, S.means, S.means ? b.zsum : nullptr, S.row_means ? b.zdot : nullptr,
+                 nullptr, 0, st);
   if ((e = cudaGetLastError())) return e;
   // 4. thresholds: the dense path's selects (own candidate gather), or the penalties
   if (is_constrained(f)) {

@@ -74,6 +74,43 @@ extern "C" am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const fl
   // every index is checked on the host before any device write can use it
   AM24_TRY(validate_csc(vals, row_ind, col_ptr, m, n));
   if (!h) return fail(AM24_ERR_INVALID_ARG, "NULL handle");
+  // canonical columns (rows strictly ascending): a column whose rows are not
+  // is sorted by row (stably) and its duplicate entries added in entry order,
+  // so that every column's rows are distinct on the device
+  std::vector<int32_t> cp2, ri2;
+  std::vector<float> v2;
+  bool canonical = true;
+  for (uint32_t c = 0; c < n && canonical; c++)
+    for (int32_t e = col_ptr[c] + 1; e < col_ptr[c + 1]; e++)
+      if (row_ind[e] <= row_ind[e - 1]) {
+        canonical = false;
+        break;
+      }
+  if (!canonical) {
+    cp2.assign((size_t)n + 1, 0);
+    ri2.reserve((size_t)col_ptr[n]);
+    v2.reserve((size_t)col_ptr[n]);
+    std::vector<int32_t> order;
+    for (uint32_t c = 0; c < n; c++) {
+      order.clear();
+      for (int32_t e = col_ptr[c]; e < col_ptr[c + 1]; e++) order.push_back(e);
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int32_t a, int32_t b2) { return row_ind[a] < row_ind[b2]; });
+      for (size_t q = 0; q < order.size(); q++) {
+        const int32_t e = order[q];
+        if (q > 0 && row_ind[e] == ri2.back())
+          v2.back() += vals[e];
+        else {
+          ri2.push_back(row_ind[e]);
+          v2.push_back(vals[e]);
+        }
+      }
+      cp2[c + 1] = (int32_t)ri2.size();
+    }
+    col_ptr = cp2.data();
+    row_ind = ri2.data();
+    vals = v2.data();
+  }
   const size_t nnz = (size_t)col_ptr[n];
   // the CSR copy, built on the host by a counting pass: within each row the
   // columns come in ascending order, as the CSC arrays list them
@@ -199,6 +236,8 @@ am24_status solve_sparse(am24_handle h, am24_matrix mat, float *x, am24_settings
   AM24_TRY(A.get(&b.nnz, k));
   AM24_TRY(A.get(&b.max_nnz, 1));
   AM24_TRY(A.get(&b.ctl, CTL_WORDS));
+  AM24_TRY(A.get(&b.work, 1));
+  AM24_TRY(A.get(&b.zgate, 1));
   AM24_TRY(A.get(&b.sum_v, k));
   AM24_TRY(A.get(&b.dot_mu, k));
   AM24_TRY(A.get(&b.zsum, k));
@@ -268,6 +307,7 @@ am24_status solve_sparse(am24_handle h, am24_matrix mat, float *x, am24_settings
     AM24_CUDA(cudaMemsetAsync(b.val, 0, sizeof(float) * k, h->stream));
     AM24_CUDA(cudaMemsetAsync(b.err, 0, sizeof(float) * k, h->stream));
     AM24_CUDA(cudaMemsetAsync(b.ctl, 0, sizeof(uint32_t) * CTL_WORDS, h->stream));
+    AM24_CUDA(cudaMemsetAsync(b.max_nnz, 0xFF, sizeof(uint32_t), h->stream));  // dense starts
     AM24_CUDA(cudaEventRecord(e0, h->stream));
     // the batch loop: finalize sets the stop word after the step the
     // reference's loop ends on; the host reads it after each step

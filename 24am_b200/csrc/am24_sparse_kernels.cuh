@@ -66,8 +66,9 @@ __global__ void __launch_bounds__(SP_THREADS) sp_spmm_kernel(
     const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
     const float *__restrict__ val, int ncols, const float *__restrict__ X, int kp, int k,
     float *__restrict__ out, int ld_out, const float *__restrict__ cvec,
-    const double *__restrict__ a, const double *__restrict__ b, const uint32_t *stop) {
-  if (*stop) return;
+    const double *__restrict__ a, const double *__restrict__ b, const uint32_t *stop,
+    const uint32_t *gate, uint32_t gate_min) {
+  if (*stop || (gate && *gate < gate_min)) return;
   __shared__ float tile[SP_TILE][SP_TILE + 1];
   __shared__ int skip[SP_TILE];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -95,13 +96,89 @@ __global__ void __launch_bounds__(SP_THREADS) sp_spmm_kernel(
   }
 }
 
+// Z = (B - centring) V once V is sparse (when sp_zgate_kernel chose this path:
+// *gate <= cap), one block per start: the
+// start's support listed in index order in shared memory, then z = sum over
+// the support of v_q B[:, q], one CSC column at a time (its rows are distinct,
+// so its entries add in parallel), and the centring as the CSR product applies
+// it.  Row i's sum runs over the same columns in the same order as in the CSR
+// product (whose other terms multiply v = 0), so the result is the same bit
+// for bit (rows the CSR product sums in segments aside), at the cost of the
+// support's entries instead of every row's.
+constexpr int SP_SCATTER_CAP = 1024;
+__global__ void __launch_bounds__(SP_THREADS) sp_scatter_z_kernel(
+    const int32_t *__restrict__ col_ptr, const int32_t *__restrict__ row_ind,
+    const float *__restrict__ cvals, const float *__restrict__ Vx,
+    const uint32_t *__restrict__ vmask, int ldn, float *__restrict__ Zs, int ldm, int m,
+    const float *__restrict__ row_means, const double *__restrict__ sum_v,
+    const double *__restrict__ dot_mu, const uint32_t *gate, uint32_t cap, const uint32_t *stop) {
+  if (*stop || *gate > cap) return;
+  __shared__ int32_t list[SP_SCATTER_CAP];
+  __shared__ uint32_t wsum[SP_THREADS / 32];
+  const int j = blockIdx.x;
+  const int words = ldn >> 5;
+  const uint32_t *mk = vmask + (size_t)j * words;
+  float *z = Zs + (size_t)j * ldm;
+  for (int i = threadIdx.x; i < m; i += SP_THREADS) z[i] = 0.f;
+  // the support in index order: a pass of SP_THREADS words at a time, each
+  // thread's word expanded at its block-wide prefix of set bits
+  int count = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int w0 = 0; w0 < words; w0 += SP_THREADS) {
+    const int w = w0 + threadIdx.x;
+    const uint32_t bits = w < words ? mk[w] : 0u;
+    const uint32_t c = __popc(bits);
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0, total = 0;
+    for (int x = 0; x < SP_THREADS / 32; x++) {
+      if (x < warp) before += wsum[x];
+      total += wsum[x];
+    }
+    uint32_t at = count + before + incl - c;
+    for (uint32_t b = bits; b; b &= b - 1u) {
+      if (at < (uint32_t)SP_SCATTER_CAP) list[at] = (w << 5) + (__ffs(b) - 1);
+      at++;
+    }
+    count += (int)total;
+    __syncthreads();
+  }
+  auto add_column = [&](int q) {
+    const float v = Vx[(size_t)j * ldn + q];
+    for (int e = col_ptr[q] + threadIdx.x; e < col_ptr[q + 1]; e += SP_THREADS) {
+      const int i = row_ind[e];
+      z[i] = fmaf(cvals[e], v, z[i]);
+    }
+    __syncthreads();
+  };
+  if (count <= SP_SCATTER_CAP) {
+    for (int t = 0; t < count; t++) add_column(list[t]);
+  } else {
+    // more loadings than the list holds (the gate's count is the finalize
+    // pass's, so this is not expected): the same order, read from the mask
+    for (int w = 0; w < words; w++)
+      for (uint32_t b = mk[w]; b; b &= b - 1u) add_column((w << 5) + (__ffs(b) - 1));
+  }
+  if (row_means || dot_mu) {
+    for (int i = threadIdx.x; i < m; i += SP_THREADS)
+      z[i] = sp_correct(z[i], i, j, row_means, sum_v, dot_mu);
+  }
+}
+
 // Long outer entries, step 1: one warp per (segment, 32 starts), the
 // segment's sum into part[s][j].
 __global__ void __launch_bounds__(SP_THREADS) sp_spmm_seg_kernel(
     const int32_t *__restrict__ seg_e0, const int32_t *__restrict__ seg_e1, int segs,
     const int32_t *__restrict__ idx, const float *__restrict__ val,
-    const float *__restrict__ X, int kp, float *__restrict__ part, const uint32_t *stop) {
-  if (*stop) return;
+    const float *__restrict__ X, int kp, float *__restrict__ part, const uint32_t *stop,
+    const uint32_t *gate, uint32_t gate_min) {
+  if (*stop || (gate && *gate < gate_min)) return;
   const int s = blockIdx.x * (SP_THREADS / 32) + (threadIdx.x >> 5);
   const int j = blockIdx.y * SP_TILE + (threadIdx.x & 31);
   if (s >= segs) return;  // whole warps leave together
@@ -114,8 +191,8 @@ __global__ void __launch_bounds__(SP_TILE) sp_spmm_long_kernel(
     const int32_t *__restrict__ outer, const int32_t *__restrict__ seg_first,
     const float *__restrict__ part, int kp, int k, float *__restrict__ out, int ld_out,
     const float *__restrict__ cvec, const double *__restrict__ a, const double *__restrict__ b,
-    const uint32_t *stop) {
-  if (*stop) return;
+    const uint32_t *stop, const uint32_t *gate, uint32_t gate_min) {
+  if (*stop || (gate && *gate < gate_min)) return;
   const int x = blockIdx.x;
   const int j = blockIdx.y * SP_TILE + threadIdx.x;
   if (j >= k) return;
@@ -126,11 +203,13 @@ __global__ void __launch_bounds__(SP_TILE) sp_spmm_long_kernel(
 }
 
 // Vt[q][j] = V's column j at row q (zero where its mask bit is clear), for
-// q < n, j < kp (columns k..kp-1 zero): the row-major X of Z = B V.
+// q < n, j < kp (columns k..kp-1 zero): the row-major X of Z = B V (dense
+// steps only: *gate >= gate_min).
 __global__ void __launch_bounds__(SP_THREADS) sp_transpose_v_kernel(
     const float *__restrict__ Vx, const uint32_t *__restrict__ mask, int ldn, int n, int k,
-    float *__restrict__ Vt, int kp, const uint32_t *stop) {
-  if (*stop) return;
+    float *__restrict__ Vt, int kp, const uint32_t *stop, const uint32_t *gate,
+    uint32_t gate_min) {
+  if (*stop || *gate < gate_min) return;
   __shared__ float tile[SP_TILE][SP_TILE + 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int q0 = blockIdx.x * SP_TILE, j0 = blockIdx.y * SP_TILE;
@@ -185,30 +264,58 @@ __device__ __forceinline__ double sp_block_sum(double v, double *red) {
 }
 
 // Per start j (one block): sum_v[j] = sum_q v_q and dot_mu[j] = sum_q mu_q v_q
-// over V's defined entries, in FP64: the rank-one corrections of Z = B V.
+// over V's defined entries, in FP64 (the rank-one corrections of Z = B V, when
+// sum_v is not null), and the number of matrix entries in the start's support
+// columns, added to *work (what a scatter of the support would touch).
 __global__ void __launch_bounds__(SP_THREADS) sp_vstats_kernel(
     const float *__restrict__ Vx, const uint32_t *__restrict__ mask, int ldn, int n,
     const float *__restrict__ means, double *__restrict__ sum_v, double *__restrict__ dot_mu,
-    const uint32_t *stop) {
+    const int32_t *__restrict__ col_ptr, unsigned long long *work, const uint32_t *stop) {
   if (*stop) return;
   __shared__ double red[SP_THREADS / 32];
   const int j = blockIdx.x;
   const int words = ldn >> 5;
-  double s = 0.0, d = 0.0;
+  double s = 0.0, d = 0.0, entries = 0.0;
   for (int q = threadIdx.x; q < n; q += SP_THREADS) {
     const uint32_t w = mask[(size_t)j * words + (q >> 5)];
     if ((w >> (q & 31)) & 1u) {
       const double v = (double)Vx[(size_t)j * ldn + q];
       s += v;
       if (means) d += (double)means[q] * v;
+      entries += (double)(col_ptr[q + 1] - col_ptr[q]);
     }
   }
-  s = sp_block_sum(s, red);
-  d = sp_block_sum(d, red);
-  if (threadIdx.x == 0) {
-    sum_v[j] = s;
-    dot_mu[j] = d;
+  entries = sp_block_sum(entries, red);
+  if (sum_v) {
+    s = sp_block_sum(s, red);
+    d = sp_block_sum(d, red);
   }
+  if (threadIdx.x == 0) {
+    if (sum_v) {
+      sum_v[j] = s;
+      dot_mu[j] = d;
+    }
+    atomicAdd(work, (unsigned long long)entries);
+  }
+}
+
+// The path of this step's Z = B V, into *zgate: 0 the scatter of each
+// support, 1 the CSR product.  The scatter needs every start's support
+// within its list (the previous step's largest count, *max_nnz, at most cap)
+// and must touch fewer matrix entries (*work over all starts) than csr_steps:
+// SP_SCATTER_PER_STEP times the steps of the CSR product's warps (nnz x k / 32,
+// one 32-start row segment per entry and chunk of starts).  A scattered entry
+// (a coalesced read of its row and value, one update of a z row that stays in
+// cache) costs about a quarter of such a warp step: measured on B200 with
+// 1024 starts, a support work of 1.4x the warp steps ran faster scattered
+// (6.5 against 9.3 ms per step), while a corpus whose supports hold its most
+// common terms (an estimated 5x) ran slower (26.9 against 24.0).
+constexpr double SP_SCATTER_PER_STEP = 4.0;
+__global__ void sp_zgate_kernel(const uint32_t *max_nnz, uint32_t cap,
+                                const unsigned long long *work, double csr_steps,
+                                uint32_t *zgate, const uint32_t *stop) {
+  if (*stop) return;
+  *zgate = (*max_nnz <= cap && (double)*work < csr_steps) ? 0u : 1u;
 }
 
 // Per start j (one block), on z = Zs[j] after the centred product:

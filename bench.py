@@ -193,6 +193,56 @@ def cpu_reference(B_host, steps, per_step_iters, starts, forms_per_step=8, first
     return total_its / total_s, cores, kind, total_its, total_s
 
 
+def fp64_oracle_check(am, M, B_host, gam, starts=64, iters=3):
+    """Per-start error of the GPU path against the FP64 oracle (checker only,
+    outside every timed region): for each formulation, `starts` reference
+    starting points stepped `iters` times on the device (am24_batch_iterate)
+    and by oracle/fast_oracle in FP64 from the same FP32 starts.  Returns, per
+    formulation, the largest and median relative difference of the per-start
+    objective and of the per-start explained variance ||B x||^2 (FP64 of each
+    side's loadings), over the starts whose steps were all well conditioned,
+    and how many were set aside."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle as po
+    import fast_oracle as fo
+    B64 = np.asarray(B_host, np.float64)
+    n = B64.shape[1]
+    out = {}
+    for f in range(8):
+        V0 = po.reference_starts(n, starts, f <= 3, S_CONS, dtype=np.float32)
+        st = am.OptimizationSettings(formulation=f, constraintParameter=S_CONS,
+                                     penaltyParameter=gam.get(f, 0.0), tolerance=0.0,
+                                     maximumIterations=iters, totalStartingPoints=starts,
+                                     batchSize=starts)
+        b = M.batch(st, starts)
+        b.load(V0)
+        b.iterate(0, iters)
+        Vg, valg, _, _ = b.read()
+        b.close()
+        V = V0.astype(np.float64)
+        val = np.zeros(starts)
+        ill = np.zeros(starts, bool)
+        for _ in range(iters):
+            r = fo.iteration(B64, V, f, S_CONS, gam.get(f, 0.0), val)
+            V, val, ill = r.V, r.val, ill | r.ill
+        ok = ~ill & np.isfinite(val) & (val != 0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            e_obj = np.abs(valg.astype(np.float64) - val) / np.abs(val)
+
+            def ev(X):
+                Xn = X / np.linalg.norm(X, axis=0, keepdims=True)
+                return np.linalg.norm(B64 @ Xn, axis=0) ** 2
+            e_ev = np.abs(ev(Vg.astype(np.float64)) - ev(V)) / ev(V)
+        o, v = e_obj[ok], e_ev[ok]
+        out[str(f)] = {"max_objective_rel_err": float(o.max()) if o.size else None,
+                       "median_objective_rel_err": float(np.median(o)) if o.size else None,
+                       "max_explained_variance_rel_err": float(v.max()) if v.size else None,
+                       "starts_compared": int(ok.sum()), "set_aside_ill_conditioned":
+                           int(starts - ok.sum())}
+    return out
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -865,6 +915,15 @@ def run_ours(args):
                "sample": f"8 formulations x {CPU_SAMPLE_ITERS} iterations x "
                          f"{CPU_SAMPLE_STARTS} starts on the full matrix ({its} start-iterations, "
                          f"{secs:.1f} s compute, reference denseDataSolver<float> + OpenBLAS)"}
+        if not args.no_oracle_check:
+            t0 = time.perf_counter()
+            cpu["fp64_oracle_check"] = {
+                "per_formulation": fp64_oracle_check(am, M, Bnp, gam, 256, CPU_SAMPLE_ITERS),
+                "how": f"256 reference starts (CTA-pair tiles, split-FP16 products, as the "
+                       f"timed steps run) x {CPU_SAMPLE_ITERS} steps on the device against the "
+                       "FP64 oracle from the same starts; starts with an ill-conditioned "
+                       "decision (FP32-size ties) set aside",
+                "seconds": time.perf_counter() - t0}
 
     if rank == 0:
         line = {"metric": "start-iterations/s", "value": value, "unit": "start-it/s",
@@ -898,6 +957,8 @@ def main():
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the per-start FP64 oracle check after the CPU baseline")
     ap.add_argument("--size", default="config1", choices=sorted(SIZES))
     ap.add_argument("--formulations", default=None,
                     help="subset for profiling runs; the headline uses all 8 "

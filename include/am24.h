@@ -161,6 +161,10 @@ void am24_default_settings(am24_settings *s);
  * s <= n, batch 0 -> total, total rounded up to whole batches. Host only. */
 am24_status am24_check_input(am24_settings *s, uint32_t n);
 
+/* A handle owns a stream on `device`.  Every entry point that takes a handle
+ * (or a server) makes that device current on the calling thread
+ * (cudaSetDevice) and leaves it current on return: a caller that drives other
+ * devices from the same thread sets its own device again afterwards. */
 am24_status am24_create(am24_handle *h, int device);
 am24_status am24_destroy(am24_handle h);
 
@@ -220,8 +224,9 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
  * the host) and the centring vectors; a solve adds 4 (3 n + 2 m) bytes per
  * start of its batch.  The centring is applied implicitly as rank-one
  * corrections of both products (the reference's doMean / doRowMean arithmetic,
- * :223-248, :277-309, here with the corrections' sums in FP64).  Duplicate
- * (row, column) entries add up.  Such a matrix is solved by
+ * :223-248, :277-309, here with the corrections' sums in FP64).  Rows within a
+ * column need not be sorted: such columns are sorted on the host and duplicate
+ * (row, column) entries added up in entry order.  Such a matrix is solved by
  * am24_solve_resident_f32 (batch mode: the dense path's iteration, both
  * products as FP32 kernels on the compressed arrays, AM24_PRECISION_MIXED runs
  * as FP32; use_otf returns AM24_ERR_UNSUPPORTED); the batch, group, deflation

@@ -231,3 +231,39 @@ def test_sparse_resident_rejections(solver):
         grp.add(M, st)
     grp.close()
     M.close()
+
+
+def test_sparse_resident_unsorted_and_duplicate_entries(solver):
+    """CSC columns with unsorted rows and repeated (row, column) entries are
+    sorted and summed on the host: the solve equals the one on the canonical
+    arrays bit for bit (values are small integers, so every sum is exact)."""
+    am = _am()
+    m, n = 120, 700
+    rng = np.random.default_rng(9)
+    A = _planted(m, n, 19, density=0.08).toarray()
+    A = np.round(A * 4.0).astype(np.float32)
+    S = sp.csc_matrix(A)
+    S.sort_indices()
+    # split every entry in two halves at random positions of its column, shuffled
+    ptr, rows, vals = [0], [], []
+    for c in range(n):
+        r = S.indices[S.indptr[c]:S.indptr[c + 1]]
+        v = S.data[S.indptr[c]:S.indptr[c + 1]]
+        half = np.floor(v / 2.0).astype(np.float32)
+        rr = np.concatenate([r, r])
+        vv = np.concatenate([half, (v - half).astype(np.float32)])
+        perm = rng.permutation(rr.size)
+        rows.extend(rr[perm])
+        vals.extend(vv[perm])
+        ptr.append(len(rows))
+    mu = np.asarray(A.mean(axis=0), np.float32)
+    kw = dict(formulation=0, constraintParameter=10, tolerance=1e-6, maximumIterations=40,
+              totalStartingPoints=64, batchSize=64)
+    M1 = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu, keep_sparse=True)
+    x1, f1, _ = M1.solve(am.OptimizationSettings(**kw))
+    M1.close()
+    M2 = am.Matrix.from_csc(solver, np.array(vals, np.float32), np.array(rows, np.int32),
+                            np.array(ptr, np.int32), m, n, means=mu, keep_sparse=True)
+    x2, f2, _ = M2.solve(am.OptimizationSettings(**kw))
+    M2.close()
+    assert f1 == f2 and np.array_equal(x1, x2)
