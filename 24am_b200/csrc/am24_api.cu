@@ -656,7 +656,7 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
 am24_status am24_matrix_deflate(am24_handle h, am24_matrix mat, const float *x,
                                 int32_t on_device) {
   if (!h || !mat || !x) return fail(AM24_ERR_INVALID_ARG, "NULL argument");
-  if (mat->sparse) return fail(AM24_ERR_UNSUPPORTED, "sparse-resident matrices are not deflated");
+  if (mat->sparse) return deflate_sparse(h, mat, x, on_device);
   AM24_CUDA(cudaSetDevice(h->device));
   MatrixDev &M = mat->d;
   Allocs local(h->stream);

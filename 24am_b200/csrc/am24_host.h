@@ -99,6 +99,12 @@ struct am24_matrix_s {
   am24host::Allocs mem;
   bool sparse = false;  // am24_matrix_create_csc_sparse_f32: kept compressed
   am24::SparseDev sp{};
+  // sparse-resident deflations: host copies of what sp's device buffers hold
+  std::vector<float> means_host;  // n, or empty
+  std::vector<float> defl_host;   // comps x n
+  std::vector<double> gram_host;  // SP_DEFL_MAX x SP_DEFL_MAX
+  float *defl_dev = nullptr;
+  double *gram_dev = nullptr, *defl_sum_dev = nullptr, *defl_mu_dev = nullptr;
 };
 
 struct am24_batch_s {
@@ -131,6 +137,9 @@ StepParams step_params(const am24_settings &s, int it, int shift);
 // non-decreasing; row indices in [0, m)); the shared rule of both CSC entry points.
 am24_status validate_csc(const float *vals, const int32_t *row_ind, const int32_t *col_ptr,
                          uint32_t m, uint32_t n);
+// am24_matrix_deflate on a sparse-resident matrix: records x as the next factor
+// (I - x x^T) of B's deflation.
+am24_status deflate_sparse(am24_handle h, am24_matrix mat, const float *x, int32_t on_device);
 // am24_solve_resident_f32 on a sparse-resident matrix (settings already checked).
 am24_status solve_sparse(am24_handle h, am24_matrix mat, float *x, am24_settings &s,
                          am24_statistics *stats, const float *start_points, float *fval_out);

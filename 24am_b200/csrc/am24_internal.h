@@ -313,7 +313,15 @@ struct SparseDev {
   float *means = nullptr;      // n floats, or null
   float *row_means = nullptr;  // m floats, or null
   SparseLong long_cols, long_rows;  // of the CSC and the CSR arrays
+  // deflation (am24_matrix_deflate): B <- B (I - x_1 x_1^T) ... (I - x_C x_C^T),
+  // applied to V before Z = B V and to B^T Z after it, never to the arrays
+  int comps = 0;
+  const float *defl = nullptr;     // comps x n: x_1 .. x_C in call order
+  const double *gram = nullptr;    // SP_DEFL_MAX x SP_DEFL_MAX: x_a^T x_b
+  const double *defl_sum = nullptr;  // comps: 1^T x_c
+  const double *defl_mu = nullptr;   // comps: means^T x_c (0 without means)
 };
+constexpr int SP_DEFL_MAX = 32;  // deflations a sparse-resident matrix takes
 
 // A batch of k starts on a sparse matrix.  Start-major planes have columns of
 // ldn (features) or ldm (samples) floats; the row-major planes Vt (n rows) and
@@ -334,6 +342,7 @@ struct SparseBatchDev {
   float *part_cols = nullptr, *part_rows = nullptr;  // segments x kp partial sums
   unsigned long long *work = nullptr;  // matrix entries in the supports' columns (this step)
   uint32_t *zgate = nullptr;           // this step's Z = B V path: 0 scatter, 1 CSR product
+  double *defl_a = nullptr;            // k x SP_DEFL_MAX: V's deflation coefficients
   int *status = nullptr;
   int *iters = nullptr, *cards = nullptr;
   int log_capacity = 0;

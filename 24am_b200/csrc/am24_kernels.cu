@@ -2955,11 +2955,18 @@ cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, cons
   // the scatter of each support when the previous step left at most
   // SP_SCATTER_CAP loadings in every start and the scatter touches fewer
   // entries than the CSR product steps through; else the CSR product
-  sp_zgate_kernel<<<1, 1, 0, st>>>(b.max_nnz, (uint32_t)SP_SCATTER_CAP, b.work,
-                                   SP_SCATTER_PER_STEP * (double)S.nnz * (double)(b.kp / 32),
-                                   b.zgate, b.ctl);
+  // deflated: the projected loadings P v are dense, so the CSR product runs
+  if (S.comps > 0)
+    sp_defl_coef_kernel<<<b.k, SP_THREADS, 0, st>>>(
+        b.Vx, b.vmask, b.ldn, S.n, S.defl, S.comps, S.gram, S.defl_sum, S.defl_mu, b.defl_a,
+        centred ? b.sum_v : nullptr, b.dot_mu, b.ctl);
+  sp_zgate_kernel<<<1, 1, 0, st>>>(
+      b.max_nnz, (uint32_t)SP_SCATTER_CAP, b.work,
+      S.comps > 0 ? -1.0 : SP_SCATTER_PER_STEP * (double)S.nnz * (double)(b.kp / 32), b.zgate,
+      b.ctl);
   sp_transpose_v_kernel<<<dim3((S.n + SP_TILE - 1) / SP_TILE, b.kp / SP_TILE), SP_THREADS, 0,
-                          st>>>(b.Vx, b.vmask, b.ldn, S.n, b.k, b.Vt, b.kp, b.ctl, b.zgate, 1u);
+                          st>>>(b.Vx, b.vmask, b.ldn, S.n, b.k, b.Vt, b.kp, b.ctl, b.zgate, 1u,
+                                S.defl, S.comps, b.defl_a);
   sparse_product(S.row_ptr, S.col_ind, S.rvals, S.m, S.long_rows, b.Vt, b.part_rows, b, b.Zs,
                  b.ldm, S.row_means, S.row_means ? b.sum_v : nullptr,
                  S.means ? b.dot_mu : nullptr, b.zgate, 1u, st);
@@ -2975,6 +2982,9 @@ cudaError_t launch_sparse_step(const SparseDev &S, const SparseBatchDev &b, cons
   sparse_product(S.col_ptr, S.row_ind, S.cvals, S.n, S.long_cols, b.Zt, b.part_cols, b, b.Vraw,
                  b.ldn, S.means, S.means ? b.zsum : nullptr, S.row_means ? b.zdot : nullptr,
                  nullptr, 0, st);
+  if (S.comps > 0)
+    sp_defl_vraw_kernel<<<b.k, SP_THREADS, 0, st>>>(b.Vraw, b.ldn, S.n, S.defl, S.comps, S.gram,
+                                                    b.ctl);
   if ((e = cudaGetLastError())) return e;
   // 4. thresholds: the dense path's selects (own candidate gather), or the penalties
   if (is_constrained(f)) {

@@ -133,6 +133,7 @@ extern "C" am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const fl
   AM24_CUDA(cudaSetDevice(h->device));
   auto *mat = new am24_matrix_s();
   mat->sparse = true;
+  if (means) mat->means_host.assign(means, means + n);
   MatrixDev &M = mat->d;
   M.m = (int)m;
   M.n = (int)n;
@@ -198,6 +199,55 @@ extern "C" am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const fl
 
 namespace am24host {
 
+am24_status deflate_sparse(am24_handle h, am24_matrix mat, const float *x, int32_t on_device) {
+  SparseDev &S = mat->sp;
+  const int n = S.n, c = S.comps;
+  if (c >= SP_DEFL_MAX)
+    return fail(AM24_ERR_INVALID_ARG, "a sparse-resident matrix takes at most " +
+                                          std::to_string(SP_DEFL_MAX) + " deflations");
+  AM24_CUDA(cudaSetDevice(h->device));
+  // work already queued on the handle's stream sees the old deflation
+  AM24_CUDA(cudaStreamSynchronize(h->stream));
+  std::vector<float> xh((size_t)n);
+  AM24_CUDA(cudaMemcpy(xh.data(), x, sizeof(float) * n,
+                       on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+  if (!mat->defl_dev) {
+    am24_status st;
+    if ((st = mat->mem.get(&mat->defl_dev, (size_t)SP_DEFL_MAX * n)) ||
+        (st = mat->mem.get(&mat->gram_dev, (size_t)SP_DEFL_MAX * SP_DEFL_MAX)) ||
+        (st = mat->mem.get(&mat->defl_sum_dev, SP_DEFL_MAX)) ||
+        (st = mat->mem.get(&mat->defl_mu_dev, SP_DEFL_MAX)))
+      return st;
+    mat->gram_host.assign((size_t)SP_DEFL_MAX * SP_DEFL_MAX, 0.0);
+  }
+  // x_c^T x_a for the earlier components and itself, 1^T x, means^T x (FP64)
+  mat->defl_host.insert(mat->defl_host.end(), xh.begin(), xh.end());
+  for (int a = 0; a <= c; a++) {
+    const float *xa = mat->defl_host.data() + (size_t)a * n;
+    double g = 0.0;
+    for (int q = 0; q < n; q++) g += (double)xa[q] * (double)xh[q];
+    mat->gram_host[(size_t)c * SP_DEFL_MAX + a] = g;
+    mat->gram_host[(size_t)a * SP_DEFL_MAX + c] = g;
+  }
+  double sum = 0.0, mu = 0.0;
+  for (int q = 0; q < n; q++) {
+    sum += (double)xh[q];
+    if (!mat->means_host.empty()) mu += (double)mat->means_host[q] * (double)xh[q];
+  }
+  AM24_CUDA(cudaMemcpy(mat->defl_dev + (size_t)c * n, xh.data(), sizeof(float) * n,
+                       cudaMemcpyHostToDevice));
+  AM24_CUDA(cudaMemcpy(mat->gram_dev, mat->gram_host.data(),
+                       sizeof(double) * mat->gram_host.size(), cudaMemcpyHostToDevice));
+  AM24_CUDA(cudaMemcpy(mat->defl_sum_dev + c, &sum, sizeof(double), cudaMemcpyHostToDevice));
+  AM24_CUDA(cudaMemcpy(mat->defl_mu_dev + c, &mu, sizeof(double), cudaMemcpyHostToDevice));
+  S.defl = mat->defl_dev;
+  S.gram = mat->gram_dev;
+  S.defl_sum = mat->defl_sum_dev;
+  S.defl_mu = mat->defl_mu_dev;
+  S.comps = c + 1;
+  return AM24_OK;
+}
+
 // The reference's batch driver (denseDataSolver's batch mode,
 // c++/src/gpower/sparse_PCA_solver.h:171-243) on a sparse-resident matrix:
 // batches of batch_size starts (reference, injected or device starts), each
@@ -250,6 +300,7 @@ am24_status solve_sparse(am24_handle h, am24_matrix mat, float *x, am24_settings
   AM24_TRY(A.get(&ev_scratch, sparse_ev_scratch(S)));
   if (S.long_cols.segs) AM24_TRY(A.get(&b.part_cols, (size_t)S.long_cols.segs * b.kp));
   if (S.long_rows.segs) AM24_TRY(A.get(&b.part_rows, (size_t)S.long_rows.segs * b.kp));
+  if (S.comps) AM24_TRY(A.get(&b.defl_a, (size_t)k * SP_DEFL_MAX));
   // every buffer starts defined: pool memory can hold an earlier call's state
   AM24_CUDA(cudaMemsetAsync(b.vmask, 0, sizeof(uint32_t) * (size_t)k * (b.ldn / 32), h->stream));
   AM24_CUDA(cudaMemsetAsync(b.Vx, 0, sizeof(float) * (size_t)k * b.ldn, h->stream));
@@ -359,11 +410,26 @@ am24_status solve_sparse(am24_handle h, am24_matrix mat, float *x, am24_settings
                                    b.ldn, (int)n, 1, xb, (int)n, h->stream));
     }
   }
-  // x <- x / ||x|| and its FP64 explained variance ||(B - centring) x||^2
+  // x <- x / ||x|| and its FP64 explained variance ||(B - centring) P x||^2
+  // (P the deflation, applied to x on the host in FP64: the last factor first)
   AM24_CUDA(launch_finalize_x(xb, (int)n, x_dev, h->stream));
-  AM24_CUDA(launch_sparse_ev(S, x_dev, ev_scratch, h->ev_out, h->stream));
   double ev = 0.0;
   AM24_CUDA(cudaMemcpyAsync(x, x_dev, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+  if (S.comps > 0) {
+    AM24_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<double> px(x, x + n);
+    for (int c = S.comps - 1; c >= 0; c--) {
+      const float *xc = mat->defl_host.data() + (size_t)c * n;
+      double a = 0.0;
+      for (unsigned q = 0; q < n; q++) a += (double)xc[q] * px[q];
+      for (unsigned q = 0; q < n; q++) px[q] -= a * (double)xc[q];
+    }
+    std::vector<float> pxf(px.begin(), px.end());
+    AM24_CUDA(cudaMemcpy(xb, pxf.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    AM24_CUDA(launch_sparse_ev(S, xb, ev_scratch, h->ev_out, h->stream));
+  } else {
+    AM24_CUDA(launch_sparse_ev(S, x_dev, ev_scratch, h->ev_out, h->stream));
+  }
   AM24_CUDA(cudaMemcpyAsync(&ev, h->ev_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   AM24_CUDA(cudaStreamSynchronize(h->stream));
   if (stats) {

@@ -205,10 +205,13 @@ __global__ void __launch_bounds__(SP_TILE) sp_spmm_long_kernel(
 // Vt[q][j] = V's column j at row q (zero where its mask bit is clear), for
 // q < n, j < kp (columns k..kp-1 zero): the row-major X of Z = B V (dense
 // steps only: *gate >= gate_min).
+// With deflations (comps > 0) the column is the projected one,
+// v - sum_c a[j][c] x_c (sp_defl_coef_kernel's coefficients).
 __global__ void __launch_bounds__(SP_THREADS) sp_transpose_v_kernel(
     const float *__restrict__ Vx, const uint32_t *__restrict__ mask, int ldn, int n, int k,
     float *__restrict__ Vt, int kp, const uint32_t *stop, const uint32_t *gate,
-    uint32_t gate_min) {
+    uint32_t gate_min, const float *__restrict__ defl, int comps,
+    const double *__restrict__ defl_a) {
   if (*stop || *gate < gate_min) return;
   __shared__ float tile[SP_TILE][SP_TILE + 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -220,6 +223,12 @@ __global__ void __launch_bounds__(SP_THREADS) sp_transpose_v_kernel(
     if (j < k && q < n) {
       const uint32_t w = mask[(size_t)j * words + (q >> 5)];
       if ((w >> (q & 31)) & 1u) v = Vx[(size_t)j * ldn + q];
+      if (comps > 0) {
+        double d = (double)v;
+        for (int c = 0; c < comps; c++)
+          d -= defl_a[(size_t)j * SP_DEFL_MAX + c] * (double)defl[(size_t)c * n + q];
+        v = (float)d;
+      }
     }
     tile[r][lane] = v;
   }
@@ -412,6 +421,82 @@ __global__ void __launch_bounds__(SP_THREADS) sp_penalty_kernel(
   if (threadIdx.x == 0) {
     obj_part[j] = (float)obj;
     nnz_part[j] = (float)cnt;
+  }
+}
+
+// Deflation, V side (one block per start): with P = (I - x_1 x_1^T) ...
+// (I - x_C x_C^T), Z = B P v applies the factors to v from the last to the
+// first: a_c = x_c^T v - sum_{c' > c} a_c' (x_c^T x_c') for c = C .. 1, and
+// P v = v - sum_c a_c x_c.  Stores a[j][c] for the transposition and corrects
+// the centring sums (when sum_v is not null) to those of P v.
+__global__ void __launch_bounds__(SP_THREADS) sp_defl_coef_kernel(
+    const float *__restrict__ Vx, const uint32_t *__restrict__ mask, int ldn, int n,
+    const float *__restrict__ defl, int comps, const double *__restrict__ gram,
+    const double *__restrict__ defl_sum, const double *__restrict__ defl_mu,
+    double *__restrict__ defl_a, double *sum_v, double *dot_mu, const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ double red[SP_THREADS / 32];
+  __shared__ double d[SP_DEFL_MAX];
+  const int j = blockIdx.x;
+  const int words = ldn >> 5;
+  for (int c = 0; c < comps; c++) {
+    double s = 0.0;
+    for (int q = threadIdx.x; q < n; q += SP_THREADS) {
+      const uint32_t w = mask[(size_t)j * words + (q >> 5)];
+      if ((w >> (q & 31)) & 1u)
+        s += (double)defl[(size_t)c * n + q] * (double)Vx[(size_t)j * ldn + q];
+    }
+    s = sp_block_sum(s, red);
+    if (threadIdx.x == 0) d[c] = s;
+  }
+  if (threadIdx.x == 0) {
+    double a[SP_DEFL_MAX];
+    double ds = 0.0, dm = 0.0;
+    for (int c = comps - 1; c >= 0; c--) {
+      double v = d[c];
+      for (int c2 = c + 1; c2 < comps; c2++) v -= a[c2] * gram[c * SP_DEFL_MAX + c2];
+      a[c] = v;
+      defl_a[(size_t)j * SP_DEFL_MAX + c] = v;
+      ds += v * defl_sum[c];
+      dm += v * defl_mu[c];
+    }
+    if (sum_v) {
+      sum_v[j] -= ds;
+      dot_mu[j] -= dm;
+    }
+  }
+}
+
+// Deflation, B^T Z side (one block per start): V = P^T B^T z applies the
+// factors to u = B^T z from the first to the last: b_c = x_c^T u -
+// sum_{c' < c} b_c' (x_c^T x_c'), then u <- u - sum_c b_c x_c, in place.
+__global__ void __launch_bounds__(SP_THREADS) sp_defl_vraw_kernel(
+    float *__restrict__ Vraw, int ldn, int n, const float *__restrict__ defl, int comps,
+    const double *__restrict__ gram, const uint32_t *stop) {
+  if (*stop) return;
+  __shared__ double red[SP_THREADS / 32];
+  __shared__ double b[SP_DEFL_MAX];
+  const int j = blockIdx.x;
+  float *u = Vraw + (size_t)j * ldn;
+  for (int c = 0; c < comps; c++) {
+    double s = 0.0;
+    for (int q = threadIdx.x; q < n; q += SP_THREADS)
+      s += (double)defl[(size_t)c * n + q] * (double)u[q];
+    s = sp_block_sum(s, red);
+    if (threadIdx.x == 0) b[c] = s;
+  }
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < comps; c++) {
+      double v = b[c];
+      for (int c2 = 0; c2 < c; c2++) v -= b[c2] * gram[c * SP_DEFL_MAX + c2];
+      b[c] = v;
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < n; q += SP_THREADS) {
+    double v = (double)u[q];
+    for (int c = 0; c < comps; c++) v -= b[c] * (double)defl[(size_t)c * n + q];
+    u[q] = (float)v;
   }
 }
 

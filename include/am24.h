@@ -229,8 +229,11 @@ am24_status am24_matrix_create_csc_f32(am24_handle h, const float *vals, const i
  * (row, column) entries added up in entry order.  Such a matrix is solved by
  * am24_solve_resident_f32 (batch mode: the dense path's iteration, both
  * products as FP32 kernels on the compressed arrays, AM24_PRECISION_MIXED runs
- * as FP32; use_otf returns AM24_ERR_UNSUPPORTED); the batch, group, deflation
- * and read entry points return AM24_ERR_UNSUPPORTED for it. */
+ * as FP32; use_otf returns AM24_ERR_UNSUPPORTED).  am24_matrix_deflate records
+ * each x as the next factor of B (I - x_1 x_1^T) ... (I - x_C x_C^T) (at most
+ * 32), applied to the loadings before Z = B V and to B^T Z after it, so the
+ * arrays stay as uploaded; the batch, group and read entry points return
+ * AM24_ERR_UNSUPPORTED for such a matrix. */
 am24_status am24_matrix_create_csc_sparse_f32(am24_handle h, const float *vals,
                                               const int32_t *row_ind, const int32_t *col_ptr,
                                               uint32_t m, uint32_t n, const float *means,
@@ -247,7 +250,8 @@ am24_status am24_solve_resident_f32(am24_handle h, am24_matrix mat, float *x,
  * Every layout the matrix holds is rebuilt in place, so batches created on it
  * stay valid; work already queued on the handle's stream sees the old B, work
  * queued after it the new one, and work on other handles must not use the
- * matrix meanwhile. */
+ * matrix meanwhile.  A sparse-resident matrix keeps its arrays and records x as
+ * the next factor instead (am24_matrix_create_csc_sparse_f32). */
 am24_status am24_matrix_deflate(am24_handle h, am24_matrix mat, const float *x,
                                 int32_t on_device);
 /* Copies the matrix's current B (m x n, column-major, leading dimension ldB >=

@@ -16,8 +16,8 @@
  *   of settings->device either densely, solved by the dense tensor-core path,
  *   or (settings->sparseResident; by default when the dense FP32 form would
  *   exceed 8 GiB or the density is below 0.5 %) compressed, with the means
- *   applied implicitly (am24_matrix_create_csc_sparse_f32; no deflation
- *   collection and no on-the-fly mode then);
+ *   applied implicitly (am24_matrix_create_csc_sparse_f32; no on-the-fly
+ *   mode then);
  * - starting points follow settings->startMode (default: the reference's
  *   dense-solver generator, rand_r per global start index), where the
  *   reference's sparse driver draws its constrained starts from the
@@ -102,7 +102,6 @@ F sparse_PCA_solver_CSC(F *B_CSC_Vals, int *B_CSC_Row_Id, int *B_CSC_Col_Ptr, F 
       o->sparseResident > 0 ||
       (o->sparseResident < 0 &&
        (dense_bytes > 8.0 * (1u << 30) || (double)nnz < 0.005 * (double)m * (double)n));
-  if (keep_sparse && !sparseDeflationCollection.list.empty()) return nan;
   if ((keep_sparse ? am24_matrix_create_csc_sparse_f32 : am24_matrix_create_csc_f32)(
           h, vals.data(), B_CSC_Row_Id, B_CSC_Col_Ptr, (uint32_t)m, (uint32_t)n,
           doMean ? mu.data() : nullptr, doRowMean ? rmu.data() : nullptr, &mat) != AM24_OK)

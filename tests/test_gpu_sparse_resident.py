@@ -211,15 +211,14 @@ def test_sparse_resident_beyond_dense_memory(solver):
 
 
 def test_sparse_resident_rejections(solver):
-    """Batches, groups, deflation and reads take dense matrices only; the
-    on-the-fly mode is not offered on a sparse-resident one."""
+    """Batches, groups and reads take dense matrices only; the on-the-fly mode
+    is not offered on a sparse-resident one."""
     am = _am()
     S = _sparse(64, 300, 5, density=0.1)
     M = am.Matrix.from_csc(solver, S, None, None, None, None, keep_sparse=True)
     st = am.OptimizationSettings(formulation=0, constraintParameter=5, totalStartingPoints=32,
                                  batchSize=32)
     for call in (lambda: M.batch(st, 32), lambda: M.read(),
-                 lambda: M.deflate(np.ones(300, np.float32) / np.sqrt(300.0)),
                  lambda: M.solve(am.OptimizationSettings(formulation=0, constraintParameter=5,
                                                          useOTF=True, totalStartingPoints=32,
                                                          batchSize=8))):
@@ -267,3 +266,36 @@ def test_sparse_resident_unsorted_and_duplicate_entries(solver):
     x2, f2, _ = M2.solve(am.OptimizationSettings(**kw))
     M2.close()
     assert f1 == f2 and np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("formulation", [0, 3, 6])
+def test_sparse_resident_deflation_matches_densified(solver, formulation):
+    """Three components, the reference's multi-component loop: after each
+    solve both matrices are deflated by the same loading (the densified
+    path's), B <- B (I - x x^T).  The densified matrix is rewritten; the
+    sparse-resident one projects the loadings instead.  Each solve's best
+    explained variance (of the deflated matrix) agrees within 1e-4."""
+    am = _am()
+    m, n, k = 300, 2500, 256
+    S = _planted(m, n, 90 + formulation, density=0.04)
+    A = S.toarray()
+    mu, _, C = _centring(A, "columns")
+    Md = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu)
+    Ms = am.Matrix.from_csc(solver, S, None, None, None, None, means=mu, keep_sparse=True)
+    for comp in range(3):
+        # the penalty from the deflated matrix, so that each solve keeps loadings
+        kw = dict(formulation=formulation, constraintParameter=12,
+                  penaltyParameter=_gamma(C, formulation), tolerance=1e-6,
+                  maximumIterations=80, totalStartingPoints=k, batchSize=k,
+                  startMode=am.START_DEVICE_UNIFORM)
+        xd, fd, sd = Md.solve(am.OptimizationSettings(**kw))
+        xs, fs, ss = Ms.solve(am.OptimizationSettings(**kw))
+        assert abs(ss.explained_variance - sd.explained_variance) <= \
+            1e-4 * sd.explained_variance, (comp, ss.explained_variance, sd.explained_variance)
+        assert abs(fs - fd) <= 1e-4 * abs(fd), (comp, fs, fd)
+        Md.deflate(xd)
+        Ms.deflate(xd)
+        x64 = xd.astype(np.float64)
+        C = C - np.outer(C @ x64, x64)
+    Md.close()
+    Ms.close()
