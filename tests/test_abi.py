@@ -24,6 +24,21 @@ def test_default_settings_are_reference_defaults(am):
     assert s.start_mode == am.START_REFERENCE and s.l1_mode == am.L1_REFERENCE_SCAN
 
 
+def test_mixed_settings_defaults_and_mirror(am):
+    """The library's MIXED options: the single-pass phase from the first
+    iteration unless a lead-in is asked for, and the Python mirror's fields
+    reaching the C struct (leadIterations in the former reserved words: the
+    struct's size and the offsets of the fields after it are unchanged)."""
+    s = am.am24_settings()
+    am.lib().am24_default_settings(C.byref(s))
+    assert (s.precision, s.stable_iterations, s.stable_share, s.lead_iterations) == (0, 5, 1.0, 0)
+    c = am.OptimizationSettings(precision=am.PRECISION_MIXED, stableIterations=3,
+                                stableShare=0.5, leadIterations=20).to_c()
+    assert (c.precision, c.stable_iterations, c.stable_share, c.lead_iterations) == (1, 3, 0.5, 20)
+    assert am.am24_settings.lead_iterations.offset == am.am24_settings.stable_share.offset + 4
+    assert am.am24_settings.reserved.offset == am.am24_settings.lead_iterations.offset + 4
+
+
 def test_check_input_matches_reference(am, po):
     """chceckInputAndModifyIt (c++/src/class/optimization_settings.h:156-168)
     against the oracle's restatement, over random settings."""
